@@ -1,0 +1,839 @@
+// Host side of the B200 IVF-flat index and its C ABI (include/harmony_b200.h).
+//
+// The index mirrors harmony::Index (src/Index.h:13-149): centroids, nlist
+// inverted lists of (id, code, norm), nprobe, train / add / search /
+// save_index / load_index.  Everything it owns lives in device memory:
+//
+//   centroids  float [nlist x dpad]          (rows zero-padded to dpad)
+//   list_off   int64 [nlist + 1]             CSR offsets of the lists
+//   codes      float [ntotal x dpad]         vectors in list order
+//   ids        int64 [ntotal]                ids in list order
+//   norms      float [ntotal]                <x, x> (the reference stores them too)
+//
+// Search runs per batch of queries, all on the index's stream:
+//   pad queries -> exact coarse distance matrix -> per-query top-nprobe
+//   -> [warm-up heap tops] -> list-major work description -> persistent
+//   exact list scan -> per-query merge of the partial top-k slots.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstdio>
+#include <fstream>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "hb_internal.hpp"
+
+namespace hb {
+
+namespace {
+thread_local std::string g_last_error;
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int pow2_floor(long long x) {
+  int p = 1;
+  while (static_cast<long long>(p) * 2 <= x && p < (1 << 30)) p <<= 1;
+  return p;
+}
+}  // namespace
+
+// Order of the dimension slices for each query block in the
+// dimension-partition mode: src/order.h:38-96 and the "period" variant of
+// src/Index.cpp:183-197.  order[b * W + t] = slice visited at hop t.
+std::vector<int32_t> block_visit_order(int W, int B, bool order_optimize, bool period) {
+  std::vector<std::vector<int>> wsbo(W + 1, std::vector<int>(B, 0));
+  if (order_optimize) {
+    if (period && B % W == 0) {
+      const int layer = B / W;
+      for (int p = 1; p <= W; ++p)
+        for (int t = (p - 1) * layer; t < p * layer; ++t) {
+          const int start = (t % layer) * W;
+          for (int r = p; r < p + W; ++r) wsbo[(r + W - 1) % W + 1][t] = start + r - p;
+        }
+    } else {
+      const int gap = (B + W - 1) / W;
+      for (int r = 1; r <= W; ++r)
+        for (int blk = 0; blk < B; ++blk) wsbo[r][(blk + gap * (r - 1)) % B] = blk;
+    }
+  } else {
+    for (int r = 1; r <= W; ++r)
+      for (int t = r - 1; t < r - 1 + B; ++t) wsbo[r][t % B] = t - (r - 1);
+  }
+  std::vector<std::vector<int>> seq(B);
+  for (int t = 0; t < B; ++t)
+    for (int r = 1; r <= W; ++r) seq[wsbo[r][t]].push_back(r - 1);
+  std::vector<int32_t> order(static_cast<size_t>(B) * W, -1);
+  for (int b = 0; b < B; ++b)
+    for (int t = 0; t < W && t < static_cast<int>(seq[b].size()); ++t) order[static_cast<size_t>(b) * W + t] = seq[b][t];
+  return order;
+}
+
+class IndexCore {
+ public:
+  IndexCore(size_t d, size_t nlist, size_t nprobe, int metric, int device)
+      : d_(d), nlist_(nlist), nprobe_(nprobe), metric_(metric), device_(device) {
+    HB_CHECK(metric == HB_METRIC_L2, HB_ERR_INVALID, "only METRIC_L2 is implemented");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      throw Error(HB_ERR_NODEVICE, "no CUDA device");
+    }
+    HB_CHECK(device >= 0 && device < ndev, HB_ERR_INVALID, "bad device ordinal");
+    HB_CUDA(cudaSetDevice(device));
+    HB_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device));
+    HB_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    reshape(d, nlist);
+  }
+  ~IndexCore() {
+    cudaSetDevice(device_);
+    if (st_) {
+      cudaStreamSynchronize(st_);
+      cudaStreamDestroy(st_);
+    }
+  }
+
+  // Index ctor state: zero centroids, empty lists (src/Index.cpp:24-43).
+  void reshape(size_t d, size_t nlist) {
+    HB_CHECK(d > 0 && d <= 1024, HB_ERR_INVALID, "d must be in [1, 1024]");
+    HB_CHECK(nlist > 0 && nlist <= (1u << 20), HB_ERR_INVALID, "nlist must be in [1, 2^20]");
+    d_ = d;
+    nlist_ = nlist;
+    dpad_ = pad_dim(d);
+    cent_.reserve(nlist_ * dpad_);
+    HB_CUDA(cudaMemsetAsync(cent_.p, 0, nlist_ * dpad_ * sizeof(float), st_));
+    list_off_.reserve(nlist_ + 1);
+    HB_CUDA(cudaMemsetAsync(list_off_.p, 0, (nlist_ + 1) * sizeof(int64_t), st_));
+    host_off_.assign(nlist_ + 1, 0);
+    ntotal_ = 0;
+    HB_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  size_t d() const { return d_; }
+  size_t nlist() const { return nlist_; }
+  size_t ntotal() const { return ntotal_; }
+  size_t nprobe() const { return nprobe_; }
+  void set_nprobe(size_t p) { nprobe_ = p; }
+  int metric() const { return metric_; }
+  cudaStream_t stream() const { return st_; }
+  uint64_t launches() const { return launches_; }
+
+  // ---- input staging -------------------------------------------------------
+
+  // Copies n x d floats (host or device) to a padded device buffer.
+  void stage_rows(const float* x, size_t n, DevBuf<float>& dst, DevBuf<float>& tmp) {
+    dst.reserve(std::max<size_t>(n * dpad_, 1));
+    if (!n) return;
+    const float* src = x;
+    if (!is_device_ptr(x)) {
+      tmp.reserve(n * d_);
+      HB_CUDA(cudaMemcpyAsync(tmp.p, x, n * d_ * sizeof(float), cudaMemcpyHostToDevice, st_));
+      src = tmp.p;
+    }
+    launch_pad_rows(src, n, static_cast<int>(d_), static_cast<int>(dpad_), dst.p, st_);
+    ++launches_;
+  }
+
+  // ---- train: src/Index.cpp:381-425 + src/Clustering.cpp:14-152 ------------
+
+  void train(size_t n, const float* x, bool lite) {
+    HB_CHECK(x || n == 0, HB_ERR_INVALID, "null training data");
+    HB_CHECK(n >= nlist_, HB_ERR_INVALID, "train needs at least nlist points");
+    HB_CHECK(n < (1ull << 31), HB_ERR_INVALID, "train supports fewer than 2^31 points");
+    HB_CUDA(cudaSetDevice(device_));
+    const int niter = lite ? 2 : 20;
+    const int seed = 6666;
+    const size_t max_pts = 256;
+    // Sampling draws exactly as the reference: std::shuffle with
+    // std::default_random_engine(seed) over the point indices, the first
+    // nlist*max_pts when n exceeds it, then a second shuffle over the
+    // sample whose first nlist entries seed the centroids.
+    size_t m = n;
+    std::vector<int64_t> sample;
+    if (n > nlist_ * max_pts) {
+      std::vector<size_t> idx(n);
+      std::iota(idx.begin(), idx.end(), 0);
+      std::shuffle(idx.begin(), idx.end(), std::default_random_engine(seed));
+      m = nlist_ * max_pts;
+      sample.assign(idx.begin(), idx.begin() + m);
+    }
+    std::vector<size_t> iidx(m);
+    std::iota(iidx.begin(), iidx.end(), 0);
+    std::shuffle(iidx.begin(), iidx.end(), std::default_random_engine(seed));
+    std::vector<int64_t> init(nlist_);
+    for (size_t c = 0; c < nlist_; ++c) init[c] = static_cast<int64_t>(iidx[c]);
+
+    DevBuf<float> xall, tmp, xs;
+    stage_rows(x, n, xall, tmp);
+    tmp.release();
+    const float* pts = xall.p;
+    if (!sample.empty()) {
+      DevBuf<int64_t> sidx;
+      sidx.reserve(m);
+      HB_CUDA(cudaMemcpyAsync(sidx.p, sample.data(), m * sizeof(int64_t), cudaMemcpyHostToDevice, st_));
+      xs.reserve(m * dpad_);
+      launch_gather_rows(xall.p, sidx.p, m, static_cast<int>(dpad_), xs.p, st_);
+      ++launches_;
+      HB_CUDA(cudaStreamSynchronize(st_));
+      xall.release();
+      pts = xs.p;
+    }
+    {
+      DevBuf<int64_t> cidx;
+      cidx.reserve(nlist_);
+      HB_CUDA(cudaMemcpyAsync(cidx.p, init.data(), nlist_ * sizeof(int64_t), cudaMemcpyHostToDevice, st_));
+      launch_gather_rows(pts, cidx.p, nlist_, static_cast<int>(dpad_), cent_.p, st_);
+      ++launches_;
+      HB_CUDA(cudaStreamSynchronize(st_));
+    }
+    DevBuf<int32_t> assign, counts;
+    DevBuf<double> sums;
+    assign.reserve(m);
+    counts.reserve(nlist_);
+    sums.reserve(nlist_ * dpad_);
+    for (int it = 0; it < niter; ++it) {
+      launch_l2_argmin(pts, static_cast<int>(m), cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), assign.p,
+                       nullptr, st_);
+      HB_CUDA(cudaMemsetAsync(sums.p, 0, nlist_ * dpad_ * sizeof(double), st_));
+      HB_CUDA(cudaMemsetAsync(counts.p, 0, nlist_ * sizeof(int32_t), st_));
+      launch_kmeans_accumulate(pts, assign.p, m, static_cast<int>(d_), static_cast<int>(dpad_), sums.p, counts.p,
+                               st_);
+      launch_kmeans_update(sums.p, counts.p, static_cast<int>(nlist_), static_cast<int>(d_), static_cast<int>(dpad_),
+                           cent_.p, st_);
+      launches_ += 3;
+    }
+    HB_CUDA(cudaStreamSynchronize(st_));
+    trained_ = true;
+  }
+
+  // ---- add: src/Index.cpp:581-698 ------------------------------------------
+
+  void add(size_t n, const float* x) {
+    if (n == 0) return;  // the reference returns before touching the lists
+    HB_CHECK(x, HB_ERR_INVALID, "null data");
+    HB_CHECK(n < (1ull << 32) - 1, HB_ERR_INVALID, "add supports fewer than 2^32 - 1 vectors");
+    HB_CUDA(cudaSetDevice(device_));
+    DevBuf<float> xpad, tmp;
+    stage_rows(x, n, xpad, tmp);
+    tmp.release();
+    DevBuf<int32_t> assign;
+    DevBuf<float> dist;
+    assign.reserve(n);
+    dist.reserve(n);
+    launch_l2_argmin(xpad.p, static_cast<int>(n), cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), assign.p,
+                     dist.p, st_);
+    DevBuf<uint64_t> k0, k1;
+    DevBuf<uint32_t> v0, v1;
+    k0.reserve(n);
+    k1.reserve(n);
+    v0.reserve(n);
+    v1.reserve(n);
+    launch_add_keys(assign.p, dist.p, n, k0.p, v0.p, st_);
+    int list_bits = 1;
+    while ((1ull << list_bits) < nlist_) ++list_bits;
+    size_t sort_bytes = 0;
+    sort_pairs_u64(k0.p, k1.p, v0.p, v1.p, n, 32 + list_bits, nullptr, &sort_bytes, st_);
+    DevBuf<unsigned char> sort_tmp;
+    sort_tmp.reserve(sort_bytes);
+    sort_pairs_u64(k0.p, k1.p, v0.p, v1.p, n, 32 + list_bits, sort_tmp.p, &sort_bytes, st_);
+    codes_.reserve(n * dpad_);
+    ids_.reserve(n);
+    norms_.reserve(n);
+    launch_scatter_sorted(xpad.p, v1.p, n, static_cast<int>(d_), static_cast<int>(dpad_), codes_.p, ids_.p, st_);
+    const size_t ob = list_offsets_tmp_bytes(static_cast<int>(nlist_));
+    DevBuf<unsigned char> otmp;
+    otmp.reserve(ob);
+    launch_list_offsets(assign.p, n, static_cast<int>(nlist_), list_off_.p, otmp.p, ob, st_);
+    launch_row_norms(codes_.p, n, static_cast<int>(d_), static_cast<int>(dpad_), norms_.p, st_);
+    launches_ += 6;
+    host_off_.resize(nlist_ + 1);
+    HB_CUDA(cudaMemcpyAsync(host_off_.data(), list_off_.p, (nlist_ + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                            st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    ntotal_ = n;
+    plan_rows_ = 0;
+  }
+
+  // ---- coarse quantizer ----------------------------------------------------
+
+  // probes_out (device, nq x P int32, ascending), cdist_out optional.
+  void coarse(const float* qpad, int nq, int P, int32_t* probes_out, float* cdist_out) {
+    dmat_.reserve(static_cast<size_t>(nq) * nlist_);
+    launch_l2_matrix(qpad, nq, cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), dmat_.p,
+                     static_cast<int>(nlist_), st_);
+    launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), P, probes_out, cdist_out, st_);
+    launches_ += 2;
+  }
+
+  // ---- search: src/Index.cpp:1638-1706 --------------------------------------
+
+  void search(size_t nq, const float* q, size_t k, const hb_search_params* prm, float* D, int64_t* I) {
+    if (nq == 0) return;
+    HB_CHECK(q && D && I, HB_ERR_INVALID, "null query or result pointer");
+    HB_CHECK(k > 0, HB_ERR_INVALID, "k must be positive");
+    HB_CUDA(cudaSetDevice(device_));
+    hb_search_params p;
+    hb_search_params_init(&p);
+    if (prm) p = *prm;
+    if (nprobe_ > nlist_) nprobe_ = nlist_;  // src/Index.cpp:1646-1648 (mutates the field)
+    HB_CHECK(p.precision == HB_PREC_FP32, HB_ERR_INVALID, "this build scans in FP32 only");
+    HB_CHECK(!p.learned_probe, HB_ERR_INVALID, "learned probe predictor not trained");
+    int mode = SCAN_PLAIN;
+    size_t P = nprobe_;
+    int W = 1, B = 1;
+    std::vector<int32_t> order;
+    bool need_tops = false;
+    switch (p.mode) {
+      case HB_MODE_ORIGINAL:
+        break;
+      case HB_MODE_BRUTE_FORCE:
+        P = nlist_;
+        break;
+      case HB_MODE_DIVIDE_IVF:
+        if (p.pruning) {
+          mode = SCAN_CHUNK4;
+          need_tops = true;
+        }
+        break;
+      case HB_MODE_DIVIDE_DIM: {
+        W = p.n_dim_blocks;
+        B = p.n_query_blocks;
+        HB_CHECK(W >= 1 && W <= 8, HB_ERR_INVALID, "n_dim_blocks must be in [1, 8]");
+        HB_CHECK(d_ % W == 0, HB_ERR_INVALID, "d must be divisible by n_dim_blocks (src/Index.cpp:125)");
+        HB_CHECK(B >= 1, HB_ERR_INVALID, "n_query_blocks must be >= 1");
+        mode = SCAN_DIMBLOCK;
+        need_tops = true;  // heap tops are always computed (src/Index.cpp:1241-1252)
+        order = block_visit_order(W, B, p.order_optimize != 0, p.period != 0);
+        break;
+      }
+      default:
+        throw Error(HB_ERR_INVALID, "search mode not supported");
+    }
+    if (p.nprobe_per_query) throw Error(HB_ERR_INVALID, "per-query nprobe needs the batched scheduler");
+
+    const bool dev_out = is_device_ptr(D) && is_device_ptr(I);
+    const bool dev_in = is_device_ptr(q);
+    const size_t bs = std::min<size_t>(nq, batch_limit(P, k));
+    const int warm_lists = p.warmup_lists;
+    const int warm_size = p.warmup_list_size > 0 ? p.warmup_list_size : static_cast<int>(k);
+    // DIVIDE_DIM query blocks cover queries [0, B * (nq / B)); the rest stay
+    // unsearched (src/Index.cpp:1189, 1266-1270).
+    const int qblock = mode == SCAN_DIMBLOCK ? static_cast<int>(nq / B) : 0;
+    if (mode == SCAN_DIMBLOCK) HB_CHECK(nq <= bs, HB_ERR_INVALID, "DIVIDE_DIM search is limited to one batch");
+    if (!order.empty()) {
+      order_dev_.reserve(order.size());
+      HB_CUDA(cudaMemcpyAsync(order_dev_.p, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
+    }
+
+    for (size_t b0 = 0; b0 < nq; b0 += bs) {
+      const int nb = static_cast<int>(std::min(bs, nq - b0));
+      float* Dd = dev_out ? D + b0 * k : nullptr;
+      int64_t* Id = dev_out ? I + b0 * k : nullptr;
+      if (!dev_out) {
+        dout_.reserve(static_cast<size_t>(nb) * k);
+        iout_.reserve(static_cast<size_t>(nb) * k);
+        Dd = dout_.p;
+        Id = iout_.p;
+      }
+      // Queries.
+      qpad_.reserve(static_cast<size_t>(nb) * dpad_);
+      const float* qsrc = q + b0 * d_;
+      if (!dev_in) {
+        qtmp_.reserve(static_cast<size_t>(nb) * d_);
+        HB_CUDA(cudaMemcpyAsync(qtmp_.p, qsrc, static_cast<size_t>(nb) * d_ * sizeof(float), cudaMemcpyHostToDevice,
+                                st_));
+        qsrc = qtmp_.p;
+      }
+      launch_pad_rows(qsrc, nb, static_cast<int>(d_), static_cast<int>(dpad_), qpad_.p, st_);
+      ++launches_;
+      if (P == 0 || ntotal_ == 0) {
+        launch_fill_results(Dd, Id, static_cast<size_t>(nb) * k, st_);
+        ++launches_;
+      } else {
+        search_batch(nb, static_cast<int>(P), static_cast<int>(k), mode, p.pruning != 0, need_tops, warm_lists,
+                     warm_size, W, B, qblock, Dd, Id);
+      }
+      if (!dev_out) {
+        HB_CUDA(cudaMemcpyAsync(D + b0 * k, Dd, static_cast<size_t>(nb) * k * sizeof(float), cudaMemcpyDeviceToHost,
+                                st_));
+        HB_CUDA(cudaMemcpyAsync(I + b0 * k, Id, static_cast<size_t>(nb) * k * sizeof(int64_t),
+                                cudaMemcpyDeviceToHost, st_));
+      }
+    }
+    HB_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  void probe_lists(size_t nq, const float* q, size_t P, int64_t* probes, float* cdist) {
+    if (nq == 0) return;
+    HB_CUDA(cudaSetDevice(device_));
+    HB_CHECK(P >= 1 && P <= nlist_, HB_ERR_INVALID, "nprobe must be in [1, nlist]");
+    DevBuf<float> qp, tmp, cd;
+    stage_rows(q, nq, qp, tmp);
+    DevBuf<int32_t> pr;
+    DevBuf<int64_t> pr64;
+    pr.reserve(nq * P);
+    pr64.reserve(nq * P);
+    cd.reserve(nq * P);
+    coarse(qp.p, static_cast<int>(nq), static_cast<int>(P), pr.p, cd.p);
+    launch_i32_to_i64(pr.p, nq * P, pr64.p, st_);
+    ++launches_;
+    HB_CUDA(cudaMemcpyAsync(probes, pr64.p, nq * P * sizeof(int64_t), cudaMemcpyDefault, st_));
+    if (cdist) HB_CUDA(cudaMemcpyAsync(cdist, cd.p, nq * P * sizeof(float), cudaMemcpyDefault, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  void warmup_tops(size_t nq, const float* q, size_t k, size_t wl, size_t wls, float* tops) {
+    if (nq == 0) return;
+    HB_CUDA(cudaSetDevice(device_));
+    size_t P = std::min(nprobe_, nlist_);
+    DevBuf<float> qp, tmp, t;
+    stage_rows(q, nq, qp, tmp);
+    DevBuf<int32_t> pr;
+    pr.reserve(std::max<size_t>(nq * P, 1));
+    t.reserve(nq);
+    if (P > 0) coarse(qp.p, static_cast<int>(nq), static_cast<int>(P), pr.p, nullptr);
+    launch_warmup_tops(qp.p, static_cast<int>(nq), pr.p, static_cast<int>(P), codes_.p, list_off_.p,
+                       static_cast<int>(dpad_), static_cast<int>(k), static_cast<int>(wl), static_cast<int>(wls), t.p,
+                       st_);
+    ++launches_;
+    HB_CUDA(cudaMemcpyAsync(tops, t.p, nq * sizeof(float), cudaMemcpyDefault, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  // ---- save / load: src/Index.cpp:1708-1770, src/IVF.cpp:76-134 --------------
+
+  void save(const char* path) {
+    HB_CUDA(cudaSetDevice(device_));
+    std::ofstream out(path, std::ios::binary);
+    HB_CHECK(out.is_open(), HB_ERR_IO, std::string("Cannot open file ") + path);
+    std::vector<float> cent(nlist_ * dpad_);
+    HB_CUDA(cudaMemcpyAsync(cent.data(), cent_.p, cent.size() * sizeof(float), cudaMemcpyDeviceToHost, st_));
+    std::vector<float> codes(ntotal_ * dpad_);
+    std::vector<int64_t> ids(ntotal_);
+    std::vector<float> norms(ntotal_);
+    if (ntotal_) {
+      HB_CUDA(cudaMemcpyAsync(codes.data(), codes_.p, codes.size() * sizeof(float), cudaMemcpyDeviceToHost, st_));
+      HB_CUDA(cudaMemcpyAsync(ids.data(), ids_.p, ids.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, st_));
+      HB_CUDA(cudaMemcpyAsync(norms.data(), norms_.p, norms.size() * sizeof(float), cudaMemcpyDeviceToHost, st_));
+    }
+    HB_CUDA(cudaStreamSynchronize(st_));
+    const size_t sub_k = 0, sub_nlist = 1, sub_nprobe = 1;
+    const int32_t metric = metric_, opt = 0;
+    out.write(reinterpret_cast<const char*>(&d_), sizeof(size_t));
+    out.write(reinterpret_cast<const char*>(&nlist_), sizeof(size_t));
+    out.write(reinterpret_cast<const char*>(&metric), sizeof(int32_t));
+    out.write(reinterpret_cast<const char*>(&opt), sizeof(int32_t));
+    out.write(reinterpret_cast<const char*>(&sub_k), sizeof(size_t));
+    out.write(reinterpret_cast<const char*>(&sub_nlist), sizeof(size_t));
+    out.write(reinterpret_cast<const char*>(&sub_nprobe), sizeof(size_t));
+    std::vector<float> row(d_);
+    for (size_t c = 0; c < nlist_; ++c)
+      out.write(reinterpret_cast<const char*>(&cent[c * dpad_]), d_ * sizeof(float));
+    for (size_t l = 0; l < nlist_; ++l) {
+      const size_t n = static_cast<size_t>(host_off_[l + 1] - host_off_[l]);
+      if (!n) continue;
+      const size_t b = static_cast<size_t>(host_off_[l]);
+      out.write(reinterpret_cast<const char*>(&l), sizeof(size_t));
+      out.write(reinterpret_cast<const char*>(&n), sizeof(size_t));
+      out.write(reinterpret_cast<const char*>(&d_), sizeof(size_t));
+      out.write(reinterpret_cast<const char*>(&sub_k), sizeof(size_t));
+      out.write(reinterpret_cast<const char*>(&opt), sizeof(int32_t));
+      for (size_t i = 0; i < n; ++i) {
+        const size_t id = static_cast<size_t>(ids[b + i]);
+        out.write(reinterpret_cast<const char*>(&id), sizeof(size_t));
+      }
+      for (size_t i = 0; i < n; ++i) out.write(reinterpret_cast<const char*>(&codes[(b + i) * dpad_]), d_ * sizeof(float));
+      out.write(reinterpret_cast<const char*>(&norms[b]), n * sizeof(float));
+    }
+    HB_CHECK(out.good(), HB_ERR_IO, std::string("write failed: ") + path);
+  }
+
+  void load(const char* path) {
+    HB_CUDA(cudaSetDevice(device_));
+    std::ifstream in(path, std::ios::binary);
+    HB_CHECK(in.is_open(), HB_ERR_IO, std::string("Cannot open file ") + path);
+    size_t d = 0, nlist = 0, sub_k = 0, sub_nlist = 0, sub_nprobe = 0;
+    int32_t metric = 0, opt = 0;
+    in.read(reinterpret_cast<char*>(&d), sizeof(size_t));
+    in.read(reinterpret_cast<char*>(&nlist), sizeof(size_t));
+    in.read(reinterpret_cast<char*>(&metric), sizeof(int32_t));
+    in.read(reinterpret_cast<char*>(&opt), sizeof(int32_t));
+    in.read(reinterpret_cast<char*>(&sub_k), sizeof(size_t));
+    in.read(reinterpret_cast<char*>(&sub_nlist), sizeof(size_t));
+    in.read(reinterpret_cast<char*>(&sub_nprobe), sizeof(size_t));
+    HB_CHECK(in.good(), HB_ERR_IO, "truncated index header");
+    HB_CHECK(metric == HB_METRIC_L2, HB_ERR_IO, "index metric is not L2");
+    HB_CHECK(d > 0 && d <= 1024 && nlist > 0 && nlist <= (1u << 20), HB_ERR_IO, "implausible index shape");
+    std::vector<float> cent(nlist * d);
+    in.read(reinterpret_cast<char*>(cent.data()), cent.size() * sizeof(float));
+    HB_CHECK(in.good(), HB_ERR_IO, "truncated centroids");
+    struct ListRec {
+      std::vector<int64_t> ids;
+      std::vector<float> codes, norms;
+    };
+    std::vector<ListRec> lists(nlist);
+    for (;;) {
+      size_t lid = 0;
+      in.read(reinterpret_cast<char*>(&lid), sizeof(size_t));
+      if (in.eof()) break;
+      HB_CHECK(in.good() && lid < nlist, HB_ERR_IO, "bad list record");
+      size_t n = 0, ld = 0, lsk = 0;
+      int32_t lopt = 0;
+      in.read(reinterpret_cast<char*>(&n), sizeof(size_t));
+      in.read(reinterpret_cast<char*>(&ld), sizeof(size_t));
+      in.read(reinterpret_cast<char*>(&lsk), sizeof(size_t));
+      in.read(reinterpret_cast<char*>(&lopt), sizeof(int32_t));
+      HB_CHECK(in.good() && ld == d && n < (1ull << 32), HB_ERR_IO, "bad list header");
+      ListRec& r = lists[lid];
+      std::vector<size_t> ids(n);
+      r.codes.resize(n * d);
+      r.norms.resize(n);
+      in.read(reinterpret_cast<char*>(ids.data()), n * sizeof(size_t));
+      in.read(reinterpret_cast<char*>(r.codes.data()), n * d * sizeof(float));
+      in.read(reinterpret_cast<char*>(r.norms.data()), n * sizeof(float));
+      r.ids.assign(ids.begin(), ids.end());
+      // Opt-level extras (src/IVF.cpp:190-211) are read and dropped.
+      size_t skip = 0;
+      if ((lopt & 1) || (lopt & 4)) skip += 2 * n * sizeof(float);
+      if (lopt & 2) skip += n * lsk * (sizeof(int64_t) + sizeof(float));
+      if (lopt & 4) skip += 2 * n * lsk * (sizeof(int64_t) + sizeof(float));
+      if (skip) in.seekg(static_cast<std::streamoff>(skip), std::ios::cur);
+      HB_CHECK(in.good(), HB_ERR_IO, "truncated list record");
+    }
+    reshape(d, nlist);
+    metric_ = metric;
+    std::vector<float> cpad(nlist * dpad_, 0.0f);
+    for (size_t c = 0; c < nlist; ++c) std::copy(&cent[c * d], &cent[c * d] + d, &cpad[c * dpad_]);
+    HB_CUDA(cudaMemcpyAsync(cent_.p, cpad.data(), cpad.size() * sizeof(float), cudaMemcpyHostToDevice, st_));
+    host_off_.assign(nlist + 1, 0);
+    for (size_t l = 0; l < nlist; ++l) host_off_[l + 1] = host_off_[l] + static_cast<int64_t>(lists[l].ids.size());
+    const size_t nt = static_cast<size_t>(host_off_[nlist]);
+    std::vector<float> codes(nt * dpad_, 0.0f);
+    std::vector<int64_t> ids(nt);
+    std::vector<float> norms(nt);
+    for (size_t l = 0; l < nlist; ++l) {
+      const size_t b = static_cast<size_t>(host_off_[l]);
+      const ListRec& r = lists[l];
+      for (size_t i = 0; i < r.ids.size(); ++i) {
+        ids[b + i] = r.ids[i];
+        norms[b + i] = r.norms[i];
+        std::copy(&r.codes[i * d], &r.codes[i * d] + d, &codes[(b + i) * dpad_]);
+      }
+    }
+    codes_.reserve(std::max<size_t>(nt * dpad_, 1));
+    ids_.reserve(std::max<size_t>(nt, 1));
+    norms_.reserve(std::max<size_t>(nt, 1));
+    if (nt) {
+      HB_CUDA(cudaMemcpyAsync(codes_.p, codes.data(), codes.size() * sizeof(float), cudaMemcpyHostToDevice, st_));
+      HB_CUDA(cudaMemcpyAsync(ids_.p, ids.data(), ids.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st_));
+      HB_CUDA(cudaMemcpyAsync(norms_.p, norms.data(), norms.size() * sizeof(float), cudaMemcpyHostToDevice, st_));
+    }
+    HB_CUDA(cudaMemcpyAsync(list_off_.p, host_off_.data(), (nlist + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                            st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    ntotal_ = nt;
+    trained_ = true;
+    plan_rows_ = 0;
+  }
+
+  void get_centroids(float* out) {
+    HB_CUDA(cudaSetDevice(device_));
+    HB_CUDA(cudaMemcpy2DAsync(out, d_ * sizeof(float), cent_.p, dpad_ * sizeof(float), d_ * sizeof(float), nlist_,
+                              cudaMemcpyDefault, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+  }
+  void get_list_sizes(int64_t* out) {
+    std::vector<int64_t> s(nlist_);
+    for (size_t l = 0; l < nlist_; ++l) s[l] = host_off_[l + 1] - host_off_[l];
+    HB_CUDA(cudaMemcpy(out, s.data(), nlist_ * sizeof(int64_t), cudaMemcpyDefault));
+  }
+
+ private:
+  // Queries per batch: bounded so the coarse matrix and the partial top-k
+  // slots stay within a few GB.
+  size_t batch_limit(size_t P, size_t k) {
+    const size_t by_matrix = std::max<size_t>(1, (size_t(1) << 30) / (nlist_ * sizeof(float)));
+    const size_t by_slots = std::max<size_t>(1, (size_t(2) << 30) / (std::max<size_t>(P, 1) * k * 8 * 2));
+    return std::max<size_t>(1, std::min<size_t>({size_t(65536), by_matrix, by_slots}));
+  }
+
+  // Chunk length of the list scan: keep at least ~4 work items per SM even
+  // for tiny batches, and at most 4096 rows per item.
+  int chunk_rows_for(int nq, int P, int tv) {
+    const double avg = ntotal_ / static_cast<double>(std::max<size_t>(nlist_, 1));
+    const long long rows = static_cast<long long>(nq) * P * std::max(avg, 1.0);
+    int cr = pow2_floor(std::max<long long>(rows / (4LL * num_sms_), 1));
+    cr = std::max(cr, tv);
+    cr = std::min(cr, 4096);
+    return cr;
+  }
+
+  // Upper bound of the output slots of a batch: nq x (sum of the P largest
+  // per-list chunk counts).
+  size_t max_slots(int nq, int P, int cr) {
+    std::vector<int64_t> ch(nlist_);
+    for (size_t l = 0; l < nlist_; ++l) ch[l] = (host_off_[l + 1] - host_off_[l] + cr - 1) / cr;
+    const size_t take = std::min<size_t>(P, nlist_);
+    std::partial_sort(ch.begin(), ch.begin() + take, ch.end(), std::greater<int64_t>());
+    int64_t s = 0;
+    for (size_t i = 0; i < take; ++i) s += ch[i];
+    return static_cast<size_t>(nq) * static_cast<size_t>(std::max<int64_t>(s, 1));
+  }
+
+  void search_batch(int nb, int P, int k, int mode, bool cut, bool need_tops, int warm_lists, int warm_size, int W,
+                    int B, int qblock, float* Dd, int64_t* Id) {
+    int tv = 0, qt = 0, qg = 0;
+    const size_t smem = scan_exact_smem_bytes(static_cast<int>(d_), static_cast<int>(dpad_), k, mode, &tv, &qt, &qg);
+    HB_CHECK(smem > 0, HB_ERR_INVALID, "k too large for the fused scan at this dimension");
+    HB_CHECK(P <= 4095, HB_ERR_INVALID, "nprobe above 4095 is not supported");
+    probes_.reserve(static_cast<size_t>(nb) * P);
+    coarse(qpad_.p, nb, P, probes_.p, nullptr);
+    if (need_tops) {
+      tops_.reserve(nb);
+      launch_warmup_tops(qpad_.p, nb, probes_.p, P, codes_.p, list_off_.p, static_cast<int>(dpad_), k, warm_lists,
+                         warm_size, tops_.p, st_);
+      ++launches_;
+    }
+    const int cr = chunk_rows_for(nb, P, tv);
+    list_cnt_.reserve(nlist_);
+    list_cursor_.reserve(nlist_);
+    list_qoff_.reserve(nlist_ + 1);
+    item_off_.reserve(nlist_ + 1);
+    list_q_.reserve(static_cast<size_t>(nb) * P);
+    slot_base_.reserve(static_cast<size_t>(nb) * P + 1);
+    const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
+    work_tmp_.reserve(wtmp);
+    launch_build_work(probes_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt_.p, list_qoff_.p,
+                      list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+    launches_ += 3;
+    part_.reserve(max_slots(nb, P, cr) * static_cast<size_t>(k));
+    counter_.reserve(1);
+    HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
+    ScanArgs a{};
+    a.codes = codes_.p;
+    a.list_off = list_off_.p;
+    a.nlist = static_cast<int>(nlist_);
+    a.d = static_cast<int>(d_);
+    a.dpad = static_cast<int>(dpad_);
+    a.q = qpad_.p;
+    a.nq = nb;
+    a.P = P;
+    a.k = k;
+    a.list_cnt = list_cnt_.p;
+    a.list_qoff = list_qoff_.p;
+    a.list_q = list_q_.p;
+    a.item_off = item_off_.p;
+    a.slot_base = slot_base_.p;
+    a.chunk_rows = cr;
+    a.qgroup = qg;
+    a.work_counter = counter_.p;
+    a.part = part_.p;
+    a.mode = mode;
+    a.tops = need_tops ? tops_.p : nullptr;
+    a.cut = cut ? 1 : 0;
+    a.nseg = W;
+    a.seg_order = order_dev_.p;
+    a.qblock = qblock;
+    a.nblocks = B;
+    launch_scan_exact(a, num_sms_, st_);
+    launch_merge(part_.p, slot_base_.p, nb, P, k, ids_.p, Dd, Id, st_);
+    launches_ += 2;
+  }
+
+  size_t d_, nlist_, nprobe_;
+  size_t dpad_ = 16;
+  int metric_;
+  int device_;
+  int num_sms_ = 148;
+  cudaStream_t st_ = nullptr;
+  bool trained_ = false;
+  size_t ntotal_ = 0;
+  size_t plan_rows_ = 0;
+  uint64_t launches_ = 0;
+  std::vector<int64_t> host_off_;
+
+  DevBuf<float> cent_, codes_, norms_;
+  DevBuf<int64_t> list_off_, ids_;
+  // search workspace
+  DevBuf<float> qpad_, qtmp_, dmat_, tops_, dout_;
+  DevBuf<int64_t> iout_, list_qoff_, item_off_, slot_base_;
+  DevBuf<int32_t> probes_, list_cnt_, list_cursor_, list_q_, order_dev_;
+  DevBuf<uint64_t> part_;
+  DevBuf<unsigned int> counter_;
+  DevBuf<unsigned char> work_tmp_;
+};
+
+}  // namespace hb
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+struct hb_index {
+  std::unique_ptr<hb::IndexCore> core;
+};
+
+namespace {
+template <class F>
+int guarded(F&& f) {
+  try {
+    hb::g_last_error.clear();
+    f();
+    return HB_OK;
+  } catch (const hb::Error& e) {
+    hb::g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    hb::g_last_error = "host allocation failed";
+    return HB_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    hb::g_last_error = e.what();
+    return HB_ERR_INVALID;
+  }
+}
+#define HB_NEED_INDEX(ix)                                           \
+  do {                                                              \
+    if (!(ix) || !(ix)->core) {                                     \
+      hb::g_last_error = "null index handle";                       \
+      return HB_ERR_INVALID;                                        \
+    }                                                               \
+  } while (0)
+}  // namespace
+
+extern "C" {
+
+void hb_search_params_init(hb_search_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->mode = HB_MODE_ORIGINAL;
+  p->pruning = 0;
+  p->order_optimize = 1;  // Param::orderOptimize default (src/Index.h:49)
+  p->period = 0;
+  p->n_dim_blocks = 1;
+  p->n_query_blocks = 1;
+  p->warmup_lists = 10;      // --warmup_list default (src/query.cpp:100-103)
+  p->warmup_list_size = 0;   // 0 -> k (src/query.cpp:330-333)
+  p->precision = HB_PREC_FP32;
+  p->rerank_mult = 4;
+  p->learned_probe = 0;
+  p->learned_target = 0.0f;
+  p->nprobe_per_query = nullptr;
+  p->max_nprobe = 0;
+}
+
+const char* hb_last_error(void) { return hb::g_last_error.c_str(); }
+
+const char* hb_version(void) { return "harmony_b200 0.1 (sm_100a)"; }
+
+int hb_create(size_t d, size_t nlist, size_t nprobe, int metric, int device, hb_index** out) {
+  if (!out) {
+    hb::g_last_error = "null output handle";
+    return HB_ERR_INVALID;
+  }
+  *out = nullptr;
+  return guarded([&] {
+    auto h = std::make_unique<hb_index>();
+    h->core = std::make_unique<hb::IndexCore>(d, nlist, nprobe, metric, device);
+    *out = h.release();
+  });
+}
+
+int hb_destroy(hb_index* ix) {
+  delete ix;
+  return HB_OK;
+}
+
+int hb_train(hb_index* ix, size_t n, const float* x, int lite) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->train(n, x, lite != 0); });
+}
+
+int hb_add(hb_index* ix, size_t n, const float* x) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->add(n, x); });
+}
+
+int hb_search(hb_index* ix, size_t nq, const float* q, size_t k, const hb_search_params* params, float* D,
+              int64_t* I) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->search(nq, q, k, params, D, I); });
+}
+
+int hb_save_index(hb_index* ix, const char* path) {
+  HB_NEED_INDEX(ix);
+  if (!path) return HB_ERR_INVALID;
+  return guarded([&] { ix->core->save(path); });
+}
+
+int hb_load_index(hb_index* ix, const char* path) {
+  HB_NEED_INDEX(ix);
+  if (!path) return HB_ERR_INVALID;
+  return guarded([&] { ix->core->load(path); });
+}
+
+int hb_set_nprobe(hb_index* ix, size_t nprobe) {
+  HB_NEED_INDEX(ix);
+  ix->core->set_nprobe(nprobe);
+  return HB_OK;
+}
+
+int hb_get_nprobe(const hb_index* ix, size_t* nprobe) {
+  HB_NEED_INDEX(ix);
+  if (!nprobe) return HB_ERR_INVALID;
+  *nprobe = ix->core->nprobe();
+  return HB_OK;
+}
+
+int hb_get_info(const hb_index* ix, size_t* d, size_t* nlist, size_t* ntotal, int* metric) {
+  HB_NEED_INDEX(ix);
+  if (d) *d = ix->core->d();
+  if (nlist) *nlist = ix->core->nlist();
+  if (ntotal) *ntotal = ix->core->ntotal();
+  if (metric) *metric = ix->core->metric();
+  return HB_OK;
+}
+
+int hb_get_centroids(const hb_index* ix, float* out) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->get_centroids(out); });
+}
+
+int hb_get_list_sizes(const hb_index* ix, int64_t* out) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->get_list_sizes(out); });
+}
+
+int hb_probe_lists(hb_index* ix, size_t nq, const float* q, size_t nprobe, int64_t* probes, float* cdist) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->probe_lists(nq, q, nprobe, probes, cdist); });
+}
+
+int hb_warmup_tops(hb_index* ix, size_t nq, const float* q, size_t k, size_t warm_lists, size_t warm_list_size,
+                   float* tops) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->warmup_tops(nq, q, k, warm_lists, warm_list_size, tops); });
+}
+
+void* hb_stream(hb_index* ix) { return (ix && ix->core) ? static_cast<void*>(ix->core->stream()) : nullptr; }
+
+uint64_t hb_launch_count(const hb_index* ix) { return (ix && ix->core) ? ix->core->launches() : 0; }
+
+int hb_train_probe_predictor(hb_index* ix, size_t, const float*, size_t, size_t, float) {
+  HB_NEED_INDEX(ix);
+  hb::g_last_error = "learned probe predictor is not built in this version";
+  return HB_ERR_INVALID;
+}
+
+}  // extern "C"

@@ -1,0 +1,157 @@
+// Internal declarations of the B200 IVF-flat core (host side + kernel
+// launchers).  Nothing here is part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/harmony_b200.h"
+
+namespace hb {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define HB_CUDA(x)                                                                          \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::hb::Error(e_ == cudaErrorMemoryAllocation ? HB_ERR_NOMEM : HB_ERR_CUDA,       \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                   \
+  } while (0)
+
+#define HB_CHECK(cond, code, msg)                     \
+  do {                                                \
+    if (!(cond)) throw ::hb::Error((code), (msg));    \
+  } while (0)
+
+// Device allocation owned by the index.  Grows, never shrinks.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  T* reserve(size_t count) {
+    if (count > n) {
+      release();
+      size_t bytes = count * sizeof(T);
+      if (bytes == 0) bytes = sizeof(T);
+      HB_CUDA(cudaMalloc(&p, bytes));
+      n = count;
+    }
+    return p;
+  }
+  T* get() const { return p; }
+};
+
+// Rows are padded to a multiple of 16 elements so that fp32, bf16 and fp8
+// rows all start on 16-byte boundaries; padding is zero in codes and queries,
+// which leaves every sequential sum unchanged (adding +0.0f is exact).
+inline size_t pad_dim(size_t d) { return (d + 15) / 16 * 16; }
+
+constexpr uint64_t kEmptyKey = ~0ull;
+
+// ---- kernel launchers (defined in the .cu files) --------------------------
+
+struct ScanPlan;  // device-resident work description of one search batch
+
+// k_exact.cu
+// Exact FP32 distance matrix D[q][c] for q < nq, c < nrows (sequential
+// unfused sums over dpad dims).
+void launch_l2_matrix(const float* q, int nq, const float* rows, int nrows, int dpad, float* D,
+                      int ldD, cudaStream_t st);
+// Exact nearest row per query (strict '<', lowest row index wins ties).
+void launch_l2_argmin(const float* q, int nq, const float* rows, int nrows, int dpad, int32_t* arg,
+                      float* dist, cudaStream_t st);
+
+// Scan modes: the reference's three per-candidate accumulations.
+enum ScanMode : int { SCAN_PLAIN = 0, SCAN_CHUNK4 = 1, SCAN_DIMBLOCK = 2 };
+
+struct ScanArgs {
+  // index
+  const float* codes;      // nb x dpad
+  const int64_t* list_off; // nlist + 1
+  int nlist;
+  int d, dpad;
+  // queries
+  const float* q;          // nq x dpad
+  int nq, P, k;
+  // work description
+  const int32_t* list_cnt;     // queries per list
+  const int64_t* list_qoff;    // exclusive scan of list_cnt (nlist + 1)
+  const int32_t* list_q;       // (query << 12 | probe rank) entries, grouped by list
+  const int64_t* item_off;     // exclusive scan of items per list (nlist + 1)
+  const int64_t* slot_base;    // nq*P + 1 exclusive scan of chunks per (q, j)
+  int chunk_rows;              // vectors per chunk
+  int qgroup;                  // queries per work item
+  unsigned int* work_counter;  // persistent scheduler counter (zeroed per launch)
+  uint64_t* part;              // slots x k partial top-k keys
+  // pruning
+  int mode;                    // ScanMode
+  const float* tops;           // per-query heap tops (CHUNK4 / DIMBLOCK)
+  int cut;                     // pruning on
+  int nseg;                    // DIMBLOCK slices
+  const int32_t* seg_order;    // DIMBLOCK: order[b * nseg + t]
+  int qblock;                  // DIMBLOCK: queries per block
+  int nblocks;                 // DIMBLOCK: blocks
+};
+void launch_scan_exact(const ScanArgs& a, int num_sms, cudaStream_t st);
+size_t scan_exact_smem_bytes(int d, int dpad, int k, int mode, int* tv, int* qt, int* qgroup);
+
+// k_select.cu
+// Row-wise selection of the k smallest (value, column) pairs of a float
+// matrix; out_idx gets columns, out_val the values, ascending.
+void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx,
+                        float* out_val, cudaStream_t st);
+// Build the list-major work description from probes (nq x P, -1 = none).
+void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist,
+                       int chunk_rows, int qgroup, int32_t* list_cnt, int64_t* list_qoff,
+                       int32_t* list_cursor, int32_t* list_q, int64_t* item_off, int64_t* slot_base,
+                       void* scan_tmp, size_t scan_tmp_bytes, cudaStream_t st);
+size_t build_work_tmp_bytes(int nq, int P, int nlist);
+// Merge partial top-k slots of each query to the final top-k.
+void launch_merge(const uint64_t* part, const int64_t* slot_base, int nq, int P, int k,
+                  const int64_t* ids, float* D, int64_t* I, cudaStream_t st);
+// Warm-up heap tops (k-th smallest distance over the warm-up candidates).
+void launch_warmup_tops(const float* q, int nq, const int32_t* probes, int P, const float* codes,
+                        const int64_t* list_off, int dpad, int k, int warm_lists,
+                        int warm_list_size, float* tops, cudaStream_t st);
+
+// k_build.cu
+void launch_pad_rows(const float* src, size_t n, int d, int dpad, float* dst, cudaStream_t st);
+void launch_gather_rows(const float* src, const int64_t* idx, size_t n, int dpad, float* dst,
+                        cudaStream_t st);
+void launch_kmeans_accumulate(const float* x, const int32_t* assign, size_t n, int d, int dpad,
+                              double* sums, int32_t* counts, cudaStream_t st);
+void launch_kmeans_update(const double* sums, const int32_t* counts, int nlist, int d, int dpad,
+                          float* cent, cudaStream_t st);
+void launch_row_norms(const float* x, size_t n, int d, int dpad, float* norms, cudaStream_t st);
+void launch_add_keys(const int32_t* assign, const float* dist, size_t n, uint64_t* keys,
+                     uint32_t* vals, cudaStream_t st);
+void sort_pairs_u64(uint64_t* keys_in, uint64_t* keys_out, uint32_t* vals_in, uint32_t* vals_out,
+                    size_t n, int end_bit, void* tmp, size_t* tmp_bytes, cudaStream_t st);
+void launch_scatter_sorted(const float* x, const uint32_t* order, size_t n, int d, int dpad,
+                           float* codes, int64_t* ids, cudaStream_t st);
+void launch_list_offsets(const int32_t* assign, size_t n, int nlist, int64_t* list_off,
+                         void* tmp, size_t tmp_bytes, cudaStream_t st);
+size_t list_offsets_tmp_bytes(int nlist);
+void launch_i64_to_i32(const int64_t* src, size_t n, int32_t* dst, cudaStream_t st);
+void launch_i32_to_i64(const int32_t* src, size_t n, int64_t* dst, cudaStream_t st);
+void launch_fill_results(float* D, int64_t* I, size_t n, cudaStream_t st);
+
+}  // namespace hb

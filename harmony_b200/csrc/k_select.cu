@@ -1,0 +1,394 @@
+// Selection and scheduling kernels of the search pipeline.
+//
+//  * select_rows_kernel -- coarse quantizer: the P smallest (distance,
+//    centroid) pairs of each query's row, ascending.  The reference keeps a
+//    max-heap of nprobe with strict '<' admission and heap-sorts it
+//    (src/IVFScan.hpp:108-138, src/Index.cpp:1440-1448); the selected set is
+//    the P smallest distances (ties broken here by the lower centroid id) and
+//    centroids at or above FLT_MAX are never admitted.
+//  * build-work kernels -- turn the probe table into the list-major work
+//    description the persistent scan consumes (which queries probe each
+//    list, items per list, output slots per (query, probe)).
+//  * merge_kernel -- the k smallest keys over all partial slots of a query
+//    (the master's heap merge of worker heaps, src/Index.cpp:1324-1343, done
+//    as one selection), decoded to (distance, id).
+//  * warmup_tops_kernel -- Index::warmUpSearch (src/Index.cpp:999-1051):
+//    k-th smallest distance over the first warm_list_size vectors of the
+//    first warm_lists probed lists; FLT_MAX when fewer than k qualify.
+//
+// All selections are radix selections over 64-bit keys (distance bits, tie)
+// followed by a bitonic sort of the k winners in shared memory.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include "hb_device.cuh"
+#include "hb_internal.hpp"
+
+namespace hb {
+namespace {
+
+constexpr int kSelThreads = 256;
+constexpr int kMaxSelect = 8192;  // largest k a single selection returns
+
+struct SelectShared {
+  int hist[256];
+  int bucket;
+  int need;
+  int count;
+  int real;
+};
+
+// Radix selection of the kk smallest non-empty keys among key_at(0..m).
+// On return s_out[0..kk) holds them (unordered) and the function returns kk.
+template <class KeyAt>
+__device__ int block_select(KeyAt key_at, int m, int kk, SelectShared& sh, uint64_t* s_out) {
+  const int tid = threadIdx.x;
+  uint64_t prefix = 0;
+  int shift = 64;
+  int need = kk;
+  // Narrow the prefix one byte at a time until the chosen bucket holds
+  // exactly the keys still needed.
+  while (shift > 0) {
+    shift -= 8;
+    for (int i = tid; i < 256; i += blockDim.x) sh.hist[i] = 0;
+    __syncthreads();
+    for (int i = tid; i < m; i += blockDim.x) {
+      const uint64_t key = key_at(i);
+      if (key == kEmpty) continue;
+      if (shift == 56 || (key >> (shift + 8)) == (prefix >> (shift + 8)))
+        atomicAdd(&sh.hist[(key >> shift) & 255], 1);
+    }
+    __syncthreads();
+    if (tid < 32) {
+      // Lane L owns bins [8L, 8L+8).
+      int loc[8];
+      int sum = 0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        loc[b] = sh.hist[tid * 8 + b];
+        sum += loc[b];
+      }
+      int incl = sum;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (tid >= off) incl += o;
+      }
+      const int excl = incl - sum;
+      const unsigned hit = __ballot_sync(0xffffffffu, incl >= need);
+      const int lane = __ffs(hit) - 1;
+      if (tid == lane) {
+        int cum = excl;
+        int b = 0;
+        for (; b < 8; ++b) {
+          if (cum + loc[b] >= need) break;
+          cum += loc[b];
+        }
+        sh.bucket = tid * 8 + b;
+        sh.need = need - cum;
+        sh.count = loc[b];
+      }
+    }
+    __syncthreads();
+    prefix |= static_cast<uint64_t>(sh.bucket) << shift;
+    need = sh.need;
+    const bool done = sh.count == need;
+    __syncthreads();
+    if (done) break;
+  }
+  // Keys whose top (64 - shift) bits are <= the prefix's are the selection.
+  if (tid == 0) sh.count = 0;
+  __syncthreads();
+  const uint64_t lim = prefix >> shift;
+  for (int i = tid; i < m; i += blockDim.x) {
+    const uint64_t key = key_at(i);
+    if (key == kEmpty) continue;
+    if ((shift == 64 ? 0 : (key >> shift)) <= lim) {
+      const int pos = atomicAdd(&sh.count, 1);
+      if (pos < kk) s_out[pos] = key;
+    }
+  }
+  __syncthreads();
+  return kk;
+}
+
+// Count keys that are not empty.
+template <class KeyAt>
+__device__ int block_count_real(KeyAt key_at, int m, SelectShared& sh) {
+  if (threadIdx.x == 0) sh.real = 0;
+  __syncthreads();
+  int c = 0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) c += key_at(i) != kEmpty;
+  for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&sh.real, c);
+  __syncthreads();
+  return sh.real;
+}
+
+// Select and sort: s_out gets the min(k, real) smallest keys ascending,
+// padded with kEmpty to pow2_ceil(k).
+template <class KeyAt>
+__device__ int block_topk_sorted(KeyAt key_at, int m, int k, SelectShared& sh, uint64_t* s_out) {
+  const int real = block_count_real(key_at, m, sh);
+  const int kk = min(k, real);
+  const int n2 = pow2_ceil(max(k, 2));
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) s_out[i] = kEmpty;
+  __syncthreads();
+  if (kk > 0) block_select(key_at, m, kk, sh, s_out);
+  block_bitonic_sort(s_out, n2);
+  return kk;
+}
+
+__global__ void __launch_bounds__(kSelThreads) select_rows_kernel(const float* __restrict__ D, int ncols,
+                                                                  int ldD, int k, int32_t* __restrict__ out_idx,
+                                                                  float* __restrict__ out_val) {
+  extern __shared__ uint64_t s_out[];
+  __shared__ SelectShared sh;
+  const float* row = D + static_cast<size_t>(blockIdx.x) * ldD;
+  auto key_at = [&](int i) -> uint64_t {
+    const float v = row[i];
+    return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(i)) : kEmpty;
+  };
+  block_topk_sorted(key_at, ncols, k, sh, s_out);
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    const uint64_t key = s_out[j];
+    const size_t o = static_cast<size_t>(blockIdx.x) * k + j;
+    out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
+    if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+  }
+}
+
+__global__ void __launch_bounds__(kSelThreads) merge_kernel(const uint64_t* __restrict__ part,
+                                                            const int64_t* __restrict__ slot_base, int P, int k,
+                                                            const int64_t* __restrict__ ids, float* __restrict__ D,
+                                                            int64_t* __restrict__ I) {
+  extern __shared__ uint64_t s_out[];
+  __shared__ SelectShared sh;
+  const int q = blockIdx.x;
+  const int64_t s0 = slot_base[static_cast<int64_t>(q) * P];
+  const int64_t s1 = slot_base[static_cast<int64_t>(q + 1) * P];
+  const uint64_t* src = part + s0 * k;
+  const int m = static_cast<int>((s1 - s0) * k);
+  auto key_at = [&](int i) -> uint64_t { return src[i]; };
+  block_topk_sorted(key_at, m, k, sh, s_out);
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    const uint64_t key = s_out[j];
+    const size_t o = static_cast<size_t>(q) * k + j;
+    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+  }
+}
+
+__global__ void __launch_bounds__(kSelThreads) warmup_tops_kernel(const float* __restrict__ q,
+                                                                  const int32_t* __restrict__ probes, int P,
+                                                                  const float* __restrict__ codes,
+                                                                  const int64_t* __restrict__ list_off, int dpad,
+                                                                  int k, int wl, int wls, float* __restrict__ tops) {
+  extern __shared__ __align__(16) unsigned char wsm[];
+  __shared__ SelectShared sh;
+  __shared__ int64_t sbeg[64];
+  __shared__ int scnt[65];
+  const int qi = blockIdx.x;
+  float* sq = reinterpret_cast<float*>(wsm);
+  float* sd = sq + dpad;
+  const int ncap = wl * wls;
+  uint64_t* s_out = reinterpret_cast<uint64_t*>(sd + ((ncap + 1) & ~1));
+  for (int c = threadIdx.x; c < dpad; c += blockDim.x) sq[c] = q[static_cast<size_t>(qi) * dpad + c];
+  if (threadIdx.x == 0) {
+    int tot = 0;
+    for (int j = 0; j < wl; ++j) {
+      const int l = probes[static_cast<size_t>(qi) * P + j];
+      int64_t n = 0;
+      if (l >= 0) {
+        sbeg[j] = list_off[l];
+        n = list_off[l + 1] - list_off[l];
+      }
+      scnt[j] = tot;
+      tot += static_cast<int>(n < wls ? n : wls);
+    }
+    scnt[wl] = tot;
+  }
+  __syncthreads();
+  const int m = scnt[wl];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    int j = 0;
+    while (scnt[j + 1] <= i) ++j;
+    const float* x = codes + static_cast<size_t>(sbeg[j] + (i - scnt[j])) * dpad;
+    float acc = 0.0f;
+    for (int c = 0; c < dpad; c += 4) {
+      const float4 v = *reinterpret_cast<const float4*>(x + c);
+      float t;
+      t = __fsub_rn(sq[c], v.x);
+      acc = __fadd_rn(acc, __fmul_rn(t, t));
+      t = __fsub_rn(sq[c + 1], v.y);
+      acc = __fadd_rn(acc, __fmul_rn(t, t));
+      t = __fsub_rn(sq[c + 2], v.z);
+      acc = __fadd_rn(acc, __fmul_rn(t, t));
+      t = __fsub_rn(sq[c + 3], v.w);
+      acc = __fadd_rn(acc, __fmul_rn(t, t));
+    }
+    sd[i] = acc;
+  }
+  __syncthreads();
+  auto key_at = [&](int i) -> uint64_t {
+    const float v = sd[i];
+    return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(i)) : kEmpty;
+  };
+  const int real = block_count_real(key_at, m, sh);
+  if (real < k) {
+    if (threadIdx.x == 0) tops[qi] = FLT_MAX;
+    return;
+  }
+  block_select(key_at, m, k, sh, s_out);
+  // The k-th smallest is the largest selected key.
+  if (threadIdx.x == 0) {
+    uint64_t mx = 0;
+    for (int i = 0; i < k; ++i) mx = s_out[i] > mx ? s_out[i] : mx;
+    tops[qi] = key_dist(mx);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Work description.
+
+__global__ void count_probes_kernel(const int32_t* __restrict__ probes, int nqp, int P,
+                                    const int64_t* __restrict__ list_off, int chunk_rows,
+                                    int32_t* __restrict__ list_cnt, int64_t* __restrict__ slot_cnt) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nqp) return;
+  const int l = probes[idx];
+  int64_t nch = 0;
+  if (l >= 0) {
+    const int64_t n = list_off[l + 1] - list_off[l];
+    if (n > 0) {
+      nch = (n + chunk_rows - 1) / chunk_rows;
+      atomicAdd(&list_cnt[l], 1);
+    }
+  }
+  slot_cnt[idx] = nch;
+}
+
+__global__ void list_items_kernel(const int32_t* __restrict__ list_cnt, const int64_t* __restrict__ list_off,
+                                  int nlist, int chunk_rows, int qgroup, int64_t* __restrict__ cnt64,
+                                  int64_t* __restrict__ items) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l > nlist) return;
+  if (l == nlist) {
+    cnt64[l] = 0;
+    items[l] = 0;
+    return;
+  }
+  const int64_t n = list_off[l + 1] - list_off[l];
+  const int64_t nch = (n + chunk_rows - 1) / chunk_rows;
+  const int64_t ng = (list_cnt[l] + qgroup - 1) / qgroup;
+  cnt64[l] = list_cnt[l];
+  items[l] = nch * ng;
+}
+
+__global__ void scatter_probes_kernel(const int32_t* __restrict__ probes, int nqp, int P,
+                                      const int64_t* __restrict__ list_off, const int64_t* __restrict__ list_qoff,
+                                      int32_t* __restrict__ cursor, int32_t* __restrict__ list_q) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nqp) return;
+  const int l = probes[idx];
+  if (l < 0 || list_off[l + 1] == list_off[l]) return;
+  const int pos = atomicAdd(&cursor[l], 1);
+  const int q = idx / P, j = idx - q * P;
+  list_q[list_qoff[l] + pos] = (q << 12) | j;
+}
+
+size_t cub_scan_bytes(size_t n) {
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, static_cast<const int64_t*>(nullptr),
+                                static_cast<int64_t*>(nullptr), static_cast<int64_t>(n));
+  return bytes;
+}
+
+void exclusive_sum(const int64_t* in, int64_t* out, size_t n, void* tmp, size_t tmp_bytes, cudaStream_t st) {
+  size_t bytes = tmp_bytes;
+  HB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, static_cast<int64_t>(n), st));
+}
+
+}  // namespace
+
+void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx, float* out_val,
+                        cudaStream_t st) {
+  if (nrows <= 0 || k <= 0) return;
+  HB_CHECK(k <= kMaxSelect, HB_ERR_INVALID, "nprobe above 8192 is not supported");
+  const size_t smem = static_cast<size_t>(pow2_ceil(k < 2 ? 2 : k)) * 8;
+  HB_CUDA(cudaFuncSetAttribute(select_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)));
+  select_rows_kernel<<<nrows, kSelThreads, smem, st>>>(D, ncols, ldD, k, out_idx, out_val);
+  HB_CUDA(cudaGetLastError());
+}
+
+size_t build_work_tmp_bytes(int nq, int P, int nlist) {
+  const size_t n1 = static_cast<size_t>(nlist) + 1;
+  const size_t n2 = static_cast<size_t>(nq) * P + 1;
+  size_t cub_bytes = std::max(cub_scan_bytes(n1), cub_scan_bytes(n2));
+  cub_bytes = (cub_bytes + 255) / 256 * 256;
+  // cub scratch + cnt64 + items64 + slot_cnt64
+  return cub_bytes + (2 * n1 + n2) * sizeof(int64_t) + 256;
+}
+
+void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist, int chunk_rows,
+                       int qgroup, int32_t* list_cnt, int64_t* list_qoff, int32_t* list_cursor, int32_t* list_q,
+                       int64_t* item_off, int64_t* slot_base, void* scan_tmp, size_t scan_tmp_bytes,
+                       cudaStream_t st) {
+  const size_t n1 = static_cast<size_t>(nlist) + 1;
+  const size_t n2 = static_cast<size_t>(nq) * P + 1;
+  size_t cub_bytes = std::max(cub_scan_bytes(n1), cub_scan_bytes(n2));
+  cub_bytes = (cub_bytes + 255) / 256 * 256;
+  HB_CHECK(scan_tmp_bytes >= cub_bytes + (2 * n1 + n2) * sizeof(int64_t), HB_ERR_INVALID,
+           "work scratch too small");
+  unsigned char* base = static_cast<unsigned char*>(scan_tmp);
+  void* cub_tmp = base;
+  int64_t* cnt64 = reinterpret_cast<int64_t*>(base + cub_bytes);
+  int64_t* items64 = cnt64 + n1;
+  int64_t* slot_cnt = items64 + n1;
+  const int nqp = nq * P;
+  HB_CUDA(cudaMemsetAsync(list_cnt, 0, sizeof(int32_t) * nlist, st));
+  HB_CUDA(cudaMemsetAsync(list_cursor, 0, sizeof(int32_t) * nlist, st));
+  HB_CUDA(cudaMemsetAsync(slot_cnt + nqp, 0, sizeof(int64_t), st));
+  const int tb = 256;
+  count_probes_kernel<<<(nqp + tb - 1) / tb, tb, 0, st>>>(probes, nqp, P, list_off, chunk_rows, list_cnt, slot_cnt);
+  list_items_kernel<<<(nlist + 1 + tb - 1) / tb, tb, 0, st>>>(list_cnt, list_off, nlist, chunk_rows, qgroup, cnt64,
+                                                              items64);
+  HB_CUDA(cudaGetLastError());
+  exclusive_sum(cnt64, list_qoff, n1, cub_tmp, cub_bytes, st);
+  exclusive_sum(items64, item_off, n1, cub_tmp, cub_bytes, st);
+  exclusive_sum(slot_cnt, slot_base, n2, cub_tmp, cub_bytes, st);
+  scatter_probes_kernel<<<(nqp + tb - 1) / tb, tb, 0, st>>>(probes, nqp, P, list_off, list_qoff, list_cursor,
+                                                            list_q);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_merge(const uint64_t* part, const int64_t* slot_base, int nq, int P, int k, const int64_t* ids,
+                  float* D, int64_t* I, cudaStream_t st) {
+  if (nq <= 0) return;
+  HB_CHECK(k <= kMaxSelect, HB_ERR_INVALID, "k above 8192 is not supported");
+  const size_t smem = static_cast<size_t>(pow2_ceil(k < 2 ? 2 : k)) * 8;
+  HB_CUDA(cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  merge_kernel<<<nq, kSelThreads, smem, st>>>(part, slot_base, P, k, ids, D, I);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_warmup_tops(const float* q, int nq, const int32_t* probes, int P, const float* codes,
+                        const int64_t* list_off, int dpad, int k, int warm_lists, int warm_list_size, float* tops,
+                        cudaStream_t st) {
+  if (nq <= 0) return;
+  const int wl = warm_lists < P ? warm_lists : P;
+  HB_CHECK(wl <= 64, HB_ERR_INVALID, "warm-up over more than 64 lists is not supported");
+  const int ncap = wl * warm_list_size;
+  HB_CHECK(ncap <= 16384, HB_ERR_INVALID, "warm-up candidate count above 16384 is not supported");
+  HB_CHECK(k <= kMaxSelect, HB_ERR_INVALID, "k above 8192 is not supported");
+  const size_t smem = static_cast<size_t>(dpad) * 4 + static_cast<size_t>((ncap + 1) & ~1) * 4 +
+                      static_cast<size_t>(k) * 8 + 16;
+  HB_CUDA(cudaFuncSetAttribute(warmup_tops_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)));
+  warmup_tops_kernel<<<nq, kSelThreads, smem, st>>>(q, probes, P, codes, list_off, dpad, k, wl, warm_list_size,
+                                                    tops);
+  HB_CUDA(cudaGetLastError());
+}
+
+}  // namespace hb

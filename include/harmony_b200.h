@@ -1,0 +1,151 @@
+/*
+ * harmony_b200 -- C ABI of the B200 IVF-flat index.
+ *
+ * This is the drop-in boundary for the IVF-flat train/add/search path of
+ * xuqianmamba/Harmony.  Each entry point replaces one member of the
+ * reference's C++ class harmony::Index (src/Index.h) and keeps its argument
+ * meaning; errors come back as status codes plus a thread-local message
+ * instead of C++ exceptions (the reference throws std::runtime_error at
+ * src/Index.cpp:60, 464, 1644, 1711, 1737).
+ *
+ * Conventions
+ *   - Every function returns HB_OK (0) or an hb_status error code; the text
+ *     of the last error on the calling thread is hb_last_error().
+ *   - Array arguments may be host or device pointers (CUDA unified
+ *     addressing tells them apart).  Results land where the caller's pointer
+ *     points.  Host arrays are copied through the index's own stream.
+ *   - One CUDA stream per index (hb_stream).  An index is not re-entrant,
+ *     like the reference (search mutates nprobe, src/Index.cpp:1646-1648).
+ *   - Vector ids are int64 (idx_t in src/common.h:83); distances are squared
+ *     L2 in float32, ascending per query; missing results are FLT_MAX / -1
+ *     (heap_init, src/heap.hpp:13-25).
+ */
+#ifndef HARMONY_B200_H
+#define HARMONY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hb_index hb_index;
+
+typedef enum {
+  HB_OK = 0,
+  HB_ERR_INVALID = 1,   /* bad argument or unsupported option            */
+  HB_ERR_CUDA = 2,      /* CUDA runtime error (message has the detail)   */
+  HB_ERR_IO = 3,        /* index file could not be opened / parsed       */
+  HB_ERR_STATE = 4,     /* call out of order (e.g. add before train)     */
+  HB_ERR_NOMEM = 5,     /* device or host allocation failed              */
+  HB_ERR_NODEVICE = 6   /* no CUDA device / library built without it     */
+} hb_status;
+
+/* MetricType, src/common.h:20-21 (same values). Only L2 is implemented. */
+enum { HB_METRIC_IP = 0, HB_METRIC_L2 = 1 };
+
+/* Index::SearchMode, src/Index.h:29-35 (same order). */
+enum {
+  HB_MODE_BRUTE_FORCE = 0,
+  HB_MODE_ORIGINAL = 1,   /* single-process search, src/Index.cpp:1664-1703   */
+  HB_MODE_DIVIDE_IVF = 2, /* list partition + warm-up pruning, node.cpp:606  */
+  HB_MODE_DIVIDE_DIM = 3, /* dimension relay + pruning, node.cpp:297-431     */
+  HB_MODE_DIVIDE_GROUP = 4
+};
+
+/* Arithmetic of the list scan. FP32 reproduces the reference's distances
+ * bit for bit; BF16 / FP8 scan on tensor cores and re-rank the widened
+ * candidate set in exact FP32. */
+enum { HB_PREC_FP32 = 0, HB_PREC_BF16 = 1, HB_PREC_FP8 = 2 };
+
+/* Search options: the fields of Index::Param that steer search
+ * (src/Index.h:48-68) plus the GPU-only knobs.  hb_search_params_init()
+ * fills the reference defaults. */
+typedef struct {
+  int32_t mode;               /* HB_MODE_*; default ORIGINAL                    */
+  int32_t pruning;            /* Param::pruning / !--disablePruning            */
+  int32_t order_optimize;     /* Param::orderOptimize                          */
+  int32_t period;             /* Param::period                                 */
+  int32_t n_dim_blocks;       /* DIVIDE_DIM workers = dimension slices (d % n == 0) */
+  int32_t n_query_blocks;     /* DIVIDE_DIM blockCount                         */
+  int32_t warmup_lists;       /* preSearch warmUpSearchList (default 10)        */
+  int32_t warmup_list_size;   /* preSearch warmUpSearchListSize (0 -> k)        */
+  int32_t precision;          /* HB_PREC_*                                     */
+  int32_t rerank_mult;        /* BF16/FP8: candidates kept = rerank_mult * k    */
+  int32_t learned_probe;      /* 1: per-query nprobe from the learned predictor */
+  float learned_target;       /* predictor target recall (0 -> trained target)   */
+  const int32_t* nprobe_per_query; /* optional nq array (host or device); overrides nprobe */
+  int32_t max_nprobe;         /* cap for per-query nprobe (0 -> index nprobe)    */
+  int32_t reserved[6];
+} hb_search_params;
+
+void hb_search_params_init(hb_search_params* p);
+
+/* Thread-local text of the last error ("" if none). */
+const char* hb_last_error(void);
+
+/* Version string and build info. */
+const char* hb_version(void);
+
+/* Index(d, nlist, nprobe, metric, ...), src/Index.h:15-25 and
+ * src/Index.cpp:24-43.  device: CUDA ordinal. */
+int hb_create(size_t d, size_t nlist, size_t nprobe, int metric, int device, hb_index** out);
+int hb_destroy(hb_index* ix);
+
+/* Index::train(n, codes), src/Index.cpp:381-425: k-means, 20 iterations
+ * (2 with lite), seed 6666, at most 256 points per centroid. */
+int hb_train(hb_index* ix, size_t n, const float* x, int lite);
+
+/* Index::add(n, codes), src/Index.cpp:581-698: replaces the lists with the
+ * n vectors, ids 0..n-1. */
+int hb_add(hb_index* ix, size_t n, const float* x);
+
+/* Index::search(n, queries, k, distances, labels), src/Index.cpp:1638-1706.
+ * params may be NULL (ORIGINAL, FP32).  D: nq*k floats, I: nq*k int64. */
+int hb_search(hb_index* ix, size_t nq, const float* q, size_t k, const hb_search_params* params,
+              float* D, int64_t* I);
+
+/* Index::save_index / load_index, src/Index.cpp:1708-1770 (byte format of
+ * the reference). */
+int hb_save_index(hb_index* ix, const char* path);
+int hb_load_index(hb_index* ix, const char* path);
+
+/* The public field Index::nprobe (mutated between searches by the
+ * reference driver, src/query.cpp:683). */
+int hb_set_nprobe(hb_index* ix, size_t nprobe);
+int hb_get_nprobe(const hb_index* ix, size_t* nprobe);
+
+/* Shape of the index. ntotal = vectors added. */
+int hb_get_info(const hb_index* ix, size_t* d, size_t* nlist, size_t* ntotal, int* metric);
+
+/* Copies of the index content (host or device destinations). */
+int hb_get_centroids(const hb_index* ix, float* out);        /* nlist * d          */
+int hb_get_list_sizes(const hb_index* ix, int64_t* out);     /* nlist              */
+
+/* Coarse quantizer only: probe lists of each query, ascending by exact
+ * centroid distance (Index::findNearNprobeOfCentroidIds,
+ * src/Index.cpp:967-995).  probes: nq*nprobe int64, cdist may be NULL. */
+int hb_probe_lists(hb_index* ix, size_t nq, const float* q, size_t nprobe, int64_t* probes,
+                   float* cdist);
+
+/* Warm-up heap tops (Index::warmUpSearch, src/Index.cpp:999-1051). */
+int hb_warmup_tops(hb_index* ix, size_t nq, const float* q, size_t k, size_t warm_lists,
+                   size_t warm_list_size, float* tops);
+
+/* The CUDA stream this index launches on (a cudaStream_t). */
+void* hb_stream(hb_index* ix);
+
+/* Number of kernels this index has launched so far (for launch accounting). */
+uint64_t hb_launch_count(const hb_index* ix);
+
+/* Learned probe predictor (no reference counterpart): train from nt training
+ * queries labelled by the plain search at nprobe = label_nprobe, for a recall
+ * target in (0, 1]. */
+int hb_train_probe_predictor(hb_index* ix, size_t nt, const float* q, size_t k, size_t label_nprobe,
+                             float target);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HARMONY_B200_H */

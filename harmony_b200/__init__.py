@@ -136,6 +136,9 @@ def lib() -> ctypes.CDLL:
     L.hb_launch_count.restype = ctypes.c_uint64
     L.hb_launch_count.argtypes = [vp]
     L.hb_train_probe_predictor.argtypes = [vp, sz, f, sz, sz, ctypes.c_float]
+    L.hb_profile_enable.argtypes = [vp, ctypes.c_int]
+    L.hb_profile_read.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
 
@@ -280,6 +283,20 @@ class Index:
 
     def launch_count(self) -> int:
         return int(self._L.hb_launch_count(self._h))
+
+    def profile(self, on: bool = True) -> None:
+        """Record CUDA events around every kernel on the index's stream."""
+        _check(self._L.hb_profile_enable(self._h, int(on)))
+
+    def profile_read(self) -> dict:
+        """{kernel name: (total ms, launches)} since the last read."""
+        names = ctypes.create_string_buffer(4096)
+        ms = np.zeros(64, np.float64)
+        cnt = np.zeros(64, np.int64)
+        n = ctypes.c_int()
+        _check(self._L.hb_profile_read(self._h, names, 4096, ms.ctypes.data, cnt.ctypes.data, 64, ctypes.byref(n)))
+        keys = names.value.decode().split("\n")[: n.value]
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(keys)}
 
     # -- train / add -------------------------------------------------------
     def train(self, n: int, codes, faiss: bool = False, lite: bool = False) -> None:

@@ -82,6 +82,13 @@ std::vector<int32_t> block_visit_order(int W, int B, bool order_optimize, bool p
   return order;
 }
 
+// Per-kernel timing with CUDA events on the index's stream (enabled by
+// hb_profile_enable; read and cleared by hb_profile_read).
+struct ProfRecord {
+  const char* name;
+  cudaEvent_t a, b;
+};
+
 class IndexCore {
  public:
   IndexCore(size_t d, size_t nlist, size_t nprobe, int metric, int device)
@@ -130,6 +137,75 @@ class IndexCore {
   int metric() const { return metric_; }
   cudaStream_t stream() const { return st_; }
   uint64_t launches() const { return launches_; }
+
+  // ---- profiling -------------------------------------------------------------
+  struct Scope {
+    IndexCore* ix;
+    const char* name;
+    cudaEvent_t a = nullptr;
+    Scope(IndexCore* i, const char* n) : ix(i), name(n) {
+      if (ix->prof_) {
+        a = ix->event();
+        cudaEventRecord(a, ix->st_);
+      }
+    }
+    ~Scope() {
+      if (a) {
+        cudaEvent_t b = ix->event();
+        cudaEventRecord(b, ix->st_);
+        ix->prof_log_.push_back({name, a, b});
+      }
+    }
+  };
+  cudaEvent_t event() {
+    if (!ev_pool_.empty()) {
+      cudaEvent_t e = ev_pool_.back();
+      ev_pool_.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    HB_CUDA(cudaEventCreate(&e));
+    return e;
+  }
+  void profile_enable(bool on) { prof_ = on; }
+  // Sums of the recorded intervals per name (ms) and their counts.
+  int profile_read(char* names, size_t names_len, double* ms, int64_t* counts, int max_entries) {
+    HB_CUDA(cudaStreamSynchronize(st_));
+    std::vector<std::string> keys;
+    std::vector<double> tot;
+    std::vector<int64_t> cnt;
+    for (auto& r : prof_log_) {
+      float t = 0.f;
+      HB_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+      size_t i = 0;
+      for (; i < keys.size(); ++i)
+        if (keys[i] == r.name) break;
+      if (i == keys.size()) {
+        keys.push_back(r.name);
+        tot.push_back(0.0);
+        cnt.push_back(0);
+      }
+      tot[i] += t;
+      cnt[i] += 1;
+      ev_pool_.push_back(r.a);
+      ev_pool_.push_back(r.b);
+    }
+    prof_log_.clear();
+    std::string joined;
+    for (size_t i = 0; i < keys.size(); ++i) {
+      if (static_cast<int>(i) < max_entries) {
+        if (ms) ms[i] = tot[i];
+        if (counts) counts[i] = cnt[i];
+      }
+      joined += keys[i];
+      joined += '\n';
+    }
+    if (names && names_len) {
+      std::strncpy(names, joined.c_str(), names_len - 1);
+      names[names_len - 1] = 0;
+    }
+    return static_cast<int>(keys.size());
+  }
 
   // ---- input staging -------------------------------------------------------
 
@@ -272,8 +348,12 @@ class IndexCore {
   // probes_out (device, nq x P int32, ascending), cdist_out optional.
   void coarse(const float* qpad, int nq, int P, int32_t* probes_out, float* cdist_out) {
     dmat_.reserve(static_cast<size_t>(nq) * nlist_);
+    {
+    Scope sc(this, "coarse_l2_matrix");
     launch_l2_matrix(qpad, nq, cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), dmat_.p,
                      static_cast<int>(nlist_), st_);
+    }
+    Scope sc(this, "coarse_select");
     launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), P, probes_out, cdist_out, st_);
     launches_ += 2;
   }
@@ -567,7 +647,7 @@ class IndexCore {
   size_t batch_limit(size_t P, size_t k) {
     const size_t by_matrix = std::max<size_t>(1, (size_t(1) << 30) / (nlist_ * sizeof(float)));
     const size_t by_slots = std::max<size_t>(1, (size_t(2) << 30) / (std::max<size_t>(P, 1) * k * 8 * 2));
-    return std::max<size_t>(1, std::min<size_t>({size_t(65536), by_matrix, by_slots}));
+    return std::max<size_t>(1, std::min<size_t>({size_t(65535), by_matrix, by_slots}));
   }
 
   // Chunk length of the list scan: keep at least ~4 work items per SM even
@@ -598,11 +678,12 @@ class IndexCore {
     int tv = 0, qt = 0, qg = 0;
     const size_t smem = scan_exact_smem_bytes(static_cast<int>(d_), static_cast<int>(dpad_), k, mode, &tv, &qt, &qg);
     HB_CHECK(smem > 0, HB_ERR_INVALID, "k too large for the fused scan at this dimension");
-    HB_CHECK(P <= 4095, HB_ERR_INVALID, "nprobe above 4095 is not supported");
+    HB_CHECK(P <= 8192, HB_ERR_INVALID, "nprobe above 8192 is not supported");
     probes_.reserve(static_cast<size_t>(nb) * P);
     coarse(qpad_.p, nb, P, probes_.p, nullptr);
     if (need_tops) {
       tops_.reserve(nb);
+      Scope sc(this, "warmup_tops");
       launch_warmup_tops(qpad_.p, nb, probes_.p, P, codes_.p, list_off_.p, static_cast<int>(dpad_), k, warm_lists,
                          warm_size, tops_.p, st_);
       ++launches_;
@@ -616,8 +697,11 @@ class IndexCore {
     slot_base_.reserve(static_cast<size_t>(nb) * P + 1);
     const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
     work_tmp_.reserve(wtmp);
+    {
+    Scope sc(this, "build_work");
     launch_build_work(probes_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt_.p, list_qoff_.p,
                       list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+    }
     launches_ += 3;
     part_.reserve(max_slots(nb, P, cr) * static_cast<size_t>(k));
     counter_.reserve(1);
@@ -648,13 +732,20 @@ class IndexCore {
     a.seg_order = order_dev_.p;
     a.qblock = qblock;
     a.nblocks = B;
-    launch_scan_exact(a, num_sms_, st_);
+    {
+      Scope sc(this, "scan_exact");
+      launch_scan_exact(a, num_sms_, st_);
+    }
+    Scope sc(this, "merge");
     launch_merge(part_.p, slot_base_.p, nb, P, k, ids_.p, Dd, Id, st_);
     launches_ += 2;
   }
 
   size_t d_, nlist_, nprobe_;
   size_t dpad_ = 16;
+  bool prof_ = false;
+  std::vector<ProfRecord> prof_log_;
+  std::vector<cudaEvent_t> ev_pool_;
   int metric_;
   int device_;
   int num_sms_ = 148;
@@ -829,6 +920,21 @@ int hb_warmup_tops(hb_index* ix, size_t nq, const float* q, size_t k, size_t war
 void* hb_stream(hb_index* ix) { return (ix && ix->core) ? static_cast<void*>(ix->core->stream()) : nullptr; }
 
 uint64_t hb_launch_count(const hb_index* ix) { return (ix && ix->core) ? ix->core->launches() : 0; }
+
+int hb_profile_enable(hb_index* ix, int on) {
+  HB_NEED_INDEX(ix);
+  ix->core->profile_enable(on != 0);
+  return HB_OK;
+}
+
+int hb_profile_read(hb_index* ix, char* names, size_t names_len, double* ms, int64_t* counts, int max_entries,
+                    int* n_entries) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] {
+    const int n = ix->core->profile_read(names, names_len, ms, counts, max_entries);
+    if (n_entries) *n_entries = n;
+  });
+}
 
 int hb_train_probe_predictor(hb_index* ix, size_t, const float*, size_t, size_t, float) {
   HB_NEED_INDEX(ix);

@@ -94,7 +94,7 @@ struct ScanArgs {
   // work description
   const int32_t* list_cnt;     // queries per list
   const int64_t* list_qoff;    // exclusive scan of list_cnt (nlist + 1)
-  const int32_t* list_q;       // (query << 12 | probe rank) entries, grouped by list
+  const int32_t* list_q;       // (query << 16 | probe rank) as uint32, grouped by list
   const int64_t* item_off;     // exclusive scan of items per list (nlist + 1)
   const int64_t* slot_base;    // nq*P + 1 exclusive scan of chunks per (q, j)
   int chunk_rows;              // vectors per chunk

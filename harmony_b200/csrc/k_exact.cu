@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kThreads, 1) scan_exact_kernel(ScanArgs a, int
   int* scnt = reinterpret_cast<int*>(sbuf + QG * cap);
   float* sthr = reinterpret_cast<float*>(scnt + QG);
   float* stop = sthr + QG;
-  int* sqid = reinterpret_cast<int*>(stop + QG);   // packed (q << 12 | j), -1 if unused
+  int* sqid = reinterpret_cast<int*>(stop + QG);   // packed (q << 16 | j) as uint32; -1 if unused
   int* sord = sqid + QG;                           // DIMBLOCK: query block index, -1 = unsearched
   __shared__ ItemShared it;
   __shared__ int sbnd[8];
@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, 1) scan_exact_kernel(ScanArgs a, int
       float top = FLT_MAX;
       if (tid < qcnt) {
         packed = a.list_q[a.list_qoff[it.list] + static_cast<int64_t>(it.group) * a.qgroup + tid];
-        const int qq = packed >> 12;
+        const int qq = static_cast<int>(static_cast<unsigned>(packed) >> 16);
         if (MODE != SCAN_PLAIN && a.tops) top = a.tops[qq];
         if (MODE == SCAN_DIMBLOCK) {
           const int b = a.qblock > 0 ? qq / a.qblock : 0;
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1) scan_exact_kernel(ScanArgs a, int
       for (int idx = tid; idx < QG * cpr; idx += kThreads) {
         const int e = idx / cpr, c = idx - e * cpr;
         const bool ok = e < qcnt;
-        const float* src = ok ? a.q + static_cast<size_t>(sqid[e] >> 12) * dpad + c * 4 : a.q;
+        const float* src = ok ? a.q + static_cast<size_t>(static_cast<unsigned>(sqid[e]) >> 16) * dpad + c * 4 : a.q;
         cp_async16(sq + e * dpad + c * 4, src, ok);
       }
     }
@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(kThreads, 1) scan_exact_kernel(ScanArgs a, int
       __syncwarp();
       warp_bitonic_sort(b, cap, lane);
       const int packed = sqid[e];
-      const int qq = packed >> 12, j = packed & 0xfff;
+      const int qq = static_cast<int>(static_cast<unsigned>(packed) >> 16), j = packed & 0xffff;
       const int64_t slot = a.slot_base[static_cast<int64_t>(qq) * a.P + j] + it.chunk;
       uint64_t* out = a.part + slot * a.k;
       for (int i = lane; i < a.k; i += 32) out[i] = b[i];

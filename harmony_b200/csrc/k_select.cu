@@ -294,7 +294,7 @@ __global__ void scatter_probes_kernel(const int32_t* __restrict__ probes, int nq
   if (l < 0 || list_off[l + 1] == list_off[l]) return;
   const int pos = atomicAdd(&cursor[l], 1);
   const int q = idx / P, j = idx - q * P;
-  list_q[list_qoff[l] + pos] = (q << 12) | j;
+  list_q[list_qoff[l] + pos] = static_cast<int32_t>((static_cast<uint32_t>(q) << 16) | static_cast<uint32_t>(j));
 }
 
 size_t cub_scan_bytes(size_t n) {

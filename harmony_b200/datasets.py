@@ -28,7 +28,7 @@ from __future__ import annotations
 
 import numpy as np
 
-CONFIG5_SPREAD = 0.55
+CONFIG5_SPREAD = 0.68
 CONFIG5_NOISE = 1.0
 
 
@@ -123,3 +123,40 @@ def write_fvecs(path: str, x: np.ndarray) -> None:
     out[:, 0] = d
     out[:, 1:] = x.view(np.int32)
     out.tofile(path)
+
+
+def device_mixture(n, d, ncomp, spread, noise=1.0, seed=0, weights=None, device="cuda", gen_chunk=1 << 22):
+    """The same Gaussian-mixture family generated on the GPU with a seeded
+    torch generator (for the 10M-vector workloads, where host generation
+    takes tens of seconds).  Returns (base, centres) as CUDA tensors.
+    Deterministic for a given seed, torch build and GPU model."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    centres = torch.randn((ncomp, d), generator=g, device=device, dtype=torch.float32) * spread
+    out = torch.empty((n, d), device=device, dtype=torch.float32)
+    w = None if weights is None else torch.as_tensor(weights, device=device, dtype=torch.float32)
+    for s in range(0, n, gen_chunk):
+        e = min(n, s + gen_chunk)
+        if w is None:
+            comp = torch.randint(0, ncomp, (e - s,), generator=g, device=device)
+        else:
+            comp = torch.multinomial(w, e - s, replacement=True, generator=g)
+        torch.randn((e - s, d), generator=g, device=device, dtype=torch.float32, out=out[s:e])
+        out[s:e].mul_(noise).add_(centres[comp])
+    return out, centres
+
+
+def config5_device(seed: int = 5, nb: int = 10_000_000, nq: int = 10_000, ntrain: int = 200_000,
+                   d: int = 128, ncomp: int = 4096, spread: float = CONFIG5_SPREAD, device="cuda"):
+    """config5 drawn on the GPU: (base, test, train) CUDA tensors."""
+    import torch
+    allx, _ = device_mixture(nb + nq + ntrain, d, ncomp, spread, CONFIG5_NOISE, seed, None, device)
+    return allx[:nb], allx[nb:nb + nq], (allx[nb + nq:] if ntrain else None)
+
+
+def config4_device(seed: int = 4, nb: int = 10_000_000, nq: int = 50_000, d: int = 96, ncomp: int = 4096,
+                   device="cuda"):
+    """config4 drawn on the GPU: (base, queries) CUDA tensors, Zipf(1.1) weights."""
+    allx, _ = device_mixture(nb + nq, d, ncomp, 4.0, 1.0, seed, zipf_weights(ncomp), device)
+    return allx[:nb], allx[nb:]

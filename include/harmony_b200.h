@@ -139,6 +139,14 @@ void* hb_stream(hb_index* ix);
 /* Number of kernels this index has launched so far (for launch accounting). */
 uint64_t hb_launch_count(const hb_index* ix);
 
+/* Per-kernel timing: when enabled, the index records CUDA events around each
+ * of its kernels on its own stream.  hb_profile_read synchronises the stream,
+ * returns per kernel name (newline-separated in `names`) the summed device
+ * time in ms and the number of launches, and clears the record. */
+int hb_profile_enable(hb_index* ix, int on);
+int hb_profile_read(hb_index* ix, char* names, size_t names_len, double* ms, int64_t* counts,
+                    int max_entries, int* n_entries);
+
 /* Learned probe predictor (no reference counterpart): train from nt training
  * queries labelled by the plain search at nprobe = label_nprobe, for a recall
  * target in (0, 1]. */

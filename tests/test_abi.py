@@ -82,3 +82,47 @@ def test_struct_layout_matches_header(tmp_path):
     size, off_ptr, off_max = map(int, subprocess.check_output([str(exe)]).split())
     S = hb._SearchParamsC
     assert (ctypes.sizeof(S), S.nprobe_per_query.offset, S.max_nprobe.offset) == (size, off_ptr, off_max)
+
+
+def test_cpp_dropin_header_compiles_and_links(tmp_path):
+    """A driver written against the reference's harmony::Index compiles against
+    include/harmony_b200_index.hpp and links libharmony_b200.so."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "driver.cpp"
+    src.write_text(r'''
+#include "harmony_b200_index.hpp"
+#include <cstdio>
+#include <vector>
+int main() {
+  try {
+    harmony::Index index(8, 4, 2, harmony::METRIC_L2, harmony::OPT_NONE, 0, 1, 1, false);
+    std::vector<float> x(64 * 8, 1.0f);
+    index.train(64, x.data());
+    index.add(64, x.data());
+    harmony::Index::Param p;
+    p.mode = harmony::Index::SearchMode::ORIGINAL;
+    index.preSearch(64, 0, 0, 0, 0, &p, "");
+    std::vector<float> D(2 * 3);
+    std::vector<harmony::idx_t> I(2 * 3);
+    index.search(2, x.data(), 3, D.data(), I.data());
+    std::printf("ok %ld\n", (long)I[0]);
+  } catch (const std::exception& e) {
+    std::printf("error %s\n", e.what());
+  }
+  return 0;
+}
+''')
+    exe = tmp_path / "driver"
+    subprocess.check_call([cxx, "-std=c++17", str(src), "-I", os.path.join(ROOT, "include"),
+                           "-L", os.path.dirname(hb.LIB_PATH), "-lharmony_b200",
+                           "-Wl,-rpath," + os.path.dirname(hb.LIB_PATH), "-o", str(exe)])
+    out = subprocess.check_output([str(exe)]).decode()
+    import torch
+    if torch.cuda.is_available():
+        assert out.startswith("ok")
+    else:
+        assert "no CUDA device" in out

@@ -136,6 +136,7 @@ def lib() -> ctypes.CDLL:
     L.hb_launch_count.restype = ctypes.c_uint64
     L.hb_launch_count.argtypes = [vp]
     L.hb_train_probe_predictor.argtypes = [vp, sz, f, sz, sz, ctypes.c_float]
+    L.hb_search_noalloc.argtypes = [vp, sz, f, sz, f, i64]
     L.hb_profile_enable.argtypes = [vp, ctypes.c_int]
     L.hb_profile_read.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_int)]

@@ -629,6 +629,102 @@ class IndexCore {
     plan_rows_ = 0;
   }
 
+  // Exact ORIGINAL search of one batch whose per-call buffers all come from
+  // the caller's device scratch; no DevBuf grows here.
+  void search_in_scratch(size_t nq, const float* q, size_t k, float* D, int64_t* I, unsigned char* scratch,
+                         size_t bytes) {
+    if (nq == 0) return;
+    HB_CHECK(q && D && I && scratch, HB_ERR_INVALID, "null query, result or scratch pointer");
+    HB_CHECK(k > 0, HB_ERR_INVALID, "k must be positive");
+    HB_CUDA(cudaSetDevice(device_));
+    HB_CHECK(is_device_ptr(q) && is_device_ptr(D) && is_device_ptr(I), HB_ERR_INVALID,
+             "queries and results must be device pointers");
+    HB_CHECK(nq <= 65535, HB_ERR_INVALID, "at most 65535 queries per call");
+    if (nprobe_ > nlist_) nprobe_ = nlist_;  // src/Index.cpp:1646-1648
+    const int P = static_cast<int>(nprobe_);
+    if (P == 0 || ntotal_ == 0) {
+      launch_fill_results(D, I, nq * k, st_);
+      HB_CUDA(cudaStreamSynchronize(st_));
+      return;
+    }
+    int tv = 0, qt = 0, qg = 0;
+    HB_CHECK(scan_exact_smem_bytes(static_cast<int>(d_), static_cast<int>(dpad_), static_cast<int>(k), SCAN_PLAIN,
+                                   &tv, &qt, &qg) > 0,
+             HB_ERR_INVALID, "k too large for the fused scan at this dimension");
+    const int nb = static_cast<int>(nq);
+    const int cr = chunk_rows_for(nb, P, tv);
+    // Slot bound without host allocation: min(P * largest chunk count,
+    // all chunks) per query.
+    int64_t max_ch = 0, all_ch = 0;
+    for (size_t l = 0; l < nlist_; ++l) {
+      const int64_t c = (host_off_[l + 1] - host_off_[l] + cr - 1) / cr;
+      max_ch = std::max(max_ch, c);
+      all_ch += c;
+    }
+    const size_t slots = nq * static_cast<size_t>(std::max<int64_t>(1, std::min<int64_t>(P * max_ch, all_ch)));
+    size_t off = 0;
+    auto carve = [&](size_t nbytes) {
+      unsigned char* p = scratch + off;
+      off += (nbytes + 255) / 256 * 256;
+      return p;
+    };
+    float* qpad = reinterpret_cast<float*>(carve(nq * dpad_ * sizeof(float)));
+    float* dmat = reinterpret_cast<float*>(carve(nq * nlist_ * sizeof(float)));
+    int32_t* probes = reinterpret_cast<int32_t*>(carve(nq * P * sizeof(int32_t)));
+    int32_t* list_cnt = reinterpret_cast<int32_t*>(carve(nlist_ * sizeof(int32_t)));
+    int32_t* cursor = reinterpret_cast<int32_t*>(carve(nlist_ * sizeof(int32_t)));
+    int64_t* list_qoff = reinterpret_cast<int64_t*>(carve((nlist_ + 1) * sizeof(int64_t)));
+    int64_t* item_off = reinterpret_cast<int64_t*>(carve((nlist_ + 1) * sizeof(int64_t)));
+    int32_t* list_q = reinterpret_cast<int32_t*>(carve(nq * P * sizeof(int32_t)));
+    int64_t* slot_base = reinterpret_cast<int64_t*>(carve((nq * P + 1) * sizeof(int64_t)));
+    const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
+    unsigned char* work_tmp = carve(wtmp);
+    uint64_t* part = reinterpret_cast<uint64_t*>(carve(slots * k * sizeof(uint64_t)));
+    unsigned int* counter = reinterpret_cast<unsigned int*>(carve(sizeof(unsigned int)));
+    if (off > bytes) {
+      char msg[200];
+      std::snprintf(msg, sizeof(msg),
+                    "this search needs %zu bytes of scratch; the fixed scratch holds %zu (use fewer queries, "
+                    "a smaller nprobe or k, or hb_search)",
+                    off, bytes);
+      throw Error(HB_ERR_INVALID, msg);
+    }
+    launch_pad_rows(q, nq, static_cast<int>(d_), static_cast<int>(dpad_), qpad, st_);
+    launch_l2_matrix(qpad, nb, cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), dmat,
+                     static_cast<int>(nlist_), st_);
+    launch_select_rows(dmat, nb, static_cast<int>(nlist_), static_cast<int>(nlist_), P, probes, nullptr, st_);
+    launch_build_work(probes, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt, list_qoff, cursor,
+                      list_q, item_off, slot_base, work_tmp, wtmp, st_);
+    HB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st_));
+    ScanArgs a{};
+    a.codes = codes_.p;
+    a.list_off = list_off_.p;
+    a.nlist = static_cast<int>(nlist_);
+    a.d = static_cast<int>(d_);
+    a.dpad = static_cast<int>(dpad_);
+    a.q = qpad;
+    a.nq = nb;
+    a.P = P;
+    a.k = static_cast<int>(k);
+    a.list_cnt = list_cnt;
+    a.list_qoff = list_qoff;
+    a.list_q = list_q;
+    a.item_off = item_off;
+    a.slot_base = slot_base;
+    a.chunk_rows = cr;
+    a.qgroup = qg;
+    a.work_counter = counter;
+    a.part = part;
+    a.mode = SCAN_PLAIN;
+    a.nseg = 1;
+    launch_scan_exact(a, num_sms_, st_);
+    launch_merge(part, slot_base, nb, P, static_cast<int>(k), ids_.p, D, I, st_);
+    launches_ += 8;
+    HB_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  int device() const { return device_; }
+
   void get_centroids(float* out) {
     HB_CUDA(cudaSetDevice(device_));
     HB_CUDA(cudaMemcpy2DAsync(out, d_ * sizeof(float), cent_.p, dpad_ * sizeof(float), d_ * sizeof(float), nlist_,
@@ -802,6 +898,20 @@ int guarded(F&& f) {
     }                                                               \
   } while (0)
 }  // namespace
+
+namespace hb {
+int index_device(const hb_index* ix) { return (ix && ix->core) ? ix->core->device() : -1; }
+
+int search_in_scratch(hb_index* ix, size_t nq, const float* q, size_t k, float* D, int64_t* I, void* scratch,
+                      size_t scratch_bytes) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] {
+    ix->core->search_in_scratch(nq, q, k, D, I, static_cast<unsigned char*>(scratch), scratch_bytes);
+  });
+}
+
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+}  // namespace hb
 
 extern "C" {
 

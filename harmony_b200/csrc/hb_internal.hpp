@@ -154,4 +154,14 @@ void launch_i64_to_i32(const int64_t* src, size_t n, int32_t* dst, cudaStream_t 
 void launch_i32_to_i64(const int32_t* src, size_t n, int64_t* dst, cudaStream_t st);
 void launch_fill_results(float* D, int64_t* I, size_t n, cudaStream_t st);
 
+// hb_index.cu: pieces the no-allocation entry point (hb_noalloc.cu) uses.
+// Device ordinal of an index (-1 for a null handle).
+int index_device(const hb_index* ix);
+// ORIGINAL-mode exact search with every per-call device buffer carved from
+// `scratch` (device memory of `scratch_bytes`); device pointers only; makes
+// no device allocation.  Returns an hb_status and sets the last error.
+int search_in_scratch(hb_index* ix, size_t nq, const float* q, size_t k, float* D, int64_t* I, void* scratch,
+                      size_t scratch_bytes);
+void set_last_error(const char* msg);
+
 }  // namespace hb

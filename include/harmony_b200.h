@@ -123,6 +123,20 @@ int hb_get_info(const hb_index* ix, size_t* d, size_t* nlist, size_t* ntotal, in
 int hb_get_centroids(const hb_index* ix, float* out);        /* nlist * d          */
 int hb_get_list_sizes(const hb_index* ix, int64_t* out);     /* nlist              */
 
+/* Exact search that allocates no device memory.  No counterpart in the
+ * reference (its search allocates freely).  For callers that cannot allocate
+ * while serving a query: a process whose device memory belongs to another
+ * allocator or a fixed pool (cudaMalloc there can fail or fragment it), or a
+ * latency-bound one (cudaFree synchronises the whole device).  Same results
+ * as hb_search in ORIGINAL mode at the index's nprobe; q, D and I must be
+ * device pointers.  All per-call scratch comes from one 32 MiB array built
+ * into the library (held on every GPU that loads it); searches needing more
+ * (about nq*nlist*4 bytes of coarse distances plus the work description and
+ * partial top-k) are rejected with HB_ERR_INVALID.  The first call for an
+ * index on a device looks the array's address up (make it before any stream
+ * capture); calls share the array, so calls whose GPU work overlaps race. */
+int hb_search_noalloc(hb_index* ix, size_t nq, const float* q, size_t k, float* D, int64_t* I);
+
 /* Coarse quantizer only: probe lists of each query, ascending by exact
  * centroid distance (Index::findNearNprobeOfCentroidIds,
  * src/Index.cpp:967-995).  probes: nq*nprobe int64, cdist may be NULL. */

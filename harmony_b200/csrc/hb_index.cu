@@ -103,6 +103,7 @@ class IndexCore {
     HB_CUDA(cudaSetDevice(device));
     HB_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device));
     HB_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    HB_CUDA(cudaMallocHost(&err_host_, sizeof(int)));
     reshape(d, nlist);
   }
   ~IndexCore() {
@@ -111,6 +112,7 @@ class IndexCore {
       cudaStreamSynchronize(st_);
       cudaStreamDestroy(st_);
     }
+    if (err_host_) cudaFreeHost(err_host_);
   }
 
   // Index ctor state: zero centroids, empty lists (src/Index.cpp:24-43).
@@ -341,6 +343,24 @@ class IndexCore {
     HB_CUDA(cudaStreamSynchronize(st_));
     ntotal_ = n;
     plan_rows_ = 0;
+    build_bf16();
+  }
+
+  // BF16 copy of the codes (rows padded to kpad = d rounded up to 64) and its
+  // TMA tensor map, for the tensor-core scan (d <= 128).
+  void build_bf16() {
+    bf16_ready_ = false;
+    kpad_ = static_cast<int>((d_ + 63) / 64 * 64);
+    if (kpad_ > 128 || ntotal_ == 0) return;
+    codes_bf16_.reserve(ntotal_ * static_cast<size_t>(kpad_));
+    launch_to_bf16(codes_.p, ntotal_, static_cast<int>(dpad_), kpad_, codes_bf16_.p, st_);
+    ++launches_;
+    make_bf16_tensor_map(tmap_, codes_bf16_.p, ntotal_, kpad_);
+    maxnorm_.reserve(1);
+    launch_max_norm(norms_.p, ntotal_, maxnorm_.p, st_);
+    launches_ += 2;
+    HB_CUDA(cudaStreamSynchronize(st_));
+    bf16_ready_ = true;
   }
 
   // ---- coarse quantizer ----------------------------------------------------
@@ -369,7 +389,19 @@ class IndexCore {
     hb_search_params_init(&p);
     if (prm) p = *prm;
     if (nprobe_ > nlist_) nprobe_ = nlist_;  // src/Index.cpp:1646-1648 (mutates the field)
-    HB_CHECK(p.precision == HB_PREC_FP32, HB_ERR_INVALID, "this build scans in FP32 only");
+    HB_CHECK(p.precision == HB_PREC_FP32 || p.precision == HB_PREC_BF16, HB_ERR_INVALID,
+             "precision must be FP32 or BF16");
+    const bool bf16 = p.precision == HB_PREC_BF16;
+    if (bf16) {
+      HB_CHECK(p.mode == HB_MODE_ORIGINAL || p.mode == HB_MODE_BRUTE_FORCE, HB_ERR_INVALID,
+               "the BF16 scan implements ORIGINAL / BRUTE_FORCE search (pruning and the dimension relay are FP32 modes)");
+      HB_CHECK(ntotal_ == 0 || bf16_ready_, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
+    }
+    const int max_R = bf16 ? scan_bf16_max_R(kpad_ > 0 ? kpad_ : 128) : 0;
+    const int R = bf16 ? std::min(max_R, std::max(static_cast<int>(k), p.rerank_mult * static_cast<int>(k))) : 0;
+    if (bf16)
+      HB_CHECK(static_cast<int>(k) <= R, HB_ERR_INVALID,
+               "BF16 search supports k up to " + std::to_string(max_R) + " at this dimension");
     HB_CHECK(!p.learned_probe, HB_ERR_INVALID, "learned probe predictor not trained");
     int mode = SCAN_PLAIN;
     size_t P = nprobe_;
@@ -443,8 +475,11 @@ class IndexCore {
         launch_fill_results(Dd, Id, static_cast<size_t>(nb) * k, st_);
         ++launches_;
       } else {
-        search_batch(nb, static_cast<int>(P), static_cast<int>(k), mode, p.pruning != 0, need_tops, warm_lists,
-                     warm_size, W, B, qblock, Dd, Id);
+        if (bf16)
+          search_batch_bf16(nb, static_cast<int>(P), static_cast<int>(k), R, Dd, Id);
+        else
+          search_batch(nb, static_cast<int>(P), static_cast<int>(k), mode, p.pruning != 0, need_tops, warm_lists,
+                       warm_size, W, B, qblock, Dd, Id);
       }
       if (!dev_out) {
         HB_CUDA(cudaMemcpyAsync(D + b0 * k, Dd, static_cast<size_t>(nb) * k * sizeof(float), cudaMemcpyDeviceToHost,
@@ -627,6 +662,7 @@ class IndexCore {
     ntotal_ = nt;
     trained_ = true;
     plan_rows_ = 0;
+    build_bf16();
   }
 
   // Exact ORIGINAL search of one batch whose per-call buffers all come from
@@ -837,8 +873,94 @@ class IndexCore {
     launches_ += 2;
   }
 
+  // One tensor-core scan pass over the probe table `probes` (nb x P):
+  // work description, then the scan into `part` (slots from `slot_base`).
+  void bf16_pass(int nb, int P, const int32_t* probes, int R, DevBuf<int64_t>& slot_base, DevBuf<uint64_t>& part) {
+    const int cr = std::max(128, chunk_rows_for(nb, P, 128));
+    list_cnt_.reserve(nlist_);
+    list_cursor_.reserve(nlist_);
+    list_qoff_.reserve(nlist_ + 1);
+    item_off_.reserve(nlist_ + 1);
+    list_q_.reserve(static_cast<size_t>(nb) * P);
+    slot_base.reserve(static_cast<size_t>(nb) * P + 1);
+    const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
+    work_tmp_.reserve(wtmp);
+    {
+      Scope sc(this, "build_work");
+      launch_build_work(probes, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p, list_qoff_.p,
+                        list_cursor_.p, list_q_.p, item_off_.p, slot_base.p, work_tmp_.p, wtmp, st_);
+    }
+    launches_ += 3;
+    part.reserve(max_slots(nb, P, cr) * static_cast<size_t>(scan_bf16_keys_per_slot(R)));
+    counter_.reserve(1);
+    HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
+    TcArgs a{};
+    a.list_off = list_off_.p;
+    a.nlist = static_cast<int>(nlist_);
+    a.kpad = kpad_;
+    a.dpad = static_cast<int>(dpad_);
+    a.q = qpad_.p;
+    a.xnorm = norms_.p;
+    a.list_cnt = list_cnt_.p;
+    a.list_qoff = list_qoff_.p;
+    a.list_q = list_q_.p;
+    a.item_off = item_off_.p;
+    a.slot_base = slot_base.p;
+    a.chunk_rows = cr;
+    a.P = P;
+    a.R = R;
+    a.work_counter = counter_.p;
+    a.part = part.p;
+    a.tau = tau_.p;
+    a.err = err_dev_.p;
+    {
+      Scope sc(this, "scan_bf16");
+      launch_scan_bf16(tmap_, a, num_sms_, st_);
+    }
+    ++launches_;
+  }
+
+  // BF16 search of one batch: exact coarse probes, a per-query bound of the
+  // R-th approximate key seeded from the nearest list, one tensor-core pass
+  // over all probes (items tighten the shared bound as they finish), and
+  // the exact FP32 re-rank.
+  void search_batch_bf16(int nb, int P, int k, int R, float* Dd, int64_t* Id) {
+    probes_.reserve(static_cast<size_t>(nb) * P);
+    coarse(qpad_.p, nb, P, probes_.p, nullptr);
+    err_dev_.reserve(1);
+    HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
+    tau_.reserve(nb);
+    {
+      Scope sc(this, "tau_seed");
+      launch_tau_seed(qpad_.p, nb, probes_.p, P, codes_.p, list_off_.p, norms_.p, static_cast<int>(dpad_), 256, R,
+                      maxnorm_.p, tau_.p, st_);
+    }
+    ++launches_;
+    bf16_pass(nb, P, probes_.p, R, slot_base_, part_);
+    {
+      Scope sc(this, "rerank");
+      launch_rerank(part_.p, slot_base_.p, nb, P, R, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd, Id,
+                    st_);
+    }
+    ++launches_;
+    HB_CUDA(cudaMemcpyAsync(err_host_, err_dev_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    if (*err_host_ != 0)
+      throw Error(HB_ERR_CUDA, "tensor-core scan gave up waiting (code " + std::to_string(*err_host_) + ")");
+  }
+
   size_t d_, nlist_, nprobe_;
   size_t dpad_ = 16;
+  int kpad_ = 0;
+  bool bf16_ready_ = false;
+  alignas(64) unsigned char tmap_[128];
+  DevBuf<uint16_t> codes_bf16_;
+  DevBuf<uint64_t> tau_, part2_;
+  DevBuf<float> maxnorm_;
+  DevBuf<int64_t> slot_base2_;
+  DevBuf<int32_t> probes1_, probes2_;
+  DevBuf<int> err_dev_;
+  int* err_host_ = nullptr;
   bool prof_ = false;
   std::vector<ProfRecord> prof_log_;
   std::vector<cudaEvent_t> ev_pool_;

@@ -154,6 +154,47 @@ void launch_i64_to_i32(const int64_t* src, size_t n, int32_t* dst, cudaStream_t 
 void launch_i32_to_i64(const int32_t* src, size_t n, int64_t* dst, cudaStream_t st);
 void launch_fill_results(float* D, int64_t* I, size_t n, cudaStream_t st);
 
+// k_tc.cu: BF16 tensor-core scan + exact FP32 re-rank.
+struct TcArgs {
+  const int64_t* list_off;
+  int nlist;
+  int kpad;                    // BF16 row length (d rounded up to 64)
+  int dpad;                    // FP32 row length of queries / codes
+  const float* q;              // nq x dpad FP32 queries
+  const float* xnorm;          // ||x||^2 per vector (list order)
+  const int32_t* list_cnt;
+  const int64_t* list_qoff;
+  const int32_t* list_q;
+  const int64_t* item_off;
+  const int64_t* slot_base;
+  int chunk_rows;              // multiple of 128
+  int P;
+  int R;                       // candidates kept per (query, chunk)
+  unsigned int* work_counter;
+  uint64_t* part;              // slots x R keys
+  uint64_t* tau;               // per query: best known R-th key (all ones = none yet)
+  int* err;                    // non-zero after a bounded wait gave up
+};
+size_t scan_bf16_smem_bytes(int kpad, int R);
+int scan_bf16_keys_per_slot(int R);  // keys each (query, chunk) slot holds
+int scan_bf16_max_R(int kpad);       // largest candidate count per query the scan holds
+void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);
+void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st);
+void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st);
+// Re-rank over the slots of one or two scan passes (part2 may be null).
+void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
+                   const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
+                   const uint64_t* part2 = nullptr, const int64_t* slot_base2 = nullptr, int P2 = 0);
+// Per-query upper bound of the R-th approximate key from the nearest list's
+// first S rows (exact FP32 + BF16 error margin); maxnorm = max ||x|| (device).
+void launch_tau_seed(const float* q, int nq, const int32_t* probes, int P, const float* codes,
+                     const int64_t* list_off, const float* xnorm, int dpad, int S, int R, const float* maxnorm,
+                     uint64_t* tau, cudaStream_t st);
+// *out = max over i of sqrt(norms[i]) (slightly rounded up), on the device.
+void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st);
+// probes (nq x P) -> first column (nq x 1) and the rest (nq x (P-1)).
+void launch_split_probes(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st);
+
 // hb_index.cu: pieces the no-allocation entry point (hb_noalloc.cu) uses.
 // Device ordinal of an index (-1 for a null handle).
 int index_device(const hb_index* ix);

@@ -1,0 +1,617 @@
+// BF16 tensor-core list scan (tcgen05 + TMA) and the exact FP32 re-rank.
+//
+// Work items are the list-major items of the exact scan (list, chunk of
+// rows, group of <= 128 queries probing the list).  Per item the CTA holds
+// the group's queries as the MMA's A operand (128 x K, BF16, K-major,
+// 128-byte swizzle, written by the epilogue warps) and streams the chunk's
+// rows as B operand tiles of 128 rows (TMA 2-D loads with the same swizzle
+// into a 3-stage ring).  One thread issues tcgen05.mma (M 128 queries x
+// N 128 rows x K 16) into one of two TMEM accumulators; four epilogue warps
+// read their TMEM lanes back (thread = query, 128 columns = rows), form
+// ||x||^2 - 2 q.x (the query's ||q||^2 does not change its ranking) and keep
+// the R smallest per query in a thread-private max-heap in shared memory.
+// The R best keys (approximate distance, row position) of every (query,
+// chunk) go to a slot; rerank_kernel takes each query's R best over its
+// slots, recomputes their distances exactly in FP32 with the reference's
+// sequential unfused loop and returns the k best -- so whenever the true
+// k nearest are among the R candidates the result equals the exact scan's.
+//
+// Warp roles (192 threads): warps 0-3 epilogue (TMEM lanes 0-127), warp 4
+// TMA producer, warp 5 MMA issuer.  Every mbarrier wait is bounded; on a
+// timeout the kernel records an error, skips the rest of the work while
+// keeping every CTA barrier, drains its copies in flight and frees TMEM.
+#include <cudaTypedefs.h>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cuda_bf16.h>
+
+#include "hb_device.cuh"
+#include "hb_internal.hpp"
+#include "hb_select.cuh"
+#include "hb_sm100.cuh"
+
+namespace hb {
+namespace {
+
+using namespace sm100;
+
+constexpr int kGroups = 2;                         // epilogue warpgroups, alternate tiles
+constexpr int kEpiThreads = 128;                   // threads per epilogue group (= queries per item)
+constexpr int kTcThreads = kGroups * kEpiThreads + 64;  // + TMA warp + MMA warp
+constexpr int kTile = 128;     // rows per B tile, queries per item (M)
+constexpr int kStages = 3;
+constexpr int kAcc = 2 * kGroups;                  // TMEM accumulators of 128 columns
+
+// Monotone map of a float to uint32 (all signs), and its inverse.
+__device__ __forceinline__ uint32_t ordered_bits(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ordered_to_float(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+struct TcShared {
+  uint64_t full[kStages];
+  uint64_t empty[kStages];
+  uint64_t accf[kAcc];
+  uint64_t acce[kAcc];
+  uint32_t tmem;
+  int done;
+  int list, chunk, group, qcnt, nrow;
+  long long row0;
+  int mma_consumed;
+};
+
+// Thread-private max-heap of R keys stored with stride kEpiThreads.  Kept
+// out of line: the epilogue's unrolled 32-column loop must stay small enough
+// for the instruction cache, and insertions are rare once the heap is warm.
+__device__ __noinline__ void heap_replace_top(uint64_t* h, int R, uint64_t key) {
+  int i = 0;
+  for (;;) {
+    const int c1 = 2 * i + 1;
+    if (c1 >= R) break;
+    const int c2 = c1 + 1;
+    uint64_t vc = h[c1 * kEpiThreads];
+    int c = c1;
+    if (c2 < R) {
+      const uint64_t v2 = h[c2 * kEpiThreads];
+      if (v2 > vc) {
+        vc = v2;
+        c = c2;
+      }
+    }
+    if (key >= vc) break;
+    h[i * kEpiThreads] = vc;
+    i = c;
+  }
+  h[i * kEpiThreads] = key;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    scan_bf16_kernel(const __grid_constant__ CUtensorMap tmap, TcArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ TcShared sh;
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int kpad = a.kpad;
+  const uint32_t kblk_bytes = kTile * 128;                 // one 64-element K block of 128 rows
+  const uint32_t tile_bytes = static_cast<uint32_t>(kpad / 64) * kblk_bytes;
+  uint8_t* A = smem;
+  uint8_t* stages = smem + tile_bytes;
+  uint64_t* heap = reinterpret_cast<uint64_t*>(stages + kStages * tile_bytes);  // [kGroups][R][128]
+  float* nrm = reinterpret_cast<float*>(heap + static_cast<size_t>(kGroups) * a.R * kEpiThreads);  // [kGroups][2][128]
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  int* err = a.err;
+
+  const int kProdWarp = kGroups * 4, kMmaWarp = kGroups * 4 + 1;
+  if (warp == kMmaWarp) tmem_alloc(&sh.tmem, 512);
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&sh.full[s], 1);
+      mbar_init(&sh.empty[s], 1);
+    }
+    for (int b = 0; b < kAcc; ++b) {
+      mbar_init(&sh.accf[b], 1);
+      mbar_init(&sh.acce[b], kEpiThreads);
+    }
+    sh.mma_consumed = 0;
+    fence_barrier_init();
+  }
+  if (warp == kProdWarp && lane == 0) prefetch_tmap(&tmap);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh.tmem;
+  const uint32_t idesc = idesc_bf16_f32(kTile, kTile);
+  const int nk = kpad / 16;
+  const int64_t total_items = a.item_off[a.nlist];
+
+  // Pipeline counters (identical tile sequences in every role).  Tile t of
+  // an item goes to epilogue group t % kGroups, accumulator
+  // 2 * group + (that group's tile count & 1).
+  uint32_t p_idx = 0, m_idx = 0;
+  uint32_t m_cnt[kGroups] = {};   // MMA: tiles issued per group
+  uint32_t e_cnt = 0;             // epilogue: tiles processed by this thread's group
+  const int grp = warp < kGroups * 4 ? warp / 4 : 0;
+  const int etid = tid - grp * kEpiThreads;  // 0..127 inside the group
+
+  for (;;) {
+    if (tid == 0) {
+      sh.done = 1;
+      if (*reinterpret_cast<volatile int*>(err) == 0) {
+        const int64_t item = static_cast<int64_t>(atomicAdd(a.work_counter, 1u));
+        if (item < total_items) {
+          int lo = 0, hi = a.nlist;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (a.item_off[mid] <= item) lo = mid; else hi = mid;
+          }
+          const int l = lo;
+          const int64_t local = item - a.item_off[l];
+          const int ng = (a.list_cnt[l] + kTile - 1) / kTile;
+          sh.list = l;
+          sh.chunk = static_cast<int>(local / ng);
+          sh.group = static_cast<int>(local % ng);
+          sh.qcnt = min(kTile, a.list_cnt[l] - sh.group * kTile);
+          sh.row0 = a.list_off[l] + static_cast<int64_t>(sh.chunk) * a.chunk_rows;
+          sh.nrow = static_cast<int>(min(static_cast<long long>(a.list_off[l + 1]), sh.row0 + static_cast<long long>(a.chunk_rows)) - sh.row0);
+          sh.done = 0;
+        }
+      }
+    }
+    __syncthreads();
+    if (sh.done) break;
+    const int qcnt = sh.qcnt;
+    const int nrow = sh.nrow;
+    const long long row0 = sh.row0;
+    const int ntiles = (nrow + kTile - 1) / kTile;
+
+    // ---- item set-up: A tile (queries, BF16, swizzled) and heaps ----------
+    int my_q = -1, my_j = 0;
+    uint64_t my_tau = kEmpty;
+    if (warp < kGroups * 4) {
+      if (etid < qcnt) {
+        const int packed = a.list_q[a.list_qoff[sh.list] + static_cast<int64_t>(sh.group) * kTile + etid];
+        my_q = static_cast<int>(static_cast<unsigned>(packed) >> 16);
+        my_j = packed & 0xffff;
+        // Best known R-th key of this query over the items finished so far:
+        // an upper bound of its overall R-th key, so the heap starts full of
+        // it and only keys below can enter.
+        my_tau = *reinterpret_cast<volatile unsigned long long*>(a.tau + my_q);
+      }
+      const float* qrow = a.q + static_cast<size_t>(my_q < 0 ? 0 : my_q) * a.dpad;
+      // The group's threads split the K range of their query row.
+#pragma unroll 2
+      for (int k = grp * 8; k < kpad; k += 8 * kGroups) {
+        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+        if (my_q >= 0 && k < a.dpad) {  // dpad is a multiple of 16: a row's 8 values are all in or all out
+          lo = *reinterpret_cast<const float4*>(qrow + k);
+          hi = *reinterpret_cast<const float4*>(qrow + k + 4);
+        }
+        __nv_bfloat162 p0 = __floats2bfloat162_rn(lo.x, lo.y), p1 = __floats2bfloat162_rn(lo.z, lo.w);
+        __nv_bfloat162 p2 = __floats2bfloat162_rn(hi.x, hi.y), p3 = __floats2bfloat162_rn(hi.z, hi.w);
+        *reinterpret_cast<uint4*>(A + sw128_offset_bf16(etid, k, kblk_bytes)) =
+            make_uint4(*reinterpret_cast<uint32_t*>(&p0), *reinterpret_cast<uint32_t*>(&p1),
+                       *reinterpret_cast<uint32_t*>(&p2), *reinterpret_cast<uint32_t*>(&p3));
+      }
+      uint64_t* hg = heap + static_cast<size_t>(grp) * a.R * kEpiThreads;
+      for (int e = 0; e < a.R; ++e) hg[e * kEpiThreads + etid] = my_tau;
+      fence_proxy_async_smem();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    if (warp == kProdWarp) {
+      // ---- TMA producer ----------------------------------------------------
+      if (lane == 0) {
+        for (int t = 0; t < ntiles; ++t, ++p_idx) {
+          const int s = p_idx % kStages;
+          const uint32_t par = ((p_idx / kStages) & 1u) ^ 1u;
+          if (!mbar_wait(&sh.empty[s], par, err, 11)) break;
+          uint8_t* dst = stages + s * tile_bytes;
+          mbar_arrive_expect_tx(&sh.full[s], tile_bytes);
+          const int r = static_cast<int>(row0) + t * kTile;
+          for (int kb = 0; kb < kpad / 64; ++kb) tma_load_2d(dst + kb * kblk_bytes, &tmap, kb * 64, r, &sh.full[s]);
+        }
+      }
+      __syncwarp();
+      p_idx = __shfl_sync(0xffffffffu, p_idx, 0);
+    } else if (warp == kMmaWarp) {
+      // ---- MMA issuer -------------------------------------------------------
+      if (lane == 0) {
+        for (int t = 0; t < ntiles; ++t, ++m_idx) {
+          const int s = m_idx % kStages;
+          if (!mbar_wait(&sh.full[s], (m_idx / kStages) & 1u, err, 12)) break;
+          const int g = t % kGroups;
+          const uint32_t c = m_cnt[g];
+          const int b = 2 * g + static_cast<int>(c & 1u);
+          if (!mbar_wait(&sh.acce[b], ((c >> 1) & 1u) ^ 1u, err, 13)) break;
+          ++m_cnt[g];
+          tc_fence_after();
+          const uint32_t a_base = smem_u32(A);
+          const uint32_t b_base = smem_u32(stages + s * tile_bytes);
+          for (int k = 0; k < nk; ++k) {
+            const uint32_t off = static_cast<uint32_t>(k >> 2) * kblk_bytes + static_cast<uint32_t>(k & 3) * 32u;
+            mma_bf16(tmem + static_cast<uint32_t>(b * kTile), desc_sw128(a_base + off), desc_sw128(b_base + off),
+                     idesc, k > 0 ? 1u : 0u);
+          }
+          mma_commit(&sh.empty[s]);
+          mma_commit(&sh.accf[b]);
+          sh.mma_consumed = static_cast<int>(m_idx + 1);
+        }
+      }
+      __syncwarp();
+      m_idx = __shfl_sync(0xffffffffu, m_idx, 0);
+      for (int g = 0; g < kGroups; ++g) m_cnt[g] = __shfl_sync(0xffffffffu, m_cnt[g], 0);
+    } else {
+      // ---- epilogue: thread = query (TMEM lane etid); group grp takes the
+      // item's tiles grp, grp + kGroups, ...
+      uint64_t* hp = heap + static_cast<size_t>(grp) * a.R * kEpiThreads + etid;
+      uint64_t top = my_tau;
+      float thr_f = top == kEmpty ? INFINITY : ordered_to_float(static_cast<uint32_t>(top >> 32));
+      const uint32_t lane_base = (32u * static_cast<uint32_t>(warp & 3)) << 16;
+      bool ok = true;
+      float nr_next = 0.f;
+      {
+        const int rn = grp * kTile + etid;
+        if (grp < ntiles && rn < nrow) nr_next = a.xnorm[row0 + rn];
+      }
+      for (int t = grp; t < ntiles; t += kGroups, ++e_cnt) {
+        const int b = 2 * grp + static_cast<int>(e_cnt & 1u);
+        float* nb = nrm + (grp * 2 + static_cast<int>(e_cnt & 1u)) * kTile;
+        nb[etid] = nr_next;
+        const int rn = (t + kGroups) * kTile + etid;
+        nr_next = (t + kGroups < ntiles && rn < nrow) ? a.xnorm[row0 + rn] : 0.f;
+        if (grp == 0) asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        else asm volatile("bar.sync 2, 128;\n" ::: "memory");
+        if (ok) ok = mbar_wait(&sh.accf[b], (e_cnt >> 1) & 1u, err, 14);
+        ok = __all_sync(0xffffffffu, ok);
+        tc_fence_after();
+        const int rows_here = min(kTile, nrow - t * kTile);
+#pragma unroll 1
+        for (int c = 0; c < kTile / 32; ++c) {
+          uint32_t r[32];
+          if (ok) {
+            tmem_ld32(tmem + lane_base + static_cast<uint32_t>(b * kTile + c * 32), r);
+            tmem_ld_wait();
+          }
+          if (ok && my_q >= 0) {
+            // v = ||x||^2 - 2 q.x as an order-preserving uint32, then the
+            // mask of columns at or under the heap's top; inserts walk the mask.
+            const float4* n4 = reinterpret_cast<const float4*>(nb + c * 32);
+            uint32_t mask = 0;
+#pragma unroll
+            for (int j4 = 0; j4 < 8; ++j4) {
+              const float4 nv = n4[j4];
+              const float v0 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 0]), nv.x);
+              const float v1 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), nv.y);
+              const float v2 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), nv.z);
+              const float v3 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), nv.w);
+              r[4 * j4 + 0] = __float_as_uint(v0);
+              r[4 * j4 + 1] = __float_as_uint(v1);
+              r[4 * j4 + 2] = __float_as_uint(v2);
+              r[4 * j4 + 3] = __float_as_uint(v3);
+              mask |= (v0 <= thr_f ? 1u : 0u) << (4 * j4 + 0);
+              mask |= (v1 <= thr_f ? 1u : 0u) << (4 * j4 + 1);
+              mask |= (v2 <= thr_f ? 1u : 0u) << (4 * j4 + 2);
+              mask |= (v3 <= thr_f ? 1u : 0u) << (4 * j4 + 3);
+            }
+            const int valid = rows_here - c * 32;
+            if (valid < 32) mask &= valid <= 0 ? 0u : ((1u << valid) - 1u);
+            const uint32_t pos0 = static_cast<uint32_t>(row0 + t * kTile + c * 32);
+            while (mask) {
+              const int j = __ffs(mask) - 1;
+              mask &= mask - 1;
+              uint32_t hv = r[0];
+#pragma unroll
+              for (int jj = 1; jj < 32; ++jj) hv = (j == jj) ? r[jj] : hv;
+              const uint64_t key = (static_cast<uint64_t>(ordered_bits(__uint_as_float(hv))) << 32) |
+                                   (pos0 + static_cast<uint32_t>(j));
+              if (key < top) {
+                heap_replace_top(hp, a.R, key);
+                top = hp[0];
+                // An all-ones top (heap not full yet) decodes to NaN: no bound.
+                thr_f = top == kEmpty ? INFINITY : ordered_to_float(static_cast<uint32_t>(top >> 32));
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&sh.acce[b]);
+      }
+      // Partial result of this (query, chunk): the group's R keys; seed
+      // entries are not results.
+      if (my_q >= 0) {
+        const int64_t slot = a.slot_base[static_cast<int64_t>(my_q) * a.P + my_j] + sh.chunk;
+        uint64_t* out = a.part + (slot * kGroups + grp) * a.R;
+        for (int e = 0; e < a.R; ++e) {
+          const uint64_t v = hp[e * kEpiThreads];
+          out[e] = v == my_tau ? kEmpty : v;
+        }
+        // A heap holding R real keys bounds the query's R-th key: publish it.
+        if (top < my_tau) atomicMin(reinterpret_cast<unsigned long long*>(a.tau + my_q), top);
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+
+  // ---- drain: copies and MMAs still in flight after an error --------------
+  if (warp == kProdWarp && lane == 0) {
+    const uint32_t consumed = static_cast<uint32_t>(*reinterpret_cast<volatile int*>(&sh.mma_consumed));
+    for (uint32_t i = consumed; i < p_idx; ++i)
+      mbar_wait(&sh.full[i % kStages], (i / kStages) & 1u, nullptr, 0, 200000000LL);
+  }
+  if (warp == kMmaWarp && lane == 0) {
+    for (int g = 0; g < kGroups; ++g)
+      if (m_cnt[g] > 0) {
+        const uint32_t last = m_cnt[g] - 1;
+        mbar_wait(&sh.accf[2 * g + static_cast<int>(last & 1u)], (last >> 1) & 1u, nullptr, 0, 200000000LL);
+      }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// Per query: R best approximate keys over its slots -> exact FP32
+// distances (sequential unfused, as the exact scan) -> k best.
+__global__ void __launch_bounds__(128) rerank_kernel(const uint64_t* __restrict__ part,
+                                                     const int64_t* __restrict__ slot_base, int P, int R, int k,
+                                                     const float* __restrict__ codes, const float* __restrict__ q,
+                                                     int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
+                                                     int64_t* __restrict__ I, const uint64_t* __restrict__ part2,
+                                                     const int64_t* __restrict__ slot_base2, int P2) {
+  extern __shared__ uint64_t s_keys[];  // pow2(R) approx, then pow2(R) exact
+  __shared__ SelectShared sh_sel;
+  const int qi = blockIdx.x;
+  const int n2 = pow2_ceil(R < 2 ? 2 : R);
+  uint64_t* s_appr = s_keys;
+  uint64_t* s_exact = s_keys + n2;
+  const int64_t s0 = slot_base[static_cast<int64_t>(qi) * P];
+  const int64_t s1 = slot_base[static_cast<int64_t>(qi + 1) * P];
+  const uint64_t* src = part + s0 * kGroups * R;
+  const int m1 = static_cast<int>((s1 - s0) * kGroups * R);
+  const uint64_t* src2 = nullptr;
+  int m2 = 0;
+  if (part2) {
+    const int64_t t0 = slot_base2[static_cast<int64_t>(qi) * P2];
+    const int64_t t1 = slot_base2[static_cast<int64_t>(qi + 1) * P2];
+    src2 = part2 + t0 * kGroups * R;
+    m2 = static_cast<int>((t1 - t0) * kGroups * R);
+  }
+  auto key_at = [&](int i) -> uint64_t { return i < m1 ? src[i] : src2[i - m1]; };
+  block_topk_sorted(key_at, m1 + m2, R, sh_sel, s_appr);
+  const float* qrow = q + static_cast<size_t>(qi) * dpad;
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+    uint64_t key = kEmpty;
+    if (i < R && s_appr[i] != kEmpty) {
+      const uint32_t pos = key_tie(s_appr[i]);
+      const float* x = codes + static_cast<size_t>(pos) * dpad;
+      float acc = 0.0f;
+      for (int c = 0; c < dpad; c += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(x + c);
+        const float4 w = *reinterpret_cast<const float4*>(qrow + c);
+        float t;
+        t = __fsub_rn(w.x, v.x);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+        t = __fsub_rn(w.y, v.y);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+        t = __fsub_rn(w.z, v.z);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+        t = __fsub_rn(w.w, v.w);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+      }
+      if (acc < FLT_MAX) key = make_key(acc, pos);
+    }
+    s_exact[i] = key;
+  }
+  __syncthreads();
+  block_bitonic_sort(s_exact, n2);
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    const uint64_t key = j < n2 ? s_exact[j] : kEmpty;
+    const size_t o = static_cast<size_t>(qi) * k + j;
+    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+  }
+}
+
+__global__ void split_probes_kernel(const int32_t* __restrict__ probes, int nq, int P, int32_t* __restrict__ first,
+                                    int32_t* __restrict__ rest) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nq * P) return;
+  const int q = idx / P, j = idx - q * P;
+  if (j == 0) first[q] = probes[idx];
+  else rest[static_cast<size_t>(q) * (P - 1) + (j - 1)] = probes[idx];
+}
+
+// Upper bound of each query's R-th approximate key before the scan: the
+// R-th smallest exact FP32 value ||x||^2 - 2 q.x over the first S rows of
+// the query's nearest list, plus a margin covering the BF16 scan's error
+// (rounding q and x to 8-bit significands changes each product by at most
+// (2u + u^2)|q_i x_i| with u = 2^-8, so the dot product by at most about
+// 2^-7 ||q|| ||x||; the margin doubles that and adds FP32 rounding).  A
+// seed therefore never drops a key that belongs to the approximate top R.
+__global__ void __launch_bounds__(128) tau_seed_kernel(const float* __restrict__ q, const int32_t* __restrict__ probes,
+                                                        int P, const float* __restrict__ codes,
+                                                        const int64_t* __restrict__ list_off,
+                                                        const float* __restrict__ xnorm, int dpad, int S, int R,
+                                                        const float* __restrict__ maxnorm,
+                                                        uint64_t* __restrict__ tau) {
+  extern __shared__ uint64_t s_seed[];  // pow2(S) keys, then dpad floats of the query
+  __shared__ SelectShared sh_sel;
+  __shared__ float s_qn;
+  const int qi = blockIdx.x;
+  const int n2 = pow2_ceil(S < 2 ? 2 : S);
+  float* sq = reinterpret_cast<float*>(s_seed + n2);
+  const float* qrow = q + static_cast<size_t>(qi) * dpad;
+  for (int c = threadIdx.x; c < dpad; c += blockDim.x) sq[c] = qrow[c];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float acc = 0.0f;
+    for (int c = 0; c < dpad; ++c) acc = __fadd_rn(acc, __fmul_rn(sq[c], sq[c]));
+    s_qn = acc;
+  }
+  const int l = probes[static_cast<size_t>(qi) * P];
+  const int64_t b = l >= 0 ? list_off[l] : 0;
+  const int n = l >= 0 ? static_cast<int>(min(static_cast<int64_t>(S), list_off[l + 1] - b)) : 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float* x = codes + static_cast<size_t>(b + i) * dpad;
+    float dot = 0.0f;
+    for (int c = 0; c < dpad; c += 4) {
+      const float4 v = *reinterpret_cast<const float4*>(x + c);
+      dot = __fadd_rn(dot, __fmul_rn(sq[c], v.x));
+      dot = __fadd_rn(dot, __fmul_rn(sq[c + 1], v.y));
+      dot = __fadd_rn(dot, __fmul_rn(sq[c + 2], v.z));
+      dot = __fadd_rn(dot, __fmul_rn(sq[c + 3], v.w));
+    }
+    const float val = fmaf(-2.0f, dot, xnorm[b + i]);
+    s_seed[i] = (static_cast<uint64_t>(ordered_bits(val)) << 32) | static_cast<uint32_t>(i);
+  }
+  __syncthreads();
+  if (n < R) {
+    if (threadIdx.x == 0) tau[qi] = kEmpty;
+    return;
+  }
+  auto key_at = [&](int i) -> uint64_t { return s_seed[i]; };
+  uint64_t* s_out = s_seed + n2 + (dpad + 1) / 2;  // after the query copy
+  block_select(key_at, n, R, sh_sel, s_out);
+  if (threadIdx.x == 0) {
+    uint64_t mx = 0;
+    for (int i = 0; i < R; ++i) mx = s_out[i] > mx ? s_out[i] : mx;
+    const float vR = ordered_to_float(static_cast<uint32_t>(mx >> 32));
+    const float mn = *maxnorm;
+    const float margin = 0.032f * sqrtf(s_qn) * mn + 2e-5f * (mn * mn + fabsf(vR)) + 1e-30f;
+    const float t = vR + margin;
+    tau[qi] = (static_cast<uint64_t>(ordered_bits(t)) << 32) | 0xffffffffull;
+  }
+}
+
+__global__ void max_norm_kernel(const float* __restrict__ norms, size_t n, float* __restrict__ out) {
+  float m = 0.0f;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    m = fmaxf(m, norms[i]);
+  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(out), __float_as_int(m));
+}
+
+__global__ void sqrt_inplace_kernel(float* v) { *v = sqrtf(*v) * 1.0001f; }
+
+__global__ void to_bf16_kernel(const float* __restrict__ src, size_t n, int dpad, int kpad,
+                               __nv_bfloat16* __restrict__ dst) {
+  const size_t total = n * static_cast<size_t>(kpad);
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t r = i / kpad;
+    const int c = static_cast<int>(i - r * kpad);
+    dst[i] = __float2bfloat16_rn(c < dpad ? src[r * dpad + c] : 0.0f);
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    HB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    HB_CHECK(p && q == cudaDriverEntryPointSuccess, HB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+size_t scan_bf16_smem_bytes(int kpad, int R) {
+  const size_t tile = static_cast<size_t>(kpad / 64) * kTile * 128;
+  return 1024 + tile * (1 + kStages) + static_cast<size_t>(kGroups) * R * kEpiThreads * 8 +
+         static_cast<size_t>(kGroups) * 2 * kTile * 4;
+}
+
+int scan_bf16_keys_per_slot(int R) { return kGroups * R; }
+
+int scan_bf16_max_R(int kpad) {
+  int R = 64;
+  while (R > 1 && scan_bf16_smem_bytes(kpad, R) > 220 * 1024) --R;
+  return R;
+}
+
+void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad) {
+  CUtensorMap* m = static_cast<CUtensorMap*>(tmap_out);
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(kpad), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(kpad) * 2};
+  cuuint32_t box[2] = {64, kTile};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = tensor_map_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(codes_bf16), dims,
+                                    strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  HB_CHECK(r == CUDA_SUCCESS, HB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+}
+
+void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st) {
+  if (!n) return;
+  size_t g = (n * kpad + 255) / 256;
+  if (g > 148u * 64u) g = 148u * 64u;
+  to_bf16_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(src, n, dpad, kpad, static_cast<__nv_bfloat16*>(dst));
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st) {
+  HB_CHECK(a.kpad == 64 || a.kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
+  HB_CHECK(a.R >= 1 && a.R <= 64, HB_ERR_INVALID, "rerank candidates per query must be in [1, 64]");
+  const size_t smem = scan_bf16_smem_bytes(a.kpad, a.R);
+  HB_CHECK(smem <= 220 * 1024, HB_ERR_INVALID, "rerank candidates too many for the BF16 scan's shared memory");
+  HB_CUDA(cudaFuncSetAttribute(scan_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  scan_bf16_kernel<<<num_sms, kTcThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap), a);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
+                   const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
+                   const uint64_t* part2, const int64_t* slot_base2, int P2) {
+  if (nq <= 0) return;
+  HB_CHECK(k <= R, HB_ERR_INVALID, "k must not exceed the re-ranked candidates");
+  const int n2 = pow2_ceil(R < 2 ? 2 : R);
+  const size_t smem = static_cast<size_t>(2 * n2) * 8 + 64;
+  rerank_kernel<<<nq, 128, smem, st>>>(part, slot_base, P, R, k, codes, q, dpad, ids, D, I, part2, slot_base2, P2);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_tau_seed(const float* q, int nq, const int32_t* probes, int P, const float* codes,
+                     const int64_t* list_off, const float* xnorm, int dpad, int S, int R, const float* maxnorm,
+                     uint64_t* tau, cudaStream_t st) {
+  if (nq <= 0) return;
+  const int n2 = pow2_ceil(S < 2 ? 2 : S);
+  const size_t smem = static_cast<size_t>(n2) * 8 + static_cast<size_t>(dpad + 1) / 2 * 8 + static_cast<size_t>(R) * 8 + 64;
+  HB_CUDA(cudaFuncSetAttribute(tau_seed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  tau_seed_kernel<<<nq, 128, smem, st>>>(q, probes, P, codes, list_off, xnorm, dpad, S, R, maxnorm, tau);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st) {
+  HB_CUDA(cudaMemsetAsync(out, 0, sizeof(float), st));
+  if (n) {
+    size_t g = (n + 255) / 256;
+    if (g > 1024) g = 1024;
+    max_norm_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(norms, n, out);
+  }
+  sqrt_inplace_kernel<<<1, 1, 0, st>>>(out);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_split_probes(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st) {
+  if (nq <= 0) return;
+  split_probes_kernel<<<(nq * P + 255) / 256, 256, 0, st>>>(probes, nq, P, first, rest);
+  HB_CUDA(cudaGetLastError());
+}
+
+}  // namespace hb

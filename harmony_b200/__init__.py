@@ -137,6 +137,7 @@ def lib() -> ctypes.CDLL:
     L.hb_launch_count.argtypes = [vp]
     L.hb_train_probe_predictor.argtypes = [vp, sz, f, sz, sz, ctypes.c_float]
     L.hb_search_noalloc.argtypes = [vp, sz, f, sz, f, i64]
+    L.hb_probe_calibration.argtypes = [vp, f, f, f, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.hb_profile_enable.argtypes = [vp, ctypes.c_int]
     L.hb_profile_read.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_int)]
@@ -183,7 +184,7 @@ class Stats:
 class SearchParams:
     """GPU search knobs beyond Index::Param (see include/harmony_b200.h)."""
     precision: Precision = Precision.FP32
-    rerank_mult: int = 4
+    rerank_mult: int = 2
     learned_probe: bool = False
     learned_target: float = 0.0
     nprobe_per_query: Optional[object] = None
@@ -405,6 +406,24 @@ class Index:
         _check(self._L.hb_warmup_tops(self._h, q.shape[0], q.ctypes.data, k, warm_lists,
                                       k if warm_list_size is None else warm_list_size, tops.ctypes.data))
         return tops
+
+    # -- learned probe predictor (no reference counterpart) -----------------
+    def train_probe_predictor(self, n: int, queries, k: int = 10, label_nprobe: int = 256,
+                              target: float = 0.95) -> None:
+        """Train the per-query nprobe predictor on n training queries labelled by
+        the exact search at nprobe = label_nprobe, calibrated to `target` recall."""
+        p, keep = _ptr(queries, np.float32)
+        _check(self._L.hb_train_probe_predictor(self._h, int(n), p, int(k), int(label_nprobe), float(target)))
+
+    def probe_calibration(self):
+        """(thresholds, recall, average nprobe) measured on the held-out split."""
+        thr = np.zeros(64, np.float32)
+        rec = np.zeros(64, np.float32)
+        avg = np.zeros(64, np.float32)
+        n = ctypes.c_int()
+        _check(self._L.hb_probe_calibration(self._h, thr.ctypes.data, rec.ctypes.data, avg.ctypes.data, 64,
+                                            ctypes.byref(n)))
+        return thr[: n.value], rec[: n.value], avg[: n.value]
 
     # -- persistence -------------------------------------------------------
     def save_index(self, path: str) -> None:

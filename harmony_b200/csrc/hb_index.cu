@@ -402,7 +402,6 @@ class IndexCore {
     if (bf16)
       HB_CHECK(static_cast<int>(k) <= R, HB_ERR_INVALID,
                "BF16 search supports k up to " + std::to_string(max_R) + " at this dimension");
-    HB_CHECK(!p.learned_probe, HB_ERR_INVALID, "learned probe predictor not trained");
     int mode = SCAN_PLAIN;
     size_t P = nprobe_;
     int W = 1, B = 1;
@@ -434,7 +433,23 @@ class IndexCore {
       default:
         throw Error(HB_ERR_INVALID, "search mode not supported");
     }
-    if (p.nprobe_per_query) throw Error(HB_ERR_INVALID, "per-query nprobe needs the batched scheduler");
+    // Per-query nprobe: the learned predictor or a caller-given array.  The
+    // coarse quantizer selects the widest probe row, each query's row is then
+    // cut at its own nprobe (cut entries become -1 and are never scanned).
+    const bool learned = p.learned_probe != 0;
+    cut_mode_ = 0;
+    if (learned) {
+      HB_CHECK(probe_.trained, HB_ERR_STATE, "learned probe predictor not trained (hb_train_probe_predictor)");
+      HB_CHECK(!p.nprobe_per_query, HB_ERR_INVALID, "learned probe and nprobe_per_query are exclusive");
+      P = std::min<size_t>(probe_.pmax, nlist_);
+      cut_mode_ = 1;
+      cut_cap_ = p.max_nprobe > 0 ? std::min<int>(p.max_nprobe, static_cast<int>(P)) : static_cast<int>(P);
+      cut_thr_ = probe_.threshold_for(p.learned_target);
+    } else if (p.nprobe_per_query) {
+      if (p.max_nprobe > 0) P = std::min<size_t>(static_cast<size_t>(p.max_nprobe), nlist_);
+      cut_mode_ = 2;
+      cut_src_ = p.nprobe_per_query;
+    }
 
     const bool dev_out = is_device_ptr(D) && is_device_ptr(I);
     const bool dev_in = is_device_ptr(q);
@@ -452,6 +467,7 @@ class IndexCore {
 
     for (size_t b0 = 0; b0 < nq; b0 += bs) {
       const int nb = static_cast<int>(std::min(bs, nq - b0));
+      cut_b0_ = b0;
       float* Dd = dev_out ? D + b0 * k : nullptr;
       int64_t* Id = dev_out ? I + b0 * k : nullptr;
       if (!dev_out) {
@@ -812,7 +828,7 @@ class IndexCore {
     HB_CHECK(smem > 0, HB_ERR_INVALID, "k too large for the fused scan at this dimension");
     HB_CHECK(P <= 8192, HB_ERR_INVALID, "nprobe above 8192 is not supported");
     probes_.reserve(static_cast<size_t>(nb) * P);
-    coarse(qpad_.p, nb, P, probes_.p, nullptr);
+    coarse_and_cut(nb, P);
     if (need_tops) {
       tops_.reserve(nb);
       Scope sc(this, "warmup_tops");
@@ -926,7 +942,7 @@ class IndexCore {
   // the exact FP32 re-rank.
   void search_batch_bf16(int nb, int P, int k, int R, float* Dd, int64_t* Id) {
     probes_.reserve(static_cast<size_t>(nb) * P);
-    coarse(qpad_.p, nb, P, probes_.p, nullptr);
+    coarse_and_cut(nb, P);
     err_dev_.reserve(1);
     HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
     tau_.reserve(nb);
@@ -948,6 +964,299 @@ class IndexCore {
     if (*err_host_ != 0)
       throw Error(HB_ERR_CUDA, "tensor-core scan gave up waiting (code " + std::to_string(*err_host_) + ")");
   }
+
+  // Coarse probes of the batch in qpad_, then the per-query cut.
+  void coarse_and_cut(int nb, int P) {
+    if (cut_mode_ == 1) {
+      cdist_.reserve(static_cast<size_t>(nb) * P);
+      coarse(qpad_.p, nb, P, probes_.p, cdist_.p);
+      Scope sc(this, "probe_mlp");
+      probe_infer(nb, qpad_.p, cdist_.p, P, probes_.p, cut_thr_, cut_cap_, nullptr);
+    } else {
+      coarse(qpad_.p, nb, P, probes_.p, nullptr);
+      if (cut_mode_ == 2) {
+        npq_.reserve(static_cast<size_t>(nb));
+        HB_CUDA(cudaMemcpyAsync(npq_.p, cut_src_ + cut_b0_, static_cast<size_t>(nb) * sizeof(int32_t), cudaMemcpyDefault,
+                                st_));
+        launch_cut_probes(npq_.p, nb, P, probes_.p, st_);
+        ++launches_;
+      }
+    }
+  }
+
+  // ---- learned probe predictor ------------------------------------------------
+  struct ProbeModel {
+    bool trained = false;
+    int F = 0, H = 256, NB = 0, C = 32, pmax = 0;
+    std::vector<int32_t> buckets;
+    DevBuf<float> W1, B1, W2, B2, W3, B3;  // BF16-rounded inference weights
+    DevBuf<float> mean, inv_std;
+    DevBuf<int32_t> bucket_val;
+    std::vector<float> cal_thr, cal_recall, cal_avgp;
+    float thr = 1.0f;
+    // Smallest-average-nprobe threshold whose validation recall reaches the
+    // target (the trained one for target 0).
+    float threshold_for(float target) const {
+      if (target <= 0.f) return thr;
+      float best = 1.0f, bestp = 1e30f;
+      for (size_t i = 0; i < cal_thr.size(); ++i)
+        if (cal_recall[i] >= target && cal_avgp[i] < bestp) {
+          bestp = cal_avgp[i];
+          best = cal_thr[i];
+        }
+      return best;
+    }
+  };
+
+  // Features -> 3 GEMMs (BF16 weights and activations, FP32 accumulation)
+  // -> per-query nprobe; probes (nb x P) are cut in place.
+  void probe_infer(int nb, const float* qpad, const float* cdist, int P, int32_t* probes, float thr, int cap,
+                   int32_t* nprobe_out) {
+    ProbeModel& m = probe_;
+    pf_.reserve(static_cast<size_t>(nb) * m.F);
+    ph1_.reserve(static_cast<size_t>(nb) * m.H);
+    ph2_.reserve(static_cast<size_t>(nb) * m.H);
+    plog_.reserve(static_cast<size_t>(nb) * m.NB);
+    mlp_features(qpad, nb, static_cast<int>(d_), static_cast<int>(dpad_), cdist, P, m.C, pf_.p, st_);
+    mlp_standardize(pf_.p, nb, m.F, m.mean.p, m.inv_std.p, true, st_);
+    mlp_gemm(nb, m.H, m.F, pf_.p, m.F, false, m.W1.p, m.F, true, ph1_.p, m.H, m.B1.p, 0.f, true, nullptr, true, st_);
+    mlp_gemm(nb, m.H, m.H, ph1_.p, m.H, false, m.W2.p, m.H, true, ph2_.p, m.H, m.B2.p, 0.f, true, nullptr, true, st_);
+    mlp_gemm(nb, m.NB, m.H, ph2_.p, m.H, false, m.W3.p, m.H, true, plog_.p, m.NB, m.B3.p, 0.f, false, nullptr, false,
+             st_);
+    mlp_choose_nprobe(plog_.p, nb, m.NB, m.bucket_val.p, thr, cap, nprobe_out, probes, P, st_);
+    launches_ += 6;
+  }
+
+ public:
+  // Trains the predictor on nt queries labelled by the exact FP32 search at
+  // nprobe = label_P: a query's label is the smallest nprobe that finds its
+  // k results (1 + the highest probe rank among their lists).  90% of the
+  // queries train the MLP (Adam), 10% calibrate the probability threshold
+  // to the recall target.
+  void train_probe(size_t nt, const float* q, size_t k, size_t label_P, float target) {
+    HB_CUDA(cudaSetDevice(device_));
+    HB_CHECK(ntotal_ > 0, HB_ERR_STATE, "train the probe predictor after add");
+    HB_CHECK(nt >= 1000, HB_ERR_INVALID, "at least 1000 training queries");
+    HB_CHECK(label_P >= 32 && label_P <= nlist_, HB_ERR_INVALID, "label nprobe must be in [32, nlist]");
+    HB_CHECK(target > 0.f && target <= 1.f, HB_ERR_INVALID, "target recall must be in (0, 1]");
+    HB_CHECK(k >= 1 && k <= 64, HB_ERR_INVALID, "k must be in [1, 64]");
+    ProbeModel& m = probe_;
+    const int P = static_cast<int>(label_P);
+    m.C = 32;
+    m.F = static_cast<int>(d_) + m.C;
+    m.H = 256;
+    m.buckets.clear();
+    for (int b : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048})
+      if (b < P) m.buckets.push_back(b);
+    m.buckets.push_back(P);
+    m.NB = static_cast<int>(m.buckets.size());
+    m.pmax = P;
+    m.trained = false;
+    // Labels from the plain exact search.
+    DevBuf<float> Dtr;
+    DevBuf<int64_t> Itr;
+    Dtr.reserve(nt * k);
+    Itr.reserve(nt * k);
+    const size_t saved = nprobe_;
+    nprobe_ = label_P;
+    hb_search_params sp;
+    hb_search_params_init(&sp);
+    search(nt, q, k, &sp, Dtr.p, Itr.p);
+    nprobe_ = saved;
+    // Probe tables with distances, and padded queries, for all nt.
+    DevBuf<float> qall, tmp, cd;
+    DevBuf<int32_t> pr;
+    stage_rows(q, nt, qall, tmp);
+    tmp.release();
+    pr.reserve(nt * P);
+    cd.reserve(nt * P);
+    const size_t cb = std::max<size_t>(1, (size_t(1) << 30) / (nlist_ * sizeof(float)));
+    for (size_t b0 = 0; b0 < nt; b0 += cb) {
+      const int nb = static_cast<int>(std::min(cb, nt - b0));
+      coarse(qall.p + b0 * dpad_, nb, P, pr.p + b0 * P, cd.p + b0 * P);
+    }
+    // id -> list, labels and per-result probe ranks.
+    std::vector<int64_t> ids_h(ntotal_);
+    HB_CUDA(cudaMemcpyAsync(ids_h.data(), ids_.p, ntotal_ * sizeof(int64_t), cudaMemcpyDeviceToHost, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    int64_t max_id = 0;
+    for (int64_t v : ids_h) max_id = std::max(max_id, v);
+    DevBuf<int32_t> lid, need, ranks;
+    lid.reserve(static_cast<size_t>(max_id) + 1);
+    HB_CUDA(cudaMemsetAsync(lid.p, 0xff, (static_cast<size_t>(max_id) + 1) * sizeof(int32_t), st_));
+    launch_list_of_id(list_off_.p, static_cast<int>(nlist_), ids_.p, lid.p, max_id + 1, st_);
+    need.reserve(nt);
+    ranks.reserve(nt * k);
+    launch_label_rank(Itr.p, static_cast<int>(nt), static_cast<int>(k), lid.p, pr.p, P, need.p, ranks.p, st_);
+    // Features.
+    DevBuf<float> X;
+    X.reserve(nt * m.F);
+    mlp_features(qall.p, static_cast<int>(nt), static_cast<int>(d_), static_cast<int>(dpad_), cd.p, P, m.C, X.p, st_);
+    m.mean.reserve(m.F);
+    m.inv_std.reserve(m.F);
+    mlp_moments(X.p, static_cast<int>(nt), m.F, m.mean.p, m.inv_std.p, st_);
+    mlp_standardize(X.p, static_cast<int>(nt), m.F, m.mean.p, m.inv_std.p, false, st_);
+    std::vector<int32_t> need_h(nt), ranks_h(nt * k);
+    HB_CUDA(cudaMemcpyAsync(need_h.data(), need.p, nt * sizeof(int32_t), cudaMemcpyDeviceToHost, st_));
+    HB_CUDA(cudaMemcpyAsync(ranks_h.data(), ranks.p, nt * k * sizeof(int32_t), cudaMemcpyDeviceToHost, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    std::vector<int32_t> y(nt);
+    for (size_t i = 0; i < nt; ++i) {
+      int b = 0;
+      while (b < m.NB - 1 && m.buckets[b] < need_h[i]) ++b;
+      y[i] = b;
+    }
+    const size_t nval = std::max<size_t>(500, nt / 10);
+    const size_t ntr = nt - nval;
+    // Parameters: Kaiming-uniform, fixed seed.
+    const int F = m.F, H = m.H, NB = m.NB;
+    const size_t n1 = static_cast<size_t>(H) * F, n2 = static_cast<size_t>(H) * H, n3 = static_cast<size_t>(NB) * H;
+    const size_t nparam = n1 + H + n2 + H + n3 + NB;
+    std::vector<float> w0(nparam, 0.f);
+    std::mt19937 rng(1234);
+    auto fill = [&](size_t off, size_t n, int fan_in) {
+      std::uniform_real_distribution<float> u(-std::sqrt(6.f / fan_in), std::sqrt(6.f / fan_in));
+      for (size_t i = 0; i < n; ++i) w0[off + i] = u(rng);
+    };
+    fill(0, n1, F);
+    fill(n1 + H, n2, H);
+    fill(n1 + H + n2 + H, n3, H);
+    DevBuf<float> W, G, Mo, Vo;
+    W.reserve(nparam);
+    G.reserve(nparam);
+    Mo.reserve(nparam);
+    Vo.reserve(nparam);
+    HB_CUDA(cudaMemcpyAsync(W.p, w0.data(), nparam * sizeof(float), cudaMemcpyHostToDevice, st_));
+    HB_CUDA(cudaMemsetAsync(Mo.p, 0, nparam * sizeof(float), st_));
+    HB_CUDA(cudaMemsetAsync(Vo.p, 0, nparam * sizeof(float), st_));
+    float *w1 = W.p, *b1 = w1 + n1, *w2 = b1 + H, *b2 = w2 + n2, *w3 = b2 + H, *b3 = w3 + n3;
+    float *g1 = G.p, *gb1 = g1 + n1, *g2 = gb1 + H, *gb2 = g2 + n2, *g3 = gb2 + H, *gb3 = g3 + n3;
+    const int B = 2048;
+    DevBuf<float> Xb, Z1, A1, Z2, A2, L, dL, dA, dZ, loss;
+    DevBuf<int32_t> yb;
+    DevBuf<int64_t> perm_d;
+    Xb.reserve(static_cast<size_t>(B) * F);
+    Z1.reserve(static_cast<size_t>(B) * H);
+    A1.reserve(static_cast<size_t>(B) * H);
+    Z2.reserve(static_cast<size_t>(B) * H);
+    A2.reserve(static_cast<size_t>(B) * H);
+    L.reserve(static_cast<size_t>(B) * NB);
+    dL.reserve(static_cast<size_t>(B) * NB);
+    dA.reserve(static_cast<size_t>(B) * H);
+    dZ.reserve(static_cast<size_t>(B) * H);
+    loss.reserve(1);
+    yb.reserve(ntr);
+    perm_d.reserve(ntr);
+    DevBuf<float> Xs;
+    Xs.reserve(ntr * F);
+    std::vector<int64_t> perm(ntr);
+    std::vector<int32_t> yperm(ntr);
+    const int epochs = 12;
+    int step = 0;
+    const float lr = 2e-3f;
+    for (int ep = 0; ep < epochs; ++ep) {
+      std::iota(perm.begin(), perm.end(), 0);
+      std::shuffle(perm.begin(), perm.end(), std::mt19937(777 + ep));
+      for (size_t i = 0; i < ntr; ++i) yperm[i] = y[perm[i]];
+      HB_CUDA(cudaMemcpyAsync(perm_d.p, perm.data(), ntr * sizeof(int64_t), cudaMemcpyHostToDevice, st_));
+      HB_CUDA(cudaMemcpyAsync(yb.p, yperm.data(), ntr * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
+      launch_gather_rows(X.p, perm_d.p, ntr, F, Xs.p, st_);
+      const float lr_ep = lr * (ep < epochs - 4 ? 1.f : 0.25f);
+      for (size_t r0 = 0; r0 + B <= ntr; r0 += B, ++step) {
+        const float* xb = Xs.p + r0 * F;
+        HB_CUDA(cudaMemsetAsync(loss.p, 0, sizeof(float), st_));
+        mlp_gemm(B, H, F, xb, F, false, w1, F, true, A1.p, H, b1, 0.f, true, Z1.p, false, st_);
+        mlp_gemm(B, H, H, A1.p, H, false, w2, H, true, A2.p, H, b2, 0.f, true, Z2.p, false, st_);
+        mlp_gemm(B, NB, H, A2.p, H, false, w3, H, true, L.p, NB, b3, 0.f, false, nullptr, false, st_);
+        mlp_softmax_ce(L.p, yb.p + r0, B, NB, dL.p, loss.p, st_);
+        // layer 3
+        mlp_gemm(NB, H, B, dL.p, NB, true, A2.p, H, false, g3, H, nullptr, 0.f, false, nullptr, false, st_);
+        mlp_colsum(dL.p, B, NB, gb3, st_);
+        mlp_gemm(B, H, NB, dL.p, NB, false, w3, H, false, dA.p, H, nullptr, 0.f, false, nullptr, false, st_);
+        mlp_gelu_backward(dA.p, Z2.p, dZ.p, static_cast<size_t>(B) * H, st_);
+        // layer 2
+        mlp_gemm(H, H, B, dZ.p, H, true, A1.p, H, false, g2, H, nullptr, 0.f, false, nullptr, false, st_);
+        mlp_colsum(dZ.p, B, H, gb2, st_);
+        mlp_gemm(B, H, H, dZ.p, H, false, w2, H, false, dA.p, H, nullptr, 0.f, false, nullptr, false, st_);
+        mlp_gelu_backward(dA.p, Z1.p, dZ.p, static_cast<size_t>(B) * H, st_);
+        // layer 1
+        mlp_gemm(H, F, B, dZ.p, H, true, xb, F, false, g1, F, nullptr, 0.f, false, nullptr, false, st_);
+        mlp_colsum(dZ.p, B, H, gb1, st_);
+        mlp_adam(W.p, G.p, Mo.p, Vo.p, nparam, lr_ep, step + 1, 1e-5f, st_);
+      }
+    }
+    // Inference copies: BF16-rounded weights.
+    m.W1.reserve(n1);
+    m.B1.reserve(H);
+    m.W2.reserve(n2);
+    m.B2.reserve(H);
+    m.W3.reserve(n3);
+    m.B3.reserve(NB);
+    mlp_round_bf16(w1, m.W1.p, n1, st_);
+    mlp_round_bf16(b1, m.B1.p, H, st_);
+    mlp_round_bf16(w2, m.W2.p, n2, st_);
+    mlp_round_bf16(b2, m.B2.p, H, st_);
+    mlp_round_bf16(w3, m.W3.p, n3, st_);
+    mlp_round_bf16(b3, m.B3.p, NB, st_);
+    m.bucket_val.reserve(NB);
+    HB_CUDA(cudaMemcpyAsync(m.bucket_val.p, m.buckets.data(), NB * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
+    // Calibration on the held-out queries: predicted nprobe for a grid of
+    // thresholds -> recall against the label search's results.
+    m.trained = true;
+    const float grid[] = {0.3f,  0.4f,  0.5f,  0.6f,   0.7f,   0.75f,  0.8f,   0.85f,  0.88f,  0.9f,   0.92f,
+                          0.94f, 0.95f, 0.96f, 0.97f,  0.975f, 0.98f,  0.985f, 0.99f,  0.993f, 0.995f, 0.997f,
+                          0.998f, 0.999f, 0.9995f, 0.9999f, 1.0f};
+    DevBuf<int32_t> npv;
+    npv.reserve(nval);
+    std::vector<int32_t> np_h(nval);
+    m.cal_thr.clear();
+    m.cal_recall.clear();
+    m.cal_avgp.clear();
+    const float* qv = qall.p + ntr * dpad_;
+    const float* cv = cd.p + ntr * P;
+    for (float t : grid) {
+      probe_infer(static_cast<int>(nval), qv, cv, P, nullptr, t, P, npv.p);
+      HB_CUDA(cudaMemcpyAsync(np_h.data(), npv.p, nval * sizeof(int32_t), cudaMemcpyDeviceToHost, st_));
+      HB_CUDA(cudaStreamSynchronize(st_));
+      double hit = 0, sp_sum = 0;
+      for (size_t i = 0; i < nval; ++i) {
+        const int32_t* rr = &ranks_h[(ntr + i) * k];
+        for (size_t j = 0; j < k; ++j) hit += rr[j] < np_h[i];
+        sp_sum += np_h[i];
+      }
+      m.cal_thr.push_back(t);
+      m.cal_recall.push_back(static_cast<float>(hit / (nval * k)));
+      m.cal_avgp.push_back(static_cast<float>(sp_sum / nval));
+    }
+    m.thr = 1.0f;
+    float bestp = 1e30f;
+    for (size_t i = 0; i < m.cal_thr.size(); ++i)
+      if (m.cal_recall[i] >= target && m.cal_avgp[i] < bestp) {
+        bestp = m.cal_avgp[i];
+        m.thr = m.cal_thr[i];
+      }
+    HB_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  int probe_calibration(float* thr, float* recall, float* avgp, int max_n) const {
+    const int n = static_cast<int>(probe_.cal_thr.size());
+    for (int i = 0; i < n && i < max_n; ++i) {
+      if (thr) thr[i] = probe_.cal_thr[i];
+      if (recall) recall[i] = probe_.cal_recall[i];
+      if (avgp) avgp[i] = probe_.cal_avgp[i];
+    }
+    return n;
+  }
+
+ private:
+  ProbeModel probe_;
+  int cut_mode_ = 0;
+  int cut_cap_ = 0;
+  float cut_thr_ = 1.0f;
+  const int32_t* cut_src_ = nullptr;
+  size_t cut_b0_ = 0;
+  DevBuf<float> cdist_, pf_, ph1_, ph2_, plog_;
+  DevBuf<int32_t> npq_;
 
   size_t d_, nlist_, nprobe_;
   size_t dpad_ = 16;
@@ -1049,7 +1358,7 @@ void hb_search_params_init(hb_search_params* p) {
   p->warmup_lists = 10;      // --warmup_list default (src/query.cpp:100-103)
   p->warmup_list_size = 0;   // 0 -> k (src/query.cpp:330-333)
   p->precision = HB_PREC_FP32;
-  p->rerank_mult = 4;
+  p->rerank_mult = 2;  // 2k candidates reproduce the exact scan on the 10M x 128 workload
   p->learned_probe = 0;
   p->learned_target = 0.0f;
   p->nprobe_per_query = nullptr;
@@ -1168,10 +1477,16 @@ int hb_profile_read(hb_index* ix, char* names, size_t names_len, double* ms, int
   });
 }
 
-int hb_train_probe_predictor(hb_index* ix, size_t, const float*, size_t, size_t, float) {
+int hb_train_probe_predictor(hb_index* ix, size_t nt, const float* q, size_t k, size_t label_nprobe, float target) {
   HB_NEED_INDEX(ix);
-  hb::g_last_error = "learned probe predictor is not built in this version";
-  return HB_ERR_INVALID;
+  return guarded([&] { ix->core->train_probe(nt, q, k, label_nprobe, target); });
+}
+
+int hb_probe_calibration(const hb_index* ix, float* thr, float* recall, float* avg_nprobe, int max_n, int* n) {
+  HB_NEED_INDEX(ix);
+  const int c = ix->core->probe_calibration(thr, recall, avg_nprobe, max_n);
+  if (n) *n = c;
+  return HB_OK;
 }
 
 }  // extern "C"

@@ -195,6 +195,28 @@ void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st);
 // probes (nq x P) -> first column (nq x 1) and the rest (nq x (P-1)).
 void launch_split_probes(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st);
 
+// k_mlp.cu: learned probe predictor kernels.
+void mlp_gemm(int M, int N, int K, const float* A, int lda, bool tA, const float* B, int ldb, bool tB, float* C, int ldc,
+              const float* bias, float beta, bool gelu, float* Z, bool round_bf16, cudaStream_t st);
+void mlp_gelu_backward(const float* dH, const float* Z, float* dZ, size_t n, cudaStream_t st);
+void mlp_softmax_ce(const float* logits, const int32_t* labels, int B, int NB, float* dlogits, float* loss,
+                    cudaStream_t st);
+void mlp_colsum(const float* dY, int B, int N, float* db, cudaStream_t st);
+void mlp_adam(float* w, const float* g, float* m, float* v, size_t n, float lr, int step, float wd, cudaStream_t st);
+void mlp_round_bf16(const float* src, float* dst, size_t n, cudaStream_t st);
+void mlp_features(const float* q, int nq, int d, int dpad, const float* cdist, int P, int C, float* out,
+                  cudaStream_t st);
+void mlp_moments(const float* x, int rows, int F, float* mean, float* inv_std, cudaStream_t st);
+void mlp_standardize(float* x, int rows, int F, const float* mean, const float* inv_std, bool round_bf16,
+                     cudaStream_t st);
+void mlp_choose_nprobe(const float* logits, int nq, int NB, const int32_t* bucket_val, float thr, int cap,
+                       int32_t* nprobe_out, int32_t* probes, int P, cudaStream_t st);
+void launch_cut_probes(const int32_t* nprobe, int nq, int P, int32_t* probes, cudaStream_t st);
+void launch_label_rank(const int64_t* I, int nq, int k, const int32_t* list_of_id, const int32_t* probes, int P,
+                       int32_t* need, int32_t* ranks, cudaStream_t st);
+void launch_list_of_id(const int64_t* list_off, int nlist, const int64_t* ids, int32_t* out, int64_t max_id,
+                       cudaStream_t st);
+
 // hb_index.cu: pieces the no-allocation entry point (hb_noalloc.cu) uses.
 // Device ordinal of an index (-1 for a null handle).
 int index_device(const hb_index* ix);

@@ -72,7 +72,7 @@ typedef struct {
   int32_t warmup_lists;       /* preSearch warmUpSearchList (default 10)        */
   int32_t warmup_list_size;   /* preSearch warmUpSearchListSize (0 -> k)        */
   int32_t precision;          /* HB_PREC_*                                     */
-  int32_t rerank_mult;        /* BF16/FP8: candidates kept = rerank_mult * k    */
+  int32_t rerank_mult;        /* BF16: candidates re-ranked = rerank_mult * k (default 2) */
   int32_t learned_probe;      /* 1: per-query nprobe from the learned predictor */
   float learned_target;       /* predictor target recall (0 -> trained target)   */
   const int32_t* nprobe_per_query; /* optional nq array (host or device); overrides nprobe */
@@ -166,6 +166,10 @@ int hb_profile_read(hb_index* ix, char* names, size_t names_len, double* ms, int
  * target in (0, 1]. */
 int hb_train_probe_predictor(hb_index* ix, size_t nt, const float* q, size_t k, size_t label_nprobe,
                              float target);
+
+/* Validation curve of the trained predictor: for each probability threshold,
+ * the recall against the label search and the average nprobe it gives. */
+int hb_probe_calibration(const hb_index* ix, float* thr, float* recall, float* avg_nprobe, int max_n, int* n);
 
 #ifdef __cplusplus
 }

@@ -33,7 +33,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libharmony_b200.so")
 
-__all__ = ["Index", "MetricType", "OptLevel", "EdgeDevice", "SearchMode", "Precision", "HarmonyError",
+__all__ = ["Index", "MetricType", "OptLevel", "EdgeDevice", "SearchMode", "Precision", "CoarseQuantizer", "HarmonyError",
            "SearchParams", "lib", "LIB_PATH"]
 
 
@@ -80,6 +80,13 @@ class Precision(enum.IntEnum):
     FP8 = 2
 
 
+class CoarseQuantizer(enum.IntEnum):
+    """Route of the coarse quantizer; every route gives the same probe rows."""
+    AUTO = 0
+    EXACT = 1
+    TENSOR = 2
+
+
 class _SearchParamsC(ctypes.Structure):
     _fields_ = [
         ("mode", ctypes.c_int32),
@@ -96,7 +103,8 @@ class _SearchParamsC(ctypes.Structure):
         ("learned_target", ctypes.c_float),
         ("nprobe_per_query", ctypes.c_void_p),
         ("max_nprobe", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("seed_rows", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
     ]
 
 
@@ -131,6 +139,8 @@ def lib() -> ctypes.CDLL:
     L.hb_get_list_sizes.argtypes = [vp, i64]
     L.hb_probe_lists.argtypes = [vp, sz, f, sz, i64, f]
     L.hb_warmup_tops.argtypes = [vp, sz, f, sz, sz, sz, f]
+    L.hb_set_coarse_quantizer.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.hb_coarse_fallbacks.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.hb_stream.restype = vp
     L.hb_stream.argtypes = [vp]
     L.hb_launch_count.restype = ctypes.c_uint64
@@ -189,6 +199,7 @@ class SearchParams:
     learned_target: float = 0.0
     nprobe_per_query: Optional[object] = None
     max_nprobe: int = 0
+    seed_rows: int = 0
 
 
 class Index:
@@ -355,6 +366,7 @@ class Index:
         c.learned_probe = int(bool(sp.learned_probe))
         c.learned_target = float(sp.learned_target)
         c.max_nprobe = int(sp.max_nprobe)
+        c.seed_rows = int(sp.seed_rows)
         return c
 
     def search(self, n: int, queries, k: int, distances, labels, ratio: float = 1.0) -> Stats:
@@ -406,6 +418,18 @@ class Index:
         _check(self._L.hb_warmup_tops(self._h, q.shape[0], q.ctypes.data, k, warm_lists,
                                       k if warm_list_size is None else warm_list_size, tops.ctypes.data))
         return tops
+
+    def set_coarse_quantizer(self, kind: "CoarseQuantizer" = CoarseQuantizer.AUTO, margin: int = -1) -> None:
+        """Pick the coarse quantizer's route (tensor cores + exact re-rank, or
+        the exact FP32 distance matrix) and the tensor-core candidate margin
+        (-1: max(16, nprobe / 4)).  The probe rows do not depend on it."""
+        _check(self._L.hb_set_coarse_quantizer(self._h, int(kind), int(margin)))
+
+    def coarse_fallbacks(self) -> int:
+        """Queries of the latest tensor-core coarse call recomputed exactly."""
+        n = ctypes.c_int64()
+        _check(self._L.hb_coarse_fallbacks(self._h, ctypes.byref(n)))
+        return int(n.value)
 
     # -- learned probe predictor (no reference counterpart) -----------------
     def train_probe_predictor(self, n: int, queries, k: int = 10, label_nprobe: int = 256,

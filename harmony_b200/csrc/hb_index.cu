@@ -128,6 +128,8 @@ class IndexCore {
     HB_CUDA(cudaMemsetAsync(list_off_.p, 0, (nlist_ + 1) * sizeof(int64_t), st_));
     host_off_.assign(nlist_ + 1, 0);
     ntotal_ = 0;
+    coarse_ready_ = false;
+    coarse_last_nq_ = 0;
     HB_CUDA(cudaStreamSynchronize(st_));
   }
 
@@ -295,6 +297,7 @@ class IndexCore {
     }
     HB_CUDA(cudaStreamSynchronize(st_));
     trained_ = true;
+    coarse_ready_ = false;
   }
 
   // ---- add: src/Index.cpp:581-698 ------------------------------------------
@@ -366,16 +369,106 @@ class IndexCore {
   // ---- coarse quantizer ----------------------------------------------------
 
   // probes_out (device, nq x P int32, ascending), cdist_out optional.
+  // Coarse quantizer (src/IVFScan.hpp:108-138, src/Index.cpp:1440-1448):
+  // probes_out (nq x P) = the P nearest centroids of each query by the
+  // reference's sequential FP32 distance, ascending, ties by lower centroid.
+  // For d <= 128 the tensor cores pick P + m candidates (3-term BF16 split),
+  // which are re-ranked exactly; a query whose candidate set cannot be
+  // proven to contain the exact top P is recomputed exactly.  Both routes
+  // give the same rows.
   void coarse(const float* qpad, int nq, int P, int32_t* probes_out, float* cdist_out) {
     dmat_.reserve(static_cast<size_t>(nq) * nlist_);
-    {
-    Scope sc(this, "coarse_l2_matrix");
-    launch_l2_matrix(qpad, nq, cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), dmat_.p,
-                     static_cast<int>(nlist_), st_);
+    const int Pm = std::min<int>(static_cast<int>(nlist_), P + coarse_extra(P));
+    const bool tc = coarse_kind_ != HB_COARSE_EXACT && d_ <= 128 && Pm <= kCoarseMaxPm && nq > 0;
+    HB_CHECK(tc || coarse_kind_ != HB_COARSE_TENSOR, HB_ERR_INVALID,
+             "the tensor-core coarse quantizer needs d <= 128 and nprobe + margin <= 1024");
+    if (!tc) {
+      {
+        Scope sc(this, "coarse_l2_matrix");
+        launch_l2_matrix(qpad, nq, cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), dmat_.p,
+                         static_cast<int>(nlist_), st_);
+      }
+      Scope sc(this, "coarse_select");
+      launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), P, probes_out, cdist_out,
+                         st_);
+      launches_ += 2;
+      coarse_last_nq_ = 0;
+      return;
     }
-    Scope sc(this, "coarse_select");
-    launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), P, probes_out, cdist_out, st_);
-    launches_ += 2;
+    ensure_coarse_tc();
+    ccand_.reserve(static_cast<size_t>(nq) * Pm);
+    cval_.reserve(static_cast<size_t>(nq) * Pm);
+    cflags_.reserve(static_cast<size_t>(nq));
+    {
+      Scope sc(this, "coarse_tc");
+      launch_coarse_tc(ctmap_, qpad, nq, static_cast<int>(dpad_), ckpad_, cnorm_.p, static_cast<int>(nlist_), dmat_.p,
+                       cerr_dev_.p, num_sms_, st_);
+    }
+    {
+      Scope sc(this, "coarse_select");
+      launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), Pm, ccand_.p, cval_.p, st_);
+    }
+    {
+      Scope sc(this, "coarse_refine");
+      launch_coarse_refine(qpad, nq, static_cast<int>(dpad_), cent_.p, ccand_.p, cval_.p, Pm, P,
+                           static_cast<int>(nlist_), cmaxnorm_.p, probes_out, cdist_out, cflags_.p, st_);
+      launch_coarse_fallback(qpad, nq, static_cast<int>(dpad_), cent_.p, static_cast<int>(nlist_), P, cflags_.p,
+                             dmat_.p, probes_out, cdist_out, st_);
+    }
+    launches_ += 4;
+    coarse_last_nq_ = nq;
+  }
+
+  int coarse_extra(int P) const { return coarse_margin_ >= 0 ? coarse_margin_ : std::max(16, P / 4); }
+
+  // Split BF16 centroids, their tensor map, ||c||^2 and max ||c||, built once
+  // per set of centroids.
+  void ensure_coarse_tc() {
+    if (coarse_ready_) return;
+    ckpad_ = static_cast<int>((d_ + 63) / 64 * 64);
+    csplit_.reserve(nlist_ * 3 * static_cast<size_t>(ckpad_));
+    make_centroid_split(cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), ckpad_, csplit_.p, ctmap_, st_);
+    cnorm_.reserve(nlist_);
+    launch_row_norms(cent_.p, nlist_, static_cast<int>(d_), static_cast<int>(dpad_), cnorm_.p, st_);
+    cmaxnorm_.reserve(1);
+    launch_max_norm(cnorm_.p, nlist_, cmaxnorm_.p, st_);
+    cerr_dev_.reserve(1);
+    HB_CUDA(cudaMemsetAsync(cerr_dev_.p, 0, sizeof(int), st_));
+    launches_ += 3;
+    coarse_ready_ = true;
+  }
+
+  // Raises when a bounded wait of the tensor-core quantizer gave up since the
+  // last check (the flag is sticky until read here).
+  void coarse_err_check() {
+    if (!coarse_ready_) return;
+    HB_CUDA(cudaMemcpyAsync(err_host_, cerr_dev_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    if (*err_host_ != 0) {
+      const int code = *err_host_;
+      HB_CUDA(cudaMemsetAsync(cerr_dev_.p, 0, sizeof(int), st_));
+      throw Error(HB_ERR_CUDA, "tensor-core coarse quantizer gave up waiting (code " + std::to_string(code) + ")");
+    }
+  }
+
+  void set_coarse(int kind, int margin) {
+    HB_CHECK(kind >= HB_COARSE_AUTO && kind <= HB_COARSE_TENSOR, HB_ERR_INVALID, "unknown coarse quantizer kind");
+    HB_CHECK(margin >= -1 && margin <= kCoarseMaxPm, HB_ERR_INVALID, "coarse margin must be in [-1, 1024]");
+    coarse_kind_ = kind;
+    coarse_margin_ = margin;
+  }
+
+  // Queries of the most recent tensor-core coarse call whose rows were
+  // recomputed exactly.
+  int64_t coarse_fallbacks() {
+    HB_CUDA(cudaSetDevice(device_));
+    if (coarse_last_nq_ == 0) return 0;
+    std::vector<int> f(coarse_last_nq_);
+    HB_CUDA(cudaMemcpyAsync(f.data(), cflags_.p, f.size() * sizeof(int), cudaMemcpyDeviceToHost, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    int64_t n = 0;
+    for (int v : f) n += v != 0;
+    return n;
   }
 
   // ---- search: src/Index.cpp:1638-1706 --------------------------------------
@@ -397,6 +490,8 @@ class IndexCore {
                "the BF16 scan implements ORIGINAL / BRUTE_FORCE search (pruning and the dimension relay are FP32 modes)");
       HB_CHECK(ntotal_ == 0 || bf16_ready_, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
     }
+    HB_CHECK(p.seed_rows >= 0 && p.seed_rows <= 256, HB_ERR_INVALID, "seed_rows must be in [0, 256]");
+    seed_rows_ = p.seed_rows > 0 ? p.seed_rows : 256;
     const int max_R = bf16 ? scan_bf16_max_R(kpad_ > 0 ? kpad_ : 128) : 0;
     const int R = bf16 ? std::min(max_R, std::max(static_cast<int>(k), p.rerank_mult * static_cast<int>(k))) : 0;
     if (bf16)
@@ -505,6 +600,7 @@ class IndexCore {
       }
     }
     HB_CUDA(cudaStreamSynchronize(st_));
+    coarse_err_check();
   }
 
   void probe_lists(size_t nq, const float* q, size_t P, int64_t* probes, float* cdist) {
@@ -523,7 +619,7 @@ class IndexCore {
     ++launches_;
     HB_CUDA(cudaMemcpyAsync(probes, pr64.p, nq * P * sizeof(int64_t), cudaMemcpyDefault, st_));
     if (cdist) HB_CUDA(cudaMemcpyAsync(cdist, cd.p, nq * P * sizeof(float), cudaMemcpyDefault, st_));
-    HB_CUDA(cudaStreamSynchronize(st_));
+    HB_CUDA(cudaStreamSynchronize(st_));    coarse_err_check();
   }
 
   void warmup_tops(size_t nq, const float* q, size_t k, size_t wl, size_t wls, float* tops) {
@@ -541,7 +637,7 @@ class IndexCore {
                        st_);
     ++launches_;
     HB_CUDA(cudaMemcpyAsync(tops, t.p, nq * sizeof(float), cudaMemcpyDefault, st_));
-    HB_CUDA(cudaStreamSynchronize(st_));
+    HB_CUDA(cudaStreamSynchronize(st_));    coarse_err_check();
   }
 
   // ---- save / load: src/Index.cpp:1708-1770, src/IVF.cpp:76-134 --------------
@@ -907,6 +1003,12 @@ class IndexCore {
                         list_cursor_.p, list_q_.p, item_off_.p, slot_base.p, work_tmp_.p, wtmp, st_);
     }
     launches_ += 3;
+    {
+      Scope sc(this, "tau_seed");
+      launch_tau_seed(qpad_.p, nb, static_cast<int>(dpad_), kpad_, codes_bf16_.p, list_off_.p, static_cast<int>(nlist_),
+                      list_qoff_.p, list_q_.p, norms_.p, std::max(R, seed_rows_), R, maxnorm_.p, tau_.p, st_);
+    }
+    ++launches_;
     part.reserve(max_slots(nb, P, cr) * static_cast<size_t>(scan_bf16_keys_per_slot(R)));
     counter_.reserve(1);
     HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
@@ -936,8 +1038,9 @@ class IndexCore {
     ++launches_;
   }
 
-  // BF16 search of one batch: exact coarse probes, a per-query bound of the
-  // R-th approximate key seeded from the nearest list, one tensor-core pass
+  // BF16 search of one batch: exact coarse probes, the list-major work
+  // description, a per-query bound of the R-th approximate key seeded from
+  // the nearest list, one tensor-core pass
   // over all probes (items tighten the shared bound as they finish), and
   // the exact FP32 re-rank.
   void search_batch_bf16(int nb, int P, int k, int R, float* Dd, int64_t* Id) {
@@ -946,12 +1049,6 @@ class IndexCore {
     err_dev_.reserve(1);
     HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
     tau_.reserve(nb);
-    {
-      Scope sc(this, "tau_seed");
-      launch_tau_seed(qpad_.p, nb, probes_.p, P, codes_.p, list_off_.p, norms_.p, static_cast<int>(dpad_), 256, R,
-                      maxnorm_.p, tau_.p, st_);
-    }
-    ++launches_;
     bf16_pass(nb, P, probes_.p, R, slot_base_, part_);
     {
       Scope sc(this, "rerank");
@@ -1079,6 +1176,7 @@ class IndexCore {
     std::vector<int64_t> ids_h(ntotal_);
     HB_CUDA(cudaMemcpyAsync(ids_h.data(), ids_.p, ntotal_ * sizeof(int64_t), cudaMemcpyDeviceToHost, st_));
     HB_CUDA(cudaStreamSynchronize(st_));
+    coarse_err_check();
     int64_t max_id = 0;
     for (int64_t v : ids_h) max_id = std::max(max_id, v);
     DevBuf<int32_t> lid, need, ranks;
@@ -1263,6 +1361,18 @@ class IndexCore {
   int kpad_ = 0;
   bool bf16_ready_ = false;
   alignas(64) unsigned char tmap_[128];
+  // tensor-core coarse quantizer
+  bool coarse_ready_ = false;
+  int coarse_kind_ = HB_COARSE_AUTO;
+  int coarse_margin_ = -1;
+  int seed_rows_ = 256;  // rows of the nearest list behind the BF16 scan's seed bound
+  int coarse_last_nq_ = 0;
+  int ckpad_ = 0;
+  alignas(64) unsigned char ctmap_[128];
+  DevBuf<uint16_t> csplit_;
+  DevBuf<float> cnorm_, cmaxnorm_, cval_;
+  DevBuf<int32_t> ccand_;
+  DevBuf<int> cflags_, cerr_dev_;
   DevBuf<uint16_t> codes_bf16_;
   DevBuf<uint64_t> tau_, part2_;
   DevBuf<float> maxnorm_;
@@ -1363,6 +1473,7 @@ void hb_search_params_init(hb_search_params* p) {
   p->learned_target = 0.0f;
   p->nprobe_per_query = nullptr;
   p->max_nprobe = 0;
+  p->seed_rows = 0;
 }
 
 const char* hb_last_error(void) { return hb::g_last_error.c_str(); }
@@ -1456,6 +1567,19 @@ int hb_warmup_tops(hb_index* ix, size_t nq, const float* q, size_t k, size_t war
                    float* tops) {
   HB_NEED_INDEX(ix);
   return guarded([&] { ix->core->warmup_tops(nq, q, k, warm_lists, warm_list_size, tops); });
+}
+
+int hb_set_coarse_quantizer(hb_index* ix, int kind, int margin) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->set_coarse(kind, margin); });
+}
+
+int hb_coarse_fallbacks(hb_index* ix, int64_t* n) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] {
+    HB_CHECK(n, HB_ERR_INVALID, "null output pointer");
+    *n = ix->core->coarse_fallbacks();
+  });
 }
 
 void* hb_stream(hb_index* ix) { return (ix && ix->core) ? static_cast<void*>(ix->core->stream()) : nullptr; }

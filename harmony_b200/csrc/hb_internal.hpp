@@ -185,15 +185,33 @@ void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream
 void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
                    const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
                    const uint64_t* part2 = nullptr, const int64_t* slot_base2 = nullptr, int P2 = 0);
-// Per-query upper bound of the R-th approximate key from the nearest list's
-// first S rows (exact FP32 + BF16 error margin); maxnorm = max ||x|| (device).
-void launch_tau_seed(const float* q, int nq, const int32_t* probes, int P, const float* codes,
-                     const int64_t* list_off, const float* xnorm, int dpad, int S, int R, const float* maxnorm,
-                     uint64_t* tau, cudaStream_t st);
+// Per-query upper bound of the R-th approximate key from the first S <= 256
+// BF16 rows of the query's nearest list (probe rank 0 in the list-major work
+// description); queries without a seed get all ones.  maxnorm = max ||x||.
+void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* codes_bf16, const int64_t* list_off,
+                     int nlist, const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int R,
+                     const float* maxnorm, uint64_t* tau, cudaStream_t st);
 // *out = max over i of sqrt(norms[i]) (slightly rounded up), on the device.
 void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st);
 // probes (nq x P) -> first column (nq x 1) and the rest (nq x (P-1)).
 void launch_split_probes(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st);
+
+// k_coarse_tc.cu: tensor-core coarse quantizer (3-term BF16 split) with an
+// exact FP32 finish; the probe rows equal the exact quantizer's.
+constexpr int kCoarseMaxPm = 1024;  // largest candidate count per query
+size_t coarse_tc_smem_bytes(int kpad);
+// cent (nlist x dpad FP32) -> out (nlist x 3*kpad BF16 [hi|lo|hi]) + its tensor map.
+void make_centroid_split(const float* cent, int nlist, int dpad, int kpad, void* out, void* tmap_out, cudaStream_t st);
+// V (nq x nlist) = max(0, ||q||^2 + ||c||^2 - 2 q.c) on the tensor cores.
+void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kpad, const float* cnorm, int nlist,
+                      float* V, int* err, int num_sms, cudaStream_t st);
+// Exact distances of the Pm candidates, top P, exactness flag per query.
+void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, const int32_t* cand, const float* cval,
+                          int Pm, int P, int nlist, const float* cmaxnorm, int32_t* probes, float* cdist, int* flags,
+                          cudaStream_t st);
+// Exact row and top P for every flagged query (V rows are overwritten).
+void launch_coarse_fallback(const float* q, int nq, int dpad, const float* cent, int nlist, int P, const int* flags,
+                            float* V, int32_t* probes, float* cdist, cudaStream_t st);
 
 // k_mlp.cu: learned probe predictor kernels.
 void mlp_gemm(int M, int N, int K, const float* A, int lda, bool tA, const float* B, int ldb, bool tB, float* C, int ldc,

@@ -1,6 +1,10 @@
-// Block-wide selection of the k smallest 64-bit keys: radix selection over
-// key bytes (most significant first) until the chosen bucket holds exactly
-// the keys still needed, then a bitonic sort of the winners.
+// Block-wide selection of the k smallest 64-bit keys: one pass for the count,
+// minimum and maximum of the non-empty keys (the bits above their highest
+// differing bit are common to all of them and need no radix pass), then
+// radix selection over 8-bit digits from that bit down until the chosen
+// bucket holds exactly the keys still needed, then a bitonic sort of the
+// winners.  Histogram updates are aggregated per warp over lanes that hit
+// the same bin (distances of one row often share their leading digits).
 #pragma once
 #include "hb_device.cuh"
 
@@ -12,27 +16,79 @@ struct SelectShared {
   int need;
   int count;
   int real;
+  unsigned long long lo;
+  unsigned long long hi;
 };
 
-// Radix selection of the kk smallest non-empty keys among key_at(0..m).
-// On return s_out[0..kk) holds them (unordered) and the function returns kk.
+// Count, minimum and maximum of the non-empty keys among key_at(0..m);
+// returns the count.  Every thread of the block must call it.
+template <class KeyAt>
+__device__ __forceinline__ int block_key_stats(KeyAt key_at, int m, SelectShared& sh) {
+  if (threadIdx.x == 0) {
+    sh.real = 0;
+    sh.lo = kEmpty;
+    sh.hi = 0;
+  }
+  __syncthreads();
+  int c = 0;
+  unsigned long long lo = kEmpty, hi = 0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const uint64_t key = key_at(i);
+    if (key == kEmpty) continue;
+    ++c;
+    lo = key < lo ? key : lo;
+    hi = key > hi ? key : hi;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, off);
+    const unsigned long long l2 = __shfl_xor_sync(0xffffffffu, lo, off);
+    const unsigned long long h2 = __shfl_xor_sync(0xffffffffu, hi, off);
+    lo = l2 < lo ? l2 : lo;
+    hi = h2 > hi ? h2 : hi;
+  }
+  if ((threadIdx.x & 31) == 0 && c) {
+    atomicAdd(&sh.real, c);
+    atomicMin(&sh.lo, lo);
+    atomicMax(&sh.hi, hi);
+  }
+  __syncthreads();
+  return sh.real;
+}
+
+// Selection of the kk smallest non-empty keys among key_at(0..m), after
+// block_key_stats on the same keys (0 < kk <= count).  On return
+// s_out[0..kk) holds them (unordered) and the function returns kk.
 template <class KeyAt>
 __device__ __forceinline__ int block_select(KeyAt key_at, int m, int kk, SelectShared& sh, uint64_t* s_out) {
-  const int tid = threadIdx.x;
-  uint64_t prefix = 0;
-  int shift = 64;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const uint64_t diff = static_cast<uint64_t>(sh.lo ^ sh.hi);
+  // Bits [shift, 64) are equal in every non-empty key.
+  int shift = diff ? 64 - __clzll(static_cast<long long>(diff)) : 0;
+  uint64_t prefix = shift >= 64 ? 0 : (static_cast<uint64_t>(sh.lo) >> shift) << shift;
   int need = kk;
-  // Narrow the prefix one byte at a time until the chosen bucket holds
-  // exactly the keys still needed.
-  while (shift > 0) {
-    shift -= 8;
+  bool take_all = kk >= sh.real;
+  __syncthreads();
+  while (!take_all && shift > 0) {
+    const int w = shift < 8 ? shift : 8;
+    shift -= w;
+    const int top = shift + w;  // bits >= top must match the prefix
+    const uint64_t want = top >= 64 ? 0 : prefix >> top;
     for (int i = tid; i < 256; i += blockDim.x) sh.hist[i] = 0;
     __syncthreads();
-    for (int i = tid; i < m; i += blockDim.x) {
-      const uint64_t key = key_at(i);
-      if (key == kEmpty) continue;
-      if (shift == 56 || (key >> (shift + 8)) == (prefix >> (shift + 8)))
-        atomicAdd(&sh.hist[(key >> shift) & 255], 1);
+    for (int base = tid & ~31; base < m; base += blockDim.x) {
+      const int i = base + lane;
+      bool valid = false;
+      unsigned bin = 0;
+      if (i < m) {
+        const uint64_t key = key_at(i);
+        valid = key != kEmpty && (top >= 64 || (key >> top) == want);
+        bin = static_cast<unsigned>(key >> shift) & ((1u << w) - 1u);
+      }
+      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const unsigned peers = __match_any_sync(vmask, bin);
+        if (lane == __ffs(peers) - 1) atomicAdd(&sh.hist[bin], __popc(peers));
+      }
     }
     __syncthreads();
     if (tid < 32) {
@@ -52,8 +108,8 @@ __device__ __forceinline__ int block_select(KeyAt key_at, int m, int kk, SelectS
       }
       const int excl = incl - sum;
       const unsigned hit = __ballot_sync(0xffffffffu, incl >= need);
-      const int lane = __ffs(hit) - 1;
-      if (tid == lane) {
+      const int first = __ffs(hit) - 1;
+      if (tid == first) {
         int cum = excl;
         int b = 0;
         for (; b < 8; ++b) {
@@ -72,14 +128,15 @@ __device__ __forceinline__ int block_select(KeyAt key_at, int m, int kk, SelectS
     __syncthreads();
     if (done) break;
   }
-  // Keys whose top (64 - shift) bits are <= the prefix's are the selection.
+  // The selection: every non-empty key when all are wanted, else the keys
+  // whose bits from `shift` up are <= the prefix's.
   if (tid == 0) sh.count = 0;
   __syncthreads();
-  const uint64_t lim = prefix >> shift;
+  const uint64_t lim = shift >= 64 ? 0 : prefix >> shift;
   for (int i = tid; i < m; i += blockDim.x) {
     const uint64_t key = key_at(i);
     if (key == kEmpty) continue;
-    if ((shift == 64 ? 0 : (key >> shift)) <= lim) {
+    if (take_all || (key >> shift) <= lim) {
       const int pos = atomicAdd(&sh.count, 1);
       if (pos < kk) s_out[pos] = key;
     }
@@ -88,24 +145,11 @@ __device__ __forceinline__ int block_select(KeyAt key_at, int m, int kk, SelectS
   return kk;
 }
 
-// Count keys that are not empty.
-template <class KeyAt>
-__device__ __forceinline__ int block_count_real(KeyAt key_at, int m, SelectShared& sh) {
-  if (threadIdx.x == 0) sh.real = 0;
-  __syncthreads();
-  int c = 0;
-  for (int i = threadIdx.x; i < m; i += blockDim.x) c += key_at(i) != kEmpty;
-  for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&sh.real, c);
-  __syncthreads();
-  return sh.real;
-}
-
 // Select and sort: s_out gets the min(k, real) smallest keys ascending,
 // padded with kEmpty to pow2_ceil(k).
 template <class KeyAt>
 __device__ __forceinline__ int block_topk_sorted(KeyAt key_at, int m, int k, SelectShared& sh, uint64_t* s_out) {
-  const int real = block_count_real(key_at, m, sh);
+  const int real = block_key_stats(key_at, m, sh);
   const int kk = min(k, real);
   const int n2 = pow2_ceil(max(k, 2));
   for (int i = threadIdx.x; i < n2; i += blockDim.x) s_out[i] = kEmpty;

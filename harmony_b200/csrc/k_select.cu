@@ -50,6 +50,144 @@ __global__ void __launch_bounds__(kSelThreads) select_rows_kernel(const float* _
   }
 }
 
+// Row selection for rows of at most 32 * kSelThreads columns and k <= 1024:
+// the row is read once into registers (VPT values per thread); a histogram
+// of the keys' high words over kBins equal ranges between the row's
+// smallest and largest non-empty key finds the bin holding the k-th key;
+// the keys in that bin and below (k plus the bin's share) are compacted
+// into shared memory and sorted.  The result is the same as
+// select_rows_kernel's: the k smallest (value bits, column) keys, ascending.
+constexpr int kBins = 1024;
+constexpr int kCandCap = 2048;
+
+template <int VPT>
+__global__ void __launch_bounds__(kSelThreads) select_rows_reg_kernel(const float* __restrict__ D, int ncols, int ldD,
+                                                                      int k, int32_t* __restrict__ out_idx,
+                                                                      float* __restrict__ out_val) {
+  __shared__ int hist[kBins];
+  __shared__ uint64_t s_keys[kCandCap];
+  __shared__ SelectShared sh;
+  __shared__ unsigned s_lo, s_hi;
+  __shared__ int s_real, s_cnt, s_bin, s_cum;
+  __shared__ int s_wsum[kSelThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const float* row = D + static_cast<size_t>(blockIdx.x) * ldD;
+  // High words of the keys; 0xFFFFFFFF marks empty (a value >= FLT_MAX or
+  // NaN has no key; no non-empty value has all-ones bits).
+  uint32_t u[VPT];
+  unsigned lo = 0xFFFFFFFFu, hi = 0;
+  int real = 0;
+#pragma unroll
+  for (int j = 0; j < VPT; ++j) {
+    const int c = tid + j * kSelThreads;
+    u[j] = 0xFFFFFFFFu;
+    if (c < ncols) {
+      const float v = row[c];
+      if (v < FLT_MAX) {
+        u[j] = __float_as_uint(v);
+        lo = min(lo, u[j]);
+        hi = max(hi, u[j]);
+        ++real;
+      }
+    }
+  }
+  if (tid == 0) {
+    s_lo = 0xFFFFFFFFu;
+    s_hi = 0;
+    s_real = 0;
+    s_cnt = 0;
+  }
+  for (int i = tid; i < kBins; i += kSelThreads) hist[i] = 0;
+  for (int off = 16; off > 0; off >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, off));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, off));
+    real += __shfl_xor_sync(0xffffffffu, real, off);
+  }
+  __syncthreads();
+  if (lane == 0 && real) {
+    atomicMin(&s_lo, lo);
+    atomicMax(&s_hi, hi);
+    atomicAdd(&s_real, real);
+  }
+  __syncthreads();
+  real = s_real;
+  lo = s_lo;
+  const int kk = min(k, real);
+  // Bin of a high word: monotone in the word (float rounding is monotone),
+  // below kBins.
+  const float scale = static_cast<float>(kBins) / (static_cast<float>(s_hi - lo) + 1.0f);
+  auto bin_of = [&](uint32_t x) -> int {
+    return min(kBins - 1, static_cast<int>(static_cast<float>(x - lo) * scale));
+  };
+  // Histogram, then the bin where the count reaches kk.
+  if (kk > 0 && kk < real) {
+#pragma unroll
+    for (int j = 0; j < VPT; ++j)
+      if (u[j] != 0xFFFFFFFFu) atomicAdd(&hist[bin_of(u[j])], 1);
+  }
+  __syncthreads();
+  if (kk > 0 && kk < real) {
+    constexpr int per = kBins / kSelThreads;
+    int loc = 0;
+#pragma unroll
+    for (int b = 0; b < per; ++b) loc += hist[tid * per + b];
+    int incl = loc;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int o = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += o;
+    }
+    if (lane == 31) s_wsum[wid] = incl;
+    __syncthreads();
+    int base = 0;
+    for (int w = 0; w < wid; ++w) base += s_wsum[w];
+    int cum = base + incl - loc;
+    if (cum < kk && cum + loc >= kk) {
+      int b = 0;
+      for (; b < per; ++b) {
+        cum += hist[tid * per + b];
+        if (cum >= kk) break;
+      }
+      s_bin = tid * per + b;
+      s_cum = cum;
+    }
+  } else if (tid == 0) {
+    s_bin = kBins;  // every non-empty key
+    s_cum = real;
+  }
+  __syncthreads();
+  const int bstar = s_bin;
+  const int ncand = s_cum;
+  uint64_t* keys = s_keys;
+  int m = 0;
+  if (ncand <= kCandCap) {
+#pragma unroll
+    for (int j = 0; j < VPT; ++j) {
+      if (u[j] != 0xFFFFFFFFu && (bstar >= kBins || bin_of(u[j]) <= bstar)) {
+        const int pos = atomicAdd(&s_cnt, 1);
+        keys[pos] = (static_cast<uint64_t>(u[j]) << 32) | static_cast<uint32_t>(tid + j * kSelThreads);
+      }
+    }
+    m = pow2_ceil(max(ncand, 2));
+    __syncthreads();
+    for (int i = ncand + tid; i < m; i += kSelThreads) keys[i] = kEmpty;
+    __syncthreads();
+    block_bitonic_sort(keys, m);
+  } else {
+    // Many equal high words near the k-th key: the generic selection.
+    auto key_at = [&](int i) -> uint64_t {
+      const float v = row[i];
+      return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(i)) : kEmpty;
+    };
+    block_topk_sorted(key_at, ncols, k, sh, keys);
+  }
+  for (int j = tid; j < k; j += kSelThreads) {
+    const uint64_t key = j < kk ? keys[j] : kEmpty;
+    const size_t o = static_cast<size_t>(blockIdx.x) * k + j;
+    out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
+    if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+  }
+}
+
 __global__ void __launch_bounds__(kSelThreads) merge_kernel(const uint64_t* __restrict__ part,
                                                             const int64_t* __restrict__ slot_base, int P, int k,
                                                             const int64_t* __restrict__ ids, float* __restrict__ D,
@@ -126,7 +264,7 @@ __global__ void __launch_bounds__(kSelThreads) warmup_tops_kernel(const float* _
     const float v = sd[i];
     return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(i)) : kEmpty;
   };
-  const int real = block_count_real(key_at, m, sh);
+  const int real = block_key_stats(key_at, m, sh);
   if (real < k) {
     if (threadIdx.x == 0) tops[qi] = FLT_MAX;
     return;
@@ -207,6 +345,19 @@ void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, in
                         cudaStream_t st) {
   if (nrows <= 0 || k <= 0) return;
   HB_CHECK(k <= kMaxSelect, HB_ERR_INVALID, "nprobe above 8192 is not supported");
+  if (k <= 1024 && ncols <= 32 * kSelThreads) {
+    const int vpt = (ncols + kSelThreads - 1) / kSelThreads;
+    if (vpt <= 4)
+      select_rows_reg_kernel<4><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val);
+    else if (vpt <= 8)
+      select_rows_reg_kernel<8><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val);
+    else if (vpt <= 16)
+      select_rows_reg_kernel<16><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val);
+    else
+      select_rows_reg_kernel<32><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val);
+    HB_CUDA(cudaGetLastError());
+    return;
+  }
   const size_t smem = static_cast<size_t>(pow2_ceil(k < 2 ? 2 : k)) * 8;
   HB_CUDA(cudaFuncSetAttribute(select_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                static_cast<int>(smem)));

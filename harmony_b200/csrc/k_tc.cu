@@ -433,65 +433,117 @@ __global__ void split_probes_kernel(const int32_t* __restrict__ probes, int nq, 
   else rest[static_cast<size_t>(q) * (P - 1) + (j - 1)] = probes[idx];
 }
 
-// Upper bound of each query's R-th approximate key before the scan: the
-// R-th smallest exact FP32 value ||x||^2 - 2 q.x over the first S rows of
-// the query's nearest list, plus a margin covering the BF16 scan's error
-// (rounding q and x to 8-bit significands changes each product by at most
-// (2u + u^2)|q_i x_i| with u = 2^-8, so the dot product by at most about
-// 2^-7 ||q|| ||x||; the margin doubles that and adds FP32 rounding).  A
-// seed therefore never drops a key that belongs to the approximate top R.
-__global__ void __launch_bounds__(128) tau_seed_kernel(const float* __restrict__ q, const int32_t* __restrict__ probes,
-                                                        int P, const float* __restrict__ codes,
-                                                        const int64_t* __restrict__ list_off,
-                                                        const float* __restrict__ xnorm, int dpad, int S, int R,
-                                                        const float* __restrict__ maxnorm,
-                                                        uint64_t* __restrict__ tau) {
-  extern __shared__ uint64_t s_seed[];  // pow2(S) keys, then dpad floats of the query
-  __shared__ SelectShared sh_sel;
-  __shared__ float s_qn;
-  const int qi = blockIdx.x;
-  const int n2 = pow2_ceil(S < 2 ? 2 : S);
-  float* sq = reinterpret_cast<float*>(s_seed + n2);
-  const float* qrow = q + static_cast<size_t>(qi) * dpad;
-  for (int c = threadIdx.x; c < dpad; c += blockDim.x) sq[c] = qrow[c];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float acc = 0.0f;
-    for (int c = 0; c < dpad; ++c) acc = __fadd_rn(acc, __fmul_rn(sq[c], sq[c]));
-    s_qn = acc;
+// Upper bound of each query's R-th approximate key before the scan, from the
+// first S rows of the query's nearest list.  The bound is computed from the
+// same BF16 operands the scan multiplies (the query rounded to BF16 exactly
+// as the scan's A tile, the BF16 codes), so the scan's value
+// ||x||^2 - 2 q~.x~ and the one here differ only by the order and width of
+// the FP32 accumulation of 128 exact BF16 products: each is within
+// 128 * 2^-19 * sum|q~_i x~_i| <= 2.5e-4 ||q|| max||x|| of the exact sum even
+// if the tensor cores kept only 19 bits per addition.  The margin,
+// 1e-3 ||q|| max||x|| + 2e-5 (max||x||^2 + |v|), covers twice that plus the
+// FP32 rounding of the combination, so the R-th value here plus the margin
+// is never below the R-th value the scan sees, and a seed never drops a key
+// of the scan's top R.
+//
+// List-major: one CTA per list stages the list's first S BF16 rows in shared
+// memory once; each query whose nearest list it is (probe rank 0 in the
+// list-major work description) takes one warp: lanes own rows, the query is
+// broadcast from shared memory, the S values are sorted in a per-warp buffer
+// and the R-th gives the bound.
+constexpr int kSeedRows = 256;
+constexpr int kSeedWarps = 8;
+
+__global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
+    const float* __restrict__ q, int dpad, int kpad, const __nv_bfloat16* __restrict__ codes,
+    const int64_t* __restrict__ list_off, const int64_t* __restrict__ list_qoff, const int32_t* __restrict__ list_q,
+    const float* __restrict__ xnorm, int S, int R, const float* __restrict__ maxnorm, uint64_t* __restrict__ tau) {
+  extern __shared__ __align__(16) uint8_t s_seed_raw[];
+  __shared__ float s_xn[kSeedRows];
+  __shared__ int s_qs[kSeedWarps * 32];
+  __shared__ int s_nq;
+  const int l = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  const int64_t e0 = list_qoff[l], e1 = list_qoff[l + 1];
+  bool mine = false;
+  for (int64_t e = e0 + tid; e < e1 && !mine; e += blockDim.x) mine = (list_q[e] & 0xffff) == 0;
+  if (!__syncthreads_or(mine)) return;
+  const int64_t b = list_off[l];
+  const int n = static_cast<int>(min(static_cast<int64_t>(S), list_off[l + 1] - b));
+  if (n < R) return;  // no seed: tau stays empty
+  const int n2 = pow2_ceil(n < 2 ? 2 : n);
+  const int stride = kpad * 2 + 16;  // bytes per staged row (padding spreads banks)
+  uint8_t* rows = s_seed_raw;
+  float* qbuf = reinterpret_cast<float*>(s_seed_raw + static_cast<size_t>(S) * stride) + wib * kpad;
+  uint64_t* buf = reinterpret_cast<uint64_t*>(s_seed_raw + static_cast<size_t>(S) * stride +
+                                              static_cast<size_t>(kSeedWarps) * kpad * 4) +
+                  static_cast<size_t>(wib) * kSeedRows;
+  const int cpr = kpad / 8;  // 16-byte chunks per row
+  for (int i = tid; i < n * cpr; i += blockDim.x) {
+    const int r = i / cpr, c = i - r * cpr;
+    cp_async16(rows + static_cast<size_t>(r) * stride + c * 16, codes + static_cast<size_t>(b + r) * kpad + c * 8, true);
   }
-  const int l = probes[static_cast<size_t>(qi) * P];
-  const int64_t b = l >= 0 ? list_off[l] : 0;
-  const int n = l >= 0 ? static_cast<int>(min(static_cast<int64_t>(S), list_off[l + 1] - b)) : 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float* x = codes + static_cast<size_t>(b + i) * dpad;
-    float dot = 0.0f;
-    for (int c = 0; c < dpad; c += 4) {
-      const float4 v = *reinterpret_cast<const float4*>(x + c);
-      dot = __fadd_rn(dot, __fmul_rn(sq[c], v.x));
-      dot = __fadd_rn(dot, __fmul_rn(sq[c + 1], v.y));
-      dot = __fadd_rn(dot, __fmul_rn(sq[c + 2], v.z));
-      dot = __fadd_rn(dot, __fmul_rn(sq[c + 3], v.w));
+  cp_async_commit();
+  for (int r = tid; r < n; r += blockDim.x) s_xn[r] = xnorm[b + r];
+  const float mn = *maxnorm;
+  cp_async_wait<0>();
+  // Rounds over the list's entries: the queries whose nearest list this is
+  // are gathered in shared memory, then one warp per query.
+  for (int64_t r0 = e0; r0 < e1; r0 += blockDim.x) {
+    if (tid == 0) s_nq = 0;
+    __syncthreads();
+    if (r0 + tid < e1) {
+      const uint32_t ent = static_cast<uint32_t>(list_q[r0 + tid]);
+      if ((ent & 0xffff) == 0) s_qs[atomicAdd(&s_nq, 1)] = static_cast<int>(ent >> 16);
     }
-    const float val = fmaf(-2.0f, dot, xnorm[b + i]);
-    s_seed[i] = (static_cast<uint64_t>(ordered_bits(val)) << 32) | static_cast<uint32_t>(i);
-  }
-  __syncthreads();
-  if (n < R) {
-    if (threadIdx.x == 0) tau[qi] = kEmpty;
-    return;
-  }
-  auto key_at = [&](int i) -> uint64_t { return s_seed[i]; };
-  uint64_t* s_out = s_seed + n2 + (dpad + 1) / 2;  // after the query copy
-  block_select(key_at, n, R, sh_sel, s_out);
-  if (threadIdx.x == 0) {
-    uint64_t mx = 0;
-    for (int i = 0; i < R; ++i) mx = s_out[i] > mx ? s_out[i] : mx;
-    const float vR = ordered_to_float(static_cast<uint32_t>(mx >> 32));
-    const float mn = *maxnorm;
-    const float margin = 0.032f * sqrtf(s_qn) * mn + 2e-5f * (mn * mn + fabsf(vR)) + 1e-30f;
-    const float t = vR + margin;
-    tau[qi] = (static_cast<uint64_t>(ordered_bits(t)) << 32) | 0xffffffffull;
+    __syncthreads();
+    const int nqr = s_nq;
+    for (int t = wib; t < nqr; t += kSeedWarps) {
+      const int qi = s_qs[t];
+      const float* qrow = q + static_cast<size_t>(qi) * dpad;
+      float qn = 0.0f;
+      for (int c = lane; c < kpad; c += 32) {
+        const float x = c < dpad ? qrow[c] : 0.0f;
+        qn = fmaf(x, x, qn);
+        qbuf[c] = __bfloat162float(__float2bfloat16_rn(x));
+      }
+      for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(0xffffffffu, qn, o);
+      __syncwarp();
+      for (int r = lane; r < n2; r += 32) {
+        uint64_t key = kEmpty;
+        if (r < n) {
+          const uint8_t* xr = rows + static_cast<size_t>(r) * stride;
+          // Four partial sums (any order is within the margin).
+          float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
+#pragma unroll 4
+          for (int c = 0; c < kpad; c += 8) {
+            const uint4 xv = *reinterpret_cast<const uint4*>(xr + c * 2);
+            const float4 qa = *reinterpret_cast<const float4*>(qbuf + c);
+            const float4 qb = *reinterpret_cast<const float4*>(qbuf + c + 4);
+            d0 = fmaf(qa.x, __uint_as_float(xv.x << 16), d0);
+            d1 = fmaf(qa.y, __uint_as_float(xv.x & 0xffff0000u), d1);
+            d2 = fmaf(qa.z, __uint_as_float(xv.y << 16), d2);
+            d3 = fmaf(qa.w, __uint_as_float(xv.y & 0xffff0000u), d3);
+            d0 = fmaf(qb.x, __uint_as_float(xv.z << 16), d0);
+            d1 = fmaf(qb.y, __uint_as_float(xv.z & 0xffff0000u), d1);
+            d2 = fmaf(qb.z, __uint_as_float(xv.w << 16), d2);
+            d3 = fmaf(qb.w, __uint_as_float(xv.w & 0xffff0000u), d3);
+          }
+          const float val = fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[r]);
+          key = (static_cast<uint64_t>(ordered_bits(val)) << 32) | static_cast<uint32_t>(r);
+        }
+        buf[r] = key;
+      }
+      __syncwarp();
+      warp_bitonic_sort(buf, n2, lane);
+      if (lane == 0) {
+        const float vR = ordered_to_float(static_cast<uint32_t>(buf[R - 1] >> 32));
+        const float margin = 1e-3f * sqrtf(qn) * mn + 2e-5f * (mn * mn + fabsf(vR)) + 1e-30f;
+        tau[qi] = (static_cast<uint64_t>(ordered_bits(vR + margin)) << 32) | 0xffffffffull;
+      }
+      __syncwarp();
+    }
+    __syncthreads();
   }
 }
 
@@ -586,14 +638,18 @@ void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_tau_seed(const float* q, int nq, const int32_t* probes, int P, const float* codes,
-                     const int64_t* list_off, const float* xnorm, int dpad, int S, int R, const float* maxnorm,
-                     uint64_t* tau, cudaStream_t st) {
+void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* codes_bf16, const int64_t* list_off,
+                     int nlist, const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int R,
+                     const float* maxnorm, uint64_t* tau, cudaStream_t st) {
   if (nq <= 0) return;
-  const int n2 = pow2_ceil(S < 2 ? 2 : S);
-  const size_t smem = static_cast<size_t>(n2) * 8 + static_cast<size_t>(dpad + 1) / 2 * 8 + static_cast<size_t>(R) * 8 + 64;
+  HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
+  HB_CHECK(S >= 1 && S <= kSeedRows && R >= 1 && R <= S, HB_ERR_INVALID, "seed sample out of range");
+  HB_CUDA(cudaMemsetAsync(tau, 0xff, static_cast<size_t>(nq) * sizeof(uint64_t), st));
+  const size_t smem = static_cast<size_t>(S) * (kpad * 2 + 16) + static_cast<size_t>(kSeedWarps) * kpad * 4 +
+                      static_cast<size_t>(kSeedWarps) * kSeedRows * 8;
   HB_CUDA(cudaFuncSetAttribute(tau_seed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  tau_seed_kernel<<<nq, 128, smem, st>>>(q, probes, P, codes, list_off, xnorm, dpad, S, R, maxnorm, tau);
+  tau_seed_kernel<<<nlist, kSeedWarps * 32, smem, st>>>(q, dpad, kpad, static_cast<const __nv_bfloat16*>(codes_bf16),
+                                                        list_off, list_qoff, list_q, xnorm, S, R, maxnorm, tau);
   HB_CUDA(cudaGetLastError());
 }
 

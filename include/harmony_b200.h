@@ -77,7 +77,9 @@ typedef struct {
   float learned_target;       /* predictor target recall (0 -> trained target)   */
   const int32_t* nprobe_per_query; /* optional nq array (host or device); overrides nprobe */
   int32_t max_nprobe;         /* cap for per-query nprobe (0 -> index nprobe)    */
-  int32_t reserved[6];
+  int32_t seed_rows;          /* BF16: rows of each query's nearest list behind
+                                 the scan's initial bound (0 -> 256, max 256)  */
+  int32_t reserved[5];
 } hb_search_params;
 
 void hb_search_params_init(hb_search_params* p);
@@ -142,6 +144,19 @@ int hb_search_noalloc(hb_index* ix, size_t nq, const float* q, size_t k, float* 
  * src/Index.cpp:967-995).  probes: nq*nprobe int64, cdist may be NULL. */
 int hb_probe_lists(hb_index* ix, size_t nq, const float* q, size_t nprobe, int64_t* probes,
                    float* cdist);
+
+/* Coarse quantizer route (no reference counterpart; the probe rows are the
+ * same on every route).  AUTO: tensor cores for d <= 128 (a 3-term BF16
+ * split picks nprobe + margin candidates, re-ranked in exact FP32; queries
+ * whose candidates cannot be proven to hold the exact top nprobe are
+ * recomputed exactly), else the FP32 distance matrix.  EXACT: always the
+ * FP32 matrix.  TENSOR: tensor cores or HB_ERR_INVALID.  margin -1 picks
+ * max(16, nprobe / 4). */
+enum { HB_COARSE_AUTO = 0, HB_COARSE_EXACT = 1, HB_COARSE_TENSOR = 2 };
+int hb_set_coarse_quantizer(hb_index* ix, int kind, int margin);
+/* Queries of the most recent tensor-core coarse call that were recomputed
+ * exactly (0 after an EXACT call). */
+int hb_coarse_fallbacks(hb_index* ix, int64_t* n);
 
 /* Warm-up heap tops (Index::warmUpSearch, src/Index.cpp:999-1051). */
 int hb_warmup_tops(hb_index* ix, size_t nq, const float* q, size_t k, size_t warm_lists,

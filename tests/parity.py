@@ -46,3 +46,31 @@ def recall_at_k(I, gt, k):
     for a, b in zip(I, gt):
         hit += len(set(a.tolist()) & set(b.tolist()))
     return hit / float(gt.shape[0] * k)
+
+
+def assert_probe_parity(P, D, Pr, Dr, dist_of=None, label=""):
+    """Probe rows of the coarse quantizer: same distances bit for bit; the
+    ids of each run of equal distances agree as sets, except the run at the
+    last position, whose ids must each lie at that distance."""
+    assert_topk_parity(D, P, Dr, Pr, dist_of, label)
+
+
+def write_index_file(path, cent, lists=()):
+    """Index file in the reference's format (src/Index.cpp:1708-1770,
+    src/IVF.cpp:76-134): header, centroids, then per non-empty list its id,
+    size, d, sub_k, opt, ids, codes and norms.  lists: (list_id, ids, codes)."""
+    import struct
+    cent = np.ascontiguousarray(cent, np.float32)
+    nlist, d = cent.shape
+    with open(path, "wb") as f:
+        f.write(struct.pack("<QQiiQQQ", d, nlist, 1, 0, 0, 1, 1))
+        f.write(cent.tobytes())
+        for l, ids, codes in lists:
+            ids = np.ascontiguousarray(ids, np.int64)
+            codes = np.ascontiguousarray(codes, np.float32).reshape(len(ids), d)
+            if len(ids) == 0:
+                continue
+            f.write(struct.pack("<QQQQi", l, len(ids), d, 0, 0))
+            f.write(ids.astype(np.uint64).tobytes())
+            f.write(codes.tobytes())
+            f.write(np.einsum("ij,ij->i", codes, codes).astype(np.float32).tobytes())

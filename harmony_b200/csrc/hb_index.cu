@@ -361,7 +361,15 @@ class IndexCore {
     make_bf16_tensor_map(tmap_, codes_bf16_.p, ntotal_, kpad_);
     maxnorm_.reserve(1);
     launch_max_norm(norms_.p, ntotal_, maxnorm_.p, st_);
-    launches_ += 2;
+    // Norms in 128-row tiles per list (+inf past each list's end), copied
+    // next to each accumulator by the scan.
+    std::vector<int64_t> toff(nlist_ + 1, 0);
+    for (size_t l = 0; l < nlist_; ++l) toff[l + 1] = toff[l] + (host_off_[l + 1] - host_off_[l] + 127) / 128;
+    tile_off_.reserve(nlist_ + 1);
+    HB_CUDA(cudaMemcpyAsync(tile_off_.p, toff.data(), toff.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st_));
+    tile_norm_.reserve(std::max<size_t>(static_cast<size_t>(toff[nlist_]) * 128, 1));
+    launch_tile_norms(norms_.p, list_off_.p, static_cast<int>(nlist_), tile_off_.p, tile_norm_.p, st_);
+    launches_ += 3;
     HB_CUDA(cudaStreamSynchronize(st_));
     bf16_ready_ = true;
   }
@@ -1018,7 +1026,9 @@ class IndexCore {
     a.kpad = kpad_;
     a.dpad = static_cast<int>(dpad_);
     a.q = qpad_.p;
-    a.xnorm = norms_.p;
+    a.tile_norm = tile_norm_.p;
+    a.tile_off = tile_off_.p;
+    a.stages = scan_bf16_stages(kpad_, R);
     a.list_cnt = list_cnt_.p;
     a.list_qoff = list_qoff_.p;
     a.list_q = list_q_.p;
@@ -1375,7 +1385,8 @@ class IndexCore {
   DevBuf<int> cflags_, cerr_dev_;
   DevBuf<uint16_t> codes_bf16_;
   DevBuf<uint64_t> tau_, part2_;
-  DevBuf<float> maxnorm_;
+  DevBuf<float> maxnorm_, tile_norm_;
+  DevBuf<int64_t> tile_off_;
   DevBuf<int64_t> slot_base2_;
   DevBuf<int32_t> probes1_, probes2_;
   DevBuf<int> err_dev_;

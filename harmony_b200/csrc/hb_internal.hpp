@@ -161,7 +161,8 @@ struct TcArgs {
   int kpad;                    // BF16 row length (d rounded up to 64)
   int dpad;                    // FP32 row length of queries / codes
   const float* q;              // nq x dpad FP32 queries
-  const float* xnorm;          // ||x||^2 per vector (list order)
+  const float* tile_norm;      // ||x||^2 per 128-row tile of each list, +inf past the list's end
+  const int64_t* tile_off;     // first tile of each list in tile_norm (nlist + 1)
   const int32_t* list_cnt;
   const int64_t* list_qoff;
   const int32_t* list_q;
@@ -174,8 +175,14 @@ struct TcArgs {
   uint64_t* part;              // slots x R keys
   uint64_t* tau;               // per query: best known R-th key (all ones = none yet)
   int* err;                    // non-zero after a bounded wait gave up
+  int stages;                  // B tile ring depth (scan_bf16_stages)
 };
-size_t scan_bf16_smem_bytes(int kpad, int R);
+size_t scan_bf16_smem_bytes(int kpad, int R, int stages);
+int scan_bf16_stages(int kpad, int R);  // deepest ring that fits beside R candidates
+// Per-tile norm array: tile_off (nlist + 1, prefix of ceil(n_l / 128)) and
+// tile_norm (tiles x 128 floats, +inf past each list's end).
+void launch_tile_norms(const float* norms, const int64_t* list_off, int nlist, const int64_t* tile_off,
+                       float* tile_norm, cudaStream_t st);
 int scan_bf16_keys_per_slot(int R);  // keys each (query, chunk) slot holds
 int scan_bf16_max_R(int kpad);       // largest candidate count per query the scan holds
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);

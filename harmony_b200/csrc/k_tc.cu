@@ -3,23 +3,33 @@
 // Work items are the list-major items of the exact scan (list, chunk of
 // rows, group of <= 128 queries probing the list).  Per item the CTA holds
 // the group's queries as the MMA's A operand (128 x K, BF16, K-major,
-// 128-byte swizzle, written by the epilogue warps) and streams the chunk's
-// rows as B operand tiles of 128 rows (TMA 2-D loads with the same swizzle
-// into a 3-stage ring).  One thread issues tcgen05.mma (M 128 queries x
-// N 128 rows x K 16) into one of two TMEM accumulators; four epilogue warps
-// read their TMEM lanes back (thread = query, 128 columns = rows), form
-// ||x||^2 - 2 q.x (the query's ||q||^2 does not change its ranking) and keep
-// the R smallest per query in a thread-private max-heap in shared memory.
-// The R best keys (approximate distance, row position) of every (query,
-// chunk) go to a slot; rerank_kernel takes each query's R best over its
-// slots, recomputes their distances exactly in FP32 with the reference's
-// sequential unfused loop and returns the k best -- so whenever the true
-// k nearest are among the R candidates the result equals the exact scan's.
+// 128-byte swizzle) and streams the chunk's rows as B operand tiles of 128
+// rows (TMA 2-D loads with the same swizzle into a ring of stages).  One
+// thread issues tcgen05.mma (M 128 queries x N 128 rows x K 16) into one of
+// four TMEM accumulators; the epilogue warps read their TMEM lanes back
+// (thread = query, 128 columns = rows), form ||x||^2 - 2 q.x (the query's
+// ||q||^2 does not change its ranking) and keep the R smallest per query in
+// a thread-private max-heap in shared memory.  The R best keys (approximate
+// distance, row position) of every (query, chunk) go to a slot;
+// rerank_kernel takes each query's R best over its slots, recomputes their
+// distances exactly in FP32 with the reference's sequential unfused loop and
+// returns the k best -- so whenever the true k nearest are among the R
+// candidates the result equals the exact scan's.
 //
-// Warp roles (192 threads): warps 0-3 epilogue (TMEM lanes 0-127), warp 4
-// TMA producer, warp 5 MMA issuer.  Every mbarrier wait is bounded; on a
-// timeout the kernel records an error, skips the rest of the work while
-// keeping every CTA barrier, drains its copies in flight and frees TMEM.
+// Warp roles (384 threads), all running ahead of each other through
+// mbarriers, with no CTA-wide barrier between items:
+//   warps 0-7   two epilogue groups (TMEM lane quarters); tile t of the
+//               CTA's global tile sequence goes to group t % 2, which keeps
+//               its own heaps per item;
+//   warp 8      TMA producer of the B tiles;
+//   warp 9      MMA issuer; it also copies each tile's 128 row norms
+//               (a padded per-tile norm array) next to the accumulator;
+//   warps 10-11 item builders: fetch the next item from the global work
+//               counter, gather its query ids and seed bounds and write its
+//               A tile into the second A buffer while the current item runs.
+// Every mbarrier wait is bounded; on a timeout the kernel records an error,
+// the roles stop taking work, copies and MMAs in flight are drained and
+// TMEM is freed.
 #include <cudaTypedefs.h>
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -38,10 +48,13 @@ using namespace sm100;
 
 constexpr int kGroups = 2;                         // epilogue warpgroups, alternate tiles
 constexpr int kEpiThreads = 128;                   // threads per epilogue group (= queries per item)
-constexpr int kTcThreads = kGroups * kEpiThreads + 64;  // + TMA warp + MMA warp
+constexpr int kBuildWarps = 2;
+constexpr int kProdWarp = kGroups * 4, kMmaWarp = kGroups * 4 + 1, kBuildWarp0 = kGroups * 4 + 2;
+constexpr int kTcThreads = (kBuildWarp0 + kBuildWarps) * 32;
 constexpr int kTile = 128;     // rows per B tile, queries per item (M)
-constexpr int kStages = 3;
+constexpr int kMaxStages = 4;
 constexpr int kAcc = 2 * kGroups;                  // TMEM accumulators of 128 columns
+constexpr size_t kSmemCap = 225 * 1024;            // dynamic shared memory budget
 
 // Monotone map of a float to uint32 (all signs), and its inverse.
 __device__ __forceinline__ uint32_t ordered_bits(float f) {
@@ -52,16 +65,23 @@ __device__ __forceinline__ float ordered_to_float(uint32_t u) {
   return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
 }
 
+struct ItemDesc {
+  int list, chunk, group, qcnt, ntiles;  // ntiles < 0: no more work
+  int row0;                              // first row (vector position) of the chunk
+  long long tile0;                       // index of the chunk's first tile in the per-tile norm array
+};
+
 struct TcShared {
-  uint64_t full[kStages];
-  uint64_t empty[kStages];
+  uint64_t full[kMaxStages];
+  uint64_t empty[kMaxStages];
   uint64_t accf[kAcc];
   uint64_t acce[kAcc];
+  uint64_t normf[kAcc];
+  uint64_t itemf[2];
+  uint64_t aempty[2];
+  uint64_t drain;
   uint32_t tmem;
-  int done;
-  int list, chunk, group, qcnt, nrow;
-  long long row0;
-  int mma_consumed;
+  ItemDesc desc[2];
 };
 
 // Thread-private max-heap of R keys stored with stride kEpiThreads.  Kept
@@ -89,35 +109,73 @@ __device__ __noinline__ void heap_replace_top(uint64_t* h, int R, uint64_t key) 
   h[i * kEpiThreads] = key;
 }
 
+// Next work item from the global counter (one thread).
+__device__ ItemDesc fetch_item(const TcArgs& a, int64_t total_items) {
+  ItemDesc d;
+  d.ntiles = -1;
+  if (*reinterpret_cast<volatile int*>(a.err) != 0) return d;
+  const int64_t item = static_cast<int64_t>(atomicAdd(a.work_counter, 1u));
+  if (item >= total_items) return d;
+  int lo = 0, hi = a.nlist;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a.item_off[mid] <= item) lo = mid; else hi = mid;
+  }
+  const int l = lo;
+  const int64_t local = item - a.item_off[l];
+  const int ng = (a.list_cnt[l] + kTile - 1) / kTile;
+  d.list = l;
+  d.chunk = static_cast<int>(local / ng);
+  d.group = static_cast<int>(local % ng);
+  d.qcnt = min(kTile, a.list_cnt[l] - d.group * kTile);
+  const int64_t lb = a.list_off[l];
+  const int64_t r0 = lb + static_cast<int64_t>(d.chunk) * a.chunk_rows;
+  const int64_t r1 = min(a.list_off[l + 1], r0 + static_cast<int64_t>(a.chunk_rows));
+  d.row0 = static_cast<int>(r0);
+  d.ntiles = static_cast<int>((r1 - r0 + kTile - 1) / kTile);
+  d.tile0 = a.tile_off[l] + static_cast<int64_t>(d.chunk) * (a.chunk_rows / kTile);
+  return d;
+}
+
 __global__ void __launch_bounds__(kTcThreads, 1)
     scan_bf16_kernel(const __grid_constant__ CUtensorMap tmap, TcArgs a) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ TcShared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int kpad = a.kpad;
+  const int S = a.stages;
   const uint32_t kblk_bytes = kTile * 128;                 // one 64-element K block of 128 rows
   const uint32_t tile_bytes = static_cast<uint32_t>(kpad / 64) * kblk_bytes;
-  uint8_t* A = smem;
-  uint8_t* stages = smem + tile_bytes;
-  uint64_t* heap = reinterpret_cast<uint64_t*>(stages + kStages * tile_bytes);  // [kGroups][R][128]
-  float* nrm = reinterpret_cast<float*>(heap + static_cast<size_t>(kGroups) * a.R * kEpiThreads);  // [kGroups][2][128]
+  uint8_t* Abuf = smem;                                    // [2] A tiles
+  uint8_t* stages = smem + 2 * tile_bytes;                 // [S] B tiles
+  uint64_t* heap = reinterpret_cast<uint64_t*>(stages + static_cast<size_t>(S) * tile_bytes);  // [kGroups][R][128]
+  float* nrm = reinterpret_cast<float*>(heap + static_cast<size_t>(kGroups) * a.R * kEpiThreads);  // [kAcc][128]
+  int* meta_q = reinterpret_cast<int*>(nrm + kAcc * kTile);                 // [2][128]
+  int* meta_j = meta_q + 2 * kTile;                                          // [2][128]
+  uint64_t* meta_tau = reinterpret_cast<uint64_t*>(meta_j + 2 * kTile);      // [2][128]
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   int* err = a.err;
 
-  const int kProdWarp = kGroups * 4, kMmaWarp = kGroups * 4 + 1;
   if (warp == kMmaWarp) tmem_alloc(&sh.tmem, 512);
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < kMaxStages; ++s) {
       mbar_init(&sh.full[s], 1);
       mbar_init(&sh.empty[s], 1);
     }
     for (int b = 0; b < kAcc; ++b) {
       mbar_init(&sh.accf[b], 1);
       mbar_init(&sh.acce[b], kEpiThreads);
+      mbar_init(&sh.normf[b], 1);
     }
-    sh.mma_consumed = 0;
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&sh.itemf[i], kBuildWarps * 32);
+      // A buffer / item slot free: the MMA warp's commit, the producer and
+      // every epilogue thread.
+      mbar_init(&sh.aempty[i], 2 + kGroups * kEpiThreads);
+    }
+    mbar_init(&sh.drain, 1);
     fence_barrier_init();
   }
   if (warp == kProdWarp && lane == 0) prefetch_tmap(&tmap);
@@ -125,114 +183,124 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sh.tmem;
-  const uint32_t idesc = idesc_bf16_f32(kTile, kTile);
-  const int nk = kpad / 16;
   const int64_t total_items = a.item_off[a.nlist];
 
-  // Pipeline counters (identical tile sequences in every role).  Tile t of
-  // an item goes to epilogue group t % kGroups, accumulator
-  // 2 * group + (that group's tile count & 1).
-  uint32_t p_idx = 0, m_idx = 0;
-  uint32_t m_cnt[kGroups] = {};   // MMA: tiles issued per group
-  uint32_t e_cnt = 0;             // epilogue: tiles processed by this thread's group
-  const int grp = warp < kGroups * 4 ? warp / 4 : 0;
-  const int etid = tid - grp * kEpiThreads;  // 0..127 inside the group
-
-  for (;;) {
-    if (tid == 0) {
-      sh.done = 1;
-      if (*reinterpret_cast<volatile int*>(err) == 0) {
-        const int64_t item = static_cast<int64_t>(atomicAdd(a.work_counter, 1u));
-        if (item < total_items) {
-          int lo = 0, hi = a.nlist;
-          while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (a.item_off[mid] <= item) lo = mid; else hi = mid;
+  if (warp >= kBuildWarp0) {
+    // ---- item builders ---------------------------------------------------
+    const int bt = tid - kBuildWarp0 * 32;
+    ItemDesc nd;
+    nd.ntiles = -1;
+    if (bt == 0) nd = fetch_item(a, total_items);
+    for (uint32_t it = 0;; ++it) {
+      const int ab = static_cast<int>(it & 1u);
+      bool okw = true;
+      if (bt == 0) {
+        okw = mbar_wait(&sh.aempty[ab], ((it >> 1) & 1u) ^ 1u, err, 31);
+        if (!okw) nd.ntiles = -1;
+        sh.desc[ab] = nd;
+      }
+      asm volatile("bar.sync 3, %0;\n" ::"n"(kBuildWarps * 32) : "memory");
+      const ItemDesc d = sh.desc[ab];
+      if (d.ntiles >= 0) {
+        const int64_t qbase = a.list_qoff[d.list] + static_cast<int64_t>(d.group) * kTile;
+        uint8_t* A = Abuf + ab * tile_bytes;
+        for (int r = bt; r < kTile; r += kBuildWarps * 32) {
+          int q = -1, j = 0;
+          uint64_t tau = kEmpty;
+          if (r < d.qcnt) {
+            const uint32_t packed = static_cast<uint32_t>(a.list_q[qbase + r]);
+            q = static_cast<int>(packed >> 16);
+            j = static_cast<int>(packed & 0xffffu);
+            // Best known R-th key of this query over the items finished so
+            // far: an upper bound of its overall R-th key.
+            tau = *reinterpret_cast<volatile unsigned long long*>(a.tau + q);
           }
-          const int l = lo;
-          const int64_t local = item - a.item_off[l];
-          const int ng = (a.list_cnt[l] + kTile - 1) / kTile;
-          sh.list = l;
-          sh.chunk = static_cast<int>(local / ng);
-          sh.group = static_cast<int>(local % ng);
-          sh.qcnt = min(kTile, a.list_cnt[l] - sh.group * kTile);
-          sh.row0 = a.list_off[l] + static_cast<int64_t>(sh.chunk) * a.chunk_rows;
-          sh.nrow = static_cast<int>(min(static_cast<long long>(a.list_off[l + 1]), sh.row0 + static_cast<long long>(a.chunk_rows)) - sh.row0);
-          sh.done = 0;
+          meta_q[ab * kTile + r] = q;
+          meta_j[ab * kTile + r] = j;
+          meta_tau[ab * kTile + r] = tau;
+          const float* qrow = a.q + static_cast<size_t>(q < 0 ? 0 : q) * a.dpad;
+#pragma unroll 4
+          for (int k = 0; k < kpad; k += 8) {
+            float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+            if (q >= 0 && k < a.dpad) {  // dpad is a multiple of 16: a row's 8 values are all in or all out
+              lo = *reinterpret_cast<const float4*>(qrow + k);
+              hi = *reinterpret_cast<const float4*>(qrow + k + 4);
+            }
+            __nv_bfloat162 p0 = __floats2bfloat162_rn(lo.x, lo.y), p1 = __floats2bfloat162_rn(lo.z, lo.w);
+            __nv_bfloat162 p2 = __floats2bfloat162_rn(hi.x, hi.y), p3 = __floats2bfloat162_rn(hi.z, hi.w);
+            *reinterpret_cast<uint4*>(A + sw128_offset_bf16(r, k, kblk_bytes)) =
+                make_uint4(*reinterpret_cast<uint32_t*>(&p0), *reinterpret_cast<uint32_t*>(&p1),
+                           *reinterpret_cast<uint32_t*>(&p2), *reinterpret_cast<uint32_t*>(&p3));
+          }
         }
+        fence_proxy_async_smem();
       }
+      mbar_arrive(&sh.itemf[ab]);
+      if (d.ntiles < 0) break;
+      if (bt == 0) nd = fetch_item(a, total_items);
     }
-    __syncthreads();
-    if (sh.done) break;
-    const int qcnt = sh.qcnt;
-    const int nrow = sh.nrow;
-    const long long row0 = sh.row0;
-    const int ntiles = (nrow + kTile - 1) / kTile;
-
-    // ---- item set-up: A tile (queries, BF16, swizzled) and heaps ----------
-    int my_q = -1, my_j = 0;
-    uint64_t my_tau = kEmpty;
-    if (warp < kGroups * 4) {
-      if (etid < qcnt) {
-        const int packed = a.list_q[a.list_qoff[sh.list] + static_cast<int64_t>(sh.group) * kTile + etid];
-        my_q = static_cast<int>(static_cast<unsigned>(packed) >> 16);
-        my_j = packed & 0xffff;
-        // Best known R-th key of this query over the items finished so far:
-        // an upper bound of its overall R-th key, so the heap starts full of
-        // it and only keys below can enter.
-        my_tau = *reinterpret_cast<volatile unsigned long long*>(a.tau + my_q);
-      }
-      const float* qrow = a.q + static_cast<size_t>(my_q < 0 ? 0 : my_q) * a.dpad;
-      // The group's threads split the K range of their query row.
-#pragma unroll 2
-      for (int k = grp * 8; k < kpad; k += 8 * kGroups) {
-        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
-        if (my_q >= 0 && k < a.dpad) {  // dpad is a multiple of 16: a row's 8 values are all in or all out
-          lo = *reinterpret_cast<const float4*>(qrow + k);
-          hi = *reinterpret_cast<const float4*>(qrow + k + 4);
-        }
-        __nv_bfloat162 p0 = __floats2bfloat162_rn(lo.x, lo.y), p1 = __floats2bfloat162_rn(lo.z, lo.w);
-        __nv_bfloat162 p2 = __floats2bfloat162_rn(hi.x, hi.y), p3 = __floats2bfloat162_rn(hi.z, hi.w);
-        *reinterpret_cast<uint4*>(A + sw128_offset_bf16(etid, k, kblk_bytes)) =
-            make_uint4(*reinterpret_cast<uint32_t*>(&p0), *reinterpret_cast<uint32_t*>(&p1),
-                       *reinterpret_cast<uint32_t*>(&p2), *reinterpret_cast<uint32_t*>(&p3));
-      }
-      uint64_t* hg = heap + static_cast<size_t>(grp) * a.R * kEpiThreads;
-      for (int e = 0; e < a.R; ++e) hg[e * kEpiThreads + etid] = my_tau;
-      fence_proxy_async_smem();
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-
-    if (warp == kProdWarp) {
-      // ---- TMA producer ----------------------------------------------------
-      if (lane == 0) {
-        for (int t = 0; t < ntiles; ++t, ++p_idx) {
-          const int s = p_idx % kStages;
-          const uint32_t par = ((p_idx / kStages) & 1u) ^ 1u;
-          if (!mbar_wait(&sh.empty[s], par, err, 11)) break;
+  } else if (warp == kProdWarp) {
+    // ---- TMA producer ------------------------------------------------------
+    uint32_t p_idx = 0;
+    if (lane == 0) {
+      for (uint32_t it = 0;; ++it) {
+        const int ab = static_cast<int>(it & 1u);
+        if (!mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 32)) break;
+        const ItemDesc d = sh.desc[ab];
+        mbar_arrive(&sh.aempty[ab]);
+        if (d.ntiles < 0) break;
+        bool ok = true;
+        for (int t = 0; t < d.ntiles; ++t, ++p_idx) {
+          const int s = static_cast<int>(p_idx % static_cast<uint32_t>(S));
+          const uint32_t par = ((p_idx / static_cast<uint32_t>(S)) & 1u) ^ 1u;
+          if (!mbar_wait(&sh.empty[s], par, err, 11)) {
+            ok = false;
+            break;
+          }
           uint8_t* dst = stages + s * tile_bytes;
           mbar_arrive_expect_tx(&sh.full[s], tile_bytes);
-          const int r = static_cast<int>(row0) + t * kTile;
+          const int r = d.row0 + t * kTile;
           for (int kb = 0; kb < kpad / 64; ++kb) tma_load_2d(dst + kb * kblk_bytes, &tmap, kb * 64, r, &sh.full[s]);
         }
+        if (!ok) break;
       }
-      __syncwarp();
-      p_idx = __shfl_sync(0xffffffffu, p_idx, 0);
-    } else if (warp == kMmaWarp) {
-      // ---- MMA issuer -------------------------------------------------------
-      if (lane == 0) {
-        for (int t = 0; t < ntiles; ++t, ++m_idx) {
-          const int s = m_idx % kStages;
-          if (!mbar_wait(&sh.full[s], (m_idx / kStages) & 1u, err, 12)) break;
-          const int g = t % kGroups;
+      // Drain: the last S loads may still be landing.
+      const uint32_t first = p_idx > static_cast<uint32_t>(S) ? p_idx - static_cast<uint32_t>(S) : 0u;
+      for (uint32_t i = first; i < p_idx; ++i)
+        mbar_wait(&sh.full[i % static_cast<uint32_t>(S)], (i / static_cast<uint32_t>(S)) & 1u, nullptr, 0,
+                  200000000LL);
+    }
+  } else if (warp == kMmaWarp) {
+    // ---- MMA issuer (+ per-tile norms) --------------------------------------
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(kTile, kTile);
+      const int nk = kpad / 16;
+      uint32_t m_idx = 0, m_cnt[kGroups] = {}, G = 0;
+      for (uint32_t it = 0;; ++it) {
+        const int ab = static_cast<int>(it & 1u);
+        if (!mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 33)) break;
+        const ItemDesc d = sh.desc[ab];
+        if (d.ntiles < 0) break;
+        tc_fence_after();
+        const uint32_t a_base = smem_u32(Abuf + ab * tile_bytes);
+        bool ok = true;
+        for (int t = 0; t < d.ntiles; ++t, ++m_idx) {
+          const int s = static_cast<int>(m_idx % static_cast<uint32_t>(S));
+          if (!mbar_wait(&sh.full[s], (m_idx / static_cast<uint32_t>(S)) & 1u, err, 12)) {
+            ok = false;
+            break;
+          }
+          const int g = static_cast<int>((G + static_cast<uint32_t>(t)) & 1u);
           const uint32_t c = m_cnt[g];
           const int b = 2 * g + static_cast<int>(c & 1u);
-          if (!mbar_wait(&sh.acce[b], ((c >> 1) & 1u) ^ 1u, err, 13)) break;
+          if (!mbar_wait(&sh.acce[b], ((c >> 1) & 1u) ^ 1u, err, 13)) {
+            ok = false;
+            break;
+          }
           ++m_cnt[g];
           tc_fence_after();
-          const uint32_t a_base = smem_u32(A);
+          mbar_arrive_expect_tx(&sh.normf[b], kTile * 4);
+          bulk_load(nrm + b * kTile, a.tile_norm + (d.tile0 + t) * kTile, kTile * 4, &sh.normf[b]);
           const uint32_t b_base = smem_u32(stages + s * tile_bytes);
           for (int k = 0; k < nk; ++k) {
             const uint32_t off = static_cast<uint32_t>(k >> 2) * kblk_bytes + static_cast<uint32_t>(k & 3) * 32u;
@@ -241,37 +309,46 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           }
           mma_commit(&sh.empty[s]);
           mma_commit(&sh.accf[b]);
-          sh.mma_consumed = static_cast<int>(m_idx + 1);
         }
+        // A buffer ab is free once these MMAs have completed.
+        mma_commit(&sh.aempty[ab]);
+        if (!ok) break;
+        G += static_cast<uint32_t>(d.ntiles);
       }
-      __syncwarp();
-      m_idx = __shfl_sync(0xffffffffu, m_idx, 0);
-      for (int g = 0; g < kGroups; ++g) m_cnt[g] = __shfl_sync(0xffffffffu, m_cnt[g], 0);
-    } else {
-      // ---- epilogue: thread = query (TMEM lane etid); group grp takes the
-      // item's tiles grp, grp + kGroups, ...
-      uint64_t* hp = heap + static_cast<size_t>(grp) * a.R * kEpiThreads + etid;
+      // Drain: every MMA done before TMEM is released.
+      mma_commit(&sh.drain);
+      mbar_wait(&sh.drain, 0, nullptr, 0, 200000000LL);
+    }
+  } else {
+    // ---- epilogue: thread = query (TMEM lane etid) ---------------------------
+    const int grp = warp >> 2;
+    const int etid = tid - grp * kEpiThreads;
+    uint64_t* hp = heap + static_cast<size_t>(grp) * a.R * kEpiThreads + etid;
+    const uint32_t lane_base = (32u * static_cast<uint32_t>(warp & 3)) << 16;
+    uint32_t e_cnt = 0, G = 0;
+    for (uint32_t it = 0;; ++it) {
+      const int ab = static_cast<int>(it & 1u);
+      bool ok = mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 34);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      const ItemDesc d = sh.desc[ab];
+      const int my_q = meta_q[ab * kTile + etid];
+      const int my_j = meta_j[ab * kTile + etid];
+      const uint64_t my_tau = meta_tau[ab * kTile + etid];
+      mbar_arrive(&sh.aempty[ab]);
+      if (d.ntiles < 0) break;
+      // The heap starts full of the query's bound: only keys below enter.
+      for (int e = 0; e < a.R; ++e) hp[e * kEpiThreads] = my_tau;
       uint64_t top = my_tau;
-      float thr_f = top == kEmpty ? INFINITY : ordered_to_float(static_cast<uint32_t>(top >> 32));
-      const uint32_t lane_base = (32u * static_cast<uint32_t>(warp & 3)) << 16;
-      bool ok = true;
-      float nr_next = 0.f;
-      {
-        const int rn = grp * kTile + etid;
-        if (grp < ntiles && rn < nrow) nr_next = a.xnorm[row0 + rn];
-      }
-      for (int t = grp; t < ntiles; t += kGroups, ++e_cnt) {
+      // An all-ones top (no bound yet) admits every finite value.
+      float thr_f = top == kEmpty ? FLT_MAX : ordered_to_float(static_cast<uint32_t>(top >> 32));
+      for (int t = static_cast<int>((static_cast<uint32_t>(grp) ^ G) & 1u); t < d.ntiles; t += kGroups, ++e_cnt) {
         const int b = 2 * grp + static_cast<int>(e_cnt & 1u);
-        float* nb = nrm + (grp * 2 + static_cast<int>(e_cnt & 1u)) * kTile;
-        nb[etid] = nr_next;
-        const int rn = (t + kGroups) * kTile + etid;
-        nr_next = (t + kGroups < ntiles && rn < nrow) ? a.xnorm[row0 + rn] : 0.f;
-        if (grp == 0) asm volatile("bar.sync 1, 128;\n" ::: "memory");
-        else asm volatile("bar.sync 2, 128;\n" ::: "memory");
-        if (ok) ok = mbar_wait(&sh.accf[b], (e_cnt >> 1) & 1u, err, 14);
+        const uint32_t par = (e_cnt >> 1) & 1u;
+        ok = ok && mbar_wait(&sh.accf[b], par, err, 14) && mbar_wait(&sh.normf[b], par, err, 15);
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
-        const int rows_here = min(kTile, nrow - t * kTile);
+        const float* nb = nrm + b * kTile;
+        const uint32_t pos_t = static_cast<uint32_t>(d.row0 + t * kTile);
 #pragma unroll 1
         for (int c = 0; c < kTile / 32; ++c) {
           uint32_t r[32];
@@ -280,10 +357,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tmem_ld_wait();
           }
           if (ok && my_q >= 0) {
-            // v = ||x||^2 - 2 q.x as an order-preserving uint32, then the
-            // mask of columns at or under the heap's top; inserts walk the mask.
+            // v = ||x||^2 - 2 q.x (rows past the list carry an infinite
+            // norm); the columns' minimum against the bound decides whether
+            // any of them needs a look.
             const float4* n4 = reinterpret_cast<const float4*>(nb + c * 32);
-            uint32_t mask = 0;
+            float mn = INFINITY;
 #pragma unroll
             for (int j4 = 0; j4 < 8; ++j4) {
               const float4 nv = n4[j4];
@@ -295,27 +373,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               r[4 * j4 + 1] = __float_as_uint(v1);
               r[4 * j4 + 2] = __float_as_uint(v2);
               r[4 * j4 + 3] = __float_as_uint(v3);
-              mask |= (v0 <= thr_f ? 1u : 0u) << (4 * j4 + 0);
-              mask |= (v1 <= thr_f ? 1u : 0u) << (4 * j4 + 1);
-              mask |= (v2 <= thr_f ? 1u : 0u) << (4 * j4 + 2);
-              mask |= (v3 <= thr_f ? 1u : 0u) << (4 * j4 + 3);
+              mn = fminf(mn, fminf(fminf(v0, v1), fminf(v2, v3)));
             }
-            const int valid = rows_here - c * 32;
-            if (valid < 32) mask &= valid <= 0 ? 0u : ((1u << valid) - 1u);
-            const uint32_t pos0 = static_cast<uint32_t>(row0 + t * kTile + c * 32);
-            while (mask) {
-              const int j = __ffs(mask) - 1;
-              mask &= mask - 1;
-              uint32_t hv = r[0];
+            if (mn <= thr_f) {
+              uint32_t mask = 0;
 #pragma unroll
-              for (int jj = 1; jj < 32; ++jj) hv = (j == jj) ? r[jj] : hv;
-              const uint64_t key = (static_cast<uint64_t>(ordered_bits(__uint_as_float(hv))) << 32) |
-                                   (pos0 + static_cast<uint32_t>(j));
-              if (key < top) {
-                heap_replace_top(hp, a.R, key);
-                top = hp[0];
-                // An all-ones top (heap not full yet) decodes to NaN: no bound.
-                thr_f = top == kEmpty ? INFINITY : ordered_to_float(static_cast<uint32_t>(top >> 32));
+              for (int j = 0; j < 32; ++j) mask |= (__uint_as_float(r[j]) <= thr_f ? 1u : 0u) << j;
+              const uint32_t pos0 = pos_t + static_cast<uint32_t>(c * 32);
+              while (mask) {
+                const int j = __ffs(mask) - 1;
+                mask &= mask - 1;
+                uint32_t hv = r[0];
+#pragma unroll
+                for (int jj = 1; jj < 32; ++jj) hv = (j == jj) ? r[jj] : hv;
+                const uint64_t key = (static_cast<uint64_t>(ordered_bits(__uint_as_float(hv))) << 32) |
+                                     (pos0 + static_cast<uint32_t>(j));
+                if (key < top) {
+                  heap_replace_top(hp, a.R, key);
+                  top = hp[0];
+                  thr_f = top == kEmpty ? FLT_MAX : ordered_to_float(static_cast<uint32_t>(top >> 32));
+                }
               }
             }
           }
@@ -326,7 +403,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // Partial result of this (query, chunk): the group's R keys; seed
       // entries are not results.
       if (my_q >= 0) {
-        const int64_t slot = a.slot_base[static_cast<int64_t>(my_q) * a.P + my_j] + sh.chunk;
+        const int64_t slot = a.slot_base[static_cast<int64_t>(my_q) * a.P + my_j] + d.chunk;
         uint64_t* out = a.part + (slot * kGroups + grp) * a.R;
         for (int e = 0; e < a.R; ++e) {
           const uint64_t v = hp[e * kEpiThreads];
@@ -335,25 +412,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // A heap holding R real keys bounds the query's R-th key: publish it.
         if (top < my_tau) atomicMin(reinterpret_cast<unsigned long long*>(a.tau + my_q), top);
       }
+      if (!ok) break;
+      G += static_cast<uint32_t>(d.ntiles);
     }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
   }
 
-  // ---- drain: copies and MMAs still in flight after an error --------------
-  if (warp == kProdWarp && lane == 0) {
-    const uint32_t consumed = static_cast<uint32_t>(*reinterpret_cast<volatile int*>(&sh.mma_consumed));
-    for (uint32_t i = consumed; i < p_idx; ++i)
-      mbar_wait(&sh.full[i % kStages], (i / kStages) & 1u, nullptr, 0, 200000000LL);
-  }
-  if (warp == kMmaWarp && lane == 0) {
-    for (int g = 0; g < kGroups; ++g)
-      if (m_cnt[g] > 0) {
-        const uint32_t last = m_cnt[g] - 1;
-        mbar_wait(&sh.accf[2 * g + static_cast<int>(last & 1u)], (last >> 1) & 1u, nullptr, 0, 200000000LL);
-      }
-  }
   tc_fence_before();
   __syncthreads();
   if (warp == kMmaWarp) {
@@ -362,8 +425,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
-// Per query: R best approximate keys over its slots -> exact FP32
-// distances (sequential unfused, as the exact scan) -> k best.
 __global__ void __launch_bounds__(128) rerank_kernel(const uint64_t* __restrict__ part,
                                                      const int64_t* __restrict__ slot_base, int P, int R, int k,
                                                      const float* __restrict__ codes, const float* __restrict__ q,
@@ -547,6 +608,17 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
   }
 }
 
+// One block per list: the list's norms in 128-row tiles, +inf past its end
+// (so rows a tile reads beyond its list can never pass a bound).
+__global__ void tile_norms_kernel(const float* __restrict__ norms, const int64_t* __restrict__ list_off,
+                                  const int64_t* __restrict__ tile_off, float* __restrict__ tile_norm) {
+  const int l = blockIdx.x;
+  const int64_t b = list_off[l], n = list_off[l + 1] - b;
+  float* dst = tile_norm + tile_off[l] * kTile;
+  const int64_t m = (tile_off[l + 1] - tile_off[l]) * kTile;
+  for (int64_t i = threadIdx.x; i < m; i += blockDim.x) dst[i] = i < n ? norms[b + i] : INFINITY;
+}
+
 __global__ void max_norm_kernel(const float* __restrict__ norms, size_t n, float* __restrict__ out) {
   float m = 0.0f;
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
@@ -583,17 +655,23 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 }  // namespace
 
-size_t scan_bf16_smem_bytes(int kpad, int R) {
+size_t scan_bf16_smem_bytes(int kpad, int R, int stages) {
   const size_t tile = static_cast<size_t>(kpad / 64) * kTile * 128;
-  return 1024 + tile * (1 + kStages) + static_cast<size_t>(kGroups) * R * kEpiThreads * 8 +
-         static_cast<size_t>(kGroups) * 2 * kTile * 4;
+  return 1024 + tile * (2 + stages) + static_cast<size_t>(kGroups) * R * kEpiThreads * 8 +
+         static_cast<size_t>(kAcc) * kTile * 4 + 2 * kTile * (4 + 4 + 8);
 }
 
 int scan_bf16_keys_per_slot(int R) { return kGroups * R; }
 
+int scan_bf16_stages(int kpad, int R) {
+  int s = kMaxStages;
+  while (s > 2 && scan_bf16_smem_bytes(kpad, R, s) > kSmemCap) --s;
+  return s;
+}
+
 int scan_bf16_max_R(int kpad) {
   int R = 64;
-  while (R > 1 && scan_bf16_smem_bytes(kpad, R) > 220 * 1024) --R;
+  while (R > 1 && scan_bf16_smem_bytes(kpad, R, 2) > kSmemCap) --R;
   return R;
 }
 
@@ -620,8 +698,10 @@ void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, c
 void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st) {
   HB_CHECK(a.kpad == 64 || a.kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
   HB_CHECK(a.R >= 1 && a.R <= 64, HB_ERR_INVALID, "rerank candidates per query must be in [1, 64]");
-  const size_t smem = scan_bf16_smem_bytes(a.kpad, a.R);
-  HB_CHECK(smem <= 220 * 1024, HB_ERR_INVALID, "rerank candidates too many for the BF16 scan's shared memory");
+  HB_CHECK(a.chunk_rows % kTile == 0, HB_ERR_INVALID, "BF16 scan chunks must be whole tiles");
+  HB_CHECK(a.stages >= 2 && a.stages <= kMaxStages, HB_ERR_INVALID, "bad stage count");
+  const size_t smem = scan_bf16_smem_bytes(a.kpad, a.R, a.stages);
+  HB_CHECK(smem <= kSmemCap, HB_ERR_INVALID, "rerank candidates too many for the BF16 scan's shared memory");
   HB_CUDA(cudaFuncSetAttribute(scan_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   scan_bf16_kernel<<<num_sms, kTcThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap), a);
   HB_CUDA(cudaGetLastError());
@@ -650,6 +730,13 @@ void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* cod
   HB_CUDA(cudaFuncSetAttribute(tau_seed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   tau_seed_kernel<<<nlist, kSeedWarps * 32, smem, st>>>(q, dpad, kpad, static_cast<const __nv_bfloat16*>(codes_bf16),
                                                         list_off, list_qoff, list_q, xnorm, S, R, maxnorm, tau);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_tile_norms(const float* norms, const int64_t* list_off, int nlist, const int64_t* tile_off,
+                       float* tile_norm, cudaStream_t st) {
+  if (nlist <= 0) return;
+  tile_norms_kernel<<<nlist, 256, 0, st>>>(norms, list_off, tile_off, tile_norm);
   HB_CUDA(cudaGetLastError());
 }
 

@@ -84,11 +84,12 @@ struct TcShared {
   ItemDesc desc[2];
 };
 
-// Thread-private max-heap of R keys stored with stride kEpiThreads.  Kept
-// out of line: the epilogue's unrolled 32-column loop must stay small enough
-// for the instruction cache, and insertions are rare once the heap is warm.
-__device__ __noinline__ void heap_replace_top(uint64_t* h, int R, uint64_t key) {
+// Thread-private max-heap of R keys stored with stride kEpiThreads: the
+// top is replaced by `key` and sifted down; returns the new top (known from
+// the sift, so no reload).
+__device__ __forceinline__ uint64_t heap_replace_top(uint64_t* h, int R, uint64_t key) {
   int i = 0;
+  uint64_t new_top = key;
   for (;;) {
     const int c1 = 2 * i + 1;
     if (c1 >= R) break;
@@ -104,9 +105,11 @@ __device__ __noinline__ void heap_replace_top(uint64_t* h, int R, uint64_t key) 
     }
     if (key >= vc) break;
     h[i * kEpiThreads] = vc;
+    if (i == 0) new_top = vc;
     i = c;
   }
   h[i * kEpiThreads] = key;
+  return new_top;
 }
 
 // Next work item from the global counter (one thread).
@@ -376,21 +379,29 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               mn = fminf(mn, fminf(fminf(v0, v1), fminf(v2, v3)));
             }
             if (mn <= thr_f) {
-              uint32_t mask = 0;
+              uint32_t mq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-              for (int j = 0; j < 32; ++j) mask |= (__uint_as_float(r[j]) <= thr_f ? 1u : 0u) << j;
+              for (int j = 0; j < 32; ++j) mq[j & 3] |= (__uint_as_float(r[j]) <= thr_f ? 1u : 0u) << j;
+              uint32_t mask = (mq[0] | mq[1]) | (mq[2] | mq[3]);
               const uint32_t pos0 = pos_t + static_cast<uint32_t>(c * 32);
               while (mask) {
                 const int j = __ffs(mask) - 1;
                 mask &= mask - 1;
-                uint32_t hv = r[0];
+                // r[j] by a 5-level select tree (no register indexing).
+                uint32_t t16[16], t8[8], t4[4], t2[2];
 #pragma unroll
-                for (int jj = 1; jj < 32; ++jj) hv = (j == jj) ? r[jj] : hv;
+                for (int i = 0; i < 16; ++i) t16[i] = (j & 1) ? r[2 * i + 1] : r[2 * i];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) t8[i] = (j & 2) ? t16[2 * i + 1] : t16[2 * i];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) t4[i] = (j & 4) ? t8[2 * i + 1] : t8[2 * i];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
+                const uint32_t hv = (j & 16) ? t2[1] : t2[0];
                 const uint64_t key = (static_cast<uint64_t>(ordered_bits(__uint_as_float(hv))) << 32) |
                                      (pos0 + static_cast<uint32_t>(j));
                 if (key < top) {
-                  heap_replace_top(hp, a.R, key);
-                  top = hp[0];
+                  top = heap_replace_top(hp, a.R, key);
                   thr_f = top == kEmpty ? FLT_MAX : ordered_to_float(static_cast<uint32_t>(top >> 32));
                 }
               }

@@ -429,6 +429,74 @@ class IndexCore {
 
   int coarse_extra(int P) const { return coarse_margin_ >= 0 ? coarse_margin_ : std::max(16, P / 4); }
 
+  bool coarse_tc_route(int P) const {
+    const int Pm = std::min<int>(static_cast<int>(nlist_), P + coarse_extra(P));
+    return coarse_kind_ != HB_COARSE_EXACT && d_ <= 128 && Pm <= kCoarseMaxPm;
+  }
+
+  // Learned probe on the tensor-core route: the exact nearest C centroids
+  // (the predictor's features) from one narrow pass, the predictor's
+  // per-query nprobe, then a second pass over the same approximate distance
+  // matrix that widens only the rows whose nprobe exceeds C (each to its own
+  // width plus margin).  probes_out (nq x P, -1 past each row's nprobe) is the
+  // exact quantizer's rows cut at the predicted nprobe, as the wide route
+  // gives.
+  void coarse_learned(const float* qpad, int nq, int P, int32_t* probes_out, float thr, int cap) {
+    const ProbeModel& m = probe_;
+    const int C = std::min<int>(m.C, P);
+    dmat_.reserve(static_cast<size_t>(nq) * nlist_);
+    ensure_coarse_tc();
+    const int nl = static_cast<int>(nlist_);
+    const int PmA = std::min(nl, C + coarse_extra(C));
+    const int PmB = std::min(nl, P + coarse_extra(P));
+    ccand_.reserve(static_cast<size_t>(nq) * PmB);
+    cval_.reserve(static_cast<size_t>(nq) * PmB);
+    cflags_.reserve(static_cast<size_t>(nq));
+    probes1_.reserve(static_cast<size_t>(nq) * C);
+    cdist_.reserve(static_cast<size_t>(nq) * C);
+    npq_.reserve(static_cast<size_t>(nq));
+    kq_.reserve(static_cast<size_t>(nq));
+    {
+      Scope sc(this, "coarse_tc");
+      launch_coarse_tc(ctmap_, qpad, nq, static_cast<int>(dpad_), ckpad_, cnorm_.p, nl, dmat_.p, cerr_dev_.p, num_sms_,
+                       st_);
+    }
+    {
+      Scope sc(this, "coarse_select");
+      launch_select_rows(dmat_.p, nq, nl, nl, PmA, ccand_.p, cval_.p, st_);
+    }
+    {
+      Scope sc(this, "coarse_refine");
+      launch_coarse_refine(qpad, nq, static_cast<int>(dpad_), cent_.p, ccand_.p, cval_.p, PmA, C, nl, cmaxnorm_.p,
+                           probes1_.p, cdist_.p, cflags_.p, st_);
+      launch_coarse_fallback(qpad, nq, static_cast<int>(dpad_), cent_.p, nl, C, cflags_.p, dmat_.p, probes1_.p,
+                             cdist_.p, st_);
+    }
+    {
+      Scope sc(this, "probe_mlp");
+      probe_infer(nq, qpad, cdist_.p, C, nullptr, thr, cap, npq_.p);
+    }
+    {
+      Scope sc(this, "coarse_widen_select");
+      launch_coarse_widths(npq_.p, nq, P, C, coarse_margin_, nl, kq_.p, st_);
+      launch_select_rows(dmat_.p, nq, nl, nl, PmB, ccand_.p, cval_.p, st_, kq_.p);
+    }
+    {
+      Scope sc(this, "coarse_widen_refine");
+      CoarseRows rows;
+      rows.width = npq_.p;
+      rows.margin = coarse_margin_;
+      rows.pre = probes1_.p;
+      rows.pre_w = C;
+      launch_coarse_refine(qpad, nq, static_cast<int>(dpad_), cent_.p, ccand_.p, cval_.p, PmB, P, nl, cmaxnorm_.p,
+                           probes_out, nullptr, cflags_.p, st_, rows);
+      launch_coarse_fallback(qpad, nq, static_cast<int>(dpad_), cent_.p, nl, P, cflags_.p, dmat_.p, probes_out, nullptr,
+                             st_, npq_.p);
+    }
+    launches_ += 12;
+    coarse_last_nq_ = nq;
+  }
+
   // Split BF16 centroids, their tensor map, ||c||^2 and max ||c||, built once
   // per set of centroids.
   void ensure_coarse_tc() {
@@ -1074,7 +1142,9 @@ class IndexCore {
 
   // Coarse probes of the batch in qpad_, then the per-query cut.
   void coarse_and_cut(int nb, int P) {
-    if (cut_mode_ == 1) {
+    if (cut_mode_ == 1 && coarse_tc_route(P) && probe_.C <= P) {
+      coarse_learned(qpad_.p, nb, P, probes_.p, cut_thr_, cut_cap_);
+    } else if (cut_mode_ == 1) {
       cdist_.reserve(static_cast<size_t>(nb) * P);
       coarse(qpad_.p, nb, P, probes_.p, cdist_.p);
       Scope sc(this, "probe_mlp");
@@ -1383,6 +1453,7 @@ class IndexCore {
   DevBuf<float> cnorm_, cmaxnorm_, cval_;
   DevBuf<int32_t> ccand_;
   DevBuf<int> cflags_, cerr_dev_;
+  DevBuf<int32_t> kq_;
   DevBuf<uint16_t> codes_bf16_;
   DevBuf<uint64_t> tau_, part2_;
   DevBuf<float> maxnorm_, tile_norm_;

@@ -117,7 +117,7 @@ size_t scan_exact_smem_bytes(int d, int dpad, int k, int mode, int* tv, int* qt,
 // Row-wise selection of the k smallest (value, column) pairs of a float
 // matrix; out_idx gets columns, out_val the values, ascending.
 void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx,
-                        float* out_val, cudaStream_t st);
+                        float* out_val, cudaStream_t st, const int32_t* k_row = nullptr);
 // Build the list-major work description from probes (nq x P, -1 = none).
 void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist,
                        int chunk_rows, int qgroup, int32_t* list_cnt, int64_t* list_qoff,
@@ -212,13 +212,27 @@ void make_centroid_split(const float* cent, int nlist, int dpad, int kpad, void*
 // V (nq x nlist) = max(0, ||q||^2 + ||c||^2 - 2 q.c) on the tensor cores.
 void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kpad, const float* cnorm, int nlist,
                       float* V, int* err, int num_sms, cudaStream_t st);
+// Per-row widths of a coarse pass: row r keeps width[r] <= P probes out of
+// width[r] + margin candidates; rows whose width is <= pre_w are copied from
+// an earlier pass of width pre_w (pre, nq x pre_w).  width == nullptr: every
+// row keeps P of Pm.
+struct CoarseRows {
+  const int32_t* width = nullptr;
+  int margin = -1;
+  const int32_t* pre = nullptr;
+  int pre_w = 0;
+};
 // Exact distances of the Pm candidates, top P, exactness flag per query.
 void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, const int32_t* cand, const float* cval,
                           int Pm, int P, int nlist, const float* cmaxnorm, int32_t* probes, float* cdist, int* flags,
-                          cudaStream_t st);
-// Exact row and top P for every flagged query (V rows are overwritten).
+                          cudaStream_t st, CoarseRows rows = CoarseRows());
+// Exact row and top P (or width[r]) for every flagged query (V rows are overwritten).
 void launch_coarse_fallback(const float* q, int nq, int dpad, const float* cent, int nlist, int P, const int* flags,
-                            float* V, int32_t* probes, float* cdist, cudaStream_t st);
+                            float* V, int32_t* probes, float* cdist, cudaStream_t st, const int32_t* width = nullptr);
+// With w = min(width[r], wmax): kq[r] = 0 if w <= pre_w, else
+// min(nlist, w + margin).
+void launch_coarse_widths(const int32_t* width, int nq, int wmax, int pre_w, int margin, int nlist, int32_t* kq,
+                          cudaStream_t st);
 
 // k_mlp.cu: learned probe predictor kernels.
 void mlp_gemm(int M, int N, int K, const float* A, int lda, bool tA, const float* B, int ldb, bool tB, float* C, int ldc,

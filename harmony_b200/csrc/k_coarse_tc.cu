@@ -248,18 +248,35 @@ __global__ void split3_kernel(const float* __restrict__ c, int n, int dpad, int 
 // One warp per query: exact distances of its Pm candidates (lane = candidate,
 // sequential over the dims), sort by (distance, centroid), keep P; flag the
 // query when the exactness bound does not hold.
+__device__ __forceinline__ int coarse_extra_dev(int P, int margin) { return margin >= 0 ? margin : max(16, P / 4); }
+
 __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restrict__ q, int nq, int dpad,
                                                             const float* __restrict__ cent,
                                                             const int32_t* __restrict__ cand, const float* __restrict__ cval,
                                                             int Pm, int P, int nlist, const float* __restrict__ cmaxnorm,
                                                             int32_t* __restrict__ probes, float* __restrict__ cdist,
-                                                            int* __restrict__ flags) {
+                                                            int* __restrict__ flags, CoarseRows rows) {
   extern __shared__ uint64_t s_ref[];  // [warps][pow2(Pm)]
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int qi = blockIdx.x * (blockDim.x >> 5) + wib;
   if (qi >= nq) return;
-  const int n2 = pow2_ceil(Pm < 2 ? 2 : Pm);
-  uint64_t* buf = s_ref + static_cast<size_t>(wib) * n2;
+  // This row's width and candidate count (P and Pm are the row strides).
+  int Pr = P, Pmr = Pm;
+  if (rows.width) {
+    Pr = min(rows.width[qi], P);
+    if (Pr <= 0 || (rows.pre && Pr <= rows.pre_w)) {
+      // Already exact from the narrower pass (or empty): copy and pad.
+      for (int j = lane; j < P; j += 32)
+        probes[static_cast<size_t>(qi) * P + j] =
+            (j < Pr && rows.pre) ? rows.pre[static_cast<size_t>(qi) * rows.pre_w + j] : -1;
+      if (lane == 0) flags[qi] = 0;
+      return;
+    }
+    Pmr = min(nlist, Pr + coarse_extra_dev(Pr, rows.margin));
+  }
+  const int n2 = pow2_ceil(Pmr < 2 ? 2 : Pmr);
+  // Per-warp buffers are laid out for the launch's widest row.
+  uint64_t* buf = s_ref + static_cast<size_t>(wib) * pow2_ceil(Pm < 2 ? 2 : Pm);
   const float* qrow = q + static_cast<size_t>(qi) * dpad;
   float qn = 0.0f;
   for (int c = lane * 4; c < dpad; c += 128) {
@@ -269,11 +286,12 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
   for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(0xffffffffu, qn, o);
   for (int i = lane; i < n2; i += 32) {
     uint64_t key = kEmpty;
-    if (i < Pm) {
+    if (i < Pmr) {
       const int c = cand[static_cast<size_t>(qi) * Pm + i];
       if (c >= 0) {
         const float* x = cent + static_cast<size_t>(c) * dpad;
         float acc = 0.0f;
+#pragma unroll 8
         for (int j = 0; j < dpad; j += 4) {
           const float4 v = *reinterpret_cast<const float4*>(x + j);
           const float4 w = *reinterpret_cast<const float4*>(qrow + j);
@@ -295,17 +313,17 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
   __syncwarp();
   warp_bitonic_sort(buf, n2, lane);
   for (int j = lane; j < P; j += 32) {
-    const uint64_t key = buf[j];
+    const uint64_t key = j < Pr ? buf[j] : kEmpty;
     probes[static_cast<size_t>(qi) * P + j] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
     if (cdist) cdist[static_cast<size_t>(qi) * P + j] = key == kEmpty ? FLT_MAX : key_dist(key);
   }
   if (lane == 0) {
     bool exact = true;
-    if (Pm < nlist) {
-      // Outside the Pm candidates every value is >= vlast, so every exact
+    if (Pmr < nlist) {
+      // Outside the Pmr candidates every value is >= vlast, so every exact
       // distance there is >= vlast - bound.
-      const float vlast = cval[static_cast<size_t>(qi) * Pm + Pm - 1];
-      const uint64_t kp = buf[P - 1];
+      const float vlast = cval[static_cast<size_t>(qi) * Pm + Pmr - 1];
+      const uint64_t kp = buf[Pr - 1];
       exact = kp != kEmpty && vlast < FLT_MAX;
       if (exact) {
         const float mn = *cmaxnorm;
@@ -323,7 +341,8 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
 __global__ void __launch_bounds__(256) coarse_fallback_kernel(const float* __restrict__ q, int nq, int dpad,
                                                               const float* __restrict__ cent, int nlist, int P,
                                                               const int* __restrict__ flags, float* __restrict__ V,
-                                                              int32_t* __restrict__ probes, float* __restrict__ cdist) {
+                                                              int32_t* __restrict__ probes, float* __restrict__ cdist,
+                                                              const int32_t* __restrict__ width) {
   extern __shared__ uint64_t s_fb[];
   __shared__ SelectShared sh_sel;
   const int qi = blockIdx.x;
@@ -344,15 +363,33 @@ __global__ void __launch_bounds__(256) coarse_fallback_kernel(const float* __res
     const float v = row[c];
     return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(c)) : kEmpty;
   };
+  const int Pr = width ? min(width[qi], P) : P;
   block_topk_sorted(key_at, nlist, P, sh_sel, s_fb);
   for (int j = threadIdx.x; j < P; j += blockDim.x) {
-    const uint64_t key = s_fb[j];
+    const uint64_t key = j < Pr ? s_fb[j] : kEmpty;
     probes[static_cast<size_t>(qi) * P + j] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
     if (cdist) cdist[static_cast<size_t>(qi) * P + j] = key == kEmpty ? FLT_MAX : key_dist(key);
   }
 }
 
+// Candidate count of each row of the wider pass: 0 where the narrower pass
+// already holds the row's width, else width + margin (at most nlist).
+__global__ void coarse_widths_kernel(const int32_t* __restrict__ width, int nq, int wmax, int pre_w, int margin,
+                                     int nlist, int32_t* __restrict__ kq) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nq) return;
+  const int w = min(width[r], wmax);
+  kq[r] = w <= pre_w ? 0 : min(nlist, w + coarse_extra_dev(w, margin));
+}
+
 }  // namespace
+
+void launch_coarse_widths(const int32_t* width, int nq, int wmax, int pre_w, int margin, int nlist, int32_t* kq,
+                          cudaStream_t st) {
+  if (nq <= 0) return;
+  coarse_widths_kernel<<<(nq + 255) / 256, 256, 0, st>>>(width, nq, wmax, pre_w, margin, nlist, kq);
+  HB_CUDA(cudaGetLastError());
+}
 
 size_t coarse_tc_smem_bytes(int kpad) {
   return 1024 + static_cast<size_t>(3 * kpad / 64 + kCStages) * kBlk;
@@ -385,7 +422,7 @@ void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kp
 
 void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, const int32_t* cand, const float* cval,
                           int Pm, int P, int nlist, const float* cmaxnorm, int32_t* probes, float* cdist, int* flags,
-                          cudaStream_t st) {
+                          cudaStream_t st, CoarseRows rows) {
   if (nq <= 0) return;
   HB_CHECK(P >= 1 && P <= Pm && Pm <= kCoarseMaxPm, HB_ERR_INVALID, "coarse candidate count out of range");
   const int n2 = pow2_ceil(Pm < 2 ? 2 : Pm);
@@ -393,16 +430,16 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
   const size_t smem = static_cast<size_t>(warps) * n2 * 8;
   HB_CUDA(cudaFuncSetAttribute(coarse_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   coarse_refine_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, st>>>(q, nq, dpad, cent, cand, cval, Pm, P, nlist,
-                                                                          cmaxnorm, probes, cdist, flags);
+                                                                          cmaxnorm, probes, cdist, flags, rows);
   HB_CUDA(cudaGetLastError());
 }
 
 void launch_coarse_fallback(const float* q, int nq, int dpad, const float* cent, int nlist, int P, const int* flags,
-                            float* V, int32_t* probes, float* cdist, cudaStream_t st) {
+                            float* V, int32_t* probes, float* cdist, cudaStream_t st, const int32_t* width) {
   if (nq <= 0) return;
   const size_t smem = static_cast<size_t>(pow2_ceil(P < 2 ? 2 : P)) * 8;
   HB_CUDA(cudaFuncSetAttribute(coarse_fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  coarse_fallback_kernel<<<nq, 256, smem, st>>>(q, nq, dpad, cent, nlist, P, flags, V, probes, cdist);
+  coarse_fallback_kernel<<<nq, 256, smem, st>>>(q, nq, dpad, cent, nlist, P, flags, V, probes, cdist, width);
   HB_CUDA(cudaGetLastError());
 }
 

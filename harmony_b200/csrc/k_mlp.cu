@@ -47,16 +47,22 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(int M, int N, int K,
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads, 4 x 4 outputs each
   float acc[4][4] = {};
   for (int k0 = 0; k0 < K; k0 += kKT) {
+    // Consecutive threads walk each operand's contiguous dimension.
     for (int i = threadIdx.x; i < kKT * kT; i += kGemmThreads) {
-      const int kk = i / kT, mm = i - kk * kT;
-      const int m = m0 + mm, k = k0 + kk;
-      float va = 0.f;
-      if (m < M && k < K) va = tA ? A[static_cast<size_t>(k) * lda + m] : A[static_cast<size_t>(m) * lda + k];
-      sA[kk][mm] = va;
-      const int n = n0 + mm;
-      float vb = 0.f;
-      if (n < N && k < K) vb = tB ? B[static_cast<size_t>(n) * ldb + k] : B[static_cast<size_t>(k) * ldb + n];
-      sB[kk][mm] = vb;
+      {
+        const int kk = tA ? i / kT : i % kKT, mm = tA ? i % kT : i / kKT;
+        const int m = m0 + mm, k = k0 + kk;
+        float va = 0.f;
+        if (m < M && k < K) va = tA ? A[static_cast<size_t>(k) * lda + m] : A[static_cast<size_t>(m) * lda + k];
+        sA[kk][mm] = va;
+      }
+      {
+        const int kk = tB ? i % kKT : i / kT, nn = tB ? i / kKT : i % kT;
+        const int n = n0 + nn, k = k0 + kk;
+        float vb = 0.f;
+        if (n < N && k < K) vb = tB ? B[static_cast<size_t>(n) * ldb + k] : B[static_cast<size_t>(k) * ldb + n];
+        sB[kk][nn] = vb;
+      }
     }
     __syncthreads();
 #pragma unroll

@@ -61,9 +61,10 @@ constexpr int kBins = 1024;
 constexpr int kCandCap = 2048;
 
 template <int VPT>
-__global__ void __launch_bounds__(kSelThreads) select_rows_reg_kernel(const float* __restrict__ D, int ncols, int ldD,
-                                                                      int k, int32_t* __restrict__ out_idx,
-                                                                      float* __restrict__ out_val) {
+__global__ void __launch_bounds__(kSelThreads, 6) select_rows_reg_kernel(const float* __restrict__ D, int ncols, int ldD,
+                                                                      int kmax, int32_t* __restrict__ out_idx,
+                                                                      float* __restrict__ out_val,
+                                                                      const int32_t* __restrict__ k_row) {
   __shared__ int hist[kBins];
   __shared__ uint64_t s_keys[kCandCap];
   __shared__ SelectShared sh;
@@ -71,6 +72,9 @@ __global__ void __launch_bounds__(kSelThreads) select_rows_reg_kernel(const floa
   __shared__ int s_real, s_cnt, s_bin, s_cum;
   __shared__ int s_wsum[kSelThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  // Row width (rows of width 0 are skipped; the output stride is kmax).
+  const int k = k_row ? min(k_row[blockIdx.x], kmax) : kmax;
+  if (k <= 0) return;
   const float* row = D + static_cast<size_t>(blockIdx.x) * ldD;
   // High words of the keys; 0xFFFFFFFF marks empty (a value >= FLT_MAX or
   // NaN has no key; no non-empty value has all-ones bits).
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(kSelThreads) select_rows_reg_kernel(const floa
   }
   for (int j = tid; j < k; j += kSelThreads) {
     const uint64_t key = j < kk ? keys[j] : kEmpty;
-    const size_t o = static_cast<size_t>(blockIdx.x) * k + j;
+    const size_t o = static_cast<size_t>(blockIdx.x) * kmax + j;
     out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
     if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
   }
@@ -342,19 +346,21 @@ void exclusive_sum(const int64_t* in, int64_t* out, size_t n, void* tmp, size_t 
 }  // namespace
 
 void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx, float* out_val,
-                        cudaStream_t st) {
+                        cudaStream_t st, const int32_t* k_row) {
   if (nrows <= 0 || k <= 0) return;
   HB_CHECK(k <= kMaxSelect, HB_ERR_INVALID, "nprobe above 8192 is not supported");
+  HB_CHECK(!k_row || (k <= 1024 && ncols <= 32 * kSelThreads), HB_ERR_INVALID,
+           "per-row widths need k <= 1024 and at most 8192 columns");
   if (k <= 1024 && ncols <= 32 * kSelThreads) {
     const int vpt = (ncols + kSelThreads - 1) / kSelThreads;
     if (vpt <= 4)
-      select_rows_reg_kernel<4><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val);
+      select_rows_reg_kernel<4><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row);
     else if (vpt <= 8)
-      select_rows_reg_kernel<8><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val);
+      select_rows_reg_kernel<8><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row);
     else if (vpt <= 16)
-      select_rows_reg_kernel<16><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val);
+      select_rows_reg_kernel<16><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row);
     else
-      select_rows_reg_kernel<32><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val);
+      select_rows_reg_kernel<32><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row);
     HB_CUDA(cudaGetLastError());
     return;
   }

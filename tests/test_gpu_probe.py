@@ -66,3 +66,27 @@ def test_learned_probe_meets_calibrated_recall(setup):
     # A higher target never lowers recall.
     D2, I2 = run(ix, test, 10, Precision.BF16, learned=True, target=0.99)
     assert recall_at_k(I2, Il, 10) >= recall_at_k(I, Il, 10) - 1e-9
+
+
+def test_learned_probe_same_on_every_coarse_route(setup):
+    """The tensor-core route computes the predictor's features from a narrow
+    exact pass and widens only the rows that need more probes; the exact
+    route selects the full width and cuts it.  Same probes, same results."""
+    from harmony_b200 import CoarseQuantizer
+    base, test, train, ix = setup
+    ix.train_probe_predictor(train.shape[0], train, k=10, label_nprobe=64, target=0.95)
+    for prec in (Precision.FP32, Precision.BF16):
+        out = {}
+        for kind in (CoarseQuantizer.TENSOR, CoarseQuantizer.EXACT):
+            ix.set_coarse_quantizer(kind, -1)
+            try:
+                out[kind] = run(ix, test, 10, prec, learned=True)
+                if kind == CoarseQuantizer.TENSOR:
+                    # The widening pass proves nearly every row exact; a row
+                    # that fails is recomputed, so many failures mean a
+                    # broken candidate set.
+                    assert ix.coarse_fallbacks() <= 0.05 * test.shape[0]
+            finally:
+                ix.set_coarse_quantizer(CoarseQuantizer.AUTO, -1)
+        (Dt, It), (De, Ie) = out[CoarseQuantizer.TENSOR], out[CoarseQuantizer.EXACT]
+        assert np.array_equal(Dt, De) and np.array_equal(It, Ie), prec

@@ -164,8 +164,9 @@ def pick_nprobe(ix, test, gt, k, target, precision):
     return NPROBE_SWEEP[-1], rec
 
 
-def time_arm(torch, ix, test, k, P, precision, steps, warmup, world, dist, learned=False, target=0.0):
-    """Device-resident timing of `steps` searches (CUDA events on the index stream)."""
+def time_arm(torch, ix, test, k, P, precision, steps, warmup, world, dist, learned=False, target=0.0, tag="arm"):
+    """Device-resident timing of `steps` searches (CUDA events on the index stream).
+    The timed loop is an NVTX range `timed_<tag>` (for `ncu --nvtx-include`)."""
     nq = test.shape[0]
     ix.nprobe = P
     ix.search_params.precision = precision
@@ -183,11 +184,13 @@ def time_arm(torch, ix, test, k, P, precision, steps, warmup, world, dist, learn
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push(f"timed_{tag}")
     e0.record(stream)
     for _ in range(steps):
         ix.search(nq, test, k, D, I)
     e1.record(stream)
     e1.synchronize()
+    torch.cuda.nvtx.range_pop()
     ms = e0.elapsed_time(e1)
     launches = ix.launch_count() - launches0
     if world > 1:
@@ -232,7 +235,7 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         for name, prec in (("fp32", Precision.FP32), ("bf16", Precision.BF16)):
             P, rec = pick_nprobe(ix, test, gt, k, args.target, prec)
-            r = time_arm(torch, ix, test, k, P, prec, args.steps, args.warmup, world, dist)
+            r = time_arm(torch, ix, test, k, P, prec, args.steps, args.warmup, world, dist, tag=name)
             r.update({"nprobe": P, "recall_at_10": recall(r.pop("I").cpu().numpy(), gt, k),
                       "qps": world * nq / (r["ms_per_step"] / 1e3)})
             arms[name] = r
@@ -249,7 +252,7 @@ def run_ours(args):
                 break
         tgt = min(tgt, 0.9999)
         r = time_arm(torch, ix, test, k, 256, Precision.BF16, args.steps, args.warmup, world, dist, learned=True,
-                     target=tgt)
+                     target=tgt, tag="learned_bf16")
         r.update({"nprobe": "learned", "predictor_target": round(tgt, 4),
                   "recall_at_10": recall(r.pop("I").cpu().numpy(), gt, k),
                   "qps": world * nq / (r["ms_per_step"] / 1e3)})

@@ -489,6 +489,96 @@ def run_reference(args):
     return res
 
 
+def run_c4(args):
+    """Config 4: 10M x 96 with Zipf(1.1) list sizes, nlist 4096, k 10, 50k
+    queries with per-query nprobe in U[4, 256], searched in batches of 1, 8,
+    64, 512 and 4096.  Each batch is one public-API call with the queries in
+    pinned host memory and the results copied back (end to end, wall clock
+    around the synchronous calls) and, separately, with queries and results
+    resident on the device (CUDA events).  QPS per batch size, FP32 exact and
+    BF16 + rerank."""
+    import torch
+    from harmony_b200 import Index, Precision, SearchMode, datasets
+    k, nq, nb, d = 10, args.nq or 50_000, args.nb or 10_000_000, 96
+    base, queries = datasets.config4_device(nb=nb, nq=nq)
+    ix = Index(d, 4096, 16)
+    t0 = time.perf_counter()
+    ix.train(base.shape[0], base)
+    ix.add(base.shape[0], base)
+    torch.cuda.synchronize()
+    build_s = round(time.perf_counter() - t0, 2)
+    sizes = ix.list_sizes()
+    npq = datasets.config4_nprobes(nq)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    # Ground truth on the first 2000 queries (FP32 exhaustive + FP64 re-rank).
+    ng = min(2000, nq)
+    gt = ground_truth(torch, ix, base, queries[:ng], k)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    q_host = torch.empty((nq, d), dtype=torch.float32).pin_memory()
+    q_host.copy_(queries.cpu())
+    npq_dev = torch.from_numpy(npq).cuda()
+    D_host = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    I_host = torch.empty((nq, k), dtype=torch.int64).pin_memory()
+    D_dev = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    I_dev = torch.empty((nq, k), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.ExternalStream(ix.stream)
+    sizes_b = [1, 8, 64, 512, 4096]
+    out = {}
+    for name, prec in (("fp32", Precision.FP32), ("bf16", Precision.BF16)):
+        sp = ix.search_params
+        sp.precision, sp.rerank_mult, sp.max_nprobe = prec, 2, 256
+        res = {}
+        for mode in ("e2e", "device"):
+            by = {}
+            for B in sizes_b:
+                calls = max(1, min(nq // B, 200 if B < 512 else 48))
+                def one(off):
+                    if mode == "device":
+                        sp.nprobe_per_query = npq_dev[off:off + B]
+                        ix.search(B, queries[off:off + B], k, D_dev[off:off + B], I_dev[off:off + B])
+                    else:
+                        sp.nprobe_per_query = npq[off:off + B]
+                        ix.search(B, q_host[off:off + B], k, D_host[off:off + B], I_host[off:off + B])
+                for c in range(3):  # warm-up
+                    one((c * B) % (nq - B + 1))
+                torch.cuda.synchronize()
+                if mode == "device":
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    for c in range(calls):
+                        one(c * B)
+                    e1.record(stream)
+                    e1.synchronize()
+                    dt = e0.elapsed_time(e1) / 1e3
+                else:
+                    t1 = time.perf_counter()
+                    for c in range(calls):
+                        one(c * B)
+                    dt = time.perf_counter() - t1
+                by[str(B)] = {"qps": round(calls * B / dt, 1), "ms_per_call": round(1e3 * dt / calls, 3),
+                              "calls": calls}
+            res[mode] = by
+        # Recall of the first 2000 queries at their own nprobe, one call.
+        sp.nprobe_per_query = npq[:ng]
+        ix.search(ng, q_host[:ng], k, D_host[:ng], I_host[:ng])
+        I_check = I_host[:ng].numpy()
+        res["recall_at_10_first_2000"] = round(recall(I_check, gt, k), 4)
+        out[name] = res
+        ix.search_params.nprobe_per_query = None
+        ix.search_params.max_nprobe = 0
+        ix.search_params.precision = Precision.FP32
+    line = {"metric": "QPS per batch size, config4 stream (10M x 96, Zipf list sizes, nlist 4096, k 10, "
+                      "per-query nprobe U[4,256], batches of 1..4096)",
+            "workload": "c4", "unit": "queries/s", "n_gpus": 1, "dtype": "f32 / bf16",
+            "data": "synthetic (seeded Zipf(1.1) Gaussian mixture drawn on the GPU)",
+            "config": {"nb": nb, "d": d, "nlist": 4096, "k": k, "nq": nq, "batch_sizes": sizes_b,
+                       "list_size_min": int(sizes.min()), "list_size_max": int(sizes.max()),
+                       "build_s": build_s},
+            "arms": out}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -501,16 +591,20 @@ def main():
     ap.add_argument("--nb", type=int, default=None, help="smaller base for profiling runs (not a bench line)")
     ap.add_argument("--nq", type=int, default=None, help="fewer queries for profiling runs (not a bench line)")
     ap.add_argument("--ntrain", type=int, default=200_000, help="training queries of the learned probe")
+    ap.add_argument("--workload", choices=["c5", "c4"], default="c5",
+                    help="c5: the headline bench line; c4: the batch-stream measurement of config 4")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.nb:
+    if args.nb and args.workload == "c5":
         WORKLOAD["nb"] = args.nb
         WORKLOAD["workload"] += f" [reduced: nb={args.nb}]"
-    if args.nq:
+    if args.nq and args.workload == "c5":
         WORKLOAD["nq"] = args.nq
         WORKLOAD["workload"] += f" [reduced: nq={args.nq}]"
-    if args.impl == "reference":
+    if args.workload == "c4":
+        run_c4(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

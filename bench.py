@@ -495,8 +495,9 @@ def run_c4(args):
     64, 512 and 4096.  Each batch is one public-API call with the queries in
     pinned host memory and the results copied back (end to end, wall clock
     around the synchronous calls) and, separately, with queries and results
-    resident on the device (CUDA events).  QPS per batch size, FP32 exact and
-    BF16 + rerank."""
+    resident on the device (CUDA events); each both as ordinary calls and as
+    one CUDA-graph launch per batch (params.use_graph).  QPS per batch size,
+    FP32 exact and BF16 + rerank."""
     import torch
     from harmony_b200 import Index, Precision, SearchMode, datasets
     k, nq, nb, d = 10, args.nq or 50_000, args.nb or 10_000_000, 96
@@ -528,12 +529,13 @@ def run_c4(args):
         sp = ix.search_params
         sp.precision, sp.rerank_mult, sp.max_nprobe = prec, 2, 256
         res = {}
-        for mode in ("e2e", "device"):
+        for mode in ("e2e", "device", "e2e_graph", "device_graph"):
+            sp.use_graph = mode.endswith("_graph")
             by = {}
             for B in sizes_b:
                 calls = max(1, min(nq // B, 200 if B < 512 else 48))
                 def one(off):
-                    if mode == "device":
+                    if mode.startswith("device"):
                         sp.nprobe_per_query = npq_dev[off:off + B]
                         ix.search(B, queries[off:off + B], k, D_dev[off:off + B], I_dev[off:off + B])
                     else:
@@ -542,7 +544,7 @@ def run_c4(args):
                 for c in range(3):  # warm-up
                     one((c * B) % (nq - B + 1))
                 torch.cuda.synchronize()
-                if mode == "device":
+                if mode.startswith("device"):
                     e0 = torch.cuda.Event(enable_timing=True)
                     e1 = torch.cuda.Event(enable_timing=True)
                     e0.record(stream)
@@ -559,6 +561,7 @@ def run_c4(args):
                 by[str(B)] = {"qps": round(calls * B / dt, 1), "ms_per_call": round(1e3 * dt / calls, 3),
                               "calls": calls}
             res[mode] = by
+        sp.use_graph = False
         # Recall of the first 2000 queries at their own nprobe, one call.
         sp.nprobe_per_query = npq[:ng]
         ix.search(ng, q_host[:ng], k, D_host[:ng], I_host[:ng])

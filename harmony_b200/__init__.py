@@ -104,7 +104,8 @@ class _SearchParamsC(ctypes.Structure):
         ("nprobe_per_query", ctypes.c_void_p),
         ("max_nprobe", ctypes.c_int32),
         ("seed_rows", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 5),
+        ("use_graph", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 
@@ -200,6 +201,7 @@ class SearchParams:
     nprobe_per_query: Optional[object] = None
     max_nprobe: int = 0
     seed_rows: int = 0
+    use_graph: bool = False
 
 
 class Index:
@@ -367,6 +369,7 @@ class Index:
         c.learned_target = float(sp.learned_target)
         c.max_nprobe = int(sp.max_nprobe)
         c.seed_rows = int(sp.seed_rows)
+        c.use_graph = 1 if sp.use_graph else 0
         return c
 
     def search(self, n: int, queries, k: int, distances, labels, ratio: float = 1.0) -> Stats:

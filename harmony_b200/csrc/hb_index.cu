@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cstdio>
 #include <fstream>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -108,6 +109,7 @@ class IndexCore {
   }
   ~IndexCore() {
     cudaSetDevice(device_);
+    drop_graphs();
     if (st_) {
       cudaStreamSynchronize(st_);
       cudaStreamDestroy(st_);
@@ -130,6 +132,7 @@ class IndexCore {
     ntotal_ = 0;
     coarse_ready_ = false;
     coarse_last_nq_ = 0;
+    drop_graphs();
     HB_CUDA(cudaStreamSynchronize(st_));
   }
 
@@ -148,7 +151,7 @@ class IndexCore {
     const char* name;
     cudaEvent_t a = nullptr;
     Scope(IndexCore* i, const char* n) : ix(i), name(n) {
-      if (ix->prof_) {
+      if (ix->prof_ && !ix->capturing_) {
         a = ix->event();
         cudaEventRecord(a, ix->st_);
       }
@@ -298,6 +301,7 @@ class IndexCore {
     HB_CUDA(cudaStreamSynchronize(st_));
     trained_ = true;
     coarse_ready_ = false;
+    drop_graphs();
   }
 
   // ---- add: src/Index.cpp:581-698 ------------------------------------------
@@ -347,6 +351,7 @@ class IndexCore {
     ntotal_ = n;
     plan_rows_ = 0;
     build_bf16();
+    drop_graphs();
   }
 
   // BF16 copy of the codes (rows padded to kpad = d rounded up to 64) and its
@@ -636,6 +641,12 @@ class IndexCore {
       HB_CUDA(cudaMemcpyAsync(order_dev_.p, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
     }
 
+    if (p.use_graph) {
+      HB_CHECK(mode == SCAN_PLAIN && (p.mode == HB_MODE_ORIGINAL || p.mode == HB_MODE_BRUTE_FORCE) && nq <= bs,
+               HB_ERR_INVALID, "graph search runs ORIGINAL / BRUTE_FORCE searches of one batch");
+      search_graph(static_cast<int>(nq), q, static_cast<int>(k), static_cast<int>(P), R, bf16, p, D, I);
+      return;
+    }
     for (size_t b0 = 0; b0 < nq; b0 += bs) {
       const int nb = static_cast<int>(std::min(bs, nq - b0));
       cut_b0_ = b0;
@@ -676,6 +687,109 @@ class IndexCore {
       }
     }
     HB_CUDA(cudaStreamSynchronize(st_));
+    coarse_err_check();
+  }
+
+  // ---- one batch as a CUDA graph --------------------------------------------
+  //
+  // The batch's inputs are copied into fixed buffers (queries, per-query
+  // nprobe), the device pipeline runs as one graph launch, and the results
+  // are copied out of fixed buffers.  A graph is captured per batch shape
+  // (batch size, k, nprobe, precision, candidate count, nprobe mode and its
+  // settings) after one ordinary run of the same shape has sized every buffer;
+  // any later device allocation of the library, and any change to the index
+  // (train / add / load), drops the cached graphs.
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t gen = 0;
+    uint64_t launches = 0;
+  };
+
+  void drop_graphs() {
+    for (auto& kv : graphs_)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs_.clear();
+  }
+
+  void run_batch_pipeline(int nb, int k, int P, int R, bool bf16) {
+    launch_pad_rows(qtmp_.p, nb, static_cast<int>(d_), static_cast<int>(dpad_), qpad_.p, st_);
+    ++launches_;
+    if (P == 0 || ntotal_ == 0) {
+      launch_fill_results(dout_.p, iout_.p, static_cast<size_t>(nb) * k, st_);
+      ++launches_;
+    } else if (bf16) {
+      search_batch_bf16(nb, P, k, R, dout_.p, iout_.p);
+    } else {
+      search_batch(nb, P, k, SCAN_PLAIN, false, false, 0, k, 1, 1, 0, dout_.p, iout_.p);
+    }
+  }
+
+  void search_graph(int nb, const float* q, int k, int P, int R, bool bf16, const hb_search_params& p, float* D,
+                    int64_t* I) {
+    qtmp_.reserve(static_cast<size_t>(nb) * d_);
+    qpad_.reserve(static_cast<size_t>(nb) * dpad_);
+    dout_.reserve(static_cast<size_t>(nb) * k);
+    iout_.reserve(static_cast<size_t>(nb) * k);
+    HB_CUDA(cudaMemcpyAsync(qtmp_.p, q, static_cast<size_t>(nb) * d_ * sizeof(float), cudaMemcpyDefault, st_));
+    if (cut_mode_ == 2) {
+      npqin_.reserve(static_cast<size_t>(nb));
+      HB_CUDA(cudaMemcpyAsync(npqin_.p, cut_src_, static_cast<size_t>(nb) * sizeof(int32_t), cudaMemcpyDefault, st_));
+      cut_src_ = npqin_.p;
+    }
+    cut_b0_ = 0;
+    char key[256];
+    std::snprintf(key, sizeof(key), "%d/%d/%d/%d/%d/%d/%d/%08x/%d/%d/%d/%d/%d", nb, k, P, R, bf16 ? 1 : 0, p.mode,
+                  cut_mode_, cut_mode_ == 1 ? *reinterpret_cast<const uint32_t*>(&cut_thr_) : 0u, cut_cap_,
+                  seed_rows_, coarse_kind_, coarse_margin_, static_cast<int>(nprobe_));
+    auto it = graphs_.find(key);
+    if (it != graphs_.end() && it->second.gen != devbuf_generation().load()) {
+      cudaGraphExecDestroy(it->second.exec);
+      graphs_.erase(it);
+      it = graphs_.end();
+    }
+    if (it != graphs_.end()) {
+      if (bf16) HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
+      HB_CUDA(cudaGraphLaunch(it->second.exec, st_));
+      launches_ += it->second.launches;
+    } else {
+      // An ordinary run sizes every buffer (and gives this call's results),
+      // then the same sequence is captured.
+      run_batch_pipeline(nb, k, P, R, bf16);
+      HB_CUDA(cudaStreamSynchronize(st_));
+      const uint64_t gen = devbuf_generation().load();
+      const uint64_t l0 = launches_;
+      HB_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeRelaxed));
+      capturing_ = true;
+      cudaGraph_t graph = nullptr;
+      try {
+        run_batch_pipeline(nb, k, P, R, bf16);
+      } catch (...) {
+        capturing_ = false;
+        cudaStreamEndCapture(st_, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        throw;
+      }
+      capturing_ = false;
+      HB_CUDA(cudaStreamEndCapture(st_, &graph));
+      if (devbuf_generation().load() == gen) {
+        GraphEntry e;
+        const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+        if (ie == cudaSuccess) {
+          e.gen = gen;
+          e.launches = launches_ - l0;
+          graphs_[key] = e;
+        } else {
+          cudaGetLastError();
+        }
+      }
+      cudaGraphDestroy(graph);
+      launches_ = l0;
+    }
+    HB_CUDA(cudaMemcpyAsync(D, dout_.p, static_cast<size_t>(nb) * k * sizeof(float), cudaMemcpyDefault, st_));
+    HB_CUDA(cudaMemcpyAsync(I, iout_.p, static_cast<size_t>(nb) * k * sizeof(int64_t), cudaMemcpyDefault, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    if (bf16) bf16_err_check();
     coarse_err_check();
   }
 
@@ -851,6 +965,7 @@ class IndexCore {
     trained_ = true;
     plan_rows_ = 0;
     build_bf16();
+    drop_graphs();
   }
 
   // Exact ORIGINAL search of one batch whose per-call buffers all come from
@@ -1082,7 +1197,7 @@ class IndexCore {
     {
       Scope sc(this, "tau_seed");
       launch_tau_seed(qpad_.p, nb, static_cast<int>(dpad_), kpad_, codes_bf16_.p, list_off_.p, static_cast<int>(nlist_),
-                      list_qoff_.p, list_q_.p, norms_.p, std::max(R, seed_rows_), R, maxnorm_.p, tau_.p, st_);
+                      list_qoff_.p, list_q_.p, norms_.p, std::max(R, seed_rows_), R, maxnorm_.p, tau_.p, st_, probes, P);
     }
     ++launches_;
     part.reserve(max_slots(nb, P, cr) * static_cast<size_t>(scan_bf16_keys_per_slot(R)));
@@ -1131,9 +1246,13 @@ class IndexCore {
     {
       Scope sc(this, "rerank");
       launch_rerank(part_.p, slot_base_.p, nb, P, R, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd, Id,
-                    st_);
+                    st_, nullptr, nullptr, 0, tau_.p);
     }
     ++launches_;
+    if (!capturing_) bf16_err_check();
+  }
+
+  void bf16_err_check() {
     HB_CUDA(cudaMemcpyAsync(err_host_, err_dev_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
     HB_CUDA(cudaStreamSynchronize(st_));
     if (*err_host_ != 0)
@@ -1453,6 +1572,9 @@ class IndexCore {
   DevBuf<float> cnorm_, cmaxnorm_, cval_;
   DevBuf<int32_t> ccand_;
   DevBuf<int> cflags_, cerr_dev_;
+  bool capturing_ = false;
+  std::map<std::string, GraphEntry> graphs_;
+  DevBuf<int32_t> npqin_;
   DevBuf<int32_t> kq_;
   DevBuf<uint16_t> codes_bf16_;
   DevBuf<uint64_t> tau_, part2_;

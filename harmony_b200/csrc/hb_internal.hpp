@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -32,6 +33,13 @@ struct Error : std::runtime_error {
     if (!(cond)) throw ::hb::Error((code), (msg));    \
   } while (0)
 
+// Bumped on every device allocation of a DevBuf: CUDA graphs that captured
+// buffer addresses are valid only while it is unchanged.
+inline std::atomic<uint64_t>& devbuf_generation() {
+  static std::atomic<uint64_t> g{0};
+  return g;
+}
+
 // Device allocation owned by the index.  Grows, never shrinks.
 template <class T>
 struct DevBuf {
@@ -53,6 +61,7 @@ struct DevBuf {
       if (bytes == 0) bytes = sizeof(T);
       HB_CUDA(cudaMalloc(&p, bytes));
       n = count;
+      devbuf_generation().fetch_add(1);
     }
     return p;
   }
@@ -188,16 +197,20 @@ int scan_bf16_max_R(int kpad);       // largest candidate count per query the sc
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);
 void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st);
 void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st);
-// Re-rank over the slots of one or two scan passes (part2 may be null).
+// Re-rank over the slots of one or two scan passes (part2 may be null);
+// tau (optional): per query an upper bound of its R-th key (the scan's final
+// bound), keys above it are skipped.
 void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
                    const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
-                   const uint64_t* part2 = nullptr, const int64_t* slot_base2 = nullptr, int P2 = 0);
+                   const uint64_t* part2 = nullptr, const int64_t* slot_base2 = nullptr, int P2 = 0,
+                   const uint64_t* tau = nullptr);
 // Per-query upper bound of the R-th approximate key from the first S <= 256
 // BF16 rows of the query's nearest list (probe rank 0 in the list-major work
 // description); queries without a seed get all ones.  maxnorm = max ||x||.
 void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* codes_bf16, const int64_t* list_off,
                      int nlist, const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int R,
-                     const float* maxnorm, uint64_t* tau, cudaStream_t st);
+                     const float* maxnorm, uint64_t* tau, cudaStream_t st, const int32_t* probes = nullptr,
+                     int P = 0);
 // *out = max over i of sqrt(norms[i]) (slightly rounded up), on the device.
 void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st);
 // probes (nq x P) -> first column (nq x 1) and the rest (nq x (P-1)).

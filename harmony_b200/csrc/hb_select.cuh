@@ -32,6 +32,7 @@ __device__ __forceinline__ int block_key_stats(KeyAt key_at, int m, SelectShared
   __syncthreads();
   int c = 0;
   unsigned long long lo = kEmpty, hi = 0;
+#pragma unroll 4
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     const uint64_t key = key_at(i);
     if (key == kEmpty) continue;
@@ -75,6 +76,7 @@ __device__ __forceinline__ int block_select(KeyAt key_at, int m, int kk, SelectS
     const uint64_t want = top >= 64 ? 0 : prefix >> top;
     for (int i = tid; i < 256; i += blockDim.x) sh.hist[i] = 0;
     __syncthreads();
+#pragma unroll 2
     for (int base = tid & ~31; base < m; base += blockDim.x) {
       const int i = base + lane;
       bool valid = false;
@@ -133,6 +135,7 @@ __device__ __forceinline__ int block_select(KeyAt key_at, int m, int kk, SelectS
   if (tid == 0) sh.count = 0;
   __syncthreads();
   const uint64_t lim = shift >= 64 ? 0 : prefix >> shift;
+#pragma unroll 4
   for (int i = tid; i < m; i += blockDim.x) {
     const uint64_t key = key_at(i);
     if (key == kEmpty) continue;

@@ -335,6 +335,86 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
   }
 }
 
+// The same refinement with one CTA per query, for small batches (a warp per
+// query leaves the GPU idle when there are few queries): threads take
+// candidates, the CTA sorts them.
+__global__ void __launch_bounds__(256) coarse_refine_block_kernel(
+    const float* __restrict__ q, int nq, int dpad, const float* __restrict__ cent, const int32_t* __restrict__ cand,
+    const float* __restrict__ cval, int Pm, int P, int nlist, const float* __restrict__ cmaxnorm,
+    int32_t* __restrict__ probes, float* __restrict__ cdist, int* __restrict__ flags, CoarseRows rows) {
+  extern __shared__ uint64_t s_blk[];  // pow2(Pm)
+  __shared__ float s_qn[8];
+  const int qi = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  int Pr = P, Pmr = Pm;
+  if (rows.width) {
+    Pr = min(rows.width[qi], P);
+    if (Pr <= 0 || (rows.pre && Pr <= rows.pre_w)) {
+      for (int j = tid; j < P; j += blockDim.x)
+        probes[static_cast<size_t>(qi) * P + j] =
+            (j < Pr && rows.pre) ? rows.pre[static_cast<size_t>(qi) * rows.pre_w + j] : -1;
+      if (tid == 0) flags[qi] = 0;
+      return;
+    }
+    Pmr = min(nlist, Pr + coarse_extra_dev(Pr, rows.margin));
+  }
+  const int n2 = pow2_ceil(Pmr < 2 ? 2 : Pmr);
+  const float* qrow = q + static_cast<size_t>(qi) * dpad;
+  float qn = 0.0f;
+  for (int c = tid; c < dpad; c += blockDim.x) qn = fmaf(qrow[c], qrow[c], qn);
+  for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(0xffffffffu, qn, o);
+  if (lane == 0) s_qn[wid] = qn;
+  for (int i = tid; i < n2; i += blockDim.x) {
+    uint64_t key = kEmpty;
+    if (i < Pmr) {
+      const int c = cand[static_cast<size_t>(qi) * Pm + i];
+      if (c >= 0) {
+        const float* x = cent + static_cast<size_t>(c) * dpad;
+        float acc = 0.0f;
+#pragma unroll 8
+        for (int j = 0; j < dpad; j += 4) {
+          const float4 v = *reinterpret_cast<const float4*>(x + j);
+          const float4 w = *reinterpret_cast<const float4*>(qrow + j);
+          float t;
+          t = __fsub_rn(w.x, v.x);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+          t = __fsub_rn(w.y, v.y);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+          t = __fsub_rn(w.z, v.z);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+          t = __fsub_rn(w.w, v.w);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+        }
+        if (acc < FLT_MAX) key = make_key(acc, static_cast<uint32_t>(c));
+      }
+    }
+    s_blk[i] = key;
+  }
+  __syncthreads();
+  block_bitonic_sort(s_blk, n2);
+  for (int j = tid; j < P; j += blockDim.x) {
+    const uint64_t key = j < Pr ? s_blk[j] : kEmpty;
+    probes[static_cast<size_t>(qi) * P + j] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
+    if (cdist) cdist[static_cast<size_t>(qi) * P + j] = key == kEmpty ? FLT_MAX : key_dist(key);
+  }
+  if (tid == 0) {
+    float qs = 0.0f;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) qs += s_qn[w];
+    bool exact = true;
+    if (Pmr < nlist) {
+      const float vlast = cval[static_cast<size_t>(qi) * Pm + Pmr - 1];
+      const uint64_t kp = s_blk[Pr - 1];
+      exact = kp != kEmpty && vlast < FLT_MAX;
+      if (exact) {
+        const float mn = *cmaxnorm;
+        const float bound = 4e-4f * sqrtf(qs) * mn + 2e-5f * (mn * mn + qs + fabsf(vlast)) + 1e-30f;
+        exact = key_dist(kp) < vlast - bound;
+      }
+    }
+    flags[qi] = exact ? 0 : 1;
+  }
+}
+
 // Exact row for each flagged query (rare): the reference's sequential FP32
 // distance to every centroid, written over the query's row of the
 // approximate matrix, then the P smallest (distance, centroid).
@@ -426,6 +506,15 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
   if (nq <= 0) return;
   HB_CHECK(P >= 1 && P <= Pm && Pm <= kCoarseMaxPm, HB_ERR_INVALID, "coarse candidate count out of range");
   const int n2 = pow2_ceil(Pm < 2 ? 2 : Pm);
+  if (nq < 512) {
+    const size_t smem = static_cast<size_t>(n2) * 8;
+    HB_CUDA(cudaFuncSetAttribute(coarse_refine_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    coarse_refine_block_kernel<<<nq, 256, smem, st>>>(q, nq, dpad, cent, cand, cval, Pm, P, nlist, cmaxnorm, probes,
+                                                      cdist, flags, rows);
+    HB_CUDA(cudaGetLastError());
+    return;
+  }
   const int warps = std::max(1, std::min(8, 65536 / (n2 * 8)));
   const size_t smem = static_cast<size_t>(warps) * n2 * 8;
   HB_CUDA(cudaFuncSetAttribute(coarse_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));

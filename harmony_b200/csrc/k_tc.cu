@@ -436,12 +436,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
-__global__ void __launch_bounds__(128) rerank_kernel(const uint64_t* __restrict__ part,
+__global__ void __launch_bounds__(256) rerank_kernel(const uint64_t* __restrict__ part,
                                                      const int64_t* __restrict__ slot_base, int P, int R, int k,
                                                      const float* __restrict__ codes, const float* __restrict__ q,
                                                      int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
                                                      int64_t* __restrict__ I, const uint64_t* __restrict__ part2,
-                                                     const int64_t* __restrict__ slot_base2, int P2) {
+                                                     const int64_t* __restrict__ slot_base2, int P2,
+                                                     const uint64_t* __restrict__ tau) {
   extern __shared__ uint64_t s_keys[];  // pow2(R) approx, then pow2(R) exact
   __shared__ SelectShared sh_sel;
   const int qi = blockIdx.x;
@@ -460,7 +461,13 @@ __global__ void __launch_bounds__(128) rerank_kernel(const uint64_t* __restrict_
     src2 = part2 + t0 * kGroups * R;
     m2 = static_cast<int>((t1 - t0) * kGroups * R);
   }
-  auto key_at = [&](int i) -> uint64_t { return i < m1 ? src[i] : src2[i - m1]; };
+  // The query's final bound is at or above its R-th key: keys above it
+  // cannot be among the R best, so they drop out of the selection.
+  const uint64_t lim = tau ? tau[qi] : kEmpty;
+  auto key_at = [&](int i) -> uint64_t {
+    const uint64_t key = i < m1 ? src[i] : src2[i - m1];
+    return key <= lim ? key : kEmpty;
+  };
   block_topk_sorted(key_at, m1 + m2, R, sh_sel, s_appr);
   const float* qrow = q + static_cast<size_t>(qi) * dpad;
   for (int i = threadIdx.x; i < n2; i += blockDim.x) {
@@ -469,6 +476,7 @@ __global__ void __launch_bounds__(128) rerank_kernel(const uint64_t* __restrict_
       const uint32_t pos = key_tie(s_appr[i]);
       const float* x = codes + static_cast<size_t>(pos) * dpad;
       float acc = 0.0f;
+#pragma unroll 8
       for (int c = 0; c < dpad; c += 4) {
         const float4 v = *reinterpret_cast<const float4*>(x + c);
         const float4 w = *reinterpret_cast<const float4*>(qrow + c);
@@ -529,17 +537,31 @@ constexpr int kSeedWarps = 8;
 __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
     const float* __restrict__ q, int dpad, int kpad, const __nv_bfloat16* __restrict__ codes,
     const int64_t* __restrict__ list_off, const int64_t* __restrict__ list_qoff, const int32_t* __restrict__ list_q,
-    const float* __restrict__ xnorm, int S, int R, const float* __restrict__ maxnorm, uint64_t* __restrict__ tau) {
+    const float* __restrict__ xnorm, int S, int R, const float* __restrict__ maxnorm, uint64_t* __restrict__ tau,
+    const int32_t* __restrict__ probes, int P) {
   extern __shared__ __align__(16) uint8_t s_seed_raw[];
   __shared__ float s_xn[kSeedRows];
   __shared__ int s_qs[kSeedWarps * 32];
   __shared__ int s_nq;
-  const int l = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
-  const int64_t e0 = list_qoff[l], e1 = list_qoff[l + 1];
-  bool mine = false;
-  for (int64_t e = e0 + tid; e < e1 && !mine; e += blockDim.x) mine = (list_q[e] & 0xffff) == 0;
-  if (!__syncthreads_or(mine)) return;
+  // One CTA per list (its rows serve every query whose nearest list it is),
+  // or, for small batches (probes given), one CTA per query.
+  const bool by_query = probes != nullptr;
+  int l;
+  int64_t e0, e1;
+  if (by_query) {
+    l = probes[static_cast<size_t>(blockIdx.x) * P];
+    if (l < 0) return;
+    e0 = 0;
+    e1 = 1;
+  } else {
+    l = blockIdx.x;
+    e0 = list_qoff[l];
+    e1 = list_qoff[l + 1];
+    bool mine = false;
+    for (int64_t e = e0 + tid; e < e1 && !mine; e += blockDim.x) mine = (list_q[e] & 0xffff) == 0;
+    if (!__syncthreads_or(mine)) return;
+  }
   const int64_t b = list_off[l];
   const int n = static_cast<int>(min(static_cast<int64_t>(S), list_off[l + 1] - b));
   if (n < R) return;  // no seed: tau stays empty
@@ -565,7 +587,8 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
     if (tid == 0) s_nq = 0;
     __syncthreads();
     if (r0 + tid < e1) {
-      const uint32_t ent = static_cast<uint32_t>(list_q[r0 + tid]);
+      const uint32_t ent =
+          by_query ? (static_cast<uint32_t>(blockIdx.x) << 16) : static_cast<uint32_t>(list_q[r0 + tid]);
       if ((ent & 0xffff) == 0) s_qs[atomicAdd(&s_nq, 1)] = static_cast<int>(ent >> 16);
     }
     __syncthreads();
@@ -720,18 +743,20 @@ void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream
 
 void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
                    const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
-                   const uint64_t* part2, const int64_t* slot_base2, int P2) {
+                   const uint64_t* part2, const int64_t* slot_base2, int P2, const uint64_t* tau) {
   if (nq <= 0) return;
   HB_CHECK(k <= R, HB_ERR_INVALID, "k must not exceed the re-ranked candidates");
   const int n2 = pow2_ceil(R < 2 ? 2 : R);
   const size_t smem = static_cast<size_t>(2 * n2) * 8 + 64;
-  rerank_kernel<<<nq, 128, smem, st>>>(part, slot_base, P, R, k, codes, q, dpad, ids, D, I, part2, slot_base2, P2);
+  // Small batches get wider CTAs (each query's selection is the whole job).
+  rerank_kernel<<<nq, nq < 1024 ? 256 : 128, smem, st>>>(part, slot_base, P, R, k, codes, q, dpad, ids, D, I, part2,
+                                                         slot_base2, P2, tau);
   HB_CUDA(cudaGetLastError());
 }
 
 void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* codes_bf16, const int64_t* list_off,
                      int nlist, const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int R,
-                     const float* maxnorm, uint64_t* tau, cudaStream_t st) {
+                     const float* maxnorm, uint64_t* tau, cudaStream_t st, const int32_t* probes, int P) {
   if (nq <= 0) return;
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
   HB_CHECK(S >= 1 && S <= kSeedRows && R >= 1 && R <= S, HB_ERR_INVALID, "seed sample out of range");
@@ -739,8 +764,10 @@ void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* cod
   const size_t smem = static_cast<size_t>(S) * (kpad * 2 + 16) + static_cast<size_t>(kSeedWarps) * kpad * 4 +
                       static_cast<size_t>(kSeedWarps) * kSeedRows * 8;
   HB_CUDA(cudaFuncSetAttribute(tau_seed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  tau_seed_kernel<<<nlist, kSeedWarps * 32, smem, st>>>(q, dpad, kpad, static_cast<const __nv_bfloat16*>(codes_bf16),
-                                                        list_off, list_qoff, list_q, xnorm, S, R, maxnorm, tau);
+  const bool by_query = probes && static_cast<long long>(nq) * 4 < nlist;
+  tau_seed_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(
+      q, dpad, kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff, list_q, xnorm, S, R, maxnorm,
+      tau, by_query ? probes : nullptr, P);
   HB_CUDA(cudaGetLastError());
 }
 

@@ -79,7 +79,10 @@ typedef struct {
   int32_t max_nprobe;         /* cap for per-query nprobe (0 -> index nprobe)    */
   int32_t seed_rows;          /* BF16: rows of each query's nearest list behind
                                  the scan's initial bound (0 -> 256, max 256)  */
-  int32_t reserved[5];
+  int32_t use_graph;          /* 1: run the batch as one CUDA-graph launch,
+                                 captured on first use per batch shape (see
+                                 hb_search); ORIGINAL / BRUTE_FORCE, one batch */
+  int32_t reserved[4];
 } hb_search_params;
 
 void hb_search_params_init(hb_search_params* p);

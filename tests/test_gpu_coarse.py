@@ -29,13 +29,15 @@ def trained(d, nlist, nb, seed, offset=0.0):
     base = centres[lab] + rng.standard_normal((nb, d)).astype(np.float32) + np.float32(offset)
     ix = Index(d, nlist, 8)
     ix.train(nb, base)
-    lab = rng.integers(0, centres.shape[0], 400)
-    q = centres[lab] + rng.standard_normal((400, d)).astype(np.float32) + np.float32(offset)
+    lab = rng.integers(0, centres.shape[0], 1200)
+    q = centres[lab] + rng.standard_normal((1200, d)).astype(np.float32) + np.float32(offset)
     return ix, np.ascontiguousarray(q, np.float32)
 
 
 @pytest.mark.parametrize("d,nlist,nq,P", [
     (128, 1000, 300, 40),
+    (128, 1000, 1100, 40),  # large batch: one warp per query in the refinement
+    (64, 500, 700, 120),
     (16, 37, 5, 8),
     (33, 300, 129, 17),
     (100, 130, 257, 64),

@@ -522,7 +522,7 @@ class IndexCore {
   // Raises when a bounded wait of the tensor-core quantizer gave up since the
   // last check (the flag is sticky until read here).
   void coarse_err_check() {
-    if (!coarse_ready_) return;
+    if (!cerr_dev_.p) return;
     HB_CUDA(cudaMemcpyAsync(err_host_, cerr_dev_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
     HB_CUDA(cudaStreamSynchronize(st_));
     if (*err_host_ != 0) {
@@ -1286,6 +1286,9 @@ class IndexCore {
     int F = 0, H = 256, NB = 0, C = 32, pmax = 0;
     std::vector<int32_t> buckets;
     DevBuf<float> W1, B1, W2, B2, W3, B3;  // BF16-rounded inference weights
+    DevBuf<uint16_t> W1b, W2b, W3b;        // the same, packed BF16 for the tensor cores
+    int K1 = 0;
+    bool tc = false;
     DevBuf<float> mean, inv_std;
     DevBuf<int32_t> bucket_val;
     std::vector<float> cal_thr, cal_recall, cal_avgp;
@@ -1309,6 +1312,26 @@ class IndexCore {
   void probe_infer(int nb, const float* qpad, const float* cdist, int P, int32_t* probes, float thr, int cap,
                    int32_t* nprobe_out) {
     ProbeModel& m = probe_;
+    if (m.tc) {
+      if (!cerr_dev_.p) {
+        cerr_dev_.reserve(1);
+        HB_CUDA(cudaMemsetAsync(cerr_dev_.p, 0, sizeof(int), st_));
+      }
+      int32_t* np = nprobe_out;
+      if (!np) {
+        npq_.reserve(static_cast<size_t>(nb));
+        np = npq_.p;
+      }
+      mlp_infer_tc(qpad, nb, static_cast<int>(d_), static_cast<int>(dpad_), cdist, P, m.C, m.mean.p, m.inv_std.p, m.K1,
+                   m.W1b.p, m.B1.p, m.W2b.p, m.B2.p, m.W3b.p, m.B3.p, m.NB, m.bucket_val.p, thr, cap, np,
+                   cerr_dev_.p, st_);
+      ++launches_;
+      if (probes) {
+        launch_cut_probes(np, nb, P, probes, st_);
+        ++launches_;
+      }
+      return;
+    }
     pf_.reserve(static_cast<size_t>(nb) * m.F);
     ph1_.reserve(static_cast<size_t>(nb) * m.H);
     ph2_.reserve(static_cast<size_t>(nb) * m.H);
@@ -1495,6 +1518,17 @@ class IndexCore {
     mlp_round_bf16(b2, m.B2.p, H, st_);
     mlp_round_bf16(w3, m.W3.p, n3, st_);
     mlp_round_bf16(b3, m.B3.p, NB, st_);
+    // Packed BF16 weights for the fused tensor-core inference.
+    m.K1 = (F + 63) / 64 * 64;
+    m.tc = m.K1 <= 256 && NB <= 32 && H == 256;
+    if (m.tc) {
+      m.W1b.reserve(static_cast<size_t>(H) * m.K1);
+      m.W2b.reserve(static_cast<size_t>(H) * H);
+      m.W3b.reserve(static_cast<size_t>(32) * H);
+      mlp_pack_bf16(m.W1.p, H, F, H, m.K1, m.W1b.p, st_);
+      mlp_pack_bf16(m.W2.p, H, H, H, H, m.W2b.p, st_);
+      mlp_pack_bf16(m.W3.p, NB, H, 32, H, m.W3b.p, st_);
+    }
     m.bucket_val.reserve(NB);
     HB_CUDA(cudaMemcpyAsync(m.bucket_val.p, m.buckets.data(), NB * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
     // Calibration on the held-out queries: predicted nprobe for a grid of

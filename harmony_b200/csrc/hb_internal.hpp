@@ -248,6 +248,14 @@ void launch_coarse_widths(const int32_t* width, int nq, int wmax, int pre_w, int
                           cudaStream_t st);
 
 // k_mlp.cu: learned probe predictor kernels.
+// Fused tensor-core inference (features -> 3 layers -> bucket choice) for
+// K1 = roundup(d + C, 64) <= 256 and NB <= 32; weights packed by
+// mlp_pack_bf16 (N x K FP32 -> Npad x Kpad BF16).
+void mlp_pack_bf16(const float* W, int N, int K, int Npad, int Kpad, void* out, cudaStream_t st);
+void mlp_infer_tc(const float* q, int nq, int d, int dpad, const float* cdist, int P, int C, const float* mean,
+                  const float* inv_std, int K1, const void* W1b, const float* b1, const void* W2b, const float* b2,
+                  const void* W3b, const float* b3, int NB, const int32_t* bucket_val, float thr, int cap,
+                  int32_t* nprobe_out, int* err, cudaStream_t st);
 void mlp_gemm(int M, int N, int K, const float* A, int lda, bool tA, const float* B, int ldb, bool tB, float* C, int ldc,
               const float* bias, float beta, bool gelu, float* Z, bool round_bf16, cudaStream_t st);
 void mlp_gelu_backward(const float* dH, const float* Z, float* dZ, size_t n, cudaStream_t st);

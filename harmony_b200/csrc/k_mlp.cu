@@ -18,6 +18,7 @@
 
 #include "hb_device.cuh"
 #include "hb_internal.hpp"
+#include "hb_sm100.cuh"
 
 namespace hb {
 namespace {
@@ -295,6 +296,211 @@ inline unsigned blocks_for(size_t n, int tb = 256, unsigned cap = 148u * 64u) {
   return static_cast<unsigned>(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
+// ---------------------------------------------------------------------------
+// Fused predictor inference on the tensor cores: one CTA per 128 queries
+// builds the standardized BF16 features in shared memory (A, K-major,
+// 128-byte swizzle), runs the three layers as tcgen05.mma chains (M 128 x
+// N 256 / 32 x K 16) into TMEM with the BF16 weights staged in shared memory,
+// applies bias + GELU + BF16 rounding between layers (written back as the
+// next layer's A operand) and ends with the bucket choice.  Same arithmetic
+// as the SIMT path (BF16 operands, FP32 accumulation, BF16 activations); the
+// accumulation order differs.
+
+using namespace sm100;
+
+constexpr int kMlpRows = 128;
+constexpr int kMlpThreads = 256;
+
+// W (N x K FP32, BF16-valued) -> Wb (Npad x Kpad BF16, zero padding).
+__global__ void pack_bf16_kernel(const float* __restrict__ W, int N, int K, int Npad, int Kpad,
+                                 __nv_bfloat16* __restrict__ out) {
+  const size_t total = static_cast<size_t>(Npad) * Kpad;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int n = static_cast<int>(i / Kpad), k = static_cast<int>(i % Kpad);
+    out[i] = __float2bfloat16_rn(n < N && k < K ? W[static_cast<size_t>(n) * K + k] : 0.0f);
+  }
+}
+
+// Copies Wb (N rows x Kpad BF16, row-major) into the swizzled K-major layout.
+__device__ __forceinline__ void stage_weights(uint8_t* dst, const __nv_bfloat16* __restrict__ Wb, int N, int Kpad) {
+  const int cpr = Kpad / 8;
+  const uint32_t kblk = static_cast<uint32_t>(N) * 128u;
+  for (int i = threadIdx.x; i < N * cpr; i += blockDim.x) {
+    const int n = i / cpr, c = i - n * cpr;
+    *reinterpret_cast<uint4*>(dst + sw128_offset_bf16(n, c * 8, kblk)) =
+        *reinterpret_cast<const uint4*>(Wb + static_cast<size_t>(n) * Kpad + c * 8);
+  }
+}
+
+__device__ __forceinline__ uint32_t pack2_bf16(float a, float b) {
+  __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&p);
+}
+
+// One layer: D[tmem] = A (128 x K) x W^T (N x K); issued by thread 0, all
+// threads wait for completion.
+__device__ __forceinline__ bool mlp_mma(uint32_t tmem, const uint8_t* A, const uint8_t* W, int N, int K,
+                                        uint64_t* bar, uint32_t parity, int* err) {
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x == 0) {
+    const uint32_t idesc = idesc_bf16_f32(kMlpRows, N);
+    const uint32_t a0 = smem_u32(A), w0 = smem_u32(W);
+    for (int k = 0; k < K / 16; ++k) {
+      const uint32_t oa = static_cast<uint32_t>(k >> 2) * (kMlpRows * 128u) + static_cast<uint32_t>(k & 3) * 32u;
+      const uint32_t ow = static_cast<uint32_t>(k >> 2) * (static_cast<uint32_t>(N) * 128u) +
+                          static_cast<uint32_t>(k & 3) * 32u;
+      mma_bf16(tmem, desc_sw128(a0 + oa), desc_sw128(w0 + ow), idesc, k > 0 ? 1u : 0u);
+    }
+    mma_commit(bar);
+  }
+  const bool ok = mbar_wait(bar, parity, err, 41);
+  tc_fence_after();
+  return ok;
+}
+
+__global__ void __launch_bounds__(kMlpThreads, 1) probe_mlp_tc_kernel(
+    const float* __restrict__ q, int nq, int d, int dpad, const float* __restrict__ cdist, int P, int C,
+    const float* __restrict__ mean, const float* __restrict__ inv_std, int K1, const __nv_bfloat16* __restrict__ W1b,
+    const float* __restrict__ b1, const __nv_bfloat16* __restrict__ W2b, const float* __restrict__ b2,
+    const __nv_bfloat16* __restrict__ W3b, const float* __restrict__ b3, int NB, const int32_t* __restrict__ bucket_val,
+    float thr, int cap, int32_t* __restrict__ nprobe_out, int* __restrict__ err) {
+  extern __shared__ uint8_t mlp_raw[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t s_tmem;
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(mlp_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* A = smem;                       // 128 x 256 BF16 (64 KB)
+  uint8_t* W = smem + kMlpRows * 256 * 2;  // up to 256 x 256 BF16 (128 KB)
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int r0 = blockIdx.x * kMlpRows;
+  const uint32_t akblk = kMlpRows * 128u;
+  if (warp == 0) tmem_alloc(&s_tmem, 256);
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  // Layer-1 weights and the features.
+  stage_weights(W, W1b, 256, K1);
+  if (tid < kMlpRows) {
+    const int r = r0 + tid;
+    const bool live = r < nq;
+    const float* qrow = q + static_cast<size_t>(live ? r : 0) * dpad;
+    const float* cd = cdist + static_cast<size_t>(live ? r : 0) * P;
+    const float l0 = logf(fmaxf(cd[0], 1e-20f));
+    const int F = d + C;
+    for (int k = 0; k < K1; k += 8) {
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int f = k + j;
+        float x = 0.0f;
+        if (live && f < F) {
+          if (f < d) {
+            x = qrow[f];
+          } else {
+            const int c = f - d;
+            if (c == 0) {
+              x = l0;
+            } else {
+              const float dj = c < P ? cd[c] : cd[P - 1];
+              x = dj < FLT_MAX ? logf(fmaxf(dj, 1e-20f)) - l0 : 0.f;
+            }
+          }
+          x = bf16r((x - mean[f]) * inv_std[f]);
+        }
+        v[j] = x;
+      }
+      *reinterpret_cast<uint4*>(A + sw128_offset_bf16(tid, k, akblk)) =
+          make_uint4(pack2_bf16(v[0], v[1]), pack2_bf16(v[2], v[3]), pack2_bf16(v[4], v[5]), pack2_bf16(v[6], v[7]));
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  // Epilogue mapping: warp w reads TMEM lanes 32 * (w % 4) (rows), columns
+  // [128 * (w / 4), +128).
+  const int row = (warp & 3) * 32 + (tid & 31);
+  const int cbase = (warp >> 2) * 128;
+  const uint32_t taddr = tmem + ((32u * static_cast<uint32_t>(warp & 3)) << 16);
+  bool ok = true;
+  uint32_t parity = 0;
+  // Layers 1 and 2: bias + GELU + BF16 back into A.
+  for (int layer = 0; layer < 2 && ok; ++layer) {
+    ok = mlp_mma(tmem, A, W, 256, layer == 0 ? K1 : 256, &bar, parity, err);
+    parity ^= 1u;
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
+    const float* bias = layer == 0 ? b1 : b2;
+    for (int c = 0; c < 4; ++c) {
+      uint32_t rr[32];
+      tmem_ld32(taddr + static_cast<uint32_t>(cbase + c * 32), rr);
+      tmem_ld_wait();
+#pragma unroll
+      for (int j8 = 0; j8 < 4; ++j8) {
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int n = cbase + c * 32 + j8 * 8 + j;
+          v[j] = bf16r(gelu_f(__uint_as_float(rr[j8 * 8 + j]) + bias[n]));
+        }
+        *reinterpret_cast<uint4*>(A + sw128_offset_bf16(row, cbase + c * 32 + j8 * 8, akblk)) =
+            make_uint4(pack2_bf16(v[0], v[1]), pack2_bf16(v[2], v[3]), pack2_bf16(v[4], v[5]),
+                       pack2_bf16(v[6], v[7]));
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    stage_weights(W, layer == 0 ? W2b : W3b, layer == 0 ? 256 : 32, 256);
+  }
+  // Layer 3 (N 32, NB used) and the bucket choice: the smallest bucket whose
+  // predicted CDF reaches thr.
+  if (ok) ok = __syncthreads_and(mlp_mma(tmem, A, W, 32, 256, &bar, parity, err));
+  if (ok && warp < 4) {
+    uint32_t rr[32];
+    tmem_ld32(taddr, rr);
+    tmem_ld_wait();
+    const int r = r0 + row;
+    if (r < nq) {
+      float z[32];
+      float mx = -INFINITY;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        z[j] = j < NB ? __uint_as_float(rr[j]) + b3[j] : -INFINITY;
+        mx = fmaxf(mx, z[j]);
+      }
+      float sum = 0.f;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < NB) sum += expf(z[j] - mx);
+      float cum = 0.f;
+      int pick = bucket_val[NB - 1];
+      bool found = false;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        if (j < NB && !found) {
+          cum += expf(z[j] - mx) / sum;
+          if (cum >= thr) {
+            pick = bucket_val[j];
+            found = true;
+          }
+        }
+      }
+      nprobe_out[r] = min(pick, cap);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
+  }
+}
+
 }  // namespace
 
 void mlp_gemm(int M, int N, int K, const float* A, int lda, bool tA, const float* B, int ldb, bool tB, float* C, int ldc,
@@ -373,6 +579,31 @@ void launch_label_rank(const int64_t* I, int nq, int k, const int32_t* list_of_i
 void launch_list_of_id(const int64_t* list_off, int nlist, const int64_t* ids, int32_t* out, int64_t max_id,
                        cudaStream_t st) {
   list_of_id_kernel<<<nlist, 128, 0, st>>>(list_off, nlist, ids, out, max_id);
+  HB_CUDA(cudaGetLastError());
+}
+
+size_t probe_mlp_tc_smem_bytes() { return 1024 + kMlpRows * 256 * 2 + 256 * 256 * 2; }
+
+void mlp_pack_bf16(const float* W, int N, int K, int Npad, int Kpad, void* out, cudaStream_t st) {
+  const size_t total = static_cast<size_t>(Npad) * Kpad;
+  pack_bf16_kernel<<<static_cast<unsigned>(std::min<size_t>((total + 255) / 256, 148u * 8u)), 256, 0, st>>>(
+      W, N, K, Npad, Kpad, static_cast<__nv_bfloat16*>(out));
+  HB_CUDA(cudaGetLastError());
+}
+
+void mlp_infer_tc(const float* q, int nq, int d, int dpad, const float* cdist, int P, int C, const float* mean,
+                  const float* inv_std, int K1, const void* W1b, const float* b1, const void* W2b, const float* b2,
+                  const void* W3b, const float* b3, int NB, const int32_t* bucket_val, float thr, int cap,
+                  int32_t* nprobe_out, int* err, cudaStream_t st) {
+  if (nq <= 0) return;
+  HB_CHECK(K1 % 64 == 0 && K1 <= 256 && NB <= 32, HB_ERR_INVALID, "predictor shape outside the tensor-core path");
+  const size_t smem = probe_mlp_tc_smem_bytes();
+  HB_CUDA(cudaFuncSetAttribute(probe_mlp_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)));
+  probe_mlp_tc_kernel<<<(nq + kMlpRows - 1) / kMlpRows, kMlpThreads, smem, st>>>(
+      q, nq, d, dpad, cdist, P, C, mean, inv_std, K1, static_cast<const __nv_bfloat16*>(W1b), b1,
+      static_cast<const __nv_bfloat16*>(W2b), b2, static_cast<const __nv_bfloat16*>(W3b), b3, NB, bucket_val, thr, cap,
+      nprobe_out, err);
   HB_CUDA(cudaGetLastError());
 }
 

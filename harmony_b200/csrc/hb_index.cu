@@ -1242,11 +1242,12 @@ class IndexCore {
     err_dev_.reserve(1);
     HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
     tau_.reserve(nb);
+    rr_over_.reserve(nb);
     bf16_pass(nb, P, probes_.p, R, slot_base_, part_);
     {
       Scope sc(this, "rerank");
       launch_rerank(part_.p, slot_base_.p, nb, P, R, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd, Id,
-                    st_, nullptr, nullptr, 0, tau_.p);
+                    st_, nullptr, nullptr, 0, tau_.p, rr_over_.p);
     }
     ++launches_;
     if (!capturing_) bf16_err_check();
@@ -1610,6 +1611,7 @@ class IndexCore {
   std::map<std::string, GraphEntry> graphs_;
   DevBuf<int32_t> npqin_;
   DevBuf<int32_t> kq_;
+  DevBuf<int> rr_over_;
   DevBuf<uint16_t> codes_bf16_;
   DevBuf<uint64_t> tau_, part2_;
   DevBuf<float> maxnorm_, tile_norm_;

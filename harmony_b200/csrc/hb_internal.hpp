@@ -203,7 +203,7 @@ void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream
 void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
                    const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
                    const uint64_t* part2 = nullptr, const int64_t* slot_base2 = nullptr, int P2 = 0,
-                   const uint64_t* tau = nullptr);
+                   const uint64_t* tau = nullptr, int* overflow = nullptr);
 // Per-query upper bound of the R-th approximate key from the first S <= 256
 // BF16 rows of the query's nearest list (probe rank 0 in the list-major work
 // description); queries without a seed get all ones.  maxnorm = max ||x||.

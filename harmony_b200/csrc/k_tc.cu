@@ -436,16 +436,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
-__global__ void __launch_bounds__(256) rerank_kernel(const uint64_t* __restrict__ part,
+__global__ void __launch_bounds__(512) rerank_kernel(const uint64_t* __restrict__ part,
                                                      const int64_t* __restrict__ slot_base, int P, int R, int k,
                                                      const float* __restrict__ codes, const float* __restrict__ q,
                                                      int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
                                                      int64_t* __restrict__ I, const uint64_t* __restrict__ part2,
                                                      const int64_t* __restrict__ slot_base2, int P2,
-                                                     const uint64_t* __restrict__ tau) {
+                                                     const uint64_t* __restrict__ tau, const int* __restrict__ only) {
   extern __shared__ uint64_t s_keys[];  // pow2(R) approx, then pow2(R) exact
   __shared__ SelectShared sh_sel;
   const int qi = blockIdx.x;
+  if (only && !only[qi]) return;
   const int n2 = pow2_ceil(R < 2 ? 2 : R);
   uint64_t* s_appr = s_keys;
   uint64_t* s_exact = s_keys + n2;
@@ -498,6 +499,93 @@ __global__ void __launch_bounds__(256) rerank_kernel(const uint64_t* __restrict_
   block_bitonic_sort(s_exact, n2);
   for (int j = threadIdx.x; j < k; j += blockDim.x) {
     const uint64_t key = j < n2 ? s_exact[j] : kEmpty;
+    const size_t o = static_cast<size_t>(qi) * k + j;
+    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+  }
+}
+
+// Re-rank with one warp per query: the keys at or under the query's final
+// bound (at most a few times R of them) are compacted by ballot into a
+// per-warp buffer, sorted, the best R recomputed exactly (sequential FP32,
+// one candidate per lane) and sorted again.  A query with more than 8192
+// slot keys or more than kRerankCap keys under its bound is flagged for the
+// CTA kernel.
+constexpr int kRerankCap = 256;
+constexpr int kRerankWarps = 8;
+
+__global__ void __launch_bounds__(kRerankWarps * 32) rerank_warp_kernel(
+    const uint64_t* __restrict__ part, const int64_t* __restrict__ slot_base, int nq, int P, int R, int k,
+    const float* __restrict__ codes, const float* __restrict__ q, int dpad, const int64_t* __restrict__ ids,
+    float* __restrict__ D, int64_t* __restrict__ I, const uint64_t* __restrict__ tau, int* __restrict__ overflow) {
+  __shared__ uint64_t s_cand[kRerankWarps][kRerankCap];
+  __shared__ uint64_t s_ex[kRerankWarps][64];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int qi = blockIdx.x * kRerankWarps + wib;
+  if (qi >= nq) return;
+  uint64_t* cand = s_cand[wib];
+  uint64_t* ex = s_ex[wib];
+  const int64_t s0 = slot_base[static_cast<int64_t>(qi) * P];
+  const int64_t s1 = slot_base[static_cast<int64_t>(qi + 1) * P];
+  const uint64_t* src = part + s0 * kGroups * R;
+  const int m = static_cast<int>((s1 - s0) * kGroups * R);
+  const uint64_t lim = tau[qi];
+  if (m > 256 * 32) {
+    // Many slots (a wide nprobe): the CTA kernel scans them faster.
+    if (lane == 0) overflow[qi] = 1;
+    return;
+  }
+  int cnt = 0;
+#pragma unroll 4
+  for (int base = 0; base < m; base += 32) {
+    const int i = base + lane;
+    const uint64_t key = i < m ? src[i] : kEmpty;
+    const bool pass = key != kEmpty && key <= lim;
+    const unsigned b = __ballot_sync(0xffffffffu, pass);
+    const int pos = cnt + __popc(b & ((1u << lane) - 1u));
+    if (pass && pos < kRerankCap) cand[pos] = key;
+    cnt += __popc(b);
+  }
+  if (cnt > kRerankCap) {
+    if (lane == 0) overflow[qi] = 1;
+    return;
+  }
+  if (lane == 0) overflow[qi] = 0;
+  const int n2 = pow2_ceil(cnt < 2 ? 2 : cnt);
+  for (int i = cnt + lane; i < n2; i += 32) cand[i] = kEmpty;
+  __syncwarp();
+  warp_bitonic_sort(cand, n2, lane);
+  const int nr = min(R, cnt);
+  const float* qrow = q + static_cast<size_t>(qi) * dpad;
+  for (int j = lane; j < 64; j += 32) {
+    uint64_t key = kEmpty;
+    if (j < nr) {
+      const uint32_t pos = key_tie(cand[j]);
+      const float* x = codes + static_cast<size_t>(pos) * dpad;
+      float acc = 0.0f;
+#pragma unroll 8
+      for (int c = 0; c < dpad; c += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(x + c);
+        const float4 w = *reinterpret_cast<const float4*>(qrow + c);
+        float t;
+        t = __fsub_rn(w.x, v.x);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+        t = __fsub_rn(w.y, v.y);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+        t = __fsub_rn(w.z, v.z);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+        t = __fsub_rn(w.w, v.w);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+      }
+      if (acc < FLT_MAX) key = make_key(acc, pos);
+    }
+    ex[j] = key;
+  }
+  __syncwarp();
+  const int e2 = pow2_ceil(nr < 2 ? 2 : nr);
+  warp_bitonic_sort(ex, e2, lane);
+  for (int j = lane; j < k; j += 32) {
+    const uint64_t key = j < e2 ? ex[j] : kEmpty;
     const size_t o = static_cast<size_t>(qi) * k + j;
     D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
     I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
@@ -743,14 +831,28 @@ void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream
 
 void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
                    const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
-                   const uint64_t* part2, const int64_t* slot_base2, int P2, const uint64_t* tau) {
+                   const uint64_t* part2, const int64_t* slot_base2, int P2, const uint64_t* tau, int* overflow) {
   if (nq <= 0) return;
+  if (tau && !part2 && overflow && R <= 64 && nq >= 1024) {
+    // Warp per query; the rare query with too many keys under its bound
+    // goes through the CTA kernel.
+    HB_CHECK(k <= R, HB_ERR_INVALID, "k must not exceed the re-ranked candidates");
+    rerank_warp_kernel<<<(nq + kRerankWarps - 1) / kRerankWarps, kRerankWarps * 32, 0, st>>>(
+        part, slot_base, nq, P, R, k, codes, q, dpad, ids, D, I, tau, overflow);
+    HB_CUDA(cudaGetLastError());
+    const int n2 = pow2_ceil(R < 2 ? 2 : R);
+    const size_t smem = static_cast<size_t>(2 * n2) * 8 + 64;
+    rerank_kernel<<<nq, 512, smem, st>>>(part, slot_base, P, R, k, codes, q, dpad, ids, D, I, nullptr, nullptr, 0, tau,
+                                         overflow);
+    HB_CUDA(cudaGetLastError());
+    return;
+  }
   HB_CHECK(k <= R, HB_ERR_INVALID, "k must not exceed the re-ranked candidates");
   const int n2 = pow2_ceil(R < 2 ? 2 : R);
   const size_t smem = static_cast<size_t>(2 * n2) * 8 + 64;
   // Small batches get wider CTAs (each query's selection is the whole job).
   rerank_kernel<<<nq, nq < 1024 ? 256 : 128, smem, st>>>(part, slot_base, P, R, k, codes, q, dpad, ids, D, I, part2,
-                                                         slot_base2, P2, tau);
+                                                         slot_base2, P2, tau, nullptr);
   HB_CUDA(cudaGetLastError());
 }
 

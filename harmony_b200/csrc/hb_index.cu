@@ -402,8 +402,9 @@ class IndexCore {
                          static_cast<int>(nlist_), st_);
       }
       Scope sc(this, "coarse_select");
+      cflags_.reserve(static_cast<size_t>(nq));
       launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), P, probes_out, cdist_out,
-                         st_);
+                         st_, nullptr, cflags_.p);
       launches_ += 2;
       coarse_last_nq_ = 0;
       return;
@@ -419,7 +420,8 @@ class IndexCore {
     }
     {
       Scope sc(this, "coarse_select");
-      launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), Pm, ccand_.p, cval_.p, st_);
+      launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), Pm, ccand_.p, cval_.p, st_,
+                         nullptr, cflags_.p);
     }
     {
       Scope sc(this, "coarse_refine");
@@ -468,7 +470,7 @@ class IndexCore {
     }
     {
       Scope sc(this, "coarse_select");
-      launch_select_rows(dmat_.p, nq, nl, nl, PmA, ccand_.p, cval_.p, st_);
+      launch_select_rows(dmat_.p, nq, nl, nl, PmA, ccand_.p, cval_.p, st_, nullptr, cflags_.p);
     }
     {
       Scope sc(this, "coarse_refine");
@@ -484,7 +486,7 @@ class IndexCore {
     {
       Scope sc(this, "coarse_widen_select");
       launch_coarse_widths(npq_.p, nq, P, C, coarse_margin_, nl, kq_.p, st_);
-      launch_select_rows(dmat_.p, nq, nl, nl, PmB, ccand_.p, cval_.p, st_, kq_.p);
+      launch_select_rows(dmat_.p, nq, nl, nl, PmB, ccand_.p, cval_.p, st_, kq_.p, cflags_.p);
     }
     {
       Scope sc(this, "coarse_widen_refine");

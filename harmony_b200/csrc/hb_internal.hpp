@@ -125,8 +125,10 @@ size_t scan_exact_smem_bytes(int d, int dpad, int k, int mode, int* tv, int* qt,
 // k_select.cu
 // Row-wise selection of the k smallest (value, column) pairs of a float
 // matrix; out_idx gets columns, out_val the values, ascending.
+// row_flags (optional, nrows ints of scratch): enables the warp-per-row
+// path for k <= 256.
 void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx,
-                        float* out_val, cudaStream_t st, const int32_t* k_row = nullptr);
+                        float* out_val, cudaStream_t st, const int32_t* k_row = nullptr, int* row_flags = nullptr);
 // Build the list-major work description from probes (nq x P, -1 = none).
 void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist,
                        int chunk_rows, int qgroup, int32_t* list_cnt, int64_t* list_qoff,

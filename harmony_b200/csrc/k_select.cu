@@ -64,7 +64,9 @@ template <int VPT>
 __global__ void __launch_bounds__(kSelThreads, 6) select_rows_reg_kernel(const float* __restrict__ D, int ncols, int ldD,
                                                                       int kmax, int32_t* __restrict__ out_idx,
                                                                       float* __restrict__ out_val,
-                                                                      const int32_t* __restrict__ k_row) {
+                                                                      const int32_t* __restrict__ k_row,
+                                                                      const int* __restrict__ only) {
+  if (only && !only[blockIdx.x]) return;
   __shared__ int hist[kBins];
   __shared__ uint64_t s_keys[kCandCap];
   __shared__ SelectShared sh;
@@ -187,6 +189,120 @@ __global__ void __launch_bounds__(kSelThreads, 6) select_rows_reg_kernel(const f
   for (int j = tid; j < k; j += kSelThreads) {
     const uint64_t key = j < kk ? keys[j] : kEmpty;
     const size_t o = static_cast<size_t>(blockIdx.x) * kmax + j;
+    out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
+    if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+  }
+}
+
+// The same selection with one warp per row (4 rows per CTA), for k <= 256
+// and rows of at most 8192 columns with 16-byte aligned rows: three passes
+// over the row from L2 (range, histogram of the keys' high words in a
+// per-warp 1024-bin table, ballot compaction of the keys in and under the
+// k-th key's bin), then a warp bitonic sort.  A row whose candidates exceed
+// kWarpCand is flagged for the CTA kernel.
+constexpr int kSelWarps = 4;
+constexpr int kWarpCand = 512;
+
+__global__ void __launch_bounds__(kSelWarps * 32) select_rows_warp_kernel(
+    const float* __restrict__ D, int nrows, int ncols, int ldD, int kmax, int32_t* __restrict__ out_idx,
+    float* __restrict__ out_val, const int32_t* __restrict__ k_row, int* __restrict__ overflow) {
+  __shared__ int s_hist[kSelWarps][kBins];
+  __shared__ uint64_t s_cand[kSelWarps][kWarpCand];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int r = blockIdx.x * kSelWarps + wib;
+  if (r >= nrows) return;
+  int* hist = s_hist[wib];
+  uint64_t* cand = s_cand[wib];
+  const int k = k_row ? min(k_row[r], kmax) : kmax;
+  overflow[r] = 0;  // every lane writes the same value
+  if (k <= 0) return;
+  const float4* row4 = reinterpret_cast<const float4*>(D + static_cast<size_t>(r) * ldD);
+  const int n4 = ncols >> 2;
+  auto word = [](float v) -> uint32_t { return v < FLT_MAX ? __float_as_uint(v) : 0xFFFFFFFFu; };
+  unsigned lo = 0xFFFFFFFFu, hi = 0;
+  int real = 0;
+#pragma unroll 4
+  for (int i = lane; i < n4; i += 32) {
+    const float4 v = row4[i];
+    const uint32_t u[4] = {word(v.x), word(v.y), word(v.z), word(v.w)};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (u[j] != 0xFFFFFFFFu) {
+        lo = min(lo, u[j]);
+        hi = max(hi, u[j]);
+        ++real;
+      }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    real += __shfl_xor_sync(0xffffffffu, real, o);
+  }
+  const int kk = min(k, real);
+  const float scale = static_cast<float>(kBins) / (static_cast<float>(hi - lo) + 1.0f);
+  auto bin_of = [&](uint32_t x) -> int { return min(kBins - 1, static_cast<int>(static_cast<float>(x - lo) * scale)); };
+  int bstar = kBins, ncand = real;
+  if (kk > 0 && kk < real) {
+    for (int i = lane; i < kBins; i += 32) hist[i] = 0;
+    __syncwarp();
+#pragma unroll 4
+    for (int i = lane; i < n4; i += 32) {
+      const float4 v = row4[i];
+      const uint32_t u[4] = {word(v.x), word(v.y), word(v.z), word(v.w)};
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (u[j] != 0xFFFFFFFFu) atomicAdd(&hist[bin_of(u[j])], 1);
+    }
+    __syncwarp();
+    // Lane L owns bins [32L, 32L + 32).
+    int loc = 0;
+    for (int b = 0; b < 32; ++b) loc += hist[lane * 32 + b];
+    int incl = loc;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int excl = incl - loc;
+    const unsigned owner = __ballot_sync(0xffffffffu, excl < kk && incl >= kk);
+    const int ol = __ffs(owner) - 1;
+    int bb = 0, cum = 0;
+    if (lane == ol) {
+      cum = excl;
+      for (; bb < 32; ++bb) {
+        cum += hist[lane * 32 + bb];
+        if (cum >= kk) break;
+      }
+    }
+    bstar = __shfl_sync(0xffffffffu, ol * 32 + bb, ol);
+    ncand = __shfl_sync(0xffffffffu, cum, ol);
+  }
+  if (ncand > kWarpCand) {
+    overflow[r] = 1;
+    return;
+  }
+  int cnt = 0;
+  for (int i = lane; i < ((n4 + 31) & ~31); i += 32) {
+    uint32_t u[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
+    if (i < n4) {
+      const float4 v = row4[i];
+      u[0] = word(v.x), u[1] = word(v.y), u[2] = word(v.z), u[3] = word(v.w);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const bool take = u[j] != 0xFFFFFFFFu && (bstar >= kBins || bin_of(u[j]) <= bstar);
+      const unsigned b = __ballot_sync(0xffffffffu, take);
+      if (take) cand[cnt + __popc(b & ((1u << lane) - 1u))] =
+          (static_cast<uint64_t>(u[j]) << 32) | static_cast<uint32_t>(4 * i + j);
+      cnt += __popc(b);
+    }
+  }
+  const int n2 = pow2_ceil(max(cnt, 2));
+  for (int i = cnt + lane; i < n2; i += 32) cand[i] = kEmpty;
+  __syncwarp();
+  warp_bitonic_sort(cand, n2, lane);
+  for (int j = lane; j < k; j += 32) {
+    const uint64_t key = j < kk ? cand[j] : kEmpty;
+    const size_t o = static_cast<size_t>(r) * kmax + j;
     out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
     if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
   }
@@ -346,21 +462,29 @@ void exclusive_sum(const int64_t* in, int64_t* out, size_t n, void* tmp, size_t 
 }  // namespace
 
 void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx, float* out_val,
-                        cudaStream_t st, const int32_t* k_row) {
+                        cudaStream_t st, const int32_t* k_row, int* row_flags) {
   if (nrows <= 0 || k <= 0) return;
+  const int* only = nullptr;
+  if (row_flags && k <= 256 && ncols <= 8192 && ncols % 4 == 0 && ldD % 4 == 0) {
+    // Warp per row; rows it flags go through the CTA kernel below.
+    select_rows_warp_kernel<<<(nrows + kSelWarps - 1) / kSelWarps, kSelWarps * 32, 0, st>>>(
+        D, nrows, ncols, ldD, k, out_idx, out_val, k_row, row_flags);
+    HB_CUDA(cudaGetLastError());
+    only = row_flags;
+  }
   HB_CHECK(k <= kMaxSelect, HB_ERR_INVALID, "nprobe above 8192 is not supported");
   HB_CHECK(!k_row || (k <= 1024 && ncols <= 32 * kSelThreads), HB_ERR_INVALID,
            "per-row widths need k <= 1024 and at most 8192 columns");
   if (k <= 1024 && ncols <= 32 * kSelThreads) {
     const int vpt = (ncols + kSelThreads - 1) / kSelThreads;
     if (vpt <= 4)
-      select_rows_reg_kernel<4><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row);
+      select_rows_reg_kernel<4><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row, only);
     else if (vpt <= 8)
-      select_rows_reg_kernel<8><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row);
+      select_rows_reg_kernel<8><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row, only);
     else if (vpt <= 16)
-      select_rows_reg_kernel<16><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row);
+      select_rows_reg_kernel<16><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row, only);
     else
-      select_rows_reg_kernel<32><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row);
+      select_rows_reg_kernel<32><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row, only);
     HB_CUDA(cudaGetLastError());
     return;
   }

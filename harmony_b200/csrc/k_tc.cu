@@ -615,10 +615,10 @@ __global__ void split_probes_kernel(const int32_t* __restrict__ probes, int nq, 
 // of the scan's top R.
 //
 // List-major: one CTA per list stages the list's first S BF16 rows in shared
-// memory once; each query whose nearest list it is (probe rank 0 in the
-// list-major work description) takes one warp: lanes own rows, the query is
-// broadcast from shared memory, the S values are sorted in a per-warp buffer
-// and the R-th gives the bound.
+// memory once; for each query whose nearest list it is (probe rank 0 in the
+// list-major work description) in turn, thread t computes row t's value with
+// the query broadcast from shared memory, and a 32-step radix selection over
+// the CTA (one barrier count per bit) finds the R-th smallest.
 constexpr int kSeedRows = 256;
 constexpr int kSeedWarps = 8;
 
@@ -631,6 +631,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
   __shared__ float s_xn[kSeedRows];
   __shared__ int s_qs[kSeedWarps * 32];
   __shared__ int s_nq;
+  __shared__ float s_qn;
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   // One CTA per list (its rows serve every query whose nearest list it is),
   // or, for small batches (probes given), one CTA per query.
@@ -653,13 +654,9 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
   const int64_t b = list_off[l];
   const int n = static_cast<int>(min(static_cast<int64_t>(S), list_off[l + 1] - b));
   if (n < R) return;  // no seed: tau stays empty
-  const int n2 = pow2_ceil(n < 2 ? 2 : n);
   const int stride = kpad * 2 + 16;  // bytes per staged row (padding spreads banks)
   uint8_t* rows = s_seed_raw;
-  float* qbuf = reinterpret_cast<float*>(s_seed_raw + static_cast<size_t>(S) * stride) + wib * kpad;
-  uint64_t* buf = reinterpret_cast<uint64_t*>(s_seed_raw + static_cast<size_t>(S) * stride +
-                                              static_cast<size_t>(kSeedWarps) * kpad * 4) +
-                  static_cast<size_t>(wib) * kSeedRows;
+  float* qbuf = reinterpret_cast<float*>(s_seed_raw + static_cast<size_t>(S) * stride);
   const int cpr = kpad / 8;  // 16-byte chunks per row
   for (int i = tid; i < n * cpr; i += blockDim.x) {
     const int r = i / cpr, c = i - r * cpr;
@@ -681,50 +678,57 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
     }
     __syncthreads();
     const int nqr = s_nq;
-    for (int t = wib; t < nqr; t += kSeedWarps) {
+    // Each query in turn, the whole CTA: thread t takes row t, then a
+    // 32-step radix selection over the CTA finds the R-th smallest value.
+    for (int t = 0; t < nqr; ++t) {
       const int qi = s_qs[t];
       const float* qrow = q + static_cast<size_t>(qi) * dpad;
-      float qn = 0.0f;
-      for (int c = lane; c < kpad; c += 32) {
-        const float x = c < dpad ? qrow[c] : 0.0f;
-        qn = fmaf(x, x, qn);
-        qbuf[c] = __bfloat162float(__float2bfloat16_rn(x));
+      for (int c = tid; c < kpad; c += blockDim.x) qbuf[c] = c < dpad ? __bfloat162float(__float2bfloat16_rn(qrow[c])) : 0.0f;
+      if (wib == 0) {
+        float qn = 0.0f;
+        for (int c = lane; c < dpad; c += 32) qn = fmaf(qrow[c], qrow[c], qn);
+        for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(0xffffffffu, qn, o);
+        if (lane == 0) s_qn = qn;
       }
-      for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(0xffffffffu, qn, o);
-      __syncwarp();
-      for (int r = lane; r < n2; r += 32) {
-        uint64_t key = kEmpty;
-        if (r < n) {
-          const uint8_t* xr = rows + static_cast<size_t>(r) * stride;
-          // Four partial sums (any order is within the margin).
-          float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
+      __syncthreads();
+      uint32_t key = 0xFFFFFFFFu;
+      if (tid < n) {
+        const uint8_t* xr = rows + static_cast<size_t>(tid) * stride;
+        // Four partial sums (any order is within the margin).
+        float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
 #pragma unroll 4
-          for (int c = 0; c < kpad; c += 8) {
-            const uint4 xv = *reinterpret_cast<const uint4*>(xr + c * 2);
-            const float4 qa = *reinterpret_cast<const float4*>(qbuf + c);
-            const float4 qb = *reinterpret_cast<const float4*>(qbuf + c + 4);
-            d0 = fmaf(qa.x, __uint_as_float(xv.x << 16), d0);
-            d1 = fmaf(qa.y, __uint_as_float(xv.x & 0xffff0000u), d1);
-            d2 = fmaf(qa.z, __uint_as_float(xv.y << 16), d2);
-            d3 = fmaf(qa.w, __uint_as_float(xv.y & 0xffff0000u), d3);
-            d0 = fmaf(qb.x, __uint_as_float(xv.z << 16), d0);
-            d1 = fmaf(qb.y, __uint_as_float(xv.z & 0xffff0000u), d1);
-            d2 = fmaf(qb.z, __uint_as_float(xv.w << 16), d2);
-            d3 = fmaf(qb.w, __uint_as_float(xv.w & 0xffff0000u), d3);
-          }
-          const float val = fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[r]);
-          key = (static_cast<uint64_t>(ordered_bits(val)) << 32) | static_cast<uint32_t>(r);
+        for (int c = 0; c < kpad; c += 8) {
+          const uint4 xv = *reinterpret_cast<const uint4*>(xr + c * 2);
+          const float4 qa = *reinterpret_cast<const float4*>(qbuf + c);
+          const float4 qb = *reinterpret_cast<const float4*>(qbuf + c + 4);
+          d0 = fmaf(qa.x, __uint_as_float(xv.x << 16), d0);
+          d1 = fmaf(qa.y, __uint_as_float(xv.x & 0xffff0000u), d1);
+          d2 = fmaf(qa.z, __uint_as_float(xv.y << 16), d2);
+          d3 = fmaf(qa.w, __uint_as_float(xv.y & 0xffff0000u), d3);
+          d0 = fmaf(qb.x, __uint_as_float(xv.z << 16), d0);
+          d1 = fmaf(qb.y, __uint_as_float(xv.z & 0xffff0000u), d1);
+          d2 = fmaf(qb.z, __uint_as_float(xv.w << 16), d2);
+          d3 = fmaf(qb.w, __uint_as_float(xv.w & 0xffff0000u), d3);
         }
-        buf[r] = key;
+        key = ordered_bits(fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[tid]));
       }
-      __syncwarp();
-      warp_bitonic_sort(buf, n2, lane);
-      if (lane == 0) {
-        const float vR = ordered_to_float(static_cast<uint32_t>(buf[R - 1] >> 32));
-        const float margin = 1e-3f * sqrtf(qn) * mn + 2e-5f * (mn * mn + fabsf(vR)) + 1e-30f;
+      uint32_t prefix = 0;
+      int need = R;
+      for (int bit = 31; bit >= 0; --bit) {
+        const uint32_t hmask = bit == 31 ? 0u : (0xFFFFFFFFu << (bit + 1));
+        const bool zero_here = (key & hmask) == prefix && ((key >> bit) & 1u) == 0u;
+        const int c0 = __syncthreads_count(zero_here);
+        if (c0 < need) {
+          need -= c0;
+          prefix |= 1u << bit;
+        }
+      }
+      if (tid == 0) {
+        const float vR = ordered_to_float(prefix);
+        const float margin = 1e-3f * sqrtf(s_qn) * mn + 2e-5f * (mn * mn + fabsf(vR)) + 1e-30f;
         tau[qi] = (static_cast<uint64_t>(ordered_bits(vR + margin)) << 32) | 0xffffffffull;
       }
-      __syncwarp();
+      __syncthreads();
     }
     __syncthreads();
   }
@@ -863,8 +867,7 @@ void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* cod
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
   HB_CHECK(S >= 1 && S <= kSeedRows && R >= 1 && R <= S, HB_ERR_INVALID, "seed sample out of range");
   HB_CUDA(cudaMemsetAsync(tau, 0xff, static_cast<size_t>(nq) * sizeof(uint64_t), st));
-  const size_t smem = static_cast<size_t>(S) * (kpad * 2 + 16) + static_cast<size_t>(kSeedWarps) * kpad * 4 +
-                      static_cast<size_t>(kSeedWarps) * kSeedRows * 8;
+  const size_t smem = static_cast<size_t>(S) * (kpad * 2 + 16) + static_cast<size_t>(kpad) * 4;
   HB_CUDA(cudaFuncSetAttribute(tau_seed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const bool by_query = probes && static_cast<long long>(nq) * 4 < nlist;
   tau_seed_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(

@@ -1615,11 +1615,10 @@ class IndexCore {
   DevBuf<int32_t> kq_;
   DevBuf<int> rr_over_;
   DevBuf<uint16_t> codes_bf16_;
-  DevBuf<uint64_t> tau_, part2_;
+  DevBuf<uint64_t> tau_;
   DevBuf<float> maxnorm_, tile_norm_;
   DevBuf<int64_t> tile_off_;
-  DevBuf<int64_t> slot_base2_;
-  DevBuf<int32_t> probes1_, probes2_;
+  DevBuf<int32_t> probes1_;
   DevBuf<int> err_dev_;
   int* err_host_ = nullptr;
   bool prof_ = false;

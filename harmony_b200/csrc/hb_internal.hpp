@@ -216,7 +216,6 @@ void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* cod
 // *out = max over i of sqrt(norms[i]) (slightly rounded up), on the device.
 void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st);
 // probes (nq x P) -> first column (nq x 1) and the rest (nq x (P-1)).
-void launch_split_probes(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st);
 
 // k_coarse_tc.cu: tensor-core coarse quantizer (3-term BF16 split) with an
 // exact FP32 finish; the probe rows equal the exact quantizer's.

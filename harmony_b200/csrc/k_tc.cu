@@ -592,15 +592,6 @@ __global__ void __launch_bounds__(kRerankWarps * 32) rerank_warp_kernel(
   }
 }
 
-__global__ void split_probes_kernel(const int32_t* __restrict__ probes, int nq, int P, int32_t* __restrict__ first,
-                                    int32_t* __restrict__ rest) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= nq * P) return;
-  const int q = idx / P, j = idx - q * P;
-  if (j == 0) first[q] = probes[idx];
-  else rest[static_cast<size_t>(q) * (P - 1) + (j - 1)] = probes[idx];
-}
-
 // Upper bound of each query's R-th approximate key before the scan, from the
 // first S rows of the query's nearest list.  The bound is computed from the
 // same BF16 operands the scan multiplies (the query rounded to BF16 exactly
@@ -891,12 +882,6 @@ void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st) 
     max_norm_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(norms, n, out);
   }
   sqrt_inplace_kernel<<<1, 1, 0, st>>>(out);
-  HB_CUDA(cudaGetLastError());
-}
-
-void launch_split_probes(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st) {
-  if (nq <= 0) return;
-  split_probes_kernel<<<(nq * P + 255) / 256, 256, 0, st>>>(probes, nq, P, first, rest);
   HB_CUDA(cudaGetLastError());
 }
 

@@ -67,6 +67,39 @@ __device__ __forceinline__ void block_bitonic_sort(uint64_t* s, int n) {
   }
 }
 
+// Monotone map of a float to uint32 (all signs), and its inverse.
+__device__ __forceinline__ uint32_t ordered_bits(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ordered_to_float(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// Squared L2 distance of one stored row and one query row (both padded to
+// dpad, a multiple of 4, with zeros) with the reference's sequential
+// unfused FP32 loop, src/utils.h:480-487: t = q - x, sum += t * t, each
+// operation rounded on its own, dimensions in order.  The zero padding adds
+// exact zeros.
+__device__ __forceinline__ float exact_l2_seq(const float* __restrict__ x, const float* __restrict__ qrow, int dpad) {
+  float acc = 0.0f;
+#pragma unroll 8
+  for (int c = 0; c < dpad; c += 4) {
+    const float4 v = *reinterpret_cast<const float4*>(x + c);
+    const float4 w = *reinterpret_cast<const float4*>(qrow + c);
+    float t;
+    t = __fsub_rn(w.x, v.x);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(w.y, v.y);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(w.z, v.z);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(w.w, v.w);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+  }
+  return acc;
+}
+
 __host__ __device__ __forceinline__ int pow2_ceil(int x) {
   int p = 1;
   while (p < x) p <<= 1;

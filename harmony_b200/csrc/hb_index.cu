@@ -355,11 +355,12 @@ class IndexCore {
   }
 
   // BF16 copy of the codes (rows padded to kpad = d rounded up to 64) and its
-  // TMA tensor map, for the tensor-core scan (d <= 128).
+  // TMA tensor map, for the tensor-core scans (the heap scan takes d <= 128,
+  // the candidate-matrix scan any d).
   void build_bf16() {
     bf16_ready_ = false;
     kpad_ = static_cast<int>((d_ + 63) / 64 * 64);
-    if (kpad_ > 128 || ntotal_ == 0) return;
+    if (ntotal_ == 0) return;
     codes_bf16_.reserve(ntotal_ * static_cast<size_t>(kpad_));
     launch_to_bf16(codes_.p, ntotal_, static_cast<int>(dpad_), kpad_, codes_bf16_.p, st_);
     ++launches_;
@@ -571,15 +572,19 @@ class IndexCore {
     if (bf16) {
       HB_CHECK(p.mode == HB_MODE_ORIGINAL || p.mode == HB_MODE_BRUTE_FORCE, HB_ERR_INVALID,
                "the BF16 scan implements ORIGINAL / BRUTE_FORCE search (pruning and the dimension relay are FP32 modes)");
-      HB_CHECK(ntotal_ == 0 || bf16_ready_, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
+      HB_CHECK(ntotal_ == 0 || bf16_ready_, HB_ERR_STATE, "BF16 codes not built");
     }
     HB_CHECK(p.seed_rows >= 0 && p.seed_rows <= 256, HB_ERR_INVALID, "seed_rows must be in [0, 256]");
     seed_rows_ = p.seed_rows > 0 ? p.seed_rows : 256;
+    // BF16 route: the shared-memory heap scan for d <= 128 and k up to its
+    // candidate capacity, else the candidate-matrix scan.
     const int max_R = bf16 ? scan_bf16_max_R(kpad_ > 0 ? kpad_ : 128) : 0;
-    const int R = bf16 ? std::min(max_R, std::max(static_cast<int>(k), p.rerank_mult * static_cast<int>(k))) : 0;
+    const int want_R = std::max(static_cast<int>(k), p.rerank_mult * static_cast<int>(k));
+    cand_path_ = bf16 && !(kpad_ <= 128 && static_cast<int>(k) <= max_R);
+    const int R = !bf16 ? 0 : cand_path_ ? std::min(kCandMaxR, want_R) : std::min(max_R, want_R);
     if (bf16)
       HB_CHECK(static_cast<int>(k) <= R, HB_ERR_INVALID,
-               "BF16 search supports k up to " + std::to_string(max_R) + " at this dimension");
+               "BF16 search supports k up to " + std::to_string(kCandMaxR));
     int mode = SCAN_PLAIN;
     size_t P = nprobe_;
     int W = 1, B = 1;
@@ -631,7 +636,8 @@ class IndexCore {
 
     const bool dev_out = is_device_ptr(D) && is_device_ptr(I);
     const bool dev_in = is_device_ptr(q);
-    const size_t bs = std::min<size_t>(nq, batch_limit(P, k));
+    size_t bs = std::min<size_t>(nq, batch_limit(P, k));
+    if (cand_path_ && P > 0) bs = std::min(bs, cand_batch_limit(P));
     const int warm_lists = p.warmup_lists;
     const int warm_size = p.warmup_list_size > 0 ? p.warmup_list_size : static_cast<int>(k);
     // DIVIDE_DIM query blocks cover queries [0, B * (nq / B)); the rest stay
@@ -1239,6 +1245,10 @@ class IndexCore {
   // over all probes (items tighten the shared bound as they finish), and
   // the exact FP32 re-rank.
   void search_batch_bf16(int nb, int P, int k, int R, float* Dd, int64_t* Id) {
+    if (cand_path_) {
+      search_batch_cand(nb, P, k, R, Dd, Id);
+      return;
+    }
     probes_.reserve(static_cast<size_t>(nb) * P);
     coarse_and_cut(nb, P);
     err_dev_.reserve(1);
@@ -1250,6 +1260,97 @@ class IndexCore {
       Scope sc(this, "rerank");
       launch_rerank(part_.p, slot_base_.p, nb, P, R, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd, Id,
                     st_, nullptr, nullptr, 0, tau_.p, rr_over_.p);
+    }
+    ++launches_;
+    if (!capturing_) bf16_err_check();
+  }
+
+  // Longest candidate row a query can have at nprobe P: the P largest lists,
+  // each rounded up to 4 entries.
+  int64_t cand_row_bound(int P) {
+    std::vector<int64_t> n(nlist_);
+    for (size_t l = 0; l < nlist_; ++l) n[l] = (host_off_[l + 1] - host_off_[l] + 3) & ~int64_t(3);
+    const size_t take = std::min<size_t>(static_cast<size_t>(P), nlist_);
+    std::partial_sort(n.begin(), n.begin() + take, n.end(), std::greater<int64_t>());
+    int64_t s = 0;
+    for (size_t i = 0; i < take; ++i) s += n[i];
+    return s;
+  }
+
+  // Queries per batch of the candidate-matrix scan: at most 2^30 candidate
+  // entries (4 GiB) and 2 GiB of gathered BF16 queries.
+  size_t cand_batch_limit(size_t P) {
+    const int64_t L = std::max<int64_t>(cand_row_bound(static_cast<int>(P)), 1);
+    HB_CHECK(L <= (int64_t(1) << 30), HB_ERR_INVALID, "candidate row of one query above 2^30 entries");
+    const size_t by_cand = static_cast<size_t>((int64_t(1) << 30) / L);
+    const size_t by_q = (size_t(2) << 30) / (P * static_cast<size_t>(kpad_) * 2);
+    return std::max<size_t>(1, std::min(by_cand, by_q));
+  }
+
+  // BF16 search of one batch through the candidate matrix: exact coarse
+  // probes, the list-major work description, every probed row's
+  // approximate value on the tensor cores, then per query the R smallest
+  // re-ranked exactly.
+  void search_batch_cand(int nb, int P, int k, int R, float* Dd, int64_t* Id) {
+    probes_.reserve(static_cast<size_t>(nb) * P);
+    coarse_and_cut(nb, P);
+    err_dev_.reserve(1);
+    HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
+    const int cr = std::max(128, chunk_rows_for(nb, P, 128));
+    const size_t nqp = static_cast<size_t>(nb) * P;
+    list_cnt_.reserve(nlist_);
+    list_cursor_.reserve(nlist_);
+    list_qoff_.reserve(nlist_ + 1);
+    item_off_.reserve(nlist_ + 1);
+    list_q_.reserve(nqp);
+    slot_base_.reserve(nqp + 1);
+    const size_t wtmp = std::max(build_work_tmp_bytes(nb, P, static_cast<int>(nlist_)), cand_segments_tmp_bytes(nb, P));
+    work_tmp_.reserve(wtmp);
+    {
+      Scope sc(this, "build_work");
+      launch_build_work(probes_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p, list_qoff_.p,
+                        list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+    }
+    launches_ += 3;
+    seg_.reserve(nqp + 1);
+    {
+      Scope sc(this, "cand_segments");
+      launch_cand_segments(probes_.p, nb, P, list_off_.p, seg_.p, work_tmp_.p, wtmp, st_);
+    }
+    launches_ += 2;
+    gq_.reserve(nqp * static_cast<size_t>(kpad_));
+    {
+      Scope sc(this, "gather_queries");
+      launch_gather_queries(qpad_.p, static_cast<int>(dpad_), kpad_, list_q_.p, list_qoff_.p + nlist_,
+                            static_cast<int64_t>(nqp), gq_.p, st_);
+    }
+    ++launches_;
+    make_bf16_tensor_map(gqmap_, gq_.p, nqp, kpad_);
+    cand_.reserve(std::max<size_t>(static_cast<size_t>(nb) * cand_row_bound(P), 1));
+    CandArgs a{};
+    a.list_off = list_off_.p;
+    a.nlist = static_cast<int>(nlist_);
+    a.kpad = kpad_;
+    a.tile_norm = tile_norm_.p;
+    a.tile_off = tile_off_.p;
+    a.list_cnt = list_cnt_.p;
+    a.list_qoff = list_qoff_.p;
+    a.list_q = list_q_.p;
+    a.item_off = item_off_.p;
+    a.chunk_rows = cr;
+    a.P = P;
+    a.seg = seg_.p;
+    a.cand = cand_.p;
+    a.err = err_dev_.p;
+    {
+      Scope sc(this, "cand_scan");
+      launch_cand_scan(gqmap_, tmap_, a, num_sms_, st_);
+    }
+    ++launches_;
+    {
+      Scope sc(this, "cand_rerank");
+      launch_cand_rerank(cand_.p, seg_.p, probes_.p, nb, P, R, k, list_off_.p, codes_.p, qpad_.p,
+                         static_cast<int>(dpad_), ids_.p, Dd, Id, st_);
     }
     ++launches_;
     if (!capturing_) bf16_err_check();
@@ -1597,6 +1698,11 @@ class IndexCore {
   int kpad_ = 0;
   bool bf16_ready_ = false;
   alignas(64) unsigned char tmap_[128];
+  alignas(64) unsigned char gqmap_[128];  // gathered BF16 queries of the candidate-matrix scan
+  bool cand_path_ = false;
+  DevBuf<int64_t> seg_;
+  DevBuf<uint16_t> gq_;
+  DevBuf<float> cand_;
   // tensor-core coarse quantizer
   bool coarse_ready_ = false;
   int coarse_kind_ = HB_COARSE_AUTO;

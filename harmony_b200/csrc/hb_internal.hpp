@@ -197,6 +197,36 @@ void launch_tile_norms(const float* norms, const int64_t* list_off, int nlist, c
 int scan_bf16_keys_per_slot(int R);  // keys each (query, chunk) slot holds
 int scan_bf16_max_R(int kpad);       // largest candidate count per query the scan holds
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);
+
+// Candidate-matrix BF16 scan (k_cand.cu): any kpad (a multiple of 64) and up
+// to kCandMaxR candidates per query.
+constexpr int kCandMaxR = 4096;
+struct CandArgs {
+  const int64_t* list_off;
+  int nlist;
+  int kpad;
+  const float* tile_norm;   // as TcArgs
+  const int64_t* tile_off;
+  const int32_t* list_cnt;  // the list-major work description (launch_build_work, groups of 128)
+  const int64_t* list_qoff;
+  const int32_t* list_q;
+  const int64_t* item_off;
+  int chunk_rows;           // multiple of 128
+  int P;
+  const int64_t* seg;       // nq x P + 1: start of each (query, probe rank) segment of `cand`
+  float* cand;              // candidate rows: ||x||^2 - 2 q~.x~, +inf padding
+  int* err;
+};
+size_t cand_segments_tmp_bytes(int nq, int P);
+void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* list_off, int64_t* seg, void* tmp,
+                          size_t tmp_bytes, cudaStream_t st);
+// Row e of G = BF16 query of list-major entry e, for e < min(*n_entries, max_rows).
+void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* list_q, const int64_t* n_entries,
+                           int64_t max_rows, void* G, cudaStream_t st);
+void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st);
+void launch_cand_rerank(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R, int k,
+                        const int64_t* list_off, const float* codes, const float* q, int dpad, const int64_t* ids,
+                        float* D, int64_t* I, cudaStream_t st);
 void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st);
 void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st);
 // Re-rank over the slots of one or two scan passes (part2 may be null);

@@ -1,0 +1,403 @@
+// BF16 tensor-core list scan through a candidate matrix, for the searches the
+// shared-memory heap scan (k_tc.cu) does not hold: vectors wider than 128
+// dimensions and more than 64 candidates per query.
+//
+//  1. gather_queries_kernel writes, for every (list, query probing it) entry
+//     of the list-major work description, the query in BF16 (K = kpad, zero
+//     padded): one row per entry, so the queries of one work item are 128
+//     consecutive rows and reach the tensor cores by plain TMA tiles.
+//  2. cand_scan_kernel: persistent, one CTA per SM, 192 threads (4 epilogue
+//     warps, a TMA warp, an MMA warp).  Work items are (list, chunk of rows,
+//     group of <= 128 queries).  For each 128-row tile of the chunk the TMA
+//     warp streams 64-column K blocks of both operands (queries: A, 128 x 64;
+//     rows: B, 128 x 64; 128-byte swizzle) into a ring of 32 KB stages, the
+//     MMA warp issues tcgen05.mma M128 x N128 x K16 into one of two TMEM
+//     accumulators, and the epilogue (thread = query, TMEM lane) writes
+//     v = ||x||^2 - 2 q~.x~ of the tile's rows into the query's candidate
+//     row: the concatenation over its probes, in probe order, of one segment
+//     per probed list (the list's length rounded up to 4; +inf past the end).
+//  3. cand_rerank_kernel: one CTA per query selects the R smallest keys
+//     (v, position) of its candidate row (block radix selection, unique keys
+//     so the choice is deterministic), maps each position back to its stored
+//     row, recomputes the distance with the reference's sequential unfused
+//     FP32 loop and returns the k best (distance, row) -- the same rule as
+//     the heap scan's rerank, so whenever the true k nearest are among the R
+//     candidates the result equals the exact scan's.
+// Every mbarrier wait is bounded; on a timeout the kernel records an error
+// code, the roles stop, copies and MMAs in flight are waited for and TMEM is
+// freed.
+#include <cudaTypedefs.h>
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cub/cub.cuh>
+
+#include "hb_device.cuh"
+#include "hb_internal.hpp"
+#include "hb_select.cuh"
+#include "hb_sm100.cuh"
+
+namespace hb {
+namespace {
+
+using namespace sm100;
+
+constexpr int kT = 128;                    // rows per tile = queries per group
+constexpr int kStg = 6;                    // ring stages
+constexpr int kThreads = 192;              // 4 epilogue warps, TMA warp, MMA warp
+constexpr uint32_t kBlk = kT * 128;        // one 128-row x 64-column BF16 block (16 KB)
+constexpr uint32_t kStageBytes = 2 * kBlk;  // A block + B block
+constexpr int kRerankThreads = 512;
+
+struct CandShared {
+  uint64_t full[kStg];
+  uint64_t empty[kStg];
+  uint64_t accf[2];
+  uint64_t acce[2];
+  uint64_t drain;
+  uint32_t tmem;
+};
+
+struct CandItem {
+  int list, chunk, group, qcnt, ntiles;
+  int64_t row0;   // first stored row of the chunk
+  int64_t tile0;  // its first 128-row norm tile
+  int64_t qrow0;  // first query row of the group in the gathered matrix
+};
+
+__device__ __forceinline__ CandItem cand_item(const CandArgs& a, int64_t item) {
+  int lo = 0, hi = a.nlist;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a.item_off[mid] <= item) lo = mid; else hi = mid;
+  }
+  CandItem d;
+  const int l = lo;
+  const int64_t local = item - a.item_off[l];
+  const int ng = (a.list_cnt[l] + kT - 1) / kT;
+  d.list = l;
+  d.chunk = static_cast<int>(local / ng);
+  d.group = static_cast<int>(local % ng);
+  d.qcnt = min(kT, a.list_cnt[l] - d.group * kT);
+  const int64_t r0 = a.list_off[l] + static_cast<int64_t>(d.chunk) * a.chunk_rows;
+  const int64_t r1 = min(a.list_off[l + 1], r0 + static_cast<int64_t>(a.chunk_rows));
+  d.row0 = r0;
+  d.ntiles = static_cast<int>((r1 - r0 + kT - 1) / kT);
+  d.tile0 = a.tile_off[l] + static_cast<int64_t>(d.chunk) * (a.chunk_rows / kT);
+  d.qrow0 = a.list_qoff[l] + static_cast<int64_t>(d.group) * kT;
+  return d;
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    cand_scan_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_x,
+                     CandArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ CandShared sh;
+  uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nkb = a.kpad / 64;
+  const int64_t total = a.item_off[a.nlist];
+
+  if (warp == 5) tmem_alloc(&sh.tmem, 256);
+  if (tid == 0) {
+    for (int s = 0; s < kStg; ++s) {
+      mbar_init(&sh.full[s], 1);
+      mbar_init(&sh.empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&sh.accf[b], 1);
+      mbar_init(&sh.acce[b], 128);
+    }
+    mbar_init(&sh.drain, 1);
+    fence_barrier_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh.tmem;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      prefetch_tmap(&tmap_q);
+      prefetch_tmap(&tmap_x);
+      int64_t it = 0;
+      bool ok = true;
+      for (int64_t item = blockIdx.x; ok && item < total; item += gridDim.x) {
+        const CandItem d = cand_item(a, item);
+        for (int t = 0; ok && t < d.ntiles; ++t) {
+          for (int kb = 0; kb < nkb; ++kb, ++it) {
+            const int s = static_cast<int>(it % kStg);
+            if (!mbar_wait(&sh.empty[s], static_cast<uint32_t>((it / kStg) & 1) ^ 1u, a.err, 31)) {
+              ok = false;
+              break;
+            }
+            uint8_t* st = ring + static_cast<size_t>(s) * kStageBytes;
+            mbar_arrive_expect_tx(&sh.full[s], kStageBytes);
+            tma_load_2d(st, &tmap_q, kb * 64, static_cast<int>(d.qrow0), &sh.full[s]);
+            tma_load_2d(st + kBlk, &tmap_x, kb * 64, static_cast<int>(d.row0 + static_cast<int64_t>(t) * kT),
+                        &sh.full[s]);
+          }
+        }
+      }
+      // Every issued copy lands before the CTA may exit: wait for the last
+      // phase issued on each stage (already complete on the normal path).
+      for (int64_t j = it - 1; j >= 0 && j >= it - kStg; --j)
+        mbar_wait(&sh.full[j % kStg], static_cast<uint32_t>((j / kStg) & 1), nullptr, 0, 200000000LL);
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(kT, kT);
+      const uint32_t rbase = smem_u32(ring);
+      int64_t it = 0, tile = 0;
+      bool ok = true;
+      for (int64_t item = blockIdx.x; ok && item < total; item += gridDim.x) {
+        const CandItem d = cand_item(a, item);
+        for (int t = 0; t < d.ntiles; ++t, ++tile) {
+          const int b = static_cast<int>(tile & 1);
+          if (!mbar_wait(&sh.acce[b], static_cast<uint32_t>((tile >> 1) & 1) ^ 1u, a.err, 33)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          for (int kb = 0; kb < nkb; ++kb, ++it) {
+            const int s = static_cast<int>(it % kStg);
+            if (!mbar_wait(&sh.full[s], static_cast<uint32_t>((it / kStg) & 1), a.err, 32)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t sa = rbase + static_cast<uint32_t>(s) * kStageBytes;
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+              mma_bf16(tmem + static_cast<uint32_t>(b * kT), desc_sw128(sa + kk * 32u),
+                       desc_sw128(sa + kBlk + kk * 32u), idesc, (kb | kk) != 0 ? 1u : 0u);
+            mma_commit(&sh.empty[s]);
+          }
+          if (!ok) break;
+          mma_commit(&sh.accf[b]);
+        }
+      }
+      // The tensor cores must be done before TMEM is released: one more
+      // commit tracks every MMA issued, on the normal and the error path.
+      if (it > 0) {
+        mma_commit(&sh.drain);
+        mbar_wait(&sh.drain, 0u, nullptr, 0, 200000000LL);
+      }
+    }
+  } else {
+    const uint32_t lane_base = (32u * static_cast<uint32_t>(warp)) << 16;
+    int64_t tile = 0;
+    bool ok = true;
+    for (int64_t item = blockIdx.x; ok && item < total; item += gridDim.x) {
+      const CandItem d = cand_item(a, item);
+      // This thread's query (lane tid of the group) and its segment.
+      int64_t sbase = 0, slen = 0;
+      if (tid < d.qcnt) {
+        const uint32_t e = static_cast<uint32_t>(a.list_q[d.qrow0 + tid]);
+        const int64_t qp = static_cast<int64_t>(e >> 16) * a.P + (e & 0xffffu);
+        sbase = a.seg[qp];
+        slen = a.seg[qp + 1] - sbase;
+      }
+      for (int t = 0; t < d.ntiles; ++t, ++tile) {
+        const int b = static_cast<int>(tile & 1);
+        if (ok) ok = mbar_wait(&sh.accf[b], static_cast<uint32_t>((tile >> 1) & 1), a.err, 34);
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        tc_fence_after();
+        const int64_t rl0 = static_cast<int64_t>(d.chunk) * a.chunk_rows + static_cast<int64_t>(t) * kT;
+        const float* tn = a.tile_norm + (d.tile0 + t) * kT;
+#pragma unroll 1
+        for (int c = 0; c < kT / 32; ++c) {
+          uint32_t r[32];
+          tmem_ld32(tmem + lane_base + static_cast<uint32_t>(b * kT + c * 32), r);
+          tmem_ld_wait();
+          const int64_t o = rl0 + c * 32;
+          if (o < slen) {
+            float* out = a.cand + sbase + o;
+#pragma unroll
+            for (int j4 = 0; j4 < 8; ++j4) {
+              if (o + 4 * j4 < slen) {
+                const float4 nm = *reinterpret_cast<const float4*>(tn + c * 32 + 4 * j4);
+                float4 v;
+                v.x = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 0]), nm.x);
+                v.y = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), nm.y);
+                v.z = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), nm.z);
+                v.w = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), nm.w);
+                *reinterpret_cast<float4*>(out + 4 * j4) = v;
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&sh.acce[b]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
+  }
+}
+
+// Row e of the gathered matrix = the query of list-major entry e in BF16
+// (columns past dpad zero).  Entries are (query << 16 | probe rank).
+__global__ void gather_queries_kernel(const float* __restrict__ q, int dpad, int kpad,
+                                      const int32_t* __restrict__ list_q, const int64_t* __restrict__ n_entries,
+                                      int64_t max_rows, __nv_bfloat16* __restrict__ G) {
+  const int64_t rows = min(*n_entries, max_rows);
+  const int per_row = kpad / 8;
+  const int64_t total = rows * per_row;
+  for (int64_t u = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; u < total;
+       u += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t e = u / per_row;
+    const int c = static_cast<int>(u - e * per_row) * 8;
+    const int qi = static_cast<int>(static_cast<uint32_t>(list_q[e]) >> 16);
+    const float* src = q + static_cast<int64_t>(qi) * dpad;
+    float x[8];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int cc = c + 4 * h;
+      float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (cc < dpad) f = *reinterpret_cast<const float4*>(src + cc);  // dpad is a multiple of 4
+      x[4 * h] = f.x, x[4 * h + 1] = f.y, x[4 * h + 2] = f.z, x[4 * h + 3] = f.w;
+    }
+    uint4 o;
+    uint32_t* ow = reinterpret_cast<uint32_t*>(&o);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      __nv_bfloat162 p = __floats2bfloat162_rn(x[2 * j], x[2 * j + 1]);
+      ow[j] = *reinterpret_cast<uint32_t*>(&p);
+    }
+    *reinterpret_cast<uint4*>(G + e * kpad + c) = o;
+  }
+}
+
+// Segment lengths: the probed list's length rounded up to 4 (0 for a cut
+// probe), in (query, probe rank) order; the exclusive sum gives the starts.
+__global__ void seg_len_kernel(const int32_t* __restrict__ probes, int nqp, const int64_t* __restrict__ list_off,
+                               int64_t* __restrict__ len) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx > nqp) return;
+  int64_t n = 0;
+  if (idx < nqp) {
+    const int l = probes[idx];
+    if (l >= 0) n = (list_off[l + 1] - list_off[l] + 3) & ~int64_t(3);
+  }
+  len[idx] = n;
+}
+
+__global__ void __launch_bounds__(kRerankThreads)
+    cand_rerank_kernel(const float* __restrict__ cand, const int64_t* __restrict__ seg,
+                       const int32_t* __restrict__ probes, int P, int R, int k, const int64_t* __restrict__ list_off,
+                       const float* __restrict__ codes, const float* __restrict__ q, int dpad,
+                       const int64_t* __restrict__ ids, float* __restrict__ D, int64_t* __restrict__ I) {
+  extern __shared__ uint64_t s_keys[];  // pow2(R) approximate keys, then pow2(R) exact keys
+  __shared__ SelectShared sh_sel;
+  const int qi = blockIdx.x;
+  const int n2 = pow2_ceil(R < 2 ? 2 : R);
+  uint64_t* s_appr = s_keys;
+  uint64_t* s_exact = s_keys + n2;
+  const int64_t* sq = seg + static_cast<int64_t>(qi) * P;
+  const int64_t r0 = sq[0];
+  const int m = static_cast<int>(sq[P] - r0);
+  const float* src = cand + r0;
+  // Key (v, position): unique, so the R chosen are the R smallest by value
+  // with ties to the earlier position.  Padding (+inf) is no candidate.
+  auto key_at = [&](int i) -> uint64_t {
+    const float v = src[i];
+    return v < INFINITY ? (static_cast<uint64_t>(ordered_bits(v)) << 32) | static_cast<uint32_t>(i) : kEmpty;
+  };
+  block_topk_sorted(key_at, m, R, sh_sel, s_appr);
+  const float* qrow = q + static_cast<size_t>(qi) * dpad;
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+    uint64_t key = kEmpty;
+    if (i < R && s_appr[i] != kEmpty) {
+      const int64_t pos = r0 + key_tie(s_appr[i]);
+      int lo = 0, hi = P;  // the last probe rank whose segment starts at or before pos
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (sq[mid] <= pos) lo = mid; else hi = mid;
+      }
+      const int l = probes[static_cast<int64_t>(qi) * P + lo];
+      const int64_t row = list_off[l] + (pos - sq[lo]);
+      const float acc = exact_l2_seq(codes + static_cast<size_t>(row) * dpad, qrow, dpad);
+      if (acc < FLT_MAX) key = make_key(acc, static_cast<uint32_t>(row));
+    }
+    s_exact[i] = key;
+  }
+  __syncthreads();
+  block_bitonic_sort(s_exact, n2);
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    const uint64_t key = j < n2 ? s_exact[j] : kEmpty;
+    const size_t o = static_cast<size_t>(qi) * k + j;
+    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+  }
+}
+
+}  // namespace
+
+size_t cand_segments_tmp_bytes(int nq, int P) {
+  const size_t n = static_cast<size_t>(nq) * P + 1;
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, static_cast<const int64_t*>(nullptr), static_cast<int64_t*>(nullptr),
+                                static_cast<int64_t>(n));
+  bytes = (bytes + 255) / 256 * 256;
+  return bytes + n * sizeof(int64_t);
+}
+
+void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* list_off, int64_t* seg, void* tmp,
+                          size_t tmp_bytes, cudaStream_t st) {
+  const int nqp = nq * P;
+  const size_t n = static_cast<size_t>(nqp) + 1;
+  size_t cub_bytes = 0;
+  HB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, static_cast<const int64_t*>(nullptr),
+                                        static_cast<int64_t*>(nullptr), static_cast<int64_t>(n)));
+  const size_t cub_pad = (cub_bytes + 255) / 256 * 256;
+  HB_CHECK(tmp_bytes >= cub_pad + n * sizeof(int64_t), HB_ERR_INVALID, "segment scratch too small");
+  int64_t* len = reinterpret_cast<int64_t*>(static_cast<unsigned char*>(tmp) + cub_pad);
+  seg_len_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(probes, nqp, list_off, len);
+  HB_CUDA(cudaGetLastError());
+  size_t bytes = cub_bytes;
+  HB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, len, seg, static_cast<int64_t>(n), st));
+}
+
+void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* list_q, const int64_t* n_entries,
+                           int64_t max_rows, void* G, cudaStream_t st) {
+  if (max_rows <= 0) return;
+  HB_CHECK(kpad % 64 == 0 && dpad % 4 == 0 && dpad <= kpad, HB_ERR_INVALID, "bad query padding");
+  int64_t g = (max_rows * (kpad / 8) + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  gather_queries_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(q, dpad, kpad, list_q, n_entries, max_rows,
+                                                                  static_cast<__nv_bfloat16*>(G));
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st) {
+  HB_CHECK(a.kpad >= 64 && a.kpad % 64 == 0, HB_ERR_INVALID, "the candidate scan needs kpad a multiple of 64");
+  HB_CHECK(a.chunk_rows >= kT && a.chunk_rows % kT == 0, HB_ERR_INVALID, "chunk rows must be a multiple of 128");
+  const size_t smem = kStg * static_cast<size_t>(kStageBytes) + 1024;
+  HB_CUDA(cudaFuncSetAttribute(cand_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  const CUtensorMap* mq = static_cast<const CUtensorMap*>(tmap_q);
+  const CUtensorMap* mx = static_cast<const CUtensorMap*>(tmap_x);
+  cand_scan_kernel<<<num_sms, kThreads, smem, st>>>(*mq, *mx, a);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_cand_rerank(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R, int k,
+                        const int64_t* list_off, const float* codes, const float* q, int dpad, const int64_t* ids,
+                        float* D, int64_t* I, cudaStream_t st) {
+  if (nq <= 0) return;
+  HB_CHECK(R >= 1 && R <= kCandMaxR && k <= R, HB_ERR_INVALID, "candidate count out of range");
+  const size_t smem = 2 * static_cast<size_t>(pow2_ceil(R < 2 ? 2 : R)) * sizeof(uint64_t);
+  HB_CUDA(cudaFuncSetAttribute(cand_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)));
+  cand_rerank_kernel<<<nq, kRerankThreads, smem, st>>>(cand, seg, probes, P, R, k, list_off, codes, q, dpad, ids, D,
+                                                       I);
+  HB_CUDA(cudaGetLastError());
+}
+
+}  // namespace hb

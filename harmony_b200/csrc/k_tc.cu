@@ -56,15 +56,6 @@ constexpr int kMaxStages = 4;
 constexpr int kAcc = 2 * kGroups;                  // TMEM accumulators of 128 columns
 constexpr size_t kSmemCap = 225 * 1024;            // dynamic shared memory budget
 
-// Monotone map of a float to uint32 (all signs), and its inverse.
-__device__ __forceinline__ uint32_t ordered_bits(float f) {
-  const uint32_t b = __float_as_uint(f);
-  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-__device__ __forceinline__ float ordered_to_float(uint32_t u) {
-  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
-
 struct ItemDesc {
   int list, chunk, group, qcnt, ntiles;  // ntiles < 0: no more work
   int row0;                              // first row (vector position) of the chunk
@@ -475,22 +466,7 @@ __global__ void __launch_bounds__(512) rerank_kernel(const uint64_t* __restrict_
     uint64_t key = kEmpty;
     if (i < R && s_appr[i] != kEmpty) {
       const uint32_t pos = key_tie(s_appr[i]);
-      const float* x = codes + static_cast<size_t>(pos) * dpad;
-      float acc = 0.0f;
-#pragma unroll 8
-      for (int c = 0; c < dpad; c += 4) {
-        const float4 v = *reinterpret_cast<const float4*>(x + c);
-        const float4 w = *reinterpret_cast<const float4*>(qrow + c);
-        float t;
-        t = __fsub_rn(w.x, v.x);
-        acc = __fadd_rn(acc, __fmul_rn(t, t));
-        t = __fsub_rn(w.y, v.y);
-        acc = __fadd_rn(acc, __fmul_rn(t, t));
-        t = __fsub_rn(w.z, v.z);
-        acc = __fadd_rn(acc, __fmul_rn(t, t));
-        t = __fsub_rn(w.w, v.w);
-        acc = __fadd_rn(acc, __fmul_rn(t, t));
-      }
+      const float acc = exact_l2_seq(codes + static_cast<size_t>(pos) * dpad, qrow, dpad);
       if (acc < FLT_MAX) key = make_key(acc, pos);
     }
     s_exact[i] = key;
@@ -561,22 +537,7 @@ __global__ void __launch_bounds__(kRerankWarps * 32) rerank_warp_kernel(
     uint64_t key = kEmpty;
     if (j < nr) {
       const uint32_t pos = key_tie(cand[j]);
-      const float* x = codes + static_cast<size_t>(pos) * dpad;
-      float acc = 0.0f;
-#pragma unroll 8
-      for (int c = 0; c < dpad; c += 4) {
-        const float4 v = *reinterpret_cast<const float4*>(x + c);
-        const float4 w = *reinterpret_cast<const float4*>(qrow + c);
-        float t;
-        t = __fsub_rn(w.x, v.x);
-        acc = __fadd_rn(acc, __fmul_rn(t, t));
-        t = __fsub_rn(w.y, v.y);
-        acc = __fadd_rn(acc, __fmul_rn(t, t));
-        t = __fsub_rn(w.z, v.z);
-        acc = __fadd_rn(acc, __fmul_rn(t, t));
-        t = __fsub_rn(w.w, v.w);
-        acc = __fadd_rn(acc, __fmul_rn(t, t));
-      }
+      const float acc = exact_l2_seq(codes + static_cast<size_t>(pos) * dpad, qrow, dpad);
       if (acc < FLT_MAX) key = make_key(acc, pos);
     }
     ex[j] = key;

@@ -91,6 +91,6 @@ def test_bf16_small_batches_and_padding(fidx):
 def test_bf16_rejects_unsupported(fidx):
     base, q, ix = fidx
     with pytest.raises(HarmonyError):
-        search(ix, q[:4], 100)  # k above the BF16 candidate capacity
+        search(ix, q[:4], 5000)  # k above the BF16 candidate capacity (4096)
     with pytest.raises(HarmonyError):
         search(ix, q[:4], 10, mode=SearchMode.DIVIDE_IVF)

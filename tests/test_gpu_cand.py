@@ -1,0 +1,155 @@
+"""GPU tests of the candidate-matrix BF16 scan (tcgen05 over any d, up to 4096
+candidates per query) with the exact FP32 re-rank: the BF16 searches the
+shared-memory heap scan does not take (d > 128, or k above 64)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from harmony_b200 import Index, Precision, SearchMode, datasets
+from tests.parity import FLT_MAX, assert_topk_parity
+
+pytestmark = pytest.mark.gpu
+
+
+def search(ix, q, k, precision=Precision.BF16, mult=4, graph=False, npq=None, max_nprobe=0):
+    q = np.ascontiguousarray(q, np.float32)
+    sp = ix.search_params
+    sp.precision, sp.rerank_mult, sp.use_graph = precision, mult, graph
+    sp.nprobe_per_query, sp.max_nprobe = npq, max_nprobe
+    D = np.empty((q.shape[0], k), np.float32)
+    I = np.empty((q.shape[0], k), np.int64)
+    try:
+        ix.search(q.shape[0], q, k, D, I)
+    finally:
+        sp.precision, sp.rerank_mult, sp.use_graph = Precision.FP32, 2, False
+        sp.nprobe_per_query, sp.max_nprobe = None, 0
+    return D, I
+
+
+def integer_mixture(rng, n, centres, sd=20.0):
+    lab = rng.integers(0, centres.shape[0], n)
+    x = centres[lab] + rng.normal(0.0, sd, (n, centres.shape[1]))
+    return np.clip(np.rint(x), 0, 255).astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def wide():
+    """500-dimensional anisotropic mixture (the shape of the 270k x 500
+    workload, scaled down)."""
+    base, q = datasets.config3(seed=71, nb=40_000, nq=300, d=500, ncomp=200)
+    ix = Index(500, 64, 8)
+    ix.train(base.shape[0], base)
+    ix.add(base.shape[0], base)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    return base, q, ix
+
+
+@pytest.mark.parametrize("nprobe,k,mult", [(8, 100, 4), (4, 10, 4), (16, 1, 8), (8, 100, 1)])
+def test_wide_matches_exact_scan(wide, restated, nprobe, k, mult):
+    base, q, ix = wide
+    ix.nprobe = nprobe
+    D, I = search(ix, q, k, mult=mult)
+    De, Ie = search(ix, q, k, precision=Precision.FP32)
+    # Every returned distance is the exact FP32 distance of its id.
+    for qi in range(0, q.shape[0], 29):
+        for j in range(0, k, max(1, k // 10)):
+            if I[qi, j] >= 0:
+                assert D[qi, j] == restated.l2(q[qi], base[I[qi, j]])
+    same = np.mean([np.array_equal(a, b) for a, b in zip(D.view(np.uint32), De.view(np.uint32))])
+    # With R = k (mult 1) only the approximate top k are re-ranked.
+    assert same >= (0.995 if mult > 1 else 0.5), same
+    assert (D[:, -1] >= De[:, -1]).all()  # never better than exact
+    assert (np.diff(D, axis=1) >= 0).all()
+
+
+def test_wide_integer_data_matches_reference(ref_lib, restated):
+    """Integer data in [0, 255] at d = 200: BF16 holds every value exactly and
+    every dot product stays below 2^24, so the approximate values rank like
+    the exact ones and the BF16 search must match the reference."""
+    rng = np.random.default_rng(17)
+    d = 200
+    centres = rng.uniform(40, 215, (40, d))
+    base = integer_mixture(rng, 8000, centres)
+    q = integer_mixture(rng, 60, centres)
+    ref = ref_lib(d, 32, 6)
+    ref.train(base)
+    ref.add(base)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "int200.index")
+        ref.save(p)
+        ix = Index()
+        ix.load_index(p)
+    ix.nprobe = 6
+    for k in (10, 100):
+        D, I = search(ix, q, k)
+        Dr, Ir = ref.search(q, k)
+        assert_topk_parity(D, I, Dr, Ir, lambda qi, i: restated.l2(q[qi], base[i]), f"cand int k={k}")
+
+
+def test_d128_large_k(restated):
+    """d = 128 with k = 100 (above the heap scan's 64 candidates) takes the
+    candidate-matrix route."""
+    base, q = datasets.config2(seed=73, nb=120_000, nq=400, ncomp=300)
+    ix = Index(128, 256, 12)
+    ix.train(base.shape[0], base)
+    ix.add(base.shape[0], base)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    for k, mult in ((100, 2), (65, 4), (300, 2)):
+        D, I = search(ix, q, k, mult=mult)
+        De, Ie = search(ix, q, k, precision=Precision.FP32)
+        same = np.mean([np.array_equal(a, b) for a, b in zip(D.view(np.uint32), De.view(np.uint32))])
+        assert same >= 0.99, (k, same)
+        assert (D[:, -1] >= De[:, -1]).all()
+        for qi in range(0, q.shape[0], 53):
+            assert D[qi, 0] == restated.l2(q[qi], base[I[qi, 0]])
+
+
+def test_wide_per_query_nprobe_and_graph(wide):
+    base, q, ix = wide
+    ix.nprobe = 8
+    rng = np.random.default_rng(9)
+    npq = rng.integers(1, 20, size=q.shape[0]).astype(np.int32)
+    D, I = search(ix, q, 50, npq=npq, max_nprobe=20)
+    De, Ie = search(ix, q, 50, precision=Precision.FP32, npq=npq, max_nprobe=20)
+    same = np.mean([np.array_equal(a, b) for a, b in zip(D.view(np.uint32), De.view(np.uint32))])
+    assert same >= 0.99, same
+    # One graph launch per batch gives the ordinary search's results, call after call.
+    for lo, n in ((0, 64), (64, 64), (128, 33), (200, 33)):
+        Dg, Ig = search(ix, q[lo:lo + n], 100, graph=True)
+        Do, Io = search(ix, q[lo:lo + n], 100)
+        assert np.array_equal(Dg, Do) and np.array_equal(Ig, Io), lo
+
+
+def test_wide_small_and_degenerate(restated):
+    rng = np.random.default_rng(23)
+    # Fewer candidates than k: padded with (FLT_MAX, -1) like heap_init.
+    b = rng.standard_normal((40, 300)).astype(np.float32)
+    small = Index(300, 4, 2)
+    small.train(40, b)
+    small.add(40, b)
+    D, I = search(small, b[:5], 50)
+    De, Ie = search(small, b[:5], 50, precision=Precision.FP32)
+    assert np.array_equal(D, De) and np.array_equal(I, Ie)
+    assert (I == -1).any() and ((I == -1) == (D == FLT_MAX)).all()
+    # Duplicated rows: equal approximate values at the candidate boundary are
+    # chosen by position, so repeated searches agree bit for bit.
+    base = np.repeat(rng.standard_normal((500, 160)).astype(np.float32), 6, axis=0)
+    ix = Index(160, 16, 4)
+    ix.train(base.shape[0], base)
+    ix.add(base.shape[0], base)
+    q = base[::97] + np.float32(0.01)
+    D1, I1 = search(ix, q, 20, mult=1)
+    D2, I2 = search(ix, q, 20, mult=1)
+    assert np.array_equal(D1, D2) and np.array_equal(I1, I2)
+    De, Ie = search(ix, q, 20, precision=Precision.FP32)
+    assert_topk_parity(D1, I1, De, Ie, lambda qi, i: restated.l2(q[qi], base[i]), "duplicates")
+    # One query, brute force over every list.
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.BRUTE_FORCE), "")
+    try:
+        D, I = search(ix, q[:1], 30)
+        De, Ie = search(ix, q[:1], 30, precision=Precision.FP32)
+        assert_topk_parity(D, I, De, Ie, lambda qi, i: restated.l2(q[qi], base[i]), "brute force")
+    finally:
+        ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")

@@ -58,8 +58,13 @@ def test_wide_matches_exact_scan(wide, restated, nprobe, k, mult):
             if I[qi, j] >= 0:
                 assert D[qi, j] == restated.l2(q[qi], base[I[qi, j]])
     same = np.mean([np.array_equal(a, b) for a, b in zip(D.view(np.uint32), De.view(np.uint32))])
-    # With R = k (mult 1) only the approximate top k are re-ranked.
-    assert same >= (0.995 if mult > 1 else 0.5), same
+    if mult > 1:
+        assert same >= 0.995, same
+    else:
+        # R = k: only the approximate top k are re-ranked, so BF16 rounding
+        # shows at the tail; the set still holds nearly all true neighbours.
+        recall = np.mean([len(set(a) & set(b)) / k for a, b in zip(I, Ie)])
+        assert recall >= 0.95, recall
     assert (D[:, -1] >= De[:, -1]).all()  # never better than exact
     assert (np.diff(D, axis=1) >= 0).all()
 
@@ -143,8 +148,9 @@ def test_wide_small_and_degenerate(restated):
     D1, I1 = search(ix, q, 20, mult=1)
     D2, I2 = search(ix, q, 20, mult=1)
     assert np.array_equal(D1, D2) and np.array_equal(I1, I2)
+    D4, I4 = search(ix, q, 20)
     De, Ie = search(ix, q, 20, precision=Precision.FP32)
-    assert_topk_parity(D1, I1, De, Ie, lambda qi, i: restated.l2(q[qi], base[i]), "duplicates")
+    assert_topk_parity(D4, I4, De, Ie, lambda qi, i: restated.l2(q[qi], base[i]), "duplicates")
     # One query, brute force over every list.
     ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.BRUTE_FORCE), "")
     try:

@@ -87,9 +87,11 @@ def test_wide_integer_data_matches_reference(ref_lib, restated):
         ix = Index()
         ix.load_index(p)
     ix.nprobe = 6
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
     for k in (10, 100):
         D, I = search(ix, q, k)
         Dr, Ir = ref.search(q, k)
+        assert (I >= 0).all()
         assert_topk_parity(D, I, Dr, Ir, lambda qi, i: restated.l2(q[qi], base[i]), f"cand int k={k}")
 
 
@@ -134,6 +136,7 @@ def test_wide_small_and_degenerate(restated):
     small = Index(300, 4, 2)
     small.train(40, b)
     small.add(40, b)
+    small.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
     D, I = search(small, b[:5], 50)
     De, Ie = search(small, b[:5], 50, precision=Precision.FP32)
     assert np.array_equal(D, De) and np.array_equal(I, Ie)
@@ -144,6 +147,7 @@ def test_wide_small_and_degenerate(restated):
     ix = Index(160, 16, 4)
     ix.train(base.shape[0], base)
     ix.add(base.shape[0], base)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
     q = base[::97] + np.float32(0.01)
     D1, I1 = search(ix, q, 20, mult=1)
     D2, I2 = search(ix, q, 20, mult=1)

@@ -1326,7 +1326,9 @@ class IndexCore {
     }
     ++launches_;
     make_bf16_tensor_map(gqmap_, gq_.p, nqp, kpad_);
-    cand_.reserve(std::max<size_t>(static_cast<size_t>(nb) * cand_row_bound(P), 1));
+    const int64_t row_bound = cand_row_bound(P);
+    cand_.reserve(std::max<size_t>(static_cast<size_t>(nb) * row_bound, 1));
+    cand_rows_.reserve(static_cast<size_t>(nb) * R);
     CandArgs a{};
     a.list_off = list_off_.p;
     a.nlist = static_cast<int>(nlist_);
@@ -1350,9 +1352,9 @@ class IndexCore {
     {
       Scope sc(this, "cand_rerank");
       launch_cand_rerank(cand_.p, seg_.p, probes_.p, nb, P, R, k, list_off_.p, codes_.p, qpad_.p,
-                         static_cast<int>(dpad_), ids_.p, Dd, Id, st_);
+                         static_cast<int>(dpad_), ids_.p, Dd, Id, cand_rows_.p, row_bound, st_);
     }
-    ++launches_;
+    launches_ += 2;
     if (!capturing_) bf16_err_check();
   }
 
@@ -1703,6 +1705,7 @@ class IndexCore {
   DevBuf<int64_t> seg_;
   DevBuf<uint16_t> gq_;
   DevBuf<float> cand_;
+  DevBuf<int64_t> cand_rows_;
   // tensor-core coarse quantizer
   bool coarse_ready_ = false;
   int coarse_kind_ = HB_COARSE_AUTO;

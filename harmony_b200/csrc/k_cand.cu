@@ -11,18 +11,20 @@
 //     group of <= 128 queries).  For each 128-row tile of the chunk the TMA
 //     warp streams 64-column K blocks of both operands (queries: A, 128 x 64;
 //     rows: B, 128 x 64; 128-byte swizzle) into a ring of 32 KB stages, the
-//     MMA warp issues tcgen05.mma M128 x N128 x K16 into one of two TMEM
+//     MMA warp issues tcgen05.mma M128 x N128 x K16 into one of four TMEM
 //     accumulators, and the epilogue (thread = query, TMEM lane) writes
 //     v = ||x||^2 - 2 q~.x~ of the tile's rows into the query's candidate
 //     row: the concatenation over its probes, in probe order, of one segment
 //     per probed list (the list's length rounded up to 4; +inf past the end).
-//  3. cand_rerank_kernel: one CTA per query selects the R smallest keys
-//     (v, position) of its candidate row (block radix selection, unique keys
-//     so the choice is deterministic), maps each position back to its stored
-//     row, recomputes the distance with the reference's sequential unfused
-//     FP32 loop and returns the k best (distance, row) -- the same rule as
-//     the heap scan's rerank, so whenever the true k nearest are among the R
-//     candidates the result equals the exact scan's.
+//  3. cand_select_kernel: one CTA per query selects the R smallest keys
+//     (v, position) of its candidate row (block radix selection over the row
+//     staged in shared memory; unique keys, so the choice is deterministic)
+//     and maps each position back to its stored row.
+//  4. cand_exact_kernel: one CTA per query recomputes the R distances with
+//     the reference's sequential unfused FP32 loop and returns the k best
+//     (distance, row) -- the same rule as the heap scan's rerank, so whenever
+//     the true k nearest are among the R candidates the result equals the
+//     exact scan's.
 // Every mbarrier wait is bounded; on a timeout the kernel records an error
 // code, the roles stop, copies and MMAs in flight are waited for and TMEM is
 // freed.
@@ -30,6 +32,8 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include <cub/cub.cuh>
 
@@ -48,13 +52,18 @@ constexpr int kStg = 6;                    // ring stages
 constexpr int kThreads = 192;              // 4 epilogue warps, TMA warp, MMA warp
 constexpr uint32_t kBlk = kT * 128;        // one 128-row x 64-column BF16 block (16 KB)
 constexpr uint32_t kStageBytes = 2 * kBlk;  // A block + B block
-constexpr int kRerankThreads = 512;
+constexpr int kAccN = 4;                    // TMEM accumulators of 128 columns (all 512)
+constexpr int kSelectThreads = 512;
+constexpr int kExactThreads = 256;
+constexpr int kExChunk = 64;                // dimensions per staged chunk of the exact re-rank
+constexpr int kExStride = kExChunk + 1;     // odd row stride: column reads hit distinct banks
+constexpr size_t kSelectSmemCap = 200 * 1024;
 
 struct CandShared {
   uint64_t full[kStg];
   uint64_t empty[kStg];
-  uint64_t accf[2];
-  uint64_t acce[2];
+  uint64_t accf[kAccN];
+  uint64_t acce[kAccN];
   uint64_t drain;
   uint32_t tmem;
 };
@@ -99,13 +108,13 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nkb = a.kpad / 64;
   const int64_t total = a.item_off[a.nlist];
 
-  if (warp == 5) tmem_alloc(&sh.tmem, 256);
+  if (warp == 5) tmem_alloc(&sh.tmem, kAccN * kT);
   if (tid == 0) {
     for (int s = 0; s < kStg; ++s) {
       mbar_init(&sh.full[s], 1);
       mbar_init(&sh.empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kAccN; ++b) {
       mbar_init(&sh.accf[b], 1);
       mbar_init(&sh.acce[b], 128);
     }
@@ -154,8 +163,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int64_t item = blockIdx.x; ok && item < total; item += gridDim.x) {
         const CandItem d = cand_item(a, item);
         for (int t = 0; t < d.ntiles; ++t, ++tile) {
-          const int b = static_cast<int>(tile & 1);
-          if (!mbar_wait(&sh.acce[b], static_cast<uint32_t>((tile >> 1) & 1) ^ 1u, a.err, 33)) {
+          const int b = static_cast<int>(tile % kAccN);
+          if (!mbar_wait(&sh.acce[b], static_cast<uint32_t>((tile / kAccN) & 1) ^ 1u, a.err, 33)) {
             ok = false;
             break;
           }
@@ -200,8 +209,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         slen = a.seg[qp + 1] - sbase;
       }
       for (int t = 0; t < d.ntiles; ++t, ++tile) {
-        const int b = static_cast<int>(tile & 1);
-        if (ok) ok = mbar_wait(&sh.accf[b], static_cast<uint32_t>((tile >> 1) & 1), a.err, 34);
+        const int b = static_cast<int>(tile % kAccN);
+        if (ok) ok = mbar_wait(&sh.accf[b], static_cast<uint32_t>((tile / kAccN) & 1), a.err, 34);
         ok = __all_sync(0xffffffffu, ok);
         if (!ok) break;
         tc_fence_after();
@@ -238,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   if (warp == 5) {
     tc_fence_after();
-    tmem_dealloc(tmem, 256);
+    tmem_dealloc(tmem, kAccN * kT);
   }
 }
 
@@ -289,49 +298,110 @@ __global__ void seg_len_kernel(const int32_t* __restrict__ probes, int nqp, cons
   len[idx] = n;
 }
 
-__global__ void __launch_bounds__(kRerankThreads)
-    cand_rerank_kernel(const float* __restrict__ cand, const int64_t* __restrict__ seg,
-                       const int32_t* __restrict__ probes, int P, int R, int k, const int64_t* __restrict__ list_off,
-                       const float* __restrict__ codes, const float* __restrict__ q, int dpad,
-                       const int64_t* __restrict__ ids, float* __restrict__ D, int64_t* __restrict__ I) {
-  extern __shared__ uint64_t s_keys[];  // pow2(R) approximate keys, then pow2(R) exact keys
+// One CTA per query: the R smallest keys (v, position) of the query's
+// candidate row -- unique, so the R chosen are the R smallest values with
+// ties to the earlier position -- mapped back to their stored rows, in
+// ascending key order (-1 past the candidates).  The row is staged in shared
+// memory when it fits (one coalesced pass over global memory; the radix
+// passes then read shared memory).  Padding (+inf) is no candidate.
+__global__ void __launch_bounds__(kSelectThreads)
+    cand_select_kernel(const float* __restrict__ cand, const int64_t* __restrict__ seg,
+                       const int32_t* __restrict__ probes, int P, int R, const int64_t* __restrict__ list_off,
+                       int stage_cap, int64_t* __restrict__ out_rows) {
+  extern __shared__ __align__(16) unsigned char smem_sel[];
   __shared__ SelectShared sh_sel;
   const int qi = blockIdx.x;
   const int n2 = pow2_ceil(R < 2 ? 2 : R);
-  uint64_t* s_appr = s_keys;
-  uint64_t* s_exact = s_keys + n2;
+  uint64_t* s_appr = reinterpret_cast<uint64_t*>(smem_sel);
+  float* s_row = reinterpret_cast<float*>(s_appr + n2);
   const int64_t* sq = seg + static_cast<int64_t>(qi) * P;
   const int64_t r0 = sq[0];
-  const int m = static_cast<int>(sq[P] - r0);
+  const int m = static_cast<int>(sq[P] - r0);  // a multiple of 4, as is r0
   const float* src = cand + r0;
-  // Key (v, position): unique, so the R chosen are the R smallest by value
-  // with ties to the earlier position.  Padding (+inf) is no candidate.
+  const bool staged = m <= stage_cap;
+  if (staged) {
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(s_row);
+#pragma unroll 4
+    for (int i = threadIdx.x; i < m / 4; i += blockDim.x) d4[i] = s4[i];
+    __syncthreads();
+  }
+  const float* rowp = staged ? s_row : src;
   auto key_at = [&](int i) -> uint64_t {
-    const float v = src[i];
+    const float v = rowp[i];
     return v < INFINITY ? (static_cast<uint64_t>(ordered_bits(v)) << 32) | static_cast<uint32_t>(i) : kEmpty;
   };
   block_topk_sorted(key_at, m, R, sh_sel, s_appr);
-  const float* qrow = q + static_cast<size_t>(qi) * dpad;
-  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-    uint64_t key = kEmpty;
-    if (i < R && s_appr[i] != kEmpty) {
+  for (int i = threadIdx.x; i < R; i += blockDim.x) {
+    int64_t row = -1;
+    if (s_appr[i] != kEmpty) {
       const int64_t pos = r0 + key_tie(s_appr[i]);
       int lo = 0, hi = P;  // the last probe rank whose segment starts at or before pos
       while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
         if (sq[mid] <= pos) lo = mid; else hi = mid;
       }
-      const int l = probes[static_cast<int64_t>(qi) * P + lo];
-      const int64_t row = list_off[l] + (pos - sq[lo]);
-      const float acc = exact_l2_seq(codes + static_cast<size_t>(row) * dpad, qrow, dpad);
-      if (acc < FLT_MAX) key = make_key(acc, static_cast<uint32_t>(row));
+      row = list_off[probes[static_cast<int64_t>(qi) * P + lo]] + (pos - sq[lo]);
     }
-    s_exact[i] = key;
+    out_rows[static_cast<int64_t>(qi) * R + i] = row;
+  }
+}
+
+// One CTA per query: exact distances of its R candidate rows with the
+// reference's sequential unfused FP32 loop (the same operations, in the same
+// order, as exact_l2_seq), then the k best (distance, row).  Thread t owns
+// candidate t of each batch of 256; the batch's rows are staged 64
+// dimensions at a time in shared memory by coalesced loads (two rows per
+// warp instruction), each thread then continues its own sum over the chunk.
+__global__ void __launch_bounds__(kExactThreads)
+    cand_exact_kernel(const int64_t* __restrict__ rows, int R, int k, const float* __restrict__ codes,
+                      const float* __restrict__ q, int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
+                      int64_t* __restrict__ I) {
+  extern __shared__ __align__(16) unsigned char smem_ex[];
+  __shared__ int64_t s_rows[kExactThreads];
+  const int qi = blockIdx.x, tid = threadIdx.x;
+  const int n2 = pow2_ceil(R < 2 ? 2 : R);
+  uint64_t* s_ex = reinterpret_cast<uint64_t*>(smem_ex);
+  float* s_tile = reinterpret_cast<float*>(s_ex + n2);  // kExactThreads x kExStride
+  const float* qrow = q + static_cast<size_t>(qi) * dpad;
+  for (int i = tid; i < n2; i += kExactThreads) s_ex[i] = kEmpty;
+  for (int b0 = 0; b0 < R; b0 += kExactThreads) {
+    const int i = b0 + tid;
+    const int64_t row = i < R ? rows[static_cast<int64_t>(qi) * R + i] : -1;
+    s_rows[tid] = row;
+    float acc = 0.0f;
+    for (int c0 = 0; c0 < dpad; c0 += kExChunk) {
+      const int w4 = min(kExChunk, dpad - c0) / 4;  // dpad is a multiple of 4
+      __syncthreads();                              // rows published / previous chunk consumed
+#pragma unroll 4
+      for (int u = tid; u < kExactThreads * (kExChunk / 4); u += kExactThreads) {
+        const int r = u / (kExChunk / 4), f = u % (kExChunk / 4);
+        const int64_t rr = s_rows[r];
+        if (rr >= 0 && f < w4) {
+          const float4 v = *reinterpret_cast<const float4*>(codes + rr * dpad + c0 + 4 * f);
+          float* dst = s_tile + r * kExStride + 4 * f;
+          dst[0] = v.x;
+          dst[1] = v.y;
+          dst[2] = v.z;
+          dst[3] = v.w;
+        }
+      }
+      __syncthreads();
+      if (row >= 0) {
+        const float* x = s_tile + tid * kExStride;
+        const int w = 4 * w4;
+        for (int c = 0; c < w; ++c) {
+          const float t = __fsub_rn(__ldg(qrow + c0 + c), x[c]);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+        }
+      }
+    }
+    if (row >= 0 && acc < FLT_MAX) s_ex[i] = make_key(acc, static_cast<uint32_t>(row));
   }
   __syncthreads();
-  block_bitonic_sort(s_exact, n2);
-  for (int j = threadIdx.x; j < k; j += blockDim.x) {
-    const uint64_t key = j < n2 ? s_exact[j] : kEmpty;
+  block_bitonic_sort(s_ex, n2);
+  for (int j = tid; j < k; j += kExactThreads) {
+    const uint64_t key = j < n2 ? s_ex[j] : kEmpty;
     const size_t o = static_cast<size_t>(qi) * k + j;
     D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
     I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
@@ -389,14 +459,22 @@ void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a,
 
 void launch_cand_rerank(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R, int k,
                         const int64_t* list_off, const float* codes, const float* q, int dpad, const int64_t* ids,
-                        float* D, int64_t* I, cudaStream_t st) {
+                        float* D, int64_t* I, int64_t* rows, int64_t row_bound, cudaStream_t st) {
   if (nq <= 0) return;
   HB_CHECK(R >= 1 && R <= kCandMaxR && k <= R, HB_ERR_INVALID, "candidate count out of range");
-  const size_t smem = 2 * static_cast<size_t>(pow2_ceil(R < 2 ? 2 : R)) * sizeof(uint64_t);
-  HB_CUDA(cudaFuncSetAttribute(cand_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem)));
-  cand_rerank_kernel<<<nq, kRerankThreads, smem, st>>>(cand, seg, probes, P, R, k, list_off, codes, q, dpad, ids, D,
-                                                       I);
+  const size_t keys = static_cast<size_t>(pow2_ceil(R < 2 ? 2 : R)) * sizeof(uint64_t);
+  // Stage rows up to the longest this batch can have, within the budget.
+  const int64_t cap_budget = static_cast<int64_t>((kSelectSmemCap - keys) / sizeof(float)) & ~int64_t(3);
+  const int stage_cap = static_cast<int>(std::min<int64_t>(std::max<int64_t>(row_bound, 0), cap_budget));
+  const size_t smem_sel = keys + static_cast<size_t>(stage_cap) * sizeof(float);
+  HB_CUDA(cudaFuncSetAttribute(cand_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem_sel)));
+  cand_select_kernel<<<nq, kSelectThreads, smem_sel, st>>>(cand, seg, probes, P, R, list_off, stage_cap, rows);
+  HB_CUDA(cudaGetLastError());
+  const size_t smem_ex = keys + static_cast<size_t>(kExactThreads) * kExStride * sizeof(float);
+  HB_CUDA(cudaFuncSetAttribute(cand_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem_ex)));
+  cand_exact_kernel<<<nq, kExactThreads, smem_ex, st>>>(rows, R, k, codes, q, dpad, ids, D, I);
   HB_CUDA(cudaGetLastError());
 }
 

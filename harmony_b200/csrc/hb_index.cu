@@ -1296,7 +1296,9 @@ class IndexCore {
     coarse_and_cut(nb, P);
     err_dev_.reserve(1);
     HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
-    const int cr = std::max(128, chunk_rows_for(nb, P, 128));
+    // One 128-row tile per work item: the queries' tile is fetched per row
+    // tile anyway, and small items balance the persistent CTAs.
+    const int cr = 128;
     const size_t nqp = static_cast<size_t>(nb) * P;
     list_cnt_.reserve(nlist_);
     list_cursor_.reserve(nlist_);
@@ -1352,7 +1354,7 @@ class IndexCore {
     {
       Scope sc(this, "cand_rerank");
       launch_cand_rerank(cand_.p, seg_.p, probes_.p, nb, P, R, k, list_off_.p, codes_.p, qpad_.p,
-                         static_cast<int>(dpad_), ids_.p, Dd, Id, cand_rows_.p, row_bound, st_);
+                         static_cast<int>(dpad_), ids_.p, Dd, Id, cand_rows_.p, st_);
     }
     launches_ += 2;
     if (!capturing_) bf16_err_check();

@@ -225,10 +225,10 @@ void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* li
                            int64_t max_rows, void* G, cudaStream_t st);
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st);
 // Selection of each query's R candidates (rows: nq x R stored rows) and
-// their exact re-rank; row_bound = the longest candidate row of the batch.
+// their exact re-rank.
 void launch_cand_rerank(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R, int k,
                         const int64_t* list_off, const float* codes, const float* q, int dpad, const int64_t* ids,
-                        float* D, int64_t* I, int64_t* rows, int64_t row_bound, cudaStream_t st);
+                        float* D, int64_t* I, int64_t* rows, cudaStream_t st);
 void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st);
 void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st);
 // Re-rank over the slots of one or two scan passes (part2 may be null);

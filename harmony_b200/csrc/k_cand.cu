@@ -8,7 +8,8 @@
 //     consecutive rows and reach the tensor cores by plain TMA tiles.
 //  2. cand_scan_kernel: persistent, one CTA per SM, 192 threads (4 epilogue
 //     warps, a TMA warp, an MMA warp).  Work items are (list, chunk of rows,
-//     group of <= 128 queries).  For each 128-row tile of the chunk the TMA
+//     group of <= 128 queries); the search uses one 128-row tile per item,
+//     so the items spread evenly over the CTAs.  For each 128-row tile of the chunk the TMA
 //     warp streams 64-column K blocks of both operands (queries: A, 128 x 64;
 //     rows: B, 128 x 64; 128-byte swizzle) into a ring of 32 KB stages, the
 //     MMA warp issues tcgen05.mma M128 x N128 x K16 into one of four TMEM
@@ -53,11 +54,11 @@ constexpr int kThreads = 192;              // 4 epilogue warps, TMA warp, MMA wa
 constexpr uint32_t kBlk = kT * 128;        // one 128-row x 64-column BF16 block (16 KB)
 constexpr uint32_t kStageBytes = 2 * kBlk;  // A block + B block
 constexpr int kAccN = 4;                    // TMEM accumulators of 128 columns (all 512)
-constexpr int kSelectThreads = 512;
+constexpr int kSelectThreads = 256;
+constexpr int kBins = 2048;                 // histogram bins of the candidate selection
 constexpr int kExactThreads = 256;
 constexpr int kExChunk = 64;                // dimensions per staged chunk of the exact re-rank
 constexpr int kExStride = kExChunk + 1;     // odd row stride: column reads hit distinct banks
-constexpr size_t kSelectSmemCap = 200 * 1024;
 
 struct CandShared {
   uint64_t full[kStg];
@@ -215,27 +216,29 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!ok) break;
         tc_fence_after();
         const int64_t rl0 = static_cast<int64_t>(d.chunk) * a.chunk_rows + static_cast<int64_t>(t) * kT;
+        // The tile's 128 row norms: one coalesced load per 32 columns, then
+        // handed to every lane by shuffles.
         const float* tn = a.tile_norm + (d.tile0 + t) * kT;
-#pragma unroll 1
+        float nrm[kT / 32];
+#pragma unroll
+        for (int c = 0; c < kT / 32; ++c) nrm[c] = tn[c * 32 + lane];
+#pragma unroll
         for (int c = 0; c < kT / 32; ++c) {
           uint32_t r[32];
           tmem_ld32(tmem + lane_base + static_cast<uint32_t>(b * kT + c * 32), r);
           tmem_ld_wait();
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            r[j] = __float_as_uint(fmaf(-2.0f, __uint_as_float(r[j]), __shfl_sync(0xffffffffu, nrm[c], j)));
           const int64_t o = rl0 + c * 32;
           if (o < slen) {
             float* out = a.cand + sbase + o;
 #pragma unroll
-            for (int j4 = 0; j4 < 8; ++j4) {
-              if (o + 4 * j4 < slen) {
-                const float4 nm = *reinterpret_cast<const float4*>(tn + c * 32 + 4 * j4);
-                float4 v;
-                v.x = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 0]), nm.x);
-                v.y = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), nm.y);
-                v.z = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), nm.z);
-                v.w = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), nm.w);
-                *reinterpret_cast<float4*>(out + 4 * j4) = v;
-              }
-            }
+            for (int j4 = 0; j4 < 8; ++j4)
+              if (o + 4 * j4 < slen)
+                *reinterpret_cast<float4*>(out + 4 * j4) =
+                    make_float4(__uint_as_float(r[4 * j4]), __uint_as_float(r[4 * j4 + 1]),
+                                __uint_as_float(r[4 * j4 + 2]), __uint_as_float(r[4 * j4 + 3]));
           }
         }
         tc_fence_before();
@@ -298,44 +301,154 @@ __global__ void seg_len_kernel(const int32_t* __restrict__ probes, int nqp, cons
   len[idx] = n;
 }
 
+// Histogram bin of a finite candidate value: 2048 equal bins over
+// [vmin, vmax]; monotone in v (each step rounds monotonically), so every
+// value in a lower bin is below every value in a higher one.
+__device__ __forceinline__ int value_bin(float v, float vmin, float scale) {
+  const float t = (v - vmin) * scale;
+  return t < static_cast<float>(kBins) ? max(0, static_cast<int>(t)) : kBins - 1;
+}
+
 // One CTA per query: the R smallest keys (v, position) of the query's
 // candidate row -- unique, so the R chosen are the R smallest values with
 // ties to the earlier position -- mapped back to their stored rows, in
-// ascending key order (-1 past the candidates).  The row is staged in shared
-// memory when it fits (one coalesced pass over global memory; the radix
-// passes then read shared memory).  Padding (+inf) is no candidate.
+// ascending key order (-1 past the candidates).  Three coalesced passes over
+// the row: the range of its finite values, a 2048-bin histogram over that
+// range, and the compaction of every key in the bins up to the one holding
+// the R-th value into shared memory, which a bitonic sort orders.  A row
+// whose compacted set would exceed the buffer (a dense bin) takes the
+// block radix selection instead.  Padding (+inf) is no candidate.
 __global__ void __launch_bounds__(kSelectThreads)
     cand_select_kernel(const float* __restrict__ cand, const int64_t* __restrict__ seg,
                        const int32_t* __restrict__ probes, int P, int R, const int64_t* __restrict__ list_off,
-                       int stage_cap, int64_t* __restrict__ out_rows) {
+                       int cap, int64_t* __restrict__ out_rows) {
   extern __shared__ __align__(16) unsigned char smem_sel[];
+  uint64_t* s_cand = reinterpret_cast<uint64_t*>(smem_sel);  // cap keys (a power of two >= 2 * pow2(R))
+  __shared__ int s_hist[kBins];
+  __shared__ unsigned int s_lo, s_hi;
+  __shared__ int s_real, s_bin, s_C, s_cnt;
   __shared__ SelectShared sh_sel;
-  const int qi = blockIdx.x;
-  const int n2 = pow2_ceil(R < 2 ? 2 : R);
-  uint64_t* s_appr = reinterpret_cast<uint64_t*>(smem_sel);
-  float* s_row = reinterpret_cast<float*>(s_appr + n2);
+  const int qi = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t* sq = seg + static_cast<int64_t>(qi) * P;
   const int64_t r0 = sq[0];
   const int m = static_cast<int>(sq[P] - r0);  // a multiple of 4, as is r0
   const float* src = cand + r0;
-  const bool staged = m <= stage_cap;
-  if (staged) {
-    const float4* s4 = reinterpret_cast<const float4*>(src);
-    float4* d4 = reinterpret_cast<float4*>(s_row);
-#pragma unroll 4
-    for (int i = threadIdx.x; i < m / 4; i += blockDim.x) d4[i] = s4[i];
-    __syncthreads();
+  for (int i = tid; i < kBins; i += kSelectThreads) s_hist[i] = 0;
+  if (tid == 0) {
+    s_lo = 0xffffffffu;
+    s_hi = 0u;
+    s_real = 0;
+    s_cnt = 0;
   }
-  const float* rowp = staged ? s_row : src;
-  auto key_at = [&](int i) -> uint64_t {
-    const float v = rowp[i];
-    return v < INFINITY ? (static_cast<uint64_t>(ordered_bits(v)) << 32) | static_cast<uint32_t>(i) : kEmpty;
-  };
-  block_topk_sorted(key_at, m, R, sh_sel, s_appr);
-  for (int i = threadIdx.x; i < R; i += blockDim.x) {
+  __syncthreads();
+  // Pass 1: count and range of the finite values.
+  {
+    unsigned int lo = 0xffffffffu, hi = 0u;
+    int c = 0;
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll 4
+    for (int i4 = tid; i4 < m / 4; i4 += kSelectThreads) {
+      const float4 v = s4[i4];
+      const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (e[j] < INFINITY) {
+          const unsigned int o = ordered_bits(e[j]);
+          ++c;
+          lo = min(lo, o);
+          hi = max(hi, o);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      c += __shfl_xor_sync(0xffffffffu, c, off);
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, off));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, off));
+    }
+    if (lane == 0 && c) {
+      atomicAdd(&s_real, c);
+      atomicMin(&s_lo, lo);
+      atomicMax(&s_hi, hi);
+    }
+  }
+  __syncthreads();
+  const int real = s_real;
+  const int need = min(R, real);
+  int C = 0;
+  if (real > 0) {
+    const float vmin = ordered_to_float(s_lo), vmax = ordered_to_float(s_hi);
+    const float range = vmax - vmin;
+    float scale = range > 0.0f ? static_cast<float>(kBins) / range : 0.0f;
+    if (!(scale < 1e30f)) scale = 0.0f;
+    // Pass 2: histogram (lanes of a warp that hit one bin add once).
+#pragma unroll 2
+    for (int base = tid & ~31; base < m; base += kSelectThreads) {
+      const int i = base + lane;
+      const float v = i < m ? src[i] : INFINITY;
+      const bool valid = v < INFINITY;
+      const int bin = valid ? value_bin(v, vmin, scale) : 0;
+      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const unsigned peers = __match_any_sync(vmask, bin);
+        if (lane == __ffs(peers) - 1) atomicAdd(&s_hist[bin], __popc(peers));
+      }
+    }
+    __syncthreads();
+    // The bin holding the need-th value: lane L sums bins [64L, 64L + 64)
+    // (read rotated so the lanes hit distinct banks).
+    if (warp == 0) {
+      int loc = 0;
+      for (int j = 0; j < kBins / 32; ++j) loc += s_hist[lane * (kBins / 32) + ((j + lane) & (kBins / 32 - 1))];
+      int incl = loc;
+      for (int off = 1; off < 32; off <<= 1) {
+        const int o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += o;
+      }
+      const unsigned hit = __ballot_sync(0xffffffffu, incl >= need);
+      if (lane == __ffs(hit) - 1) {
+        int cum = incl - loc, b = lane * (kBins / 32);
+        for (;; ++b) {
+          cum += s_hist[b];
+          if (cum >= need) break;
+        }
+        s_bin = b;
+        s_C = cum;
+      }
+    }
+    __syncthreads();
+    C = s_C;
+    if (C <= cap) {
+      // Pass 3: every key in bins <= s_bin, in any order (the keys are unique).
+      const int bsel = s_bin;
+#pragma unroll 2
+      for (int base = tid & ~31; base < m; base += kSelectThreads) {
+        const int i = base + lane;
+        const float v = i < m ? src[i] : INFINITY;
+        const bool take = v < INFINITY && value_bin(v, vmin, scale) <= bsel;
+        const unsigned tm = __ballot_sync(0xffffffffu, take);
+        int pos0 = 0;
+        if (lane == 0 && tm) pos0 = atomicAdd(&s_cnt, __popc(tm));
+        pos0 = __shfl_sync(0xffffffffu, pos0, 0);
+        if (take)
+          s_cand[pos0 + __popc(tm & ((1u << lane) - 1u))] =
+              (static_cast<uint64_t>(ordered_bits(v)) << 32) | static_cast<uint32_t>(i);
+      }
+      const int c2 = pow2_ceil(C < 2 ? 2 : C);
+      for (int i = C + tid; i < c2; i += kSelectThreads) s_cand[i] = kEmpty;
+      __syncthreads();
+      block_bitonic_sort(s_cand, c2);
+    } else {
+      // A dense bin: radix selection over the whole row.
+      auto key_at = [&](int i) -> uint64_t {
+        const float v = src[i];
+        return v < INFINITY ? (static_cast<uint64_t>(ordered_bits(v)) << 32) | static_cast<uint32_t>(i) : kEmpty;
+      };
+      block_topk_sorted(key_at, m, R, sh_sel, s_cand);
+    }
+  }
+  for (int i = tid; i < R; i += kSelectThreads) {
     int64_t row = -1;
-    if (s_appr[i] != kEmpty) {
-      const int64_t pos = r0 + key_tie(s_appr[i]);
+    if (i < need) {
+      const int64_t pos = r0 + key_tie(s_cand[i]);
       int lo = 0, hi = P;  // the last probe rank whose segment starts at or before pos
       while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
@@ -373,7 +486,7 @@ __global__ void __launch_bounds__(kExactThreads)
     for (int c0 = 0; c0 < dpad; c0 += kExChunk) {
       const int w4 = min(kExChunk, dpad - c0) / 4;  // dpad is a multiple of 4
       __syncthreads();                              // rows published / previous chunk consumed
-#pragma unroll 4
+#pragma unroll
       for (int u = tid; u < kExactThreads * (kExChunk / 4); u += kExactThreads) {
         const int r = u / (kExChunk / 4), f = u % (kExChunk / 4);
         const int64_t rr = s_rows[r];
@@ -459,17 +572,16 @@ void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a,
 
 void launch_cand_rerank(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R, int k,
                         const int64_t* list_off, const float* codes, const float* q, int dpad, const int64_t* ids,
-                        float* D, int64_t* I, int64_t* rows, int64_t row_bound, cudaStream_t st) {
+                        float* D, int64_t* I, int64_t* rows, cudaStream_t st) {
   if (nq <= 0) return;
   HB_CHECK(R >= 1 && R <= kCandMaxR && k <= R, HB_ERR_INVALID, "candidate count out of range");
   const size_t keys = static_cast<size_t>(pow2_ceil(R < 2 ? 2 : R)) * sizeof(uint64_t);
-  // Stage rows up to the longest this batch can have, within the budget.
-  const int64_t cap_budget = static_cast<int64_t>((kSelectSmemCap - keys) / sizeof(float)) & ~int64_t(3);
-  const int stage_cap = static_cast<int>(std::min<int64_t>(std::max<int64_t>(row_bound, 0), cap_budget));
-  const size_t smem_sel = keys + static_cast<size_t>(stage_cap) * sizeof(float);
+  // Compaction buffer: at least 2048 keys and four times the R kept.
+  const int cap = std::max(2048, 4 * pow2_ceil(R < 2 ? 2 : R));
+  const size_t smem_sel = static_cast<size_t>(cap) * sizeof(uint64_t);
   HB_CUDA(cudaFuncSetAttribute(cand_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                static_cast<int>(smem_sel)));
-  cand_select_kernel<<<nq, kSelectThreads, smem_sel, st>>>(cand, seg, probes, P, R, list_off, stage_cap, rows);
+  cand_select_kernel<<<nq, kSelectThreads, smem_sel, st>>>(cand, seg, probes, P, R, list_off, cap, rows);
   HB_CUDA(cudaGetLastError());
   const size_t smem_ex = keys + static_cast<size_t>(kExactThreads) * kExStride * sizeof(float);
   HB_CUDA(cudaFuncSetAttribute(cand_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -1352,9 +1352,12 @@ class IndexCore {
     }
     ++launches_;
     {
-      Scope sc(this, "cand_rerank");
-      launch_cand_rerank(cand_.p, seg_.p, probes_.p, nb, P, R, k, list_off_.p, codes_.p, qpad_.p,
-                         static_cast<int>(dpad_), ids_.p, Dd, Id, cand_rows_.p, st_);
+      Scope sc(this, "cand_select");
+      launch_cand_select(cand_.p, seg_.p, probes_.p, nb, P, R, list_off_.p, cand_rows_.p, st_);
+    }
+    {
+      Scope sc(this, "cand_exact");
+      launch_cand_exact(cand_rows_.p, nb, R, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd, Id, st_);
     }
     launches_ += 2;
     if (!capturing_) bf16_err_check();

@@ -224,11 +224,12 @@ void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* l
 void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* list_q, const int64_t* n_entries,
                            int64_t max_rows, void* G, cudaStream_t st);
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st);
-// Selection of each query's R candidates (rows: nq x R stored rows) and
-// their exact re-rank.
-void launch_cand_rerank(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R, int k,
-                        const int64_t* list_off, const float* codes, const float* q, int dpad, const int64_t* ids,
-                        float* D, int64_t* I, int64_t* rows, cudaStream_t st);
+// Selection of each query's R candidates (rows: nq x R stored rows, -1 past
+// the candidates), then their exact re-rank to the k best.
+void launch_cand_select(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R,
+                        const int64_t* list_off, int64_t* rows, cudaStream_t st);
+void launch_cand_exact(const int64_t* rows, int nq, int R, int k, const float* codes, const float* q, int dpad,
+                       const int64_t* ids, float* D, int64_t* I, cudaStream_t st);
 void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st);
 void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st);
 // Re-rank over the slots of one or two scan passes (part2 may be null);

@@ -570,12 +570,10 @@ void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a,
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_cand_rerank(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R, int k,
-                        const int64_t* list_off, const float* codes, const float* q, int dpad, const int64_t* ids,
-                        float* D, int64_t* I, int64_t* rows, cudaStream_t st) {
+void launch_cand_select(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R,
+                        const int64_t* list_off, int64_t* rows, cudaStream_t st) {
   if (nq <= 0) return;
-  HB_CHECK(R >= 1 && R <= kCandMaxR && k <= R, HB_ERR_INVALID, "candidate count out of range");
-  const size_t keys = static_cast<size_t>(pow2_ceil(R < 2 ? 2 : R)) * sizeof(uint64_t);
+  HB_CHECK(R >= 1 && R <= kCandMaxR, HB_ERR_INVALID, "candidate count out of range");
   // Compaction buffer: at least 2048 keys and four times the R kept.
   const int cap = std::max(2048, 4 * pow2_ceil(R < 2 ? 2 : R));
   const size_t smem_sel = static_cast<size_t>(cap) * sizeof(uint64_t);
@@ -583,6 +581,13 @@ void launch_cand_rerank(const float* cand, const int64_t* seg, const int32_t* pr
                                static_cast<int>(smem_sel)));
   cand_select_kernel<<<nq, kSelectThreads, smem_sel, st>>>(cand, seg, probes, P, R, list_off, cap, rows);
   HB_CUDA(cudaGetLastError());
+}
+
+void launch_cand_exact(const int64_t* rows, int nq, int R, int k, const float* codes, const float* q, int dpad,
+                       const int64_t* ids, float* D, int64_t* I, cudaStream_t st) {
+  if (nq <= 0) return;
+  HB_CHECK(R >= 1 && R <= kCandMaxR && k <= R, HB_ERR_INVALID, "candidate count out of range");
+  const size_t keys = static_cast<size_t>(pow2_ceil(R < 2 ? 2 : R)) * sizeof(uint64_t);
   const size_t smem_ex = keys + static_cast<size_t>(kExactThreads) * kExStride * sizeof(float);
   HB_CUDA(cudaFuncSetAttribute(cand_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                static_cast<int>(smem_ex)));

@@ -56,6 +56,7 @@ constexpr uint32_t kStageBytes = 2 * kBlk;  // A block + B block
 constexpr int kAccN = 4;                    // TMEM accumulators of 128 columns (all 512)
 constexpr int kSelectThreads = 256;
 constexpr int kBins = 2048;                 // histogram bins of the candidate selection
+constexpr int kSelUnroll = 4;               // 32-value runs a warp loads at once
 constexpr int kExactThreads = 256;
 constexpr int kExChunk = 64;                // dimensions per staged chunk of the exact re-rank
 constexpr int kExStride = kExChunk + 1;     // odd row stride: column reads hit distinct banks
@@ -379,17 +380,24 @@ __global__ void __launch_bounds__(kSelectThreads)
     const float range = vmax - vmin;
     float scale = range > 0.0f ? static_cast<float>(kBins) / range : 0.0f;
     if (!(scale < 1e30f)) scale = 0.0f;
-    // Pass 2: histogram (lanes of a warp that hit one bin add once).
-#pragma unroll 2
-    for (int base = tid & ~31; base < m; base += kSelectThreads) {
-      const int i = base + lane;
-      const float v = i < m ? src[i] : INFINITY;
-      const bool valid = v < INFINITY;
-      const int bin = valid ? value_bin(v, vmin, scale) : 0;
-      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        const unsigned peers = __match_any_sync(vmask, bin);
-        if (lane == __ffs(peers) - 1) atomicAdd(&s_hist[bin], __popc(peers));
+    // Pass 2: histogram (lanes of a warp that hit one bin add once); each
+    // warp loads four 32-value runs before it bins them.
+    for (int base = tid & ~31; base < m; base += kSelUnroll * kSelectThreads) {
+      float vv[kSelUnroll];
+#pragma unroll
+      for (int u = 0; u < kSelUnroll; ++u) {
+        const int i = base + u * kSelectThreads + lane;
+        vv[u] = i < m ? src[i] : INFINITY;
+      }
+#pragma unroll
+      for (int u = 0; u < kSelUnroll; ++u) {
+        const bool valid = vv[u] < INFINITY;
+        const int bin = valid ? value_bin(vv[u], vmin, scale) : 0;
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+          const unsigned peers = __match_any_sync(vmask, bin);
+          if (lane == __ffs(peers) - 1) atomicAdd(&s_hist[bin], __popc(peers));
+        }
       }
     }
     __syncthreads();
@@ -419,18 +427,25 @@ __global__ void __launch_bounds__(kSelectThreads)
     if (C <= cap) {
       // Pass 3: every key in bins <= s_bin, in any order (the keys are unique).
       const int bsel = s_bin;
-#pragma unroll 2
-      for (int base = tid & ~31; base < m; base += kSelectThreads) {
-        const int i = base + lane;
-        const float v = i < m ? src[i] : INFINITY;
-        const bool take = v < INFINITY && value_bin(v, vmin, scale) <= bsel;
-        const unsigned tm = __ballot_sync(0xffffffffu, take);
-        int pos0 = 0;
-        if (lane == 0 && tm) pos0 = atomicAdd(&s_cnt, __popc(tm));
-        pos0 = __shfl_sync(0xffffffffu, pos0, 0);
-        if (take)
-          s_cand[pos0 + __popc(tm & ((1u << lane) - 1u))] =
-              (static_cast<uint64_t>(ordered_bits(v)) << 32) | static_cast<uint32_t>(i);
+      for (int base = tid & ~31; base < m; base += kSelUnroll * kSelectThreads) {
+        float vv[kSelUnroll];
+#pragma unroll
+        for (int u = 0; u < kSelUnroll; ++u) {
+          const int i = base + u * kSelectThreads + lane;
+          vv[u] = i < m ? src[i] : INFINITY;
+        }
+#pragma unroll
+        for (int u = 0; u < kSelUnroll; ++u) {
+          const int i = base + u * kSelectThreads + lane;
+          const bool take = vv[u] < INFINITY && value_bin(vv[u], vmin, scale) <= bsel;
+          const unsigned tm = __ballot_sync(0xffffffffu, take);
+          int pos0 = 0;
+          if (lane == 0 && tm) pos0 = atomicAdd(&s_cnt, __popc(tm));
+          pos0 = __shfl_sync(0xffffffffu, pos0, 0);
+          if (take)
+            s_cand[pos0 + __popc(tm & ((1u << lane) - 1u))] =
+                (static_cast<uint64_t>(ordered_bits(vv[u])) << 32) | static_cast<uint32_t>(i);
+        }
       }
       const int c2 = pow2_ceil(C < 2 ? 2 : C);
       for (int i = C + tid; i < c2; i += kSelectThreads) s_cand[i] = kEmpty;
@@ -463,22 +478,24 @@ __global__ void __launch_bounds__(kSelectThreads)
 // One CTA per query: exact distances of its R candidate rows with the
 // reference's sequential unfused FP32 loop (the same operations, in the same
 // order, as exact_l2_seq), then the k best (distance, row).  Thread t owns
-// candidate t of each batch of 256; the batch's rows are staged 64
-// dimensions at a time in shared memory by coalesced loads (two rows per
-// warp instruction), each thread then continues its own sum over the chunk.
+// candidate t of each batch of blockDim.x (R rounded up to a warp, 64 to
+// 256); the batch's rows and the query are staged 64 dimensions at a time
+// in shared memory by coalesced loads (two rows per warp instruction), and
+// each thread continues its own sum over the chunk from shared memory.
 __global__ void __launch_bounds__(kExactThreads)
     cand_exact_kernel(const int64_t* __restrict__ rows, int R, int k, const float* __restrict__ codes,
                       const float* __restrict__ q, int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
                       int64_t* __restrict__ I) {
   extern __shared__ __align__(16) unsigned char smem_ex[];
   __shared__ int64_t s_rows[kExactThreads];
-  const int qi = blockIdx.x, tid = threadIdx.x;
+  __shared__ __align__(16) float s_q[kExChunk];
+  const int qi = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   const int n2 = pow2_ceil(R < 2 ? 2 : R);
   uint64_t* s_ex = reinterpret_cast<uint64_t*>(smem_ex);
-  float* s_tile = reinterpret_cast<float*>(s_ex + n2);  // kExactThreads x kExStride
+  float* s_tile = reinterpret_cast<float*>(s_ex + n2);  // nt x kExStride
   const float* qrow = q + static_cast<size_t>(qi) * dpad;
-  for (int i = tid; i < n2; i += kExactThreads) s_ex[i] = kEmpty;
-  for (int b0 = 0; b0 < R; b0 += kExactThreads) {
+  for (int i = tid; i < n2; i += nt) s_ex[i] = kEmpty;
+  for (int b0 = 0; b0 < R; b0 += nt) {
     const int i = b0 + tid;
     const int64_t row = i < R ? rows[static_cast<int64_t>(qi) * R + i] : -1;
     s_rows[tid] = row;
@@ -486,8 +503,9 @@ __global__ void __launch_bounds__(kExactThreads)
     for (int c0 = 0; c0 < dpad; c0 += kExChunk) {
       const int w4 = min(kExChunk, dpad - c0) / 4;  // dpad is a multiple of 4
       __syncthreads();                              // rows published / previous chunk consumed
-#pragma unroll
-      for (int u = tid; u < kExactThreads * (kExChunk / 4); u += kExactThreads) {
+      if (tid < w4) *reinterpret_cast<float4*>(s_q + 4 * tid) = *reinterpret_cast<const float4*>(qrow + c0 + 4 * tid);
+#pragma unroll 4
+      for (int u = tid; u < nt * (kExChunk / 4); u += nt) {
         const int r = u / (kExChunk / 4), f = u % (kExChunk / 4);
         const int64_t rr = s_rows[r];
         if (rr >= 0 && f < w4) {
@@ -502,9 +520,16 @@ __global__ void __launch_bounds__(kExactThreads)
       __syncthreads();
       if (row >= 0) {
         const float* x = s_tile + tid * kExStride;
-        const int w = 4 * w4;
-        for (int c = 0; c < w; ++c) {
-          const float t = __fsub_rn(__ldg(qrow + c0 + c), x[c]);
+        for (int c = 0; c < 4 * w4; c += 4) {
+          const float4 qq = *reinterpret_cast<const float4*>(s_q + c);
+          const float x0 = x[c], x1 = x[c + 1], x2 = x[c + 2], x3 = x[c + 3];
+          float t = __fsub_rn(qq.x, x0);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+          t = __fsub_rn(qq.y, x1);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+          t = __fsub_rn(qq.z, x2);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+          t = __fsub_rn(qq.w, x3);
           acc = __fadd_rn(acc, __fmul_rn(t, t));
         }
       }
@@ -513,7 +538,7 @@ __global__ void __launch_bounds__(kExactThreads)
   }
   __syncthreads();
   block_bitonic_sort(s_ex, n2);
-  for (int j = tid; j < k; j += kExactThreads) {
+  for (int j = tid; j < k; j += nt) {
     const uint64_t key = j < n2 ? s_ex[j] : kEmpty;
     const size_t o = static_cast<size_t>(qi) * k + j;
     D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
@@ -588,10 +613,11 @@ void launch_cand_exact(const int64_t* rows, int nq, int R, int k, const float* c
   if (nq <= 0) return;
   HB_CHECK(R >= 1 && R <= kCandMaxR && k <= R, HB_ERR_INVALID, "candidate count out of range");
   const size_t keys = static_cast<size_t>(pow2_ceil(R < 2 ? 2 : R)) * sizeof(uint64_t);
-  const size_t smem_ex = keys + static_cast<size_t>(kExactThreads) * kExStride * sizeof(float);
+  const int nt = std::min(kExactThreads, std::max(64, (R + 31) / 32 * 32));
+  const size_t smem_ex = keys + static_cast<size_t>(nt) * kExStride * sizeof(float);
   HB_CUDA(cudaFuncSetAttribute(cand_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                static_cast<int>(smem_ex)));
-  cand_exact_kernel<<<nq, kExactThreads, smem_ex, st>>>(rows, R, k, codes, q, dpad, ids, D, I);
+  cand_exact_kernel<<<nq, nt, smem_ex, st>>>(rows, R, k, codes, q, dpad, ids, D, I);
   HB_CUDA(cudaGetLastError());
 }
 

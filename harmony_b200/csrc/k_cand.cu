@@ -58,7 +58,7 @@ constexpr int kSelectThreads = 256;
 constexpr int kBins = 2048;                 // histogram bins of the candidate selection
 constexpr int kSelUnroll = 4;               // 32-value runs a warp loads at once
 constexpr int kExactThreads = 256;
-constexpr int kExChunk = 64;                // dimensions per staged chunk of the exact re-rank
+constexpr int kExChunk = 32;                // dimensions per staged chunk of the exact re-rank
 constexpr int kExStride = kExChunk + 1;     // odd row stride: column reads hit distinct banks
 
 struct CandShared {
@@ -380,8 +380,9 @@ __global__ void __launch_bounds__(kSelectThreads)
     const float range = vmax - vmin;
     float scale = range > 0.0f ? static_cast<float>(kBins) / range : 0.0f;
     if (!(scale < 1e30f)) scale = 0.0f;
-    // Pass 2: histogram (lanes of a warp that hit one bin add once); each
-    // warp loads four 32-value runs before it bins them.
+    // Pass 2: histogram (one shared atomic per value: the values of a run
+    // spread over the bins); each warp loads four 32-value runs before it
+    // bins them.
     for (int base = tid & ~31; base < m; base += kSelUnroll * kSelectThreads) {
       float vv[kSelUnroll];
 #pragma unroll
@@ -390,15 +391,8 @@ __global__ void __launch_bounds__(kSelectThreads)
         vv[u] = i < m ? src[i] : INFINITY;
       }
 #pragma unroll
-      for (int u = 0; u < kSelUnroll; ++u) {
-        const bool valid = vv[u] < INFINITY;
-        const int bin = valid ? value_bin(vv[u], vmin, scale) : 0;
-        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-        if (valid) {
-          const unsigned peers = __match_any_sync(vmask, bin);
-          if (lane == __ffs(peers) - 1) atomicAdd(&s_hist[bin], __popc(peers));
-        }
-      }
+      for (int u = 0; u < kSelUnroll; ++u)
+        if (vv[u] < INFINITY) atomicAdd(&s_hist[value_bin(vv[u], vmin, scale)], 1);
     }
     __syncthreads();
     // The bin holding the need-th value: lane L sums bins [64L, 64L + 64)
@@ -479,9 +473,10 @@ __global__ void __launch_bounds__(kSelectThreads)
 // reference's sequential unfused FP32 loop (the same operations, in the same
 // order, as exact_l2_seq), then the k best (distance, row).  Thread t owns
 // candidate t of each batch of blockDim.x (R rounded up to a warp, 64 to
-// 256); the batch's rows and the query are staged 64 dimensions at a time
-// in shared memory by coalesced loads (two rows per warp instruction), and
-// each thread continues its own sum over the chunk from shared memory.
+// 256); the batch's rows and the query are staged 32 dimensions at a time
+// in shared memory by coalesced loads (four 128-byte rows per warp
+// instruction, all of a thread's loads in flight at once), and each thread
+// continues its own sum over the chunk from shared memory.
 __global__ void __launch_bounds__(kExactThreads)
     cand_exact_kernel(const int64_t* __restrict__ rows, int R, int k, const float* __restrict__ codes,
                       const float* __restrict__ q, int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
@@ -504,8 +499,9 @@ __global__ void __launch_bounds__(kExactThreads)
       const int w4 = min(kExChunk, dpad - c0) / 4;  // dpad is a multiple of 4
       __syncthreads();                              // rows published / previous chunk consumed
       if (tid < w4) *reinterpret_cast<float4*>(s_q + 4 * tid) = *reinterpret_cast<const float4*>(qrow + c0 + 4 * tid);
-#pragma unroll 4
-      for (int u = tid; u < nt * (kExChunk / 4); u += nt) {
+#pragma unroll
+      for (int j = 0; j < kExChunk / 4; ++j) {
+        const int u = tid + j * nt;
         const int r = u / (kExChunk / 4), f = u % (kExChunk / 4);
         const int64_t rr = s_rows[r];
         if (rr >= 0 && f < w4) {

@@ -582,6 +582,102 @@ def run_c4(args):
     print(json.dumps(line))
 
 
+def run_c3(args):
+    """Config 3: 270k x 500 anisotropic mixture (per-dimension variance
+    proportional to (j + 1)^-1.2), nlist 512, nprobe 32, k 100, 5000 queries.
+    Arms: the exact FP32 scan and the BF16 candidate-matrix scan with the exact
+    FP32 re-rank of the 2k (rerank_mult 2) and 4k best.  Each arm is timed with
+    queries and results resident on the device (CUDA events on the index
+    stream) and end to end (pinned host queries and results, wall clock around
+    the synchronous calls).  Recall@100 and the largest relative distance error
+    are taken against FP64 ground truth on the first 1000 queries; same_as_fp32
+    is the fraction of queries whose k results equal the exact scan's bit for
+    bit."""
+    import torch
+    from harmony_b200 import Index, Precision, SearchMode, datasets
+    k, nq, nb, d, nlist, P = 100, args.nq or 5000, args.nb or 270_000, 500, 512, 32
+    base_np, q_np = datasets.config3(nb=nb, nq=nq)
+    base = torch.from_numpy(base_np).cuda()
+    queries = torch.from_numpy(q_np).cuda()
+    ix = Index(d, nlist, P)
+    t0 = time.perf_counter()
+    ix.train(nb, base)
+    ix.add(nb, base)
+    torch.cuda.synchronize()
+    build_s = round(time.perf_counter() - t0, 2)
+    # FP64 ground truth of the first 1000 queries: exhaustive FP32 top 128,
+    # re-ranked in FP64.
+    ng = min(1000, nq)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.BRUTE_FORCE), "")
+    GI = torch.empty((ng, 128), dtype=torch.int64, device="cuda")
+    G = torch.empty((ng, 128), dtype=torch.float32, device="cuda")
+    ix.search(ng, queries[:ng], 128, G, GI)
+    cand = base[GI.reshape(-1)].double().reshape(ng, 128, d)
+    d64 = ((cand - queries[:ng].double()[:, None, :]) ** 2).sum(-1)
+    order = torch.argsort(d64, dim=1, stable=True)
+    gt = torch.gather(GI, 1, order)[:, :k].cpu().numpy()
+    del cand, d64
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    ix.nprobe = P
+    q_host = torch.empty((nq, d), dtype=torch.float32).pin_memory()
+    q_host.copy_(queries.cpu())
+    D_host = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    I_host = torch.empty((nq, k), dtype=torch.int64).pin_memory()
+    D_dev = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    I_dev = torch.empty((nq, k), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.ExternalStream(ix.stream)
+    arms, ref = {}, None
+    for name, prec, mult in (("fp32", Precision.FP32, 2), ("bf16_rerank2k", Precision.BF16, 2),
+                             ("bf16_rerank4k", Precision.BF16, 4)):
+        sp = ix.search_params
+        sp.precision, sp.rerank_mult = prec, mult
+        reps = 3 if prec == Precision.FP32 else 10
+        for _ in range(3):
+            ix.search(nq, queries, k, D_dev, I_dev)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            ix.search(nq, queries, k, D_dev, I_dev)
+        e1.record(stream)
+        e1.synchronize()
+        ms_dev = e0.elapsed_time(e1) / reps
+        t1 = time.perf_counter()
+        for _ in range(reps):
+            ix.search(nq, q_host, k, D_host, I_host)
+        ms_e2e = 1e3 * (time.perf_counter() - t1) / reps
+        ix.profile(True)
+        ix.search(nq, queries, k, D_dev, I_dev)
+        kern = {kk: round(v[0], 3) for kk, v in ix.profile_read().items()}
+        ix.profile(False)
+        Dn, In = D_dev.cpu().numpy(), I_dev.cpu().numpy()
+        # Largest relative error of the returned distances against FP64.
+        sel = torch.from_numpy(In[:ng]).cuda()
+        x = base[sel.reshape(-1)].double().reshape(ng, k, d)
+        e64 = ((x - queries[:ng].double()[:, None, :]) ** 2).sum(-1).cpu().numpy()
+        del x
+        err = float(np.max(np.abs(Dn[:ng].astype(np.float64) - e64) / np.maximum(e64, 1e-30)))
+        arm = {"ms_device": round(ms_dev, 3), "qps_device": round(nq / ms_dev * 1e3, 1),
+               "ms_e2e": round(ms_e2e, 3), "qps_e2e": round(nq / ms_e2e * 1e3, 1),
+               "recall_at_100_vs_fp64_first_1000": round(recall(In[:ng], gt, k), 4),
+               "max_rel_dist_err_vs_fp64": err, "kernels_ms": kern}
+        if ref is None:
+            ref = Dn
+        else:
+            arm["same_as_fp32"] = round(float(np.mean([np.array_equal(a, b) for a, b in
+                                                       zip(Dn.view(np.uint32), ref.view(np.uint32))])), 4)
+        arms[name] = arm
+    ix.search_params.precision = Precision.FP32
+    line = {"metric": "QPS, config3 (270k x 500 anisotropic mixture, nlist 512, nprobe 32, k 100, 5000 queries)",
+            "workload": "c3", "unit": "queries/s", "n_gpus": 1, "dtype": "f32 / bf16",
+            "data": "synthetic (seeded anisotropic Gaussian mixture; stands in for nuswide's shape)",
+            "config": {"nb": nb, "d": d, "nlist": nlist, "nprobe": P, "k": k, "nq": nq, "build_s": build_s,
+                       "inputs": "8.6 MB of queries per step; the index (540 MB FP32 + 276 MB BF16) exceeds L2"},
+            "arms": arms}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -594,8 +690,9 @@ def main():
     ap.add_argument("--nb", type=int, default=None, help="smaller base for profiling runs (not a bench line)")
     ap.add_argument("--nq", type=int, default=None, help="fewer queries for profiling runs (not a bench line)")
     ap.add_argument("--ntrain", type=int, default=200_000, help="training queries of the learned probe")
-    ap.add_argument("--workload", choices=["c5", "c4"], default="c5",
-                    help="c5: the headline bench line; c4: the batch-stream measurement of config 4")
+    ap.add_argument("--workload", choices=["c5", "c4", "c3"], default="c5",
+                    help="c5: the headline bench line; c4: the batch-stream measurement of config 4; "
+                         "c3: the 500-dimensional k = 100 measurement of config 3")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -607,6 +704,8 @@ def main():
         WORKLOAD["workload"] += f" [reduced: nq={args.nq}]"
     if args.workload == "c4":
         run_c4(args)
+    elif args.workload == "c3":
+        run_c3(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

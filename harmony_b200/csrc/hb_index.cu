@@ -1346,25 +1346,6 @@ class IndexCore {
     a.seg = seg_.p;
     a.cand = cand_.p;
     a.err = err_dev_.p;
-    // Items = sum over lists of tiles x ceil(queries / 128)
-    //      <= (largest tile count) x (entries / 128) + (total tiles).
-    int64_t max_tiles = 0, all_tiles = 0;
-    for (size_t l = 0; l < nlist_; ++l) {
-      const int64_t t = (host_off_[l + 1] - host_off_[l] + 127) / 128;
-      max_tiles = std::max(max_tiles, t);
-      all_tiles += t;
-    }
-    const int64_t item_cap = std::max<int64_t>(1, max_tiles * static_cast<int64_t>((nqp + 127) / 128) + all_tiles);
-    cand_items_.reserve(static_cast<size_t>(item_cap));
-    cand_sbase_.reserve(static_cast<size_t>(item_cap) * 128);
-    a.items = cand_items_.p;
-    a.item_sbase = cand_sbase_.p;
-    a.item_cap = item_cap;
-    {
-      Scope sc(this, "cand_items");
-      launch_cand_items(a, st_);
-    }
-    ++launches_;
     {
       Scope sc(this, "cand_scan");
       launch_cand_scan(gqmap_, tmap_, a, num_sms_, st_);
@@ -1730,8 +1711,6 @@ class IndexCore {
   DevBuf<uint16_t> gq_;
   DevBuf<float> cand_;
   DevBuf<int64_t> cand_rows_;
-  DevBuf<CandItemDesc> cand_items_;
-  DevBuf<int64_t> cand_sbase_;
   // tensor-core coarse quantizer
   bool coarse_ready_ = false;
   int coarse_kind_ = HB_COARSE_AUTO;

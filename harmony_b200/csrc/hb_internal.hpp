@@ -201,17 +201,6 @@ void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, i
 // Candidate-matrix BF16 scan (k_cand.cu): any kpad (a multiple of 64) and up
 // to kCandMaxR candidates per query.
 constexpr int kCandMaxR = 4096;
-// One work item of the candidate scan, written by launch_cand_items so that
-// the scan's roles read it with one load (64 bytes).
-struct CandItemDesc {
-  int32_t list, qcnt, ntiles, pad;
-  int64_t row0;   // first stored row of the item's rows
-  int64_t tile0;  // its first 128-row norm tile
-  int64_t qrow0;  // first row of its query group in the gathered matrix
-  int64_t rl0;    // position of its first row within the list
-  int64_t slen;   // the list's segment length (rows rounded up to 4)
-  int64_t pad2;
-};
 struct CandArgs {
   const int64_t* list_off;
   int nlist;
@@ -227,13 +216,7 @@ struct CandArgs {
   const int64_t* seg;       // nq x P + 1: start of each (query, probe rank) segment of `cand`
   float* cand;              // candidate rows: ||x||^2 - 2 q~.x~, +inf padding
   int* err;
-  CandItemDesc* items;      // item table (item_cap entries)
-  int64_t* item_sbase;      // per item, the segment start of each of its 128 query lanes
-  int64_t item_cap;
 };
-// Item table of the candidate scan (one CTA per list); sets err to 35 when
-// the batch has more items than item_cap.
-void launch_cand_items(const CandArgs& a, cudaStream_t st);
 size_t cand_segments_tmp_bytes(int nq, int P);
 void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* list_off, int64_t* seg, void* tmp,
                           size_t tmp_bytes, cudaStream_t st);

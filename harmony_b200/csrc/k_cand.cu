@@ -6,10 +6,7 @@
 //     of the list-major work description, the query in BF16 (K = kpad, zero
 //     padded): one row per entry, so the queries of one work item are 128
 //     consecutive rows and reach the tensor cores by plain TMA tiles.
-//  2. cand_items_kernel writes the table of work items (one descriptor per
-//     item and the segment start of each of its query lanes), so that the
-//     scan's roles read an item with one load instead of a search.
-//  3. cand_scan_kernel: persistent, one CTA per SM, 192 threads (4 epilogue
+//  2. cand_scan_kernel: persistent, one CTA per SM, 192 threads (4 epilogue
 //     warps, a TMA warp, an MMA warp).  Work items are (list, chunk of rows,
 //     group of <= 128 queries); the search uses one 128-row tile per item,
 //     so the items spread evenly over the CTAs.  For each 128-row tile of the chunk the TMA
@@ -20,11 +17,11 @@
 //     v = ||x||^2 - 2 q~.x~ of the tile's rows into the query's candidate
 //     row: the concatenation over its probes, in probe order, of one segment
 //     per probed list (the list's length rounded up to 4; +inf past the end).
-//  4. cand_select_kernel: one CTA per query selects the R smallest keys
+//  3. cand_select_kernel: one CTA per query selects the R smallest keys
 //     (v, position) of its candidate row (block radix selection over the row
 //     staged in shared memory; unique keys, so the choice is deterministic)
 //     and maps each position back to its stored row.
-//  5. cand_exact_kernel: one CTA per query recomputes the R distances with
+//  4. cand_exact_kernel: one CTA per query recomputes the R distances with
 //     the reference's sequential unfused FP32 loop and returns the k best
 //     (distance, row) -- the same rule as the heap scan's rerank, so whenever
 //     the true k nearest are among the R candidates the result equals the
@@ -73,6 +70,36 @@ struct CandShared {
   uint32_t tmem;
 };
 
+struct CandItem {
+  int list, chunk, group, qcnt, ntiles;
+  int64_t row0;   // first stored row of the chunk
+  int64_t tile0;  // its first 128-row norm tile
+  int64_t qrow0;  // first query row of the group in the gathered matrix
+};
+
+__device__ __forceinline__ CandItem cand_item(const CandArgs& a, int64_t item) {
+  int lo = 0, hi = a.nlist;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a.item_off[mid] <= item) lo = mid; else hi = mid;
+  }
+  CandItem d;
+  const int l = lo;
+  const int64_t local = item - a.item_off[l];
+  const int ng = (a.list_cnt[l] + kT - 1) / kT;
+  d.list = l;
+  d.chunk = static_cast<int>(local / ng);
+  d.group = static_cast<int>(local % ng);
+  d.qcnt = min(kT, a.list_cnt[l] - d.group * kT);
+  const int64_t r0 = a.list_off[l] + static_cast<int64_t>(d.chunk) * a.chunk_rows;
+  const int64_t r1 = min(a.list_off[l + 1], r0 + static_cast<int64_t>(a.chunk_rows));
+  d.row0 = r0;
+  d.ntiles = static_cast<int>((r1 - r0 + kT - 1) / kT);
+  d.tile0 = a.tile_off[l] + static_cast<int64_t>(d.chunk) * (a.chunk_rows / kT);
+  d.qrow0 = a.list_qoff[l] + static_cast<int64_t>(d.group) * kT;
+  return d;
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     cand_scan_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_x,
                      CandArgs a) {
@@ -81,9 +108,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nkb = a.kpad / 64;
-  // A batch with more items than the table holds was flagged (code 35) by
-  // cand_items_kernel and is not scanned.
-  const int64_t total = a.item_off[a.nlist] <= a.item_cap ? a.item_off[a.nlist] : 0;
+  const int64_t total = a.item_off[a.nlist];
 
   if (warp == 5) tmem_alloc(&sh.tmem, kAccN * kT);
   if (tid == 0) {
@@ -110,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       int64_t it = 0;
       bool ok = true;
       for (int64_t item = blockIdx.x; ok && item < total; item += gridDim.x) {
-        const CandItemDesc d = a.items[item];
+        const CandItem d = cand_item(a, item);
         for (int t = 0; ok && t < d.ntiles; ++t) {
           for (int kb = 0; kb < nkb; ++kb, ++it) {
             const int s = static_cast<int>(it % kStg);
@@ -138,8 +163,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       int64_t it = 0, tile = 0;
       bool ok = true;
       for (int64_t item = blockIdx.x; ok && item < total; item += gridDim.x) {
-        const int nt = a.items[item].ntiles;
-        for (int t = 0; t < nt; ++t, ++tile) {
+        const CandItem d = cand_item(a, item);
+        for (int t = 0; t < d.ntiles; ++t, ++tile) {
           const int b = static_cast<int>(tile % kAccN);
           if (!mbar_wait(&sh.acce[b], static_cast<uint32_t>((tile / kAccN) & 1) ^ 1u, a.err, 33)) {
             ok = false;
@@ -175,30 +200,23 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t lane_base = (32u * static_cast<uint32_t>(warp)) << 16;
     int64_t tile = 0;
     bool ok = true;
-    // The item and this lane's segment start come from the item table; the
-    // next item's are loaded before the current item's tiles are written.
-    CandItemDesc d{};
-    int64_t sb = 0;
-    if (blockIdx.x < total) {
-      d = a.items[blockIdx.x];
-      sb = a.item_sbase[static_cast<int64_t>(blockIdx.x) * kT + tid];
-    }
     for (int64_t item = blockIdx.x; ok && item < total; item += gridDim.x) {
-      const int64_t nx = item + gridDim.x;
-      CandItemDesc dn{};
-      int64_t sbn = 0;
-      if (nx < total) {
-        dn = a.items[nx];
-        sbn = a.item_sbase[nx * kT + tid];
+      const CandItem d = cand_item(a, item);
+      // This thread's query (lane tid of the group) and its segment.
+      int64_t sbase = 0, slen = 0;
+      if (tid < d.qcnt) {
+        const uint32_t e = static_cast<uint32_t>(a.list_q[d.qrow0 + tid]);
+        const int64_t qp = static_cast<int64_t>(e >> 16) * a.P + (e & 0xffffu);
+        sbase = a.seg[qp];
+        slen = a.seg[qp + 1] - sbase;
       }
-      const int64_t sbase = sb, slen = tid < d.qcnt ? d.slen : 0;  // lanes past the group write nothing
       for (int t = 0; t < d.ntiles; ++t, ++tile) {
         const int b = static_cast<int>(tile % kAccN);
         if (ok) ok = mbar_wait(&sh.accf[b], static_cast<uint32_t>((tile / kAccN) & 1), a.err, 34);
         ok = __all_sync(0xffffffffu, ok);
         if (!ok) break;
         tc_fence_after();
-        const int64_t rl0 = d.rl0 + static_cast<int64_t>(t) * kT;
+        const int64_t rl0 = static_cast<int64_t>(d.chunk) * a.chunk_rows + static_cast<int64_t>(t) * kT;
         // The tile's 128 row norms: one coalesced load per 32 columns, then
         // handed to every lane by shuffles.
         const float* tn = a.tile_norm + (d.tile0 + t) * kT;
@@ -227,8 +245,6 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_before();
         mbar_arrive(&sh.acce[b]);
       }
-      d = dn;
-      sb = sbn;
     }
   }
   tc_fence_before();
@@ -236,48 +252,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 5) {
     tc_fence_after();
     tmem_dealloc(tmem, kAccN * kT);
-  }
-}
-
-// Item table: one CTA (128 threads) per list writes each of the list's
-// items (chunk-major, then query group) and, per query lane, the start of
-// that query's segment for the list.
-__global__ void __launch_bounds__(kT) cand_items_kernel(CandArgs a) {
-  const int l = blockIdx.x, t = threadIdx.x;
-  const int64_t i0 = a.item_off[l], i1 = a.item_off[l + 1];
-  if (i0 == i1) return;
-  if (i1 > a.item_cap) {
-    if (t == 0) atomicCAS(a.err, 0, 35);
-    return;
-  }
-  const int cnt = a.list_cnt[l];
-  const int ng = (cnt + kT - 1) / kT;
-  const int64_t lb = a.list_off[l], le = a.list_off[l + 1];
-  for (int64_t it = i0; it < i1; ++it) {
-    const int64_t local = it - i0;
-    const int chunk = static_cast<int>(local / ng), group = static_cast<int>(local % ng);
-    const int qcnt = min(kT, cnt - group * kT);
-    const int64_t r0 = lb + static_cast<int64_t>(chunk) * a.chunk_rows;
-    const int64_t r1 = min(le, r0 + static_cast<int64_t>(a.chunk_rows));
-    const int64_t qrow0 = a.list_qoff[l] + static_cast<int64_t>(group) * kT;
-    if (t == 0) {
-      CandItemDesc d;
-      d.list = l;
-      d.qcnt = qcnt;
-      d.ntiles = static_cast<int>((r1 - r0 + kT - 1) / kT);
-      d.pad = 0;
-      d.row0 = r0;
-      d.tile0 = a.tile_off[l] + static_cast<int64_t>(chunk) * (a.chunk_rows / kT);
-      d.qrow0 = qrow0;
-      d.rl0 = static_cast<int64_t>(chunk) * a.chunk_rows;
-      d.slen = (le - lb + 3) & ~int64_t(3);
-      d.pad2 = 0;
-      a.items[it] = d;
-    }
-    if (t < qcnt) {
-      const uint32_t e = static_cast<uint32_t>(a.list_q[qrow0 + t]);
-      a.item_sbase[it * kT + t] = a.seg[static_cast<int64_t>(e >> 16) * a.P + (e & 0xffffu)];
-    }
   }
 }
 
@@ -593,12 +567,6 @@ void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* l
   HB_CUDA(cudaGetLastError());
   size_t bytes = cub_bytes;
   HB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, len, seg, static_cast<int64_t>(n), st));
-}
-
-void launch_cand_items(const CandArgs& a, cudaStream_t st) {
-  if (a.nlist <= 0) return;
-  cand_items_kernel<<<a.nlist, kT, 0, st>>>(a);
-  HB_CUDA(cudaGetLastError());
 }
 
 void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* list_q, const int64_t* n_entries,

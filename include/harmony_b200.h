@@ -72,7 +72,9 @@ typedef struct {
   int32_t warmup_lists;       /* preSearch warmUpSearchList (default 10)        */
   int32_t warmup_list_size;   /* preSearch warmUpSearchListSize (0 -> k)        */
   int32_t precision;          /* HB_PREC_*                                     */
-  int32_t rerank_mult;        /* BF16: candidates re-ranked = rerank_mult * k (default 2) */
+  int32_t rerank_mult;        /* BF16: candidates re-ranked = rerank_mult * k (default 2;
+                                 at most 64 on the d <= 128 heap scan, else at most 4096;
+                                 k itself up to 4096) */
   int32_t learned_probe;      /* 1: per-query nprobe from the learned predictor */
   float learned_target;       /* predictor target recall (0 -> trained target)   */
   const int32_t* nprobe_per_query; /* optional nq array (host or device); overrides nprobe */

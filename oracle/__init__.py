@@ -235,6 +235,17 @@ class RefIndex:
             L.ref_heap_topk.argtypes = [_sz, _f, _sz, _f, _i]
             L.ref_l2.restype = ctypes.c_float
             L.ref_l2.argtypes = [_f, _f, _sz]
+            _cp, _ip32 = ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)
+            L.ref_load_fvecs.restype = _sz
+            L.ref_load_fvecs.argtypes = [_cp, ctypes.c_int, ctypes.c_int, _f, _ip32]
+            L.ref_load_bvecs.restype = _sz
+            L.ref_load_bvecs.argtypes = [_cp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), _ip32]
+            L.ref_load_xvecs.restype = _sz
+            L.ref_load_xvecs.argtypes = [_cp, ctypes.c_int, ctypes.c_int, _f, _ip32]
+            for fn in ("ref_calculate_recall", "ref_calculate_recall_loose", "ref_calculate_r2"):
+                getattr(L, fn).restype = ctypes.c_float
+                getattr(L, fn).argtypes = [_i, _f, _i, _f, _sz, _sz, _sz]
+            L.ref_stats_csv.argtypes = [_cp, ctypes.c_int, _cp, _cp, ctypes.c_int, _i, _d]
             L.ref_set_threads.argtypes = [ctypes.c_int]
             L.ref_max_threads.restype = ctypes.c_int
             cls._L = L
@@ -351,6 +362,63 @@ class RefIndex:
         I = np.empty(k, np.int64)
         cls.lib().ref_heap_topk(vals.size, _fp(vals), k, _fp(D), _ip(I))
         return D, I
+
+    # ---- the query driver's evaluation helpers (src/utils.h, src/stats.h) ----
+
+    @classmethod
+    def _load(cls, fn, path, bounds, dtype):
+        d = ctypes.c_int()
+        p = path.encode()
+        n = fn(p, bounds[0], bounds[1], None, ctypes.byref(d))
+        out = np.empty((n, d.value), dtype)
+        fn(p, bounds[0], bounds[1], out.ctypes.data_as(ctypes.POINTER(np.ctypeslib.as_ctypes_type(dtype))),
+           ctypes.byref(d))
+        return out
+
+    @classmethod
+    def load_fvecs(cls, path, bounds=(1, 0)):
+        return cls._load(cls.lib().ref_load_fvecs, path, bounds, np.float32)
+
+    @classmethod
+    def load_bvecs(cls, path, bounds=(1, 0)):
+        return cls._load(cls.lib().ref_load_bvecs, path, bounds, np.uint8)
+
+    @classmethod
+    def load_xvecs(cls, path, bounds=(1, 0)):
+        return cls._load(cls.lib().ref_load_xvecs, path, bounds, np.float32)
+
+    @classmethod
+    def _measure(cls, fn, I, D, GT, GD, k, gt_k):
+        I, GT = _i64(I), _i64(GT)
+        D, GD = _f32(D), _f32(GD)
+        return np.float32(fn(_ip(I), _fp(D), _ip(GT), _fp(GD), I.size // k, k, gt_k))
+
+    @classmethod
+    def calculate_recall(cls, I, D, GT, GD, k, gt_k=0):
+        return cls._measure(cls.lib().ref_calculate_recall, I, D, GT, GD, k, gt_k)
+
+    @classmethod
+    def calculate_recall_loose(cls, I, D, GT, GD, k, gt_k=0):
+        return cls._measure(cls.lib().ref_calculate_recall_loose, I, D, GT, GD, k, gt_k)
+
+    @classmethod
+    def calculate_r2(cls, I, D, GT, GD, k, gt_k=0):
+        return cls._measure(cls.lib().ref_calculate_r2, I, D, GT, GD, k, gt_k)
+
+    _STATS_INT = ["nlist", "nprobe", "opt_level", "total_count", "skip_triangle_count", "skip_triangle_large_count",
+                  "skip_subnn_L2_count", "skip_subnn_IP_count", "simi_update_count", "check_subnn_L2_ele_count",
+                  "check_subnn_IP_ele_count", "check_subnn_L2_count", "check_subnn_IP_count", "nb", "nq", "d", "k",
+                  "divideIVF", "disableOrderOptimize", "blockSend", "pruning", "block", "worker", "group", "team"]
+    _STATS_DBL = ["simi_ratio", "faiss_query_time", "query_time", "original_time", "recall", "r2", "variance",
+                  "trainTime", "addTime", "preSearchTime", "inBalanceRatio", "inBalanceRatioTeam", "brute_ratio"]
+
+    @classmethod
+    def stats_csv(cls, path, append, dataset, record, my=False):
+        """The reference's Stats::toCsv / myToCsv of the fields of `record`."""
+        iv = np.array([int(getattr(record, f)) for f in cls._STATS_INT], np.int64)
+        dv = np.array([float(getattr(record, f)) for f in cls._STATS_DBL], np.float64)
+        cls.lib().ref_stats_csv(path.encode(), int(append), dataset.encode(), record.mode.encode(), int(my),
+                                _ip(iv), dv.ctypes.data_as(_d))
 
     @classmethod
     def l2(cls, a, b):

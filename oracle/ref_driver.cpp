@@ -200,4 +200,103 @@ void ref_heap_topk(size_t n, const float* vals, size_t k, float* D, int64_t* I) 
 
 float ref_l2(const float* a, const float* b, size_t d) { return calculatedEuclideanDistance(a, b, d); }
 
+// The query driver's evaluation helpers (src/utils.h:187-407, 631-755;
+// src/stats.h:101-125), exposed for the harness tests.  Loaders copy rows
+// a..b (1-based, inclusive; b = 0 for all) into out when out is non-null
+// and return the row count, *d_out the dimension.
+size_t ref_load_fvecs(const char* path, int a, int b, float* out, int* d_out) {
+  auto [v, n, d] = loadFvecs(path, {a, b});
+  *d_out = d;
+  if (out && v) std::memcpy(out, v.get(), n * static_cast<size_t>(d) * sizeof(float));
+  return n;
+}
+
+size_t ref_load_bvecs(const char* path, int a, int b, uint8_t* out, int* d_out) {
+  auto [v, n, d] = loadBvecs(path, {a, b});
+  *d_out = d;
+  if (out && v) std::memcpy(out, v.get(), n * static_cast<size_t>(d));
+  return n;
+}
+
+size_t ref_load_xvecs(const char* path, int a, int b, float* out, int* d_out) {
+  auto [v, n, d] = loadXvecs(path, {a, b});
+  *d_out = d;
+  if (out && v) std::memcpy(out, v.get(), n * static_cast<size_t>(d) * sizeof(float));
+  return n;
+}
+
+float ref_calculate_recall(const int64_t* I, const float* D, const int64_t* GT, const float* GD, size_t nq,
+                           size_t k, size_t gt_k) {
+  QuietStdout quiet;
+  return calculate_recall(I, D, GT, GD, nq, k, METRIC_L2, gt_k);
+}
+
+float ref_calculate_recall_loose(const int64_t* I, const float* D, const int64_t* GT, const float* GD, size_t nq,
+                                 size_t k, size_t gt_k) {
+  QuietStdout quiet;
+  return calculate_recall_loose(I, D, GT, GD, nq, k, METRIC_L2, gt_k);
+}
+
+float ref_calculate_r2(const int64_t* I, const float* D, const int64_t* GT, const float* GD, size_t nq, size_t k,
+                       size_t gt_k) {
+  return calculate_r2(I, D, GT, GD, nq, k, METRIC_L2, gt_k);
+}
+
+// Stats::toCsv (which = 0) or Stats::myToCsv (which = 1) of a Stats whose
+// fields are iv = {nlist, nprobe, opt_level, total_count, skip_triangle_count,
+// skip_triangle_large_count, skip_subnn_L2_count, skip_subnn_IP_count,
+// simi_update_count, check_subnn_L2_ele_count, check_subnn_IP_ele_count,
+// check_subnn_L2_count, check_subnn_IP_count, nb, nq, d, k, divideIVF,
+// disableOrderOptimize, blockSend, pruning, block, worker, group, team} and
+// dv = {simi_ratio, faiss_query_time, query_time, original_time, recall, r2,
+// variance, trainTime, addTime, preSearchTime, inBalanceRatio,
+// inBalanceRatioTeam, brute_ratio}.
+void ref_stats_csv(const char* path, int append, const char* dataset, const char* mode, int which,
+                   const int64_t* iv, const double* dv) {
+  Stats s;
+  s.nlist = iv[0];
+  s.nprobe = iv[1];
+  s.opt_level = static_cast<OptLevel>(iv[2]);
+  s.total_count = iv[3];
+  s.skip_triangle_count = iv[4];
+  s.skip_triangle_large_count = iv[5];
+  s.skip_subnn_L2_count = iv[6];
+  s.skip_subnn_IP_count = iv[7];
+  s.simi_update_count = iv[8];
+  s.check_subnn_L2_ele_count = iv[9];
+  s.check_subnn_IP_ele_count = iv[10];
+  s.check_subnn_L2_count = iv[11];
+  s.check_subnn_IP_count = iv[12];
+  s.nb = iv[13];
+  s.nq = iv[14];
+  s.d = iv[15];
+  s.k = iv[16];
+  s.divideIVF = iv[17] != 0;
+  s.disableOrderOptimize = iv[18] != 0;
+  s.blockSend = iv[19] != 0;
+  s.pruning = iv[20] != 0;
+  s.block = iv[21];
+  s.worker = iv[22];
+  s.group = iv[23];
+  s.team = iv[24];
+  s.simi_ratio = static_cast<float>(dv[0]);
+  s.faiss_query_time = dv[1];
+  s.query_time = dv[2];
+  s.original_time = dv[3];
+  s.recall = dv[4];
+  s.r2 = dv[5];
+  s.variance = dv[6];
+  s.trainTime = dv[7];
+  s.addTime = dv[8];
+  s.preSearchTime = dv[9];
+  s.inBalanceRatio = dv[10];
+  s.inBalanceRatioTeam = dv[11];
+  s.brute_ratio = dv[12];
+  s.mode = mode;
+  if (which == 0)
+    s.toCsv(path, append != 0, dataset);
+  else
+    s.myToCsv(path, append != 0, dataset);
+}
+
 }  // extern "C"

@@ -148,6 +148,8 @@ def lib() -> ctypes.CDLL:
     L.hb_launch_count.argtypes = [vp]
     L.hb_train_probe_predictor.argtypes = [vp, sz, f, sz, sz, ctypes.c_float]
     L.hb_search_noalloc.argtypes = [vp, sz, f, sz, f, i64]
+    L.hb_retain_lists.argtypes = [vp, sz, sz]
+    L.hb_merge_topk.argtypes = [vp, sz, sz, sz, f, i64, f, i64]
     L.hb_probe_calibration.argtypes = [vp, f, f, f, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.hb_profile_enable.argtypes = [vp, ctypes.c_int]
     L.hb_profile_read.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
@@ -290,6 +292,25 @@ class Index:
         out = np.empty(nl, np.int64)
         _check(self._L.hb_get_list_sizes(self._h, out.ctypes.data))
         return out
+
+    def retain_lists(self, first: int, count: int) -> None:
+        """Keep lists [first, first + count) and empty the others: one rank's
+        share of the reference's DIVIDE_IVF partition (src/Index.cpp:79-104).
+        Ids are unchanged."""
+        _check(self._L.hb_retain_lists(self._h, int(first), int(count)))
+
+    def merge_topk(self, D_parts, I_parts, D, I) -> None:
+        """Merge per-shard results (device tensors of shape (parts, nq, k)) into
+        D, I (nq, k) with the reference master's heap rule
+        (src/Index.cpp:1327-1341), on this index's stream."""
+        parts, nq, k = D_parts.shape
+        for t in (D_parts, I_parts, D, I):
+            if not (hasattr(t, "is_cuda") and t.is_cuda and t.is_contiguous()):
+                raise TypeError("merge_topk takes contiguous CUDA tensors")
+        if tuple(I_parts.shape) != (parts, nq, k) or tuple(D.shape) != (nq, k) or tuple(I.shape) != (nq, k):
+            raise ValueError("shape mismatch")
+        _check(self._L.hb_merge_topk(self._h, parts, nq, k, D_parts.data_ptr(), I_parts.data_ptr(), D.data_ptr(),
+                                     I.data_ptr()))
 
     @property
     def stream(self) -> int:

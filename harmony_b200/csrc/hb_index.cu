@@ -1078,6 +1078,57 @@ class IndexCore {
                               cudaMemcpyDefault, st_));
     HB_CUDA(cudaStreamSynchronize(st_));
   }
+  // Keep lists [first, first + count) and empty the others (one rank's share
+  // of the reference's DIVIDE_IVF partition, src/Index.cpp:79-104): the kept
+  // lists are one contiguous block of rows, moved to the front with their
+  // ids (which stay the index's own), norms and offsets.
+  void retain_lists(size_t first, size_t count) {
+    HB_CHECK(trained_, HB_ERR_STATE, "index not trained");
+    HB_CHECK(first <= nlist_ && count <= nlist_ - first, HB_ERR_INVALID, "list range outside the index");
+    HB_CUDA(cudaSetDevice(device_));
+    const int64_t r0 = host_off_[first], r1 = host_off_[first + count];
+    const size_t kept = static_cast<size_t>(r1 - r0);
+    if (kept && r0 > 0) {
+      DevBuf<float> c;
+      DevBuf<int64_t> i;
+      DevBuf<float> n;
+      c.reserve(kept * dpad_);
+      i.reserve(kept);
+      n.reserve(kept);
+      HB_CUDA(cudaMemcpyAsync(c.p, codes_.p + r0 * dpad_, kept * dpad_ * sizeof(float), cudaMemcpyDeviceToDevice,
+                              st_));
+      HB_CUDA(cudaMemcpyAsync(i.p, ids_.p + r0, kept * sizeof(int64_t), cudaMemcpyDeviceToDevice, st_));
+      HB_CUDA(cudaMemcpyAsync(n.p, norms_.p + r0, kept * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+      HB_CUDA(cudaMemcpyAsync(codes_.p, c.p, kept * dpad_ * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+      HB_CUDA(cudaMemcpyAsync(ids_.p, i.p, kept * sizeof(int64_t), cudaMemcpyDeviceToDevice, st_));
+      HB_CUDA(cudaMemcpyAsync(norms_.p, n.p, kept * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+      HB_CUDA(cudaStreamSynchronize(st_));
+    }
+    for (size_t l = 0; l <= nlist_; ++l) {
+      const int64_t o = host_off_[l];
+      host_off_[l] = l <= first ? 0 : (l >= first + count ? r1 - r0 : o - r0);
+    }
+    HB_CUDA(cudaMemcpyAsync(list_off_.p, host_off_.data(), (nlist_ + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                            st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    ntotal_ = kept;
+    plan_rows_ = 0;
+    build_bf16();
+    drop_graphs();
+  }
+
+  // The reference master's merge of per-worker results (src/Index.cpp:1327-1341)
+  // on the index stream; device arrays only.
+  void merge_parts(size_t nparts, size_t nq, size_t k, const float* Dp, const int64_t* Ip, float* D, int64_t* I) {
+    HB_CHECK(nparts >= 1 && k >= 1, HB_ERR_INVALID, "need at least one part and k >= 1");
+    HB_CHECK(is_device_ptr(Dp) && is_device_ptr(Ip) && is_device_ptr(D) && is_device_ptr(I), HB_ERR_INVALID,
+             "merge takes device arrays");
+    HB_CUDA(cudaSetDevice(device_));
+    launch_merge_parts(Dp, Ip, static_cast<int>(nparts), static_cast<int64_t>(nq), static_cast<int>(k), D, I, st_);
+    ++launches_;
+    HB_CUDA(cudaStreamSynchronize(st_));
+  }
+
   void get_list_sizes(int64_t* out) {
     std::vector<int64_t> s(nlist_);
     for (size_t l = 0; l < nlist_; ++l) s[l] = host_off_[l + 1] - host_off_[l];
@@ -1906,6 +1957,21 @@ int hb_get_info(const hb_index* ix, size_t* d, size_t* nlist, size_t* ntotal, in
 int hb_get_centroids(const hb_index* ix, float* out) {
   HB_NEED_INDEX(ix);
   return guarded([&] { ix->core->get_centroids(out); });
+}
+
+int hb_retain_lists(hb_index* ix, size_t first, size_t count) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] { ix->core->retain_lists(first, count); });
+}
+
+int hb_merge_topk(hb_index* ix, size_t nparts, size_t nq, size_t k, const float* D_parts, const int64_t* I_parts,
+                  float* D, int64_t* I) {
+  HB_NEED_INDEX(ix);
+  if (nq == 0) return HB_OK;
+  return guarded([&] {
+    HB_CHECK(D_parts && I_parts && D && I, HB_ERR_INVALID, "null pointer");
+    ix->core->merge_parts(nparts, nq, k, D_parts, I_parts, D, I);
+  });
 }
 
 int hb_get_list_sizes(const hb_index* ix, int64_t* out) {

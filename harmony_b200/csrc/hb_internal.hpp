@@ -135,6 +135,10 @@ void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list
                        int32_t* list_cursor, int32_t* list_q, int64_t* item_off, int64_t* slot_base,
                        void* scan_tmp, size_t scan_tmp_bytes, cudaStream_t st);
 size_t build_work_tmp_bytes(int nq, int P, int nlist);
+// The reference master's heap merge of nparts result rows per query
+// (Dp, Ip: nparts x nq x k, part-major) into D, I (nq x k, ascending).
+void launch_merge_parts(const float* Dp, const int64_t* Ip, int nparts, int64_t nq, int k, float* D, int64_t* I,
+                        cudaStream_t st);
 // Merge partial top-k slots of each query to the final top-k.
 void launch_merge(const uint64_t* part, const int64_t* slot_base, int nq, int P, int k,
                   const int64_t* ids, float* D, int64_t* I, cudaStream_t st);

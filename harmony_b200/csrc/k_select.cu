@@ -447,6 +447,56 @@ __global__ void scatter_probes_kernel(const int32_t* __restrict__ probes, int nq
   list_q[list_qoff[l] + pos] = static_cast<int32_t>((static_cast<uint32_t>(q) << 16) | static_cast<uint32_t>(j));
 }
 
+// Binary max-heap of (value, id) rows in place, restating the reference's
+// heap_replace_top / heap_sort (src/heap.hpp:36-80) 0-based: the new value
+// sinks from the root; at each level it goes to the left child when there is
+// no right child or the left value is the greater, else to the right child,
+// and stops when it is greater than that child.
+__device__ __forceinline__ void heap_sink(float* hv, int64_t* hi, int64_t k, float val, int64_t id) {
+  int64_t j = 0;
+  for (;;) {
+    int64_t c = 2 * j + 1;
+    if (c >= k) break;
+    if (c + 1 < k && !(hv[c] > hv[c + 1])) ++c;
+    if (val > hv[c]) break;
+    hv[j] = hv[c];
+    hi[j] = hi[c];
+    j = c;
+  }
+  hv[j] = val;
+  hi[j] = id;
+}
+
+// One thread per query: the reference master's merge of the workers' result
+// rows (src/Index.cpp:1327-1341): heap of k (FLT_MAX, -1), then for each part
+// in order and each of its k entries in order, admit a value strictly below
+// the top; finally heap-sort ascending.  The output row is the heap.
+__global__ void merge_parts_kernel(const float* __restrict__ Dp, const int64_t* __restrict__ Ip, int nparts,
+                                   int64_t nq, int k, float* __restrict__ D, int64_t* __restrict__ I) {
+  const int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (q >= nq) return;
+  float* hv = D + q * k;
+  int64_t* hi = I + q * k;
+  for (int i = 0; i < k; ++i) {
+    hv[i] = FLT_MAX;
+    hi[i] = -1;
+  }
+  for (int p = 0; p < nparts; ++p) {
+    const int64_t base = (static_cast<int64_t>(p) * nq + q) * k;
+    for (int i = 0; i < k; ++i) {
+      const float v = Dp[base + i];
+      if (v < hv[0]) heap_sink(hv, hi, k, v, Ip[base + i]);
+    }
+  }
+  for (int64_t i = k - 1; i >= 0; --i) {
+    const float v = hv[i];
+    const int64_t id = hi[i];
+    hv[i] = hv[0];
+    hi[i] = hi[0];
+    heap_sink(hv, hi, i, v, id);
+  }
+}
+
 size_t cub_scan_bytes(size_t n) {
   size_t bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, bytes, static_cast<const int64_t*>(nullptr),
@@ -492,6 +542,13 @@ void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, in
   HB_CUDA(cudaFuncSetAttribute(select_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                static_cast<int>(smem)));
   select_rows_kernel<<<nrows, kSelThreads, smem, st>>>(D, ncols, ldD, k, out_idx, out_val);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_merge_parts(const float* Dp, const int64_t* Ip, int nparts, int64_t nq, int k, float* D, int64_t* I,
+                        cudaStream_t st) {
+  if (nq <= 0) return;
+  merge_parts_kernel<<<static_cast<unsigned>((nq + 127) / 128), 128, 0, st>>>(Dp, Ip, nparts, nq, k, D, I);
   HB_CUDA(cudaGetLastError());
 }
 

@@ -130,6 +130,19 @@ int hb_get_info(const hb_index* ix, size_t* d, size_t* nlist, size_t* ntotal, in
 int hb_get_centroids(const hb_index* ix, float* out);        /* nlist * d          */
 int hb_get_list_sizes(const hb_index* ix, int64_t* out);     /* nlist              */
 
+/* List sharding across GPUs (the reference's DIVIDE_IVF partition,
+ * src/Index.cpp:79-104 and 1279-1347, with the merge on the device).
+ * hb_retain_lists keeps lists [first, first + count) and empties the others;
+ * ids are unchanged, so every shard reports the full index's ids.
+ * hb_merge_topk merges nparts result rows per query (D_parts, I_parts:
+ * nparts x nq x k, part-major, device memory) into D, I (nq x k, device) with
+ * the reference master's rule (src/Index.cpp:1327-1341): a max-heap of k,
+ * parts in order, a value admitted when strictly below the top, then sorted
+ * ascending.  Runs on the index's stream and returns when done. */
+int hb_retain_lists(hb_index* ix, size_t first, size_t count);
+int hb_merge_topk(hb_index* ix, size_t nparts, size_t nq, size_t k, const float* D_parts, const int64_t* I_parts,
+                  float* D, int64_t* I);
+
 /* Exact search that allocates no device memory.  No counterpart in the
  * reference (its search allocates freely).  For callers that cannot allocate
  * while serving a query: a process whose device memory belongs to another

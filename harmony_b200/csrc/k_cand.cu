@@ -13,12 +13,10 @@
 //     warp streams 64-column K blocks of both operands (queries: A, 128 x 64;
 //     rows: B, 128 x 64; 128-byte swizzle) into a ring of 32 KB stages, the
 //     MMA warp issues tcgen05.mma M128 x N128 x K16 into one of four TMEM
-//     accumulators, and the epilogue (thread = query, TMEM lane) forms
-//     v = ||x||^2 - 2 q~.x~ of the tile's rows and, transposed through shared
-//     memory so that each store is a 128-byte run of one query, writes them
-//     into the query's candidate row: the concatenation over its probes, in
-//     probe order, of one segment per probed list (the list's length rounded
-//     up to 4; +inf past the end).
+//     accumulators, and the epilogue (thread = query, TMEM lane) writes
+//     v = ||x||^2 - 2 q~.x~ of the tile's rows into the query's candidate
+//     row: the concatenation over its probes, in probe order, of one segment
+//     per probed list (the list's length rounded up to 4; +inf past the end).
 //  3. cand_select_kernel: one CTA per query selects the R smallest keys
 //     (v, position) of its candidate row (block radix selection over the row
 //     staged in shared memory; unique keys, so the choice is deterministic)
@@ -56,8 +54,6 @@ constexpr int kThreads = 192;              // 4 epilogue warps, TMA warp, MMA wa
 constexpr uint32_t kBlk = kT * 128;        // one 128-row x 64-column BF16 block (16 KB)
 constexpr uint32_t kStageBytes = 2 * kBlk;  // A block + B block
 constexpr int kAccN = 4;                    // TMEM accumulators of 128 columns (all 512)
-constexpr int kTwStride = 33;               // staging row stride (odd: conflict-free both ways)
-constexpr size_t kTwBytes = 4 * 32 * kTwStride * sizeof(float);  // 4 epilogue warps
 constexpr int kSelectThreads = 256;
 constexpr int kBins = 2048;                 // histogram bins of the candidate selection
 constexpr int kSelUnroll = 4;               // 32-value runs a warp loads at once
@@ -202,9 +198,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     const uint32_t lane_base = (32u * static_cast<uint32_t>(warp)) << 16;
-    // This warp's 32 x 33 staging block (after the ring) for the transposed
-    // candidate stores.
-    float* tw = reinterpret_cast<float*>(ring + static_cast<size_t>(kStg) * kStageBytes) + warp * 32 * kTwStride;
     int64_t tile = 0;
     bool ok = true;
     for (int64_t item = blockIdx.x; ok && item < total; item += gridDim.x) {
@@ -238,20 +231,16 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
           for (int j = 0; j < 32; ++j)
             r[j] = __float_as_uint(fmaf(-2.0f, __uint_as_float(r[j]), __shfl_sync(0xffffffffu, nrm[c], j)));
-          // Transpose through shared memory, then query by query the warp
-          // writes 32 consecutive values: one 128-byte run per store.
           const int64_t o = rl0 + c * 32;
+          if (o < slen) {
+            float* out = a.cand + sbase + o;
 #pragma unroll
-          for (int j = 0; j < 32; ++j) tw[lane * kTwStride + j] = __uint_as_float(r[j]);
-          __syncwarp();
-          if (__any_sync(0xffffffffu, o < slen)) {
-            for (int l = 0; l < 32; ++l) {
-              const int64_t sb_l = __shfl_sync(0xffffffffu, sbase, l);
-              const int64_t sl_l = __shfl_sync(0xffffffffu, slen, l);
-              if (o + lane < sl_l) a.cand[sb_l + o + lane] = tw[l * kTwStride + lane];
-            }
+            for (int j4 = 0; j4 < 8; ++j4)
+              if (o + 4 * j4 < slen)
+                *reinterpret_cast<float4*>(out + 4 * j4) =
+                    make_float4(__uint_as_float(r[4 * j4]), __uint_as_float(r[4 * j4 + 1]),
+                                __uint_as_float(r[4 * j4 + 2]), __uint_as_float(r[4 * j4 + 3]));
           }
-          __syncwarp();
         }
         tc_fence_before();
         mbar_arrive(&sh.acce[b]);
@@ -594,7 +583,7 @@ void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* li
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st) {
   HB_CHECK(a.kpad >= 64 && a.kpad % 64 == 0, HB_ERR_INVALID, "the candidate scan needs kpad a multiple of 64");
   HB_CHECK(a.chunk_rows >= kT && a.chunk_rows % kT == 0, HB_ERR_INVALID, "chunk rows must be a multiple of 128");
-  const size_t smem = kStg * static_cast<size_t>(kStageBytes) + kTwBytes + 1024;
+  const size_t smem = kStg * static_cast<size_t>(kStageBytes) + 1024;
   HB_CUDA(cudaFuncSetAttribute(cand_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const CUtensorMap* mq = static_cast<const CUtensorMap*>(tmap_q);
   const CUtensorMap* mx = static_cast<const CUtensorMap*>(tmap_x);

@@ -16,6 +16,8 @@ every step touches every list, so no L2 flush is needed between steps.
   python bench.py [--steps K] [--warmup W] [--gpus N]        (our CUDA path)
   python bench.py --impl reference                           (the reference's
         own CPU search, oracle/_ref, on the same frozen index and queries)
+  python bench.py --workload c4     (10M x 96, Zipf list sizes, batches of 1..4096)
+  python bench.py --workload c3     (270k x 500, k 100: the candidate-matrix BF16 path)
 
 Multi-GPU: the path is query-parallel with no exchange step, so N ranks run
 N independent replicas (weak scaling, each rank its own 10k queries).

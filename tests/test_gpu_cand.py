@@ -163,3 +163,25 @@ def test_wide_small_and_degenerate(restated):
         assert_topk_parity(D, I, De, Ie, lambda qi, i: restated.l2(q[qi], base[i]), "brute force")
     finally:
         ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+
+
+def test_dense_bin_takes_the_radix_fallback(restated):
+    """3000 identical rows next to the query put more than 2048 keys in the
+    histogram bin of the R-th value: the selection falls back to the block
+    radix selection, and the result is still the exact one (every returned
+    row at the tied distance)."""
+    rng = np.random.default_rng(31)
+    d = 160
+    same = np.repeat(rng.standard_normal((1, d)).astype(np.float32), 3000, axis=0)
+    other = (rng.standard_normal((3000, d)) * 3 + 10).astype(np.float32)
+    base = np.concatenate([same, other])
+    ix = Index(d, 8, 8)
+    ix.train(base.shape[0], base)
+    ix.add(base.shape[0], base)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    q = same[:3] + np.float32(0.05)
+    for k in (10, 100):
+        D, I = search(ix, q, k)
+        De, Ie = search(ix, q, k, precision=Precision.FP32)
+        assert_topk_parity(D, I, De, Ie, lambda qi, i: restated.l2(q[qi], base[i]), f"dense bin k={k}")
+        assert (I < 3000).all()  # all from the identical rows

@@ -159,3 +159,26 @@ def test_stats_csv_matches_reference(ref_lib, tmp, my):
     ref_lib.stats_csv(theirs, False, "x", record(), my=my)
     with open(ours, "rb") as a, open(theirs, "rb") as b:
         assert a.read() == b.read()
+
+
+def test_stats_record_from_search(tmp):
+    """A record filled from one search call carries the index's shape and the
+    call's Stats, and writes a row the reference's reader would parse."""
+    from harmony_b200 import Stats
+
+    class FakeIndex:
+        def _info(self):
+            return 128, 1024, 1_000_000, 0
+
+    st = Stats(query_time=0.25, nprobe=32, k=10, nq=10_000)
+    rec = harness.StatsRecord.from_search(FakeIndex(), st, recall=0.95, mode="ORIGINAL")
+    assert (rec.d, rec.nlist, rec.nb, rec.nprobe, rec.k, rec.nq) == (128, 1024, 1_000_000, 32, 10, 10_000)
+    p = os.path.join(tmp, "s.csv")
+    rec.my_to_csv(p, True, "c5")
+    rec.my_to_csv(p, True, "c5")
+    lines = open(p).read().splitlines()
+    assert len(lines) == 3 and lines[0].startswith("dataset,mode,nb,nq,d,nlist,nprobe,k,")
+    row = dict(zip(lines[0].split(","), lines[1].split(",")))
+    assert row["recall"] == "0.9500000000000000" and row["query_time"] == "0.2500000000000000"
+    with pytest.raises(AttributeError):
+        harness.StatsRecord.from_search(FakeIndex(), st, no_such_field=1)

@@ -359,7 +359,6 @@ class IndexCore {
   // the candidate-matrix scan any d).
   void build_bf16() {
     bf16_ready_ = false;
-    planes_ready_ = false;
     kpad_ = static_cast<int>((d_ + 63) / 64 * 64);
     if (ntotal_ == 0) return;
     codes_bf16_.reserve(ntotal_ * static_cast<size_t>(kpad_));
@@ -1317,19 +1316,6 @@ class IndexCore {
     if (!capturing_) bf16_err_check();
   }
 
-  // Plane-major BF16 copy of the codes for the candidate-matrix scan, built
-  // on its first search after the lists change (an ordinary call sizes it
-  // before any graph capture).
-  void ensure_planes() {
-    if (planes_ready_) return;
-    HB_CHECK(!capturing_, HB_ERR_STATE, "BF16 planes must be built before a graph capture");
-    codes_planes_.reserve(std::max<size_t>(ntotal_ * static_cast<size_t>(kpad_), 1));
-    launch_to_bf16_planes(codes_.p, ntotal_, static_cast<int>(dpad_), kpad_, codes_planes_.p, st_);
-    ++launches_;
-    make_bf16_plane_map(pmap_, codes_planes_.p, std::max<size_t>(ntotal_, 1), kpad_);
-    planes_ready_ = true;
-  }
-
   // Longest candidate row a query can have at nprobe P: the P largest lists,
   // each rounded up to 4 entries.
   int64_t cand_row_bound(int P) {
@@ -1357,7 +1343,6 @@ class IndexCore {
   // approximate value on the tensor cores, then per query the R smallest
   // re-ranked exactly.
   void search_batch_cand(int nb, int P, int k, int R, float* Dd, int64_t* Id) {
-    ensure_planes();
     probes_.reserve(static_cast<size_t>(nb) * P);
     coarse_and_cut(nb, P);
     err_dev_.reserve(1);
@@ -1393,7 +1378,7 @@ class IndexCore {
                             static_cast<int64_t>(nqp), gq_.p, st_);
     }
     ++launches_;
-    make_bf16_plane_map(gqmap_, gq_.p, nqp, kpad_);
+    make_bf16_tensor_map(gqmap_, gq_.p, nqp, kpad_);
     const int64_t row_bound = cand_row_bound(P);
     cand_.reserve(std::max<size_t>(static_cast<size_t>(nb) * row_bound, 1));
     cand_rows_.reserve(static_cast<size_t>(nb) * R);
@@ -1414,7 +1399,7 @@ class IndexCore {
     a.err = err_dev_.p;
     {
       Scope sc(this, "cand_scan");
-      launch_cand_scan(gqmap_, pmap_, a, num_sms_, st_);
+      launch_cand_scan(gqmap_, tmap_, a, num_sms_, st_);
     }
     ++launches_;
     {
@@ -1772,9 +1757,6 @@ class IndexCore {
   bool bf16_ready_ = false;
   alignas(64) unsigned char tmap_[128];
   alignas(64) unsigned char gqmap_[128];  // gathered BF16 queries of the candidate-matrix scan
-  alignas(64) unsigned char pmap_[128];   // plane-major BF16 codes of the candidate-matrix scan
-  bool planes_ready_ = false;
-  DevBuf<uint16_t> codes_planes_;
   bool cand_path_ = false;
   DevBuf<int64_t> seg_;
   DevBuf<uint16_t> gq_;

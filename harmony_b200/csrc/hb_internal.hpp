@@ -201,11 +201,6 @@ void launch_tile_norms(const float* norms, const int64_t* list_off, int nlist, c
 int scan_bf16_keys_per_slot(int R);  // keys each (query, chunk) slot holds
 int scan_bf16_max_R(int kpad);       // largest candidate count per query the scan holds
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);
-// BF16 planes (plane p = columns [64p, 64p + 64) of every row, 128 bytes per
-// row) and their 3-D map: box 64 x 128 rows x 1 plane, 128-byte swizzle, the
-// same shared-memory image as a 64 x 128 box of the row-major copy.
-void launch_to_bf16_planes(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st);
-void make_bf16_plane_map(void* tmap_out, const void* planes, size_t rows, int kpad);
 
 // Candidate-matrix BF16 scan (k_cand.cu): any kpad (a multiple of 64) and up
 // to kCandMaxR candidates per query.
@@ -229,8 +224,7 @@ struct CandArgs {
 size_t cand_segments_tmp_bytes(int nq, int P);
 void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* list_off, int64_t* seg, void* tmp,
                           size_t tmp_bytes, cudaStream_t st);
-// Row e of G = BF16 query of list-major entry e, for e < min(*n_entries, max_rows);
-// G in planes of max_rows rows (as launch_to_bf16_planes).
+// Row e of G = BF16 query of list-major entry e, for e < min(*n_entries, max_rows).
 void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* list_q, const int64_t* n_entries,
                            int64_t max_rows, void* G, cudaStream_t st);
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st);

@@ -11,8 +11,7 @@
 //     group of <= 128 queries); the search uses one 128-row tile per item,
 //     so the items spread evenly over the CTAs.  For each 128-row tile of the chunk the TMA
 //     warp streams 64-column K blocks of both operands (queries: A, 128 x 64;
-//     rows: B, 128 x 64; 128-byte swizzle) from plane-major BF16 copies, where
-//     a K block of 128 rows is 16 KB of contiguous memory, into a ring of 32 KB stages, the
+//     rows: B, 128 x 64; 128-byte swizzle) into a ring of 32 KB stages, the
 //     MMA warp issues tcgen05.mma M128 x N128 x K16 into one of four TMEM
 //     accumulators, and the epilogue (thread = query, TMEM lane) writes
 //     v = ||x||^2 - 2 q~.x~ of the tile's rows into the query's candidate
@@ -146,8 +145,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             uint8_t* st = ring + static_cast<size_t>(s) * kStageBytes;
             mbar_arrive_expect_tx(&sh.full[s], kStageBytes);
-            tma_load_3d(st, &tmap_q, 0, static_cast<int>(d.qrow0), kb, &sh.full[s]);
-            tma_load_3d(st + kBlk, &tmap_x, 0, static_cast<int>(d.row0 + static_cast<int64_t>(t) * kT), kb,
+            tma_load_2d(st, &tmap_q, kb * 64, static_cast<int>(d.qrow0), &sh.full[s]);
+            tma_load_2d(st + kBlk, &tmap_x, kb * 64, static_cast<int>(d.row0 + static_cast<int64_t>(t) * kT),
                         &sh.full[s]);
           }
         }
@@ -257,8 +256,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // Row e of the gathered matrix = the query of list-major entry e in BF16
-// (columns past dpad zero), stored in planes of 64 columns (plane p at
-// p * max_rows * 64).  Entries are (query << 16 | probe rank).
+// (columns past dpad zero).  Entries are (query << 16 | probe rank).
 __global__ void gather_queries_kernel(const float* __restrict__ q, int dpad, int kpad,
                                       const int32_t* __restrict__ list_q, const int64_t* __restrict__ n_entries,
                                       int64_t max_rows, __nv_bfloat16* __restrict__ G) {
@@ -286,7 +284,7 @@ __global__ void gather_queries_kernel(const float* __restrict__ q, int dpad, int
       __nv_bfloat162 p = __floats2bfloat162_rn(x[2 * j], x[2 * j + 1]);
       ow[j] = *reinterpret_cast<uint32_t*>(&p);
     }
-    *reinterpret_cast<uint4*>(G + (static_cast<int64_t>(c / 64) * max_rows + e) * 64 + (c % 64)) = o;
+    *reinterpret_cast<uint4*>(G + e * kpad + c) = o;
   }
 }
 

@@ -719,22 +719,6 @@ __global__ void to_bf16_kernel(const float* __restrict__ src, size_t n, int dpad
   }
 }
 
-// BF16 planes: plane p holds columns [64p, 64p + 64) of every row, rows
-// 128 bytes apart, so a 128-row box of one K block is 16 KB of contiguous
-// memory.
-__global__ void to_bf16_planes_kernel(const float* __restrict__ src, size_t n, int dpad, int kpad,
-                                      __nv_bfloat16* __restrict__ dst) {
-  const size_t total = n * static_cast<size_t>(kpad);
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const size_t plane = i / (n * 64);
-    const size_t rem = i - plane * n * 64;
-    const size_t r = rem / 64;
-    const int c = static_cast<int>(plane * 64 + (rem - r * 64));
-    dst[i] = __float2bfloat16_rn(c < dpad ? src[r * dpad + c] : 0.0f);
-  }
-}
-
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -779,27 +763,6 @@ void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, i
                                     strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   HB_CHECK(r == CUDA_SUCCESS, HB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-}
-
-void make_bf16_plane_map(void* tmap_out, const void* planes, size_t rows, int kpad) {
-  CUtensorMap* m = static_cast<CUtensorMap*>(tmap_out);
-  cuuint64_t dims[3] = {64, static_cast<cuuint64_t>(rows), static_cast<cuuint64_t>(kpad / 64)};
-  cuuint64_t strides[2] = {128, static_cast<cuuint64_t>(rows) * 128};
-  cuuint32_t box[3] = {64, kTile, 1};
-  cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = tensor_map_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(planes), dims, strides,
-                                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  HB_CHECK(r == CUDA_SUCCESS, HB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-}
-
-void launch_to_bf16_planes(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st) {
-  if (!n) return;
-  size_t g = (n * kpad + 255) / 256;
-  if (g > 148u * 64u) g = 148u * 64u;
-  to_bf16_planes_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(src, n, dpad, kpad,
-                                                                 static_cast<__nv_bfloat16*>(dst));
-  HB_CUDA(cudaGetLastError());
 }
 
 void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st) {

@@ -3,7 +3,7 @@ library give numbers and CSV rows that compare directly with the reference's:
 
 * the vector-file loaders of src/utils.h:187-407 (fvecs, bvecs, text rows,
   and the extension dispatch), with the reference's 1-based inclusive row
-  bounds;
+  bounds, and its result / ground-truth files (src/utils.h:565-620);
 * the recall measures and r2 of src/utils.h:631-755;
 * the Stats CSV rows of src/stats.h:101-125 (``toCsv`` and ``myToCsv``),
   with the reference's column names and number formatting.
@@ -145,6 +145,49 @@ def load_xvecs(path: str, bounds: Tuple[int, int] = (1, 0), reference_offsets: b
     if path.endswith(".txt"):
         return load_tvecs(path)
     raise ValueError("no support file")
+
+
+def write_results(I, D, path: str) -> None:
+    """writeResultsToFile (src/utils.h:565-594): a result or ground-truth file.
+    A path ending in "txt" gets one line per query of "label distance" pairs
+    (distances fixed to 6 decimals); any other path gets the int64 labels then
+    the float32 distances, raw.  Missing parent directories are created."""
+    I = np.ascontiguousarray(I, np.int64)
+    D = np.ascontiguousarray(D, np.float32)
+    if I.shape != D.shape or I.ndim != 2:
+        raise ValueError("labels and distances must both be nq x k")
+    parent = os.path.dirname(path)
+    if parent:
+        os.makedirs(parent, exist_ok=True)
+    if path.endswith("txt"):
+        with open(path, "w") as f:
+            for li, di in zip(I, D):
+                f.write(" ".join(f"{int(a)} {float(b):.6f}" for a, b in zip(li, di)) + "\n")
+    else:
+        with open(path, "wb") as f:
+            f.write(I.tobytes())
+            f.write(D.tobytes())
+
+
+def load_results(path: str, nq: int, k: int) -> Tuple[np.ndarray, np.ndarray]:
+    """loadResults (src/utils.h:596-620): (labels int64, distances float32),
+    each nq x k, from a file written by write_results or by the reference."""
+    if path.endswith("txt"):
+        with open(path, "r") as f:
+            tok = f.read().split()
+        if len(tok) < 2 * nq * k:
+            raise ValueError(f"{path}: {len(tok) // 2} pairs, {nq * k} expected")
+        pairs = np.array(tok[:2 * nq * k], dtype=object).reshape(nq * k, 2)
+        I = np.array([int(t) for t in pairs[:, 0]], np.int64).reshape(nq, k)
+        D = np.array([float(t) for t in pairs[:, 1]], np.float32).reshape(nq, k)
+        return I, D
+    raw = np.fromfile(path, dtype=np.uint8)
+    need = nq * k * 12
+    if raw.size < need:
+        raise ValueError(f"{path}: {raw.size} bytes, {need} expected")
+    I = raw[:nq * k * 8].view(np.int64).reshape(nq, k).copy()
+    D = raw[nq * k * 8:need].view(np.float32).reshape(nq, k).copy()
+    return I, D
 
 
 def _valid_prefix(I: np.ndarray) -> np.ndarray:

@@ -246,6 +246,8 @@ class RefIndex:
                 getattr(L, fn).restype = ctypes.c_float
                 getattr(L, fn).argtypes = [_i, _f, _i, _f, _sz, _sz, _sz]
             L.ref_stats_csv.argtypes = [_cp, ctypes.c_int, _cp, _cp, ctypes.c_int, _i, _d]
+            L.ref_write_results.argtypes = [_i, _f, _sz, _sz, _cp]
+            L.ref_load_results.argtypes = [_cp, _i, _f, _sz, _sz]
             L.ref_set_threads.argtypes = [ctypes.c_int]
             L.ref_max_threads.restype = ctypes.c_int
             cls._L = L
@@ -404,6 +406,19 @@ class RefIndex:
     @classmethod
     def calculate_r2(cls, I, D, GT, GD, k, gt_k=0):
         return cls._measure(cls.lib().ref_calculate_r2, I, D, GT, GD, k, gt_k)
+
+    @classmethod
+    def write_results(cls, I, D, path):
+        I, D = _i64(I), _f32(D)
+        nq, k = I.shape
+        cls.lib().ref_write_results(_ip(I), _fp(D), nq, k, path.encode())
+
+    @classmethod
+    def load_results(cls, path, nq, k):
+        I = np.zeros((nq, k), np.int64)
+        D = np.zeros((nq, k), np.float32)
+        cls.lib().ref_load_results(path.encode(), _ip(I), _fp(D), nq, k)
+        return I, D
 
     _STATS_INT = ["nlist", "nprobe", "opt_level", "total_count", "skip_triangle_count", "skip_triangle_large_count",
                   "skip_subnn_L2_count", "skip_subnn_IP_count", "simi_update_count", "check_subnn_L2_ele_count",

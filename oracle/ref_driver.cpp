@@ -242,6 +242,17 @@ float ref_calculate_r2(const int64_t* I, const float* D, const int64_t* GT, cons
   return calculate_r2(I, D, GT, GD, nq, k, METRIC_L2, gt_k);
 }
 
+// Result files of the query driver (src/utils.h:565-620): ground truth and
+// search results, text ("...txt": "label distance" pairs) or binary (labels
+// then distances).
+void ref_write_results(const int64_t* I, const float* D, size_t nq, size_t k, const char* path) {
+  writeResultsToFile(I, D, nq, k, path);
+}
+
+void ref_load_results(const char* path, int64_t* I, float* D, size_t nq, size_t k) {
+  loadResults(path, I, D, nq, k);
+}
+
 // Stats::toCsv (which = 0) or Stats::myToCsv (which = 1) of a Stats whose
 // fields are iv = {nlist, nprobe, opt_level, total_count, skip_triangle_count,
 // skip_triangle_large_count, skip_subnn_L2_count, skip_subnn_IP_count,

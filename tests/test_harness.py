@@ -182,3 +182,24 @@ def test_stats_record_from_search(tmp):
     assert row["recall"] == "0.9500000000000000" and row["query_time"] == "0.2500000000000000"
     with pytest.raises(AttributeError):
         harness.StatsRecord.from_search(FakeIndex(), st, no_such_field=1)
+
+
+@pytest.mark.parametrize("ext", ["txt", "bin"])
+def test_result_files_match_reference(ref_lib, tmp, ext):
+    rng = np.random.default_rng(9)
+    I = rng.integers(-1, 1_000_000, (13, 7)).astype(np.int64)
+    D = (rng.standard_normal((13, 7)) * 1000).astype(np.float32)
+    D[0, -1] = np.finfo(np.float32).max  # padding slots as searches leave them
+    ours = os.path.join(tmp, "sub", f"gt_7.{ext}")
+    theirs = os.path.join(tmp, "ref", f"gt_7.{ext}")
+    harness.write_results(I, D, ours)
+    ref_lib.write_results(I, D, theirs)
+    with open(ours, "rb") as a, open(theirs, "rb") as b:
+        assert a.read() == b.read()
+    for path in (ours, theirs):
+        Ia, Da = harness.load_results(path, 13, 7)
+        Ib, Db = ref_lib.load_results(path, 13, 7)
+        assert np.array_equal(Ia, Ib) and np.array_equal(Da.view(np.uint32), Db.view(np.uint32))
+        assert np.array_equal(Ia, I)
+        if ext == "bin":
+            assert np.array_equal(Da, D)

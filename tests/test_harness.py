@@ -203,3 +203,28 @@ def test_result_files_match_reference(ref_lib, tmp, ext):
         assert np.array_equal(Ia, I)
         if ext == "bin":
             assert np.array_equal(Da, D)
+
+
+def test_golden_harness_fixtures(tmp):
+    """The reference's outputs stored by tests/golden/make_golden_harness.py:
+    the harness reproduces them without the reference library present."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_harness.npz"))
+    p = os.path.join(tmp, "g.bvecs")
+    g["bvecs_file"].tofile(p)
+    assert np.array_equal(harness.load_bvecs(p, (1, 0), reference_offsets=True), g["bvecs_all"])
+    assert np.array_equal(harness.load_bvecs(p, (3, 9), reference_offsets=True), g["bvecs_3_9"])
+    for name, (k, gt_k) in {"k10": (10, 10), "k10_gt100": (10, 100)}.items():
+        args = [g[f"recall_{name}_{s}"] for s in ("I", "D", "GT", "GD")]
+        got = np.array([harness.calculate_recall(*args, k, gt_k), harness.calculate_recall_loose(*args, k, gt_k),
+                        harness.calculate_r2(*args, k, gt_k)], np.float32)
+        assert got.tobytes() == g[f"recall_{name}_values"].tobytes(), name
+    rec = record(skip_triangle_large_count=0, check_subnn_IP_ele_count=0, check_subnn_IP_count=0,
+                 disableOrderOptimize=False, blockSend=False)
+    for name, my in (("csv_to", False), ("csv_my", True)):
+        p = os.path.join(tmp, f"{name}.csv")
+        (rec.my_to_csv if my else rec.to_csv)(p, False, "sift1m")
+        (rec.my_to_csv if my else rec.to_csv)(p, True, "sift1m")
+        assert open(p, "rb").read() == g[name].tobytes(), name
+    p = os.path.join(tmp, "r.txt")
+    harness.write_results(g["results_I"], g["results_D"], p)
+    assert open(p, "rb").read() == g["results_txt"].tobytes()

@@ -150,6 +150,35 @@ def recall(I, gt, k):
     return float(np.mean([len(set(a.tolist()) & set(b.tolist())) / k for a, b in zip(I, gt)]))
 
 
+def parity_count(D, I, Dr, Ir):
+    """Queries whose top-k equals the other result's: distances identical bit
+    for bit, and ids identical except among those at the k-th distance (an
+    exact tie across the boundary, where the reference's heap history decides,
+    src/IVFScan.hpp:267).  Returns (identical queries, queries)."""
+    D, Dr = np.ascontiguousarray(D, np.float32), np.ascontiguousarray(Dr, np.float32)
+    I, Ir = np.asarray(I), np.asarray(Ir)
+    same_d = np.all(D.view(np.uint32) == Dr.view(np.uint32), axis=1)
+    ok = 0
+    for q in np.nonzero(same_d)[0]:
+        if np.array_equal(I[q], Ir[q]):
+            ok += 1
+            continue
+        below = Dr[q] < Dr[q, -1]
+        ok += set(I[q][below].tolist()) == set(Ir[q][below].tolist())
+    return int(ok), int(D.shape[0])
+
+
+def max_rel_err_vs_fp64(torch, base, test, D, I):
+    """Largest relative error of returned distances against FP64 recomputation."""
+    Dt = torch.as_tensor(np.asarray(D)).cuda().double()
+    It = torch.as_tensor(np.asarray(I)).cuda()
+    valid = It >= 0
+    x = base[It.clamp(min=0).reshape(-1)].double().reshape(It.shape[0], It.shape[1], -1)
+    d64 = ((x - test.double()[:, None, :]) ** 2).sum(-1)
+    err = ((Dt - d64).abs() / d64.clamp(min=1e-30))[valid]
+    return float(err.max().item()) if err.numel() else 0.0
+
+
 def pick_nprobe(ix, test, gt, k, target, precision):
     import torch
     nq = test.shape[0]
@@ -205,7 +234,7 @@ def time_arm(torch, ix, test, k, P, precision, steps, warmup, world, dist, learn
         ix.search(nq, test, k, D, I)
     prof = ix.profile_read()
     ix.profile(False)
-    return {"ms_per_step": ms / steps, "launches_per_step": launches / steps, "I": I,
+    return {"ms_per_step": ms / steps, "launches_per_step": launches / steps, "I": I, "D": D,
             "kernel_ms": {n: v[0] / steps for n, v in prof.items()}}
 
 
@@ -233,12 +262,13 @@ def run_ours(args):
     build["probe_train_queries"] = int(train.shape[0])
     del train
 
-    arms = {}
+    arms, outs = {}, {}
     with ClockSampler(local) as clk:
         for name, prec in (("fp32", Precision.FP32), ("bf16", Precision.BF16)):
             P, rec = pick_nprobe(ix, test, gt, k, args.target, prec)
             r = time_arm(torch, ix, test, k, P, prec, args.steps, args.warmup, world, dist, tag=name)
-            r.update({"nprobe": P, "recall_at_10": recall(r.pop("I").cpu().numpy(), gt, k),
+            outs[name] = (r.pop("D").cpu().numpy(), r.pop("I").cpu().numpy())
+            r.update({"nprobe": P, "recall_at_10": recall(outs[name][1], gt, k),
                       "qps": world * nq / (r["ms_per_step"] / 1e3)})
             arms[name] = r
         # Learned nprobe + BF16: raise the predictor's target until the test
@@ -255,8 +285,9 @@ def run_ours(args):
         tgt = min(tgt, 0.9999)
         r = time_arm(torch, ix, test, k, 256, Precision.BF16, args.steps, args.warmup, world, dist, learned=True,
                      target=tgt, tag="learned_bf16")
+        outs["learned_bf16"] = (r.pop("D").cpu().numpy(), r.pop("I").cpu().numpy())
         r.update({"nprobe": "learned", "predictor_target": round(tgt, 4),
-                  "recall_at_10": recall(r.pop("I").cpu().numpy(), gt, k),
+                  "recall_at_10": recall(outs["learned_bf16"][1], gt, k),
                   "qps": world * nq / (r["ms_per_step"] / 1e3)})
         thr, crec, cavg = ix.probe_calibration()
         i_sel = int(np.argmin(np.where(crec >= tgt, cavg, 1e9)))
@@ -300,6 +331,35 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_recall = recall(Ih_np, gt, k)
+
+    # Parity at this configuration (untimed).  The BF16 arms against the exact
+    # FP32 scan over the same probe lists: the fixed-nprobe arm at its nprobe,
+    # the learned arm with the same predicted per-query nprobe (the predictor
+    # cuts the probe rows the same way for either precision).  The FP32 scan
+    # against the reference's own Index::search is checked on the CPU-baseline
+    # sample below.
+    def exact_fp32(P, learned=False, target=0.0):
+        sp = ix.search_params
+        sp.precision, sp.learned_probe, sp.learned_target = Precision.FP32, learned, target
+        ix.nprobe = P
+        Dx = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+        Ix = torch.empty((nq, k), dtype=torch.int64, device="cuda")
+        ix.search(nq, test, k, Dx, Ix)
+        return Dx.cpu().numpy(), Ix.cpu().numpy()
+
+    Pf, Pb = arms["fp32"]["nprobe"], arms["bf16"]["nprobe"]
+    ref_b = outs["fp32"] if Pb == Pf else exact_fp32(Pb)
+    ok_b, n_b = parity_count(*outs["bf16"], *ref_b)
+    ref_l = exact_fp32(256, learned=True, target=tgt)
+    ok_l, n_l = parity_count(*outs["learned_bf16"], *ref_l)
+    Dh, Ih = outs["learned_bf16"] if head is arms["learned_bf16"] else outs["bf16"]
+    parity = {
+        "rule": "per query: distances bit-identical, ids identical except among ties at the k-th distance",
+        "bf16_fixed_vs_fp32_exact": {"nprobe": Pb, "identical": ok_b, "queries": n_b},
+        "learned_bf16_vs_learned_fp32_exact": {"identical": ok_l, "queries": n_l},
+        "headline_max_rel_dist_err_vs_fp64": max_rel_err_vs_fp64(torch, base, test, Dh, Ih),
+        "fp32_max_rel_dist_err_vs_fp64": max_rel_err_vs_fp64(torch, base, test, *outs["fp32"]),
+    }
 
     # Roofline of the headline step's dominant kernel.
     hbm_peak, bf16_peak, peak_kind = load_peaks()
@@ -377,14 +437,21 @@ def run_ours(args):
             "e2e": {"value": round(world * nq / (e2e_ms / 1e3), 1), "unit": "queries/s",
                     "h2d_bytes_per_step": nq * d * 4, "d2h_bytes_per_step": nq * k * 12,
                     "recall_at_10": round(e2e_recall, 4)},
+            "parity": parity,
             "roofline": roof,
             "kernel_ms_per_step": {n: round(v, 4) for n, v in kms.items()},
             "gpu_launches": int(round(head["launches_per_step"] * args.steps)),
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:
-            ix.search_params.precision = Precision.FP32
-            result["cpu_baseline"] = cpu_baseline(ix, test.cpu().numpy(), fp["nprobe"], k, gt)
+            ix.search_params.precision, ix.search_params.learned_probe = Precision.FP32, False
+            cb, Dr, Ir = cpu_baseline(ix, test.cpu().numpy(), fp["nprobe"], k, gt)
+            result["cpu_baseline"] = cb
+            n = Dr.shape[0]
+            ok_r, _ = parity_count(outs["fp32"][0][:n], outs["fp32"][1][:n], Dr, Ir)
+            parity["fp32_vs_reference_index_search"] = {
+                "nprobe": fp["nprobe"], "identical": ok_r, "queries": n,
+                "reference": "Index::search (ORIGINAL) of oracle/_ref on the same frozen index, the CPU-baseline sample"}
         print(json.dumps(result), flush=True)
     if world > 1:
         dist.barrier()
@@ -424,23 +491,25 @@ def cpu_baseline(ix, test_np, P, k, gt, budget_s=12.0):
     t0 = time.perf_counter()
     Dr, Ir = ref.search(sample, k)
     t = time.perf_counter() - t0
-    return {"value": round(n / t, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
-            "sample": f"first {n} of the 10k test queries, nprobe {P}, k {k}, one Index::search call "
-                      f"(ORIGINAL mode, OpenMP over {cores} threads)",
-            "recall_at_10": round(recall(Ir, gt[:n], k), 4)}
+    model, _, _ = oracle.host_cpu()
+    return ({"value": round(n / t, 1), "unit": "queries/s", "cores": cores, "kind": "reference", "cpu_model": model,
+             "reference_build": oracle.RefIndex.build_kind,
+             "sample": f"first {n} of the 10k test queries, nprobe {P}, k {k}, one Index::search call "
+                       f"(ORIGINAL mode, OpenMP over {cores} threads)",
+             "recall_at_10": round(recall(Ir, gt[:n], k), 4)}, Dr, Ir)
 
 
-def run_reference(args):
-    world, rank, local = dist_setup()
-    if rank != 0:
-        return None
+def freeze_index(args):
+    """Child process of the reference arm: build the 10M x 128 index on the GPU
+    (the reference's CPU k-means over 10M x 4096 would take hours), pick the
+    smallest nprobe whose exact search reaches the recall target against the
+    FP64 ground truth, and write the frozen index in the reference's file
+    format with the queries and ground truth into args.freeze_to."""
     import torch
-    import oracle
     from harmony_b200 import Index, SearchMode
+    _, _, local = dist_setup()
     torch.cuda.set_device(local)
     k, nq = WORKLOAD["k"], WORKLOAD["nq"]
-    # Frozen index built on the GPU (the reference's CPU k-means over 10M x
-    # 4096 takes hours); the timed path below is the reference's own search.
     ix, base, test, build = build_index(torch, seed=5)
     gt = ground_truth(torch, ix, base, test, k)
     ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
@@ -453,13 +522,44 @@ def run_reference(args):
         if recall(I.cpu().numpy(), gt, k) >= args.target:
             P = p
             break
-    test_np = test.cpu().numpy()
-    ref = _ref_from_index(ix)
-    del ix, base
-    torch.cuda.empty_cache()
+    ix.save_index(os.path.join(args.freeze_to, "index"))
+    np.save(os.path.join(args.freeze_to, "test.npy"), test.cpu().numpy())
+    np.save(os.path.join(args.freeze_to, "gt.npy"), gt)
+    with open(os.path.join(args.freeze_to, "meta.json"), "w") as f:
+        json.dump({"nprobe": P, **build}, f)
+
+
+def run_reference(args):
+    """The reference's own CPU search (oracle/_ref: Index::search, ORIGINAL
+    mode, OpenMP over every host core) on the frozen index.  The index is
+    built and frozen by a child process, so this process loads only the
+    reference library (no torch, no CUDA library of this project)."""
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return None
+    import shutil
+    import oracle
+    k, nq = WORKLOAD["k"], WORKLOAD["nq"]
+    d = tempfile.mkdtemp(prefix="hb_ref_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        cmd = [sys.executable, os.path.abspath(__file__), "--freeze-to", d, "--target", str(args.target)]
+        if args.nb:
+            cmd += ["--nb", str(args.nb)]
+        subprocess.run(cmd, check=True)
+        with open(os.path.join(d, "meta.json")) as f:
+            meta = json.load(f)
+        test_np = np.load(os.path.join(d, "test.npy"))
+        gt = np.load(os.path.join(d, "gt.npy"))
+        if not oracle.RefIndex.available():
+            oracle.build(reference=True)
+        ref = oracle.RefIndex.load(os.path.join(d, "index"))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    P = int(meta.pop("nprobe"))
     ref.nprobe = P
     cores = os.cpu_count() or 1
     oracle.RefIndex.set_threads(cores)
+    model, _, _ = oracle.host_cpu()
     # Bounded sample per step so the whole run stays within a few minutes.
     t0 = time.perf_counter()
     ref.search(test_np[:64], k)
@@ -482,9 +582,11 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Gaussian mixture drawn on the GPU)",
         "config": {"workload": WORKLOAD["workload"], "nprobe": P, "queries_per_step": n,
-                   "recall_at_10": round(recall(Ir, gt[:n], k), 4), **build},
+                   "recall_at_10": round(recall(Ir, gt[:n], k), 4), **meta},
         "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
-                         "sample": f"first {n} test queries per step; reference Index::search, ORIGINAL mode"},
+                         "cpu_model": model, "reference_build": oracle.RefIndex.build_kind,
+                         "sample": f"first {n} test queries per step; reference Index::search, ORIGINAL mode; "
+                                   f"index frozen by a child process, loaded with the reference's load_index"},
         "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(res), flush=True)
@@ -692,6 +794,7 @@ def main():
     ap.add_argument("--nb", type=int, default=None, help="smaller base for profiling runs (not a bench line)")
     ap.add_argument("--nq", type=int, default=None, help="fewer queries for profiling runs (not a bench line)")
     ap.add_argument("--ntrain", type=int, default=200_000, help="training queries of the learned probe")
+    ap.add_argument("--freeze-to", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["c5", "c4", "c3"], default="c5",
                     help="c5: the headline bench line; c4: the batch-stream measurement of config 4; "
                          "c3: the 500-dimensional k = 100 measurement of config 3")
@@ -704,7 +807,9 @@ def main():
     if args.nq and args.workload == "c5":
         WORKLOAD["nq"] = args.nq
         WORKLOAD["workload"] += f" [reduced: nq={args.nq}]"
-    if args.workload == "c4":
+    if args.freeze_to:
+        freeze_index(args)
+    elif args.workload == "c4":
         run_c4(args)
     elif args.workload == "c3":
         run_c3(args)

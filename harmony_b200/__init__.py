@@ -105,7 +105,9 @@ class _SearchParamsC(ctypes.Structure):
         ("max_nprobe", ctypes.c_int32),
         ("seed_rows", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("full_warmup", ctypes.c_int32),
+        ("heap_tops", ctypes.c_void_p),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -146,6 +148,9 @@ def lib() -> ctypes.CDLL:
     L.hb_stream.argtypes = [vp]
     L.hb_launch_count.restype = ctypes.c_uint64
     L.hb_launch_count.argtypes = [vp]
+    L.hb_device_allocations.restype = ctypes.c_uint64
+    L.hb_device_allocations.argtypes = []
+    L.hb_selftest_bounded_wait.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     L.hb_train_probe_predictor.argtypes = [vp, sz, f, sz, sz, ctypes.c_float]
     L.hb_search_noalloc.argtypes = [vp, sz, f, sz, f, i64]
     L.hb_retain_lists.argtypes = [vp, sz, sz]
@@ -161,6 +166,19 @@ def lib() -> ctypes.CDLL:
 def _check(code: int) -> None:
     if code != 0:
         raise HarmonyError(code, lib().hb_last_error().decode(errors="replace"))
+
+
+def _wait_for_torch(stream_handle: int, *arrays) -> None:
+    """Order the index's stream after torch's current stream when any of
+    `arrays` is a CUDA tensor.  The library launches on its own non-blocking
+    stream and never waits on other streams, so a tensor that torch is still
+    producing (or a buffer a collective is still filling) must be finished
+    on that stream before the library reads it."""
+    if not any(getattr(a, "is_cuda", False) for a in arrays):
+        return
+    import torch
+    dev = next(a.device for a in arrays if getattr(a, "is_cuda", False))
+    torch.cuda.ExternalStream(stream_handle, device=dev).wait_stream(torch.cuda.current_stream(dev))
 
 
 def _ptr(a, dtype, writable=False):
@@ -213,12 +231,16 @@ class Index:
 
     @dataclass
     class Param:
-        """Index::Param (src/Index.h:48-68): the fields that steer search."""
+        """Index::Param (src/Index.h:48-68): the fields that steer search.
+        fullWarmUp with heapTops (nq floats, e.g. each query's k-th ground-truth
+        distance as src/query.cpp:716-725 fills it) replaces the warm-up search's
+        pruning thresholds in DIVIDE_DIM (src/Index.cpp:1235-1241)."""
         orderOptimize: bool = True
         mode: SearchMode = SearchMode.ORIGINAL
         pruning: bool = False
         period: bool = False
         fullWarmUp: bool = False
+        heapTops: Optional[object] = None
         block_dim: int = 0
         groupCount: int = 0
         teamCount: int = 0
@@ -309,6 +331,8 @@ class Index:
                 raise TypeError("merge_topk takes contiguous CUDA tensors")
         if tuple(I_parts.shape) != (parts, nq, k) or tuple(D.shape) != (nq, k) or tuple(I.shape) != (nq, k):
             raise ValueError("shape mismatch")
+        # The parts usually come from a collective queued on torch's stream.
+        _wait_for_torch(self.stream, D_parts, I_parts, D, I)
         _check(self._L.hb_merge_topk(self._h, parts, nq, k, D_parts.data_ptr(), I_parts.data_ptr(), D.data_ptr(),
                                      I.data_ptr()))
 
@@ -377,6 +401,7 @@ class Index:
         c.pruning = int(bool(prm.pruning))
         c.order_optimize = int(bool(prm.orderOptimize))
         c.period = int(bool(prm.period))
+        c.full_warmup = int(bool(prm.fullWarmUp))
         if prm.mode == SearchMode.DIVIDE_DIM:
             c.n_dim_blocks = max(1, self.workerCount)
             c.n_query_blocks = max(1, self.blockCount)
@@ -413,6 +438,11 @@ class Index:
         if self.search_params.nprobe_per_query is not None:
             pq, keep_pq = _ptr(self.search_params.nprobe_per_query, np.int32)
             c.nprobe_per_query = pq
+        keep_tops = None
+        if getattr(self.param, "fullWarmUp", False) and self.param.heapTops is not None:
+            tp, keep_tops = _ptr(self.param.heapTops, np.float32)
+            c.heap_tops = tp
+        _wait_for_torch(self.stream, queries, distances, labels, keep_pq, keep_tops)
         _check(self._L.hb_search(self._h, int(n), qp, int(k), ctypes.byref(c), dp, ip))
         return Stats(query_time=time.perf_counter() - t0, nprobe=self.nprobe, k=k, nq=n)
 

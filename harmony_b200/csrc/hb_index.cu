@@ -616,6 +616,14 @@ class IndexCore {
       default:
         throw Error(HB_ERR_INVALID, "search mode not supported");
     }
+    // Param::fullWarmUp: the dimension relay prunes against the caller's heap
+    // tops instead of the warm-up search's (src/Index.cpp:1235-1241); the
+    // reference reads the flag in no other mode.
+    ext_tops_ = nullptr;
+    if (p.mode == HB_MODE_DIVIDE_DIM && p.full_warmup) {
+      HB_CHECK(p.heap_tops, HB_ERR_INVALID, "fullWarmUp needs heap_tops (the reference exits: heapTop not exist)");
+      ext_tops_ = p.heap_tops;
+    }
     // Per-query nprobe: the learned predictor or a caller-given array.  The
     // coarse quantizer selects the widest probe row, each query's row is then
     // cut at its own nprobe (cut entries become -1 and are never scanned).
@@ -1072,6 +1080,25 @@ class IndexCore {
 
   int device() const { return device_; }
 
+  // Self-test of the device waits' give-up path: a kernel waits on an
+  // mbarrier that nothing arrives on, with a budget of `budget` cycles, and
+  // must return with its error code recorded; the host turns the code into
+  // HB_ERR_CUDA exactly as after a real scan.
+  void wait_selftest(long long budget, long long* waited) {
+    HB_CUDA(cudaSetDevice(device_));
+    DevBuf<long long> w;
+    w.reserve(1);
+    err_dev_.reserve(1);
+    HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
+    launch_wait_selftest(budget, 99, err_dev_.p, w.p, st_);
+    ++launches_;
+    long long wh = 0;
+    HB_CUDA(cudaMemcpyAsync(&wh, w.p, sizeof(long long), cudaMemcpyDeviceToHost, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    if (waited) *waited = wh;
+    bf16_err_check();
+  }
+
   void get_centroids(float* out) {
     HB_CUDA(cudaSetDevice(device_));
     HB_CUDA(cudaMemcpy2DAsync(out, d_ * sizeof(float), cent_.p, dpad_ * sizeof(float), d_ * sizeof(float), nlist_,
@@ -1177,10 +1204,15 @@ class IndexCore {
     coarse_and_cut(nb, P);
     if (need_tops) {
       tops_.reserve(nb);
-      Scope sc(this, "warmup_tops");
-      launch_warmup_tops(qpad_.p, nb, probes_.p, P, codes_.p, list_off_.p, static_cast<int>(dpad_), k, warm_lists,
-                         warm_size, tops_.p, st_);
-      ++launches_;
+      if (ext_tops_) {
+        HB_CUDA(cudaMemcpyAsync(tops_.p, ext_tops_ + cut_b0_, static_cast<size_t>(nb) * sizeof(float),
+                                cudaMemcpyDefault, st_));
+      } else {
+        Scope sc(this, "warmup_tops");
+        launch_warmup_tops(qpad_.p, nb, probes_.p, P, codes_.p, list_off_.p, static_cast<int>(dpad_), k, warm_lists,
+                           warm_size, tops_.p, st_);
+        ++launches_;
+      }
     }
     const int cr = chunk_rows_for(nb, P, tv);
     list_cnt_.reserve(nlist_);
@@ -1743,6 +1775,7 @@ class IndexCore {
 
  private:
   ProbeModel probe_;
+  const float* ext_tops_ = nullptr;  // caller's heap tops (fullWarmUp) for the current search
   int cut_mode_ = 0;
   int cut_cap_ = 0;
   float cut_thr_ = 1.0f;
@@ -2006,6 +2039,22 @@ int hb_coarse_fallbacks(hb_index* ix, int64_t* n) {
 void* hb_stream(hb_index* ix) { return (ix && ix->core) ? static_cast<void*>(ix->core->stream()) : nullptr; }
 
 uint64_t hb_launch_count(const hb_index* ix) { return (ix && ix->core) ? ix->core->launches() : 0; }
+
+uint64_t hb_device_allocations(void) { return hb::devbuf_generation().load(); }
+
+int hb_selftest_bounded_wait(hb_index* ix, int64_t budget_cycles, int64_t* waited_cycles) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] {
+    long long w = 0;
+    try {
+      ix->core->wait_selftest(budget_cycles, &w);
+    } catch (...) {
+      if (waited_cycles) *waited_cycles = w;
+      throw;
+    }
+    if (waited_cycles) *waited_cycles = w;
+  });
+}
 
 int hb_profile_enable(hb_index* ix, int on) {
   HB_NEED_INDEX(ix);

@@ -250,6 +250,10 @@ void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* cod
                      int nlist, const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int R,
                      const float* maxnorm, uint64_t* tau, cudaStream_t st, const int32_t* probes = nullptr,
                      int P = 0);
+// One thread waits on an mbarrier nothing arrives on, with a budget of
+// `budget` cycles: *err gets `code` and *waited the cycles spent (-1 if the
+// wait had completed, which cannot happen).
+void launch_wait_selftest(long long budget, int code, int* err, long long* waited, cudaStream_t st);
 // *out = max over i of sqrt(norms[i]) (slightly rounded up), on the device.
 void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st);
 // probes (nq x P) -> first column (nq x 1) and the rest (nq x (P-1)).

@@ -719,6 +719,20 @@ __global__ void to_bf16_kernel(const float* __restrict__ src, size_t n, int dpad
   }
 }
 
+// Self-test of the bounded mbarrier wait: one thread initialises an mbarrier
+// that nothing ever arrives on and waits for its first phase with a budget of
+// `budget` clock cycles.  No copy or MMA is in flight, so giving up is the
+// only way out; the wait records `code` in *err and the kernel returns.
+__global__ void wait_selftest_kernel(long long budget, int code, int* err, long long* waited) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  fence_barrier_init();
+  const long long t0 = clock64();
+  const bool done = mbar_wait(&bar, 0u, err, code, budget);
+  *waited = done ? -1 : clock64() - t0;
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -825,6 +839,12 @@ void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* cod
   tau_seed_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(
       q, dpad, kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff, list_q, xnorm, S, R, maxnorm,
       tau, by_query ? probes : nullptr, P);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_wait_selftest(long long budget, int code, int* err, long long* waited, cudaStream_t st) {
+  HB_CHECK(budget >= 0, HB_ERR_INVALID, "wait budget must be non-negative");
+  wait_selftest_kernel<<<1, 32, 0, st>>>(budget, code, err, waited);
   HB_CUDA(cudaGetLastError());
 }
 

@@ -84,7 +84,14 @@ typedef struct {
   int32_t use_graph;          /* 1: run the batch as one CUDA-graph launch,
                                  captured on first use per batch shape (see
                                  hb_search); ORIGINAL / BRUTE_FORCE, one batch */
-  int32_t reserved[4];
+  int32_t full_warmup;        /* Param::fullWarmUp: DIVIDE_DIM prunes against the
+                                 caller's heap_tops instead of running the warm-up
+                                 search (src/Index.cpp:1235-1241); the other modes
+                                 ignore it, as the reference does                */
+  const float* heap_tops;     /* Param::heapTops: nq floats (host or device); must
+                                 be set when full_warmup is (the reference exits
+                                 with "heapTop not exist"; here HB_ERR_INVALID)   */
+  int32_t reserved[2];
 } hb_search_params;
 
 void hb_search_params_init(hb_search_params* p);
@@ -185,6 +192,21 @@ void* hb_stream(hb_index* ix);
 
 /* Number of kernels this index has launched so far (for launch accounting). */
 uint64_t hb_launch_count(const hb_index* ix);
+
+/* Device allocations (cudaMalloc calls) the library has made in this process,
+ * over all indexes.  No reference counterpart: a diagnostic that lets a
+ * caller check that a call allocated nothing. */
+uint64_t hb_device_allocations(void);
+
+/* Self-test of the device-side bounded waits (no reference counterpart).
+ * Every mbarrier wait in the tensor-core kernels gives up after a clock
+ * budget, records an error code in a device flag and lets its kernel return,
+ * and the host reports HB_ERR_CUDA.  This launches one kernel whose single
+ * thread waits, with budget_cycles, on an mbarrier nothing arrives on (no
+ * copy or MMA in flight), so it returns HB_ERR_CUDA with "gave up waiting
+ * (code 99)" and the cycles the wait took in *waited_cycles; the index stays
+ * usable afterwards. */
+int hb_selftest_bounded_wait(hb_index* ix, int64_t budget_cycles, int64_t* waited_cycles);
 
 /* Per-kernel timing: when enabled, the index records CUDA events around each
  * of its kernels on its own stream.  hb_profile_read synchronises the stream,

@@ -37,6 +37,7 @@ class Index {
     bool pruning = false;
     bool period = false;
     bool fullWarmUp = false;
+    float* heapTops = nullptr;  // per-query pruning thresholds used when fullWarmUp (DIVIDE_DIM)
   };
 
   Index(size_t d = 0, size_t nlist = 0, size_t nprobe = 0, MetricType metric = METRIC_L2,
@@ -87,6 +88,8 @@ class Index {
       sp.n_query_blocks = static_cast<int32_t>(blockCount ? blockCount : 1);
       if (warmUpSearchList) sp.warmup_lists = static_cast<int32_t>(warmUpSearchList);
       sp.warmup_list_size = static_cast<int32_t>(warmUpSearchListSize);
+      sp.full_warmup = param->fullWarmUp ? 1 : 0;
+      sp.heap_tops = param->heapTops;
     }
     check(hb_search(h_, n, queries, k, &sp, distances, labels));
     size_t np = 0;

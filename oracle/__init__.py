@@ -24,7 +24,33 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libivf_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libharmony_ref.so")
-REFERENCE_SRC = "/root/reference"
+REF_RELEASE_SO = os.path.join(HERE, "_ref", "libharmony_ref_release.so")
+# Where the reference sources lie (only the build reads them).
+REFERENCE_SRC = os.environ.get("HARMONY_REFERENCE", "/root/reference")
+_AVX512 = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
+
+
+def host_cpu():
+    """(model name, logical cores, has the AVX-512 subsets x86-64-v4 needs)."""
+    model, flags = "unknown", set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and model == "unknown":
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags") and not flags:
+                    flags = set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return model, os.cpu_count() or 1, all(f in flags for f in _AVX512)
+
+
+def reference_build():
+    """(path, description) of the reference library this host loads: the
+    Release-flag build where the CPU has AVX-512, else the portable one."""
+    if os.path.exists(REF_RELEASE_SO) and host_cpu()[2]:
+        return REF_RELEASE_SO, "release flags (-Ofast -mavx512f -march=x86-64-v4 -O3 -DNDEBUG)"
+    return REF_SO, "portable flags (-O3 -DNDEBUG -ffp-contract=off)"
 
 _f = ctypes.POINTER(ctypes.c_float)
 _d = ctypes.POINTER(ctypes.c_double)
@@ -200,13 +226,15 @@ class RefIndex:
     """The reference's own harmony::Index (ORIGINAL mode), via oracle/_ref."""
 
     _L = None
+    build_kind = ""
 
     @classmethod
     def lib(cls):
         if cls._L is None:
-            if not os.path.exists(REF_SO):
-                raise FileNotFoundError(f"reference oracle not built: {REF_SO}")
-            L = ctypes.CDLL(REF_SO)
+            path, cls.build_kind = reference_build()
+            if not os.path.exists(path):
+                raise FileNotFoundError(f"reference oracle not built: {path}")
+            L = ctypes.CDLL(path)
             L.ref_index_new.restype = _vp
             L.ref_index_new.argtypes = [_sz, _sz, _sz]
             L.ref_index_free.argtypes = [_vp]

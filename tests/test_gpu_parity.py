@@ -175,6 +175,31 @@ def test_config2_pruned_and_dimblock(c2small, restated):
         assert_topk_parity(D, I, Do, Io, label=f"dimblock W={W} B={B}")
 
 
+def test_config2_dimblock_full_warmup(c2small, restated):
+    """Param::fullWarmUp: DIVIDE_DIM prunes against the caller's heap tops --
+    the query driver fills them with each query's k-th ground-truth distance
+    (src/query.cpp:716-725) -- and runs no warm-up search
+    (src/Index.cpp:1235-1241)."""
+    import torch
+    base, q, ix, ref = c2small
+    k = 100
+    ix.nprobe = ref.nprobe = 16
+    Dgt, _ = search(ix, q, k, Index.Param(mode=SearchMode.BRUTE_FORCE))
+    tops = np.ascontiguousarray(Dgt[:, k - 1])
+    data = ref.index_data()
+    probes = ref.probe_lists(q)
+    for W, B, opt in ((4, 4, True), (8, 3, False)):
+        order = restated.block_order(W, B, opt)
+        Do, Io = restated.search_dimblock(data, q, probes, tops, k, W, B, order, cut=True)
+        for t in (tops, torch.from_numpy(tops).cuda()):
+            prm = Index.Param(mode=SearchMode.DIVIDE_DIM, pruning=True, orderOptimize=opt, fullWarmUp=True,
+                              heapTops=t)
+            D, I = search(ix, q, k, prm, workers=W, blocks=B)
+            assert_topk_parity(D, I, Do, Io, label=f"full warm-up W={W} B={B}")
+    with pytest.raises(HarmonyError, match="heapTop"):
+        search(ix, q, k, Index.Param(mode=SearchMode.DIVIDE_DIM, pruning=True, fullWarmUp=True), workers=4, blocks=4)
+
+
 def test_single_query_batches_split_lists(c2small):
     """A one-query batch splits every list into many chunks (many slots)."""
     base, q, ix, ref = c2small

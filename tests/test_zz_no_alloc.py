@@ -61,6 +61,36 @@ def test_noalloc_matches_search_on_two_calls_in_a_row(built, k):
         assert np.array_equal(D.view(np.uint32), D0.view(np.uint32)) and np.array_equal(I, I0)
 
 
+def test_noalloc_allocates_nothing(built):
+    """The reason the entry point exists: after the first call (which looks the
+    fixed array's address up), a call makes no device allocation -- the
+    library's own allocation counter and the device's free memory are the same
+    before and after it, with the caller's buffers allocated beforehand."""
+    import torch
+    from harmony_b200 import lib
+    ix, q, qd = built
+    L = lib()
+    k = 10
+    nq = qd.shape[0]
+    D = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    I = torch.empty((nq, k), dtype=torch.int64, device="cuda")
+    assert L.hb_search_noalloc(ix._h, nq, qd.data_ptr(), k, D.data_ptr(), I.data_ptr()) == 0
+    torch.cuda.synchronize()
+    allocs0 = L.hb_device_allocations()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert L.hb_search_noalloc(ix._h, nq, qd.data_ptr(), k, D.data_ptr(), I.data_ptr()) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert L.hb_device_allocations() == allocs0
+    assert free1 == free0
+    # The ordinary search of a new shape does allocate (the counter works).
+    D2 = torch.empty((nq, 77), dtype=torch.float32, device="cuda")
+    I2 = torch.empty((nq, 77), dtype=torch.int64, device="cuda")
+    ix.search(nq, qd, 77, D2, I2)
+    assert L.hb_device_allocations() > allocs0
+
+
 def test_noalloc_smaller_call_after_larger_one(built):
     """The scratch keeps the previous call's contents; a smaller search after
     a larger one must not see them."""

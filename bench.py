@@ -18,6 +18,7 @@ every step touches every list, so no L2 flush is needed between steps.
         own CPU search, oracle/_ref, on the same frozen index and queries)
   python bench.py --workload c4     (10M x 96, Zipf list sizes, batches of 1..4096)
   python bench.py --workload c3     (270k x 500, k 100: the candidate-matrix BF16 path)
+  python bench.py --workload c2     (1M x 128, nlist 1024, k 100: the nprobe 8..128 sweep)
 
 Multi-GPU: the path is query-parallel with no exchange step, so N ranks run
 N independent replicas (weak scaling, each rank its own 10k queries).
@@ -782,6 +783,102 @@ def run_c3(args):
     print(json.dumps(line))
 
 
+def run_c2(args):
+    """Config 2: 1,000,000 x 128 (1000 unit-variance components, centres
+    N(0, 4^2)), 10,000 queries, nlist 1024, k 100, the reference driver's
+    nprobe sweep 8 / 16 / 32 / 64 / 128 (src/query.cpp:680-777).  Per nprobe:
+    the plain FP32 scan (the reference's arithmetic) and the bounded BF16 scan
+    (whose result must equal it), device-timed (CUDA events on the index
+    stream, queries and results resident), with the scan kernel's own time,
+    its algorithmic bytes (every probed list read once per probing query, the
+    reference's traffic) and its FP32-pipe fraction (3 FP32 operations per
+    element pair against SMs x 128 lanes x 2 (packed f32x2) x the sampled
+    clock); recall@100 against FP64 ground truth on the first 1000 queries."""
+    import torch
+    from harmony_b200 import Index, Precision, SearchMode, datasets
+    k, nq, nb, d, nlist = 100, args.nq or 10_000, args.nb or 1_000_000, 128, 1024
+    base_np, q_np = datasets.config2(nb=nb, nq=nq)
+    base = torch.from_numpy(base_np).cuda()
+    queries = torch.from_numpy(q_np).cuda()
+    ix = Index(d, nlist, 8)
+    t0 = time.perf_counter()
+    ix.train(nb, base)
+    ix.add(nb, base)
+    torch.cuda.synchronize()
+    build_s = round(time.perf_counter() - t0, 2)
+    ng = min(1000, nq)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.BRUTE_FORCE), "")
+    GI = torch.empty((ng, 128), dtype=torch.int64, device="cuda")
+    G = torch.empty((ng, 128), dtype=torch.float32, device="cuda")
+    ix.search(ng, queries[:ng], 128, G, GI)
+    cand = base[GI.reshape(-1)].double().reshape(ng, 128, d)
+    d64 = ((cand - queries[:ng].double()[:, None, :]) ** 2).sum(-1)
+    gt = torch.gather(GI, 1, torch.argsort(d64, dim=1, stable=True))[:, :k].cpu().numpy()
+    del cand, d64
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    sizes = ix.list_sizes()
+    D = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    I = torch.empty((nq, k), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.ExternalStream(ix.stream)
+    sweep = []
+    with ClockSampler(0) as clk:
+        for P in (8, 16, 32, 64, 128):
+            ix.nprobe = P
+            probes, _ = ix.probe_lists(q_np, P)
+            pairs = int(sizes[probes].sum())
+            row = {"nprobe": P, "probed_vectors_per_query": round(pairs / nq, 1)}
+            outs = {}
+            for name, prec in (("fp32", Precision.FP32), ("bf16", Precision.BF16)):
+                ix.search_params.precision = prec
+                reps = 3 if prec == Precision.FP32 else 10
+                for _ in range(3):
+                    ix.search(nq, queries, k, D, I)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    ix.search(nq, queries, k, D, I)
+                e1.record(stream)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                ix.profile(True)
+                ix.search(nq, queries, k, D, I)
+                kern = {kk: round(v[0], 4) for kk, v in ix.profile_read().items()}
+                ix.profile(False)
+                outs[name] = (D.cpu().numpy().copy(), I.cpu().numpy().copy())
+                arm = {"ms": round(ms, 3), "qps": round(nq / ms * 1e3, 1), "kernels_ms": kern,
+                       "recall_at_100_first_1000": round(recall(outs[name][1][:ng], gt, k), 4)}
+                scan = kern.get("scan_exact" if prec == Precision.FP32 else "scan_bf16")
+                if scan:
+                    elem = 2 if prec == Precision.BF16 else 4
+                    arm["scan_bytes_alg_gbs"] = round(pairs * d * elem / (scan / 1e3) / 1e9, 1)
+                    if prec == Precision.FP32:
+                        arm["scan_fp32_ops_per_s"] = 3.0 * pairs * d / (scan / 1e3)
+                row[name] = arm
+            ok, n = parity_count(*outs["bf16"], *outs["fp32"])
+            row["bf16_identical_to_fp32"] = {"identical": ok, "queries": n}
+            sweep.append(row)
+        ix.search_params.precision = Precision.FP32
+    ck = clk.summary()
+    sm = ck.get("sm_mhz") or 1965.0
+    peak = 148 * 128 * 2 * sm * 1e6
+    for row in sweep:
+        v = row["fp32"].get("scan_fp32_ops_per_s")
+        if v:
+            row["fp32"]["scan_fp32_pipe_frac"] = round(v / peak, 3)
+            row["fp32"]["scan_fp32_ops_per_s"] = round(v / 1e12, 2)
+    line = {"metric": "QPS per nprobe, config2 (1M x 128, nlist 1024, k 100, 10k queries)",
+            "workload": "c2", "unit": "queries/s", "n_gpus": 1, "dtype": "f32 / bf16",
+            "data": "synthetic (seeded 1000-component Gaussian mixture, centres N(0, 4^2); stands in for sift1m's shape)",
+            "config": {"nb": nb, "d": d, "nlist": nlist, "k": k, "nq": nq, "build_s": build_s,
+                       "list_size_min": int(sizes.min()), "list_size_max": int(sizes.max()),
+                       "fp32_pipe_peak": "148 SMs x 128 lanes x 2 (f32x2) x sampled SM clock, 3 ops per element pair",
+                       "inputs": "512 MB of FP32 codes > L2; every step reads each probed list"},
+            "clocks": ck, "sweep": sweep}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -795,9 +892,9 @@ def main():
     ap.add_argument("--nq", type=int, default=None, help="fewer queries for profiling runs (not a bench line)")
     ap.add_argument("--ntrain", type=int, default=200_000, help="training queries of the learned probe")
     ap.add_argument("--freeze-to", default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", choices=["c5", "c4", "c3"], default="c5",
+    ap.add_argument("--workload", choices=["c5", "c4", "c3", "c2"], default="c5",
                     help="c5: the headline bench line; c4: the batch-stream measurement of config 4; "
-                         "c3: the 500-dimensional k = 100 measurement of config 3")
+                         "c3: the 500-dimensional k = 100 measurement of config 3; c2: the 1M x 128 nprobe sweep")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -813,6 +910,8 @@ def main():
         run_c4(args)
     elif args.workload == "c3":
         run_c3(args)
+    elif args.workload == "c2":
+        run_c2(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -151,6 +151,8 @@ def lib() -> ctypes.CDLL:
     L.hb_device_allocations.restype = ctypes.c_uint64
     L.hb_device_allocations.argtypes = []
     L.hb_selftest_bounded_wait.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    L.hb_set_wait_budget.argtypes = [vp, ctypes.c_int64]
+    L.hb_bf16_fallbacks.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.hb_train_probe_predictor.argtypes = [vp, sz, f, sz, sz, ctypes.c_float]
     L.hb_search_noalloc.argtypes = [vp, sz, f, sz, f, i64]
     L.hb_retain_lists.argtypes = [vp, sz, sz]
@@ -478,6 +480,18 @@ class Index:
         the exact FP32 distance matrix) and the tensor-core candidate margin
         (-1: max(16, nprobe / 4)).  The probe rows do not depend on it."""
         _check(self._L.hb_set_coarse_quantizer(self._h, int(kind), int(margin)))
+
+    def bf16_fallbacks(self) -> int:
+        """Queries of the latest BF16 search (d <= 128, k <= 256) whose candidate
+        buffer overflowed and were searched again with the exact scan."""
+        n = ctypes.c_int64()
+        _check(self._L.hb_bf16_fallbacks(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def set_wait_budget(self, cycles: int = 0) -> None:
+        """Clock cycles a device wait of the BF16 scan spends before giving up
+        (0: the default)."""
+        _check(self._L.hb_set_wait_budget(self._h, int(cycles)))
 
     def coarse_fallbacks(self) -> int:
         """Queries of the latest tensor-core coarse call recomputed exactly."""

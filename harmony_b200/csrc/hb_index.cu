@@ -535,6 +535,9 @@ class IndexCore {
     }
   }
 
+  void set_wait_budget(long long cycles) { wait_budget_ = cycles > 0 ? cycles : kDefaultWaitBudget; }
+  int last_overflow() const { return last_overflow_; }
+
   void set_coarse(int kind, int margin) {
     HB_CHECK(kind >= HB_COARSE_AUTO && kind <= HB_COARSE_TENSOR, HB_ERR_INVALID, "unknown coarse quantizer kind");
     HB_CHECK(margin >= -1 && margin <= kCoarseMaxPm, HB_ERR_INVALID, "coarse margin must be in [-1, 1024]");
@@ -576,13 +579,15 @@ class IndexCore {
     }
     HB_CHECK(p.seed_rows >= 0 && p.seed_rows <= 256, HB_ERR_INVALID, "seed_rows must be in [0, 256]");
     seed_rows_ = p.seed_rows > 0 ? p.seed_rows : 256;
-    // BF16 route: the shared-memory heap scan for d <= 128 and k up to its
-    // candidate capacity, else the candidate-matrix scan.
-    const int max_R = bf16 ? scan_bf16_max_R(kpad_ > 0 ? kpad_ : 128) : 0;
+    // BF16 route: the bounded filter scan (exact result) for d <= 128 and
+    // k <= 256, else the candidate-matrix scan with a fixed re-rank width.
     const int want_R = std::max(static_cast<int>(k), p.rerank_mult * static_cast<int>(k));
-    cand_path_ = bf16 && !(kpad_ <= 128 && static_cast<int>(k) <= max_R);
-    const int R = !bf16 ? 0 : cand_path_ ? std::min(kCandMaxR, want_R) : std::min(max_R, want_R);
-    if (bf16)
+    int etv = 0, eqt = 0, eqg = 0;
+    const bool exact_k = scan_exact_smem_bytes(static_cast<int>(d_), static_cast<int>(dpad_), static_cast<int>(k),
+                                               SCAN_PLAIN, &etv, &eqt, &eqg) > 0;
+    cand_path_ = bf16 && !(kpad_ <= 128 && static_cast<int>(k) <= kFilterMaxK && exact_k);
+    const int R = cand_path_ ? std::min(kCandMaxR, want_R) : 0;
+    if (cand_path_)
       HB_CHECK(static_cast<int>(k) <= R, HB_ERR_INVALID,
                "BF16 search supports k up to " + std::to_string(kCandMaxR));
     int mode = SCAN_PLAIN;
@@ -646,6 +651,8 @@ class IndexCore {
     const bool dev_in = is_device_ptr(q);
     size_t bs = std::min<size_t>(nq, batch_limit(P, k));
     if (cand_path_ && P > 0) bs = std::min(bs, cand_batch_limit(P));
+    if (bf16 && !cand_path_)
+      bs = std::min(bs, std::max<size_t>(1, (size_t(1) << 30) / (static_cast<size_t>(filter_cap(k)) * 8)));
     const int warm_lists = p.warmup_lists;
     const int warm_size = p.warmup_list_size > 0 ? p.warmup_list_size : static_cast<int>(k);
     // DIVIDE_DIM query blocks cover queries [0, B * (nq / B)); the rest stay
@@ -801,6 +808,10 @@ class IndexCore {
       }
       cudaGraphDestroy(graph);
       launches_ = l0;
+    }
+    if (bf16 && !cand_path_) {
+      bf16_err_check();
+      fix_overflow(nb, P, k, dout_.p, iout_.p);
     }
     HB_CUDA(cudaMemcpyAsync(D, dout_.p, static_cast<size_t>(nb) * k * sizeof(float), cudaMemcpyDefault, st_));
     HB_CUDA(cudaMemcpyAsync(I, iout_.p, static_cast<size_t>(nb) * k * sizeof(int64_t), cudaMemcpyDefault, st_));
@@ -1214,6 +1225,16 @@ class IndexCore {
         ++launches_;
       }
     }
+    scan_exact_from(nb, P, k, qpad_.p, probes_.p, mode, cut, need_tops ? tops_.p : nullptr, W, B, qblock, Dd, Id);
+  }
+
+  // The exact list scan and merge of nb queries (qpad, nb x dpad) over the
+  // probe table `probes` (nb x P).
+  void scan_exact_from(int nb, int P, int k, const float* qpad, const int32_t* probes, int mode, bool cut,
+                       const float* tops, int W, int B, int qblock, float* Dd, int64_t* Id) {
+    int tv = 0, qt = 0, qg = 0;
+    const size_t smem = scan_exact_smem_bytes(static_cast<int>(d_), static_cast<int>(dpad_), k, mode, &tv, &qt, &qg);
+    HB_CHECK(smem > 0, HB_ERR_INVALID, "k too large for the fused scan at this dimension");
     const int cr = chunk_rows_for(nb, P, tv);
     list_cnt_.reserve(nlist_);
     list_cursor_.reserve(nlist_);
@@ -1224,9 +1245,9 @@ class IndexCore {
     const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
     work_tmp_.reserve(wtmp);
     {
-    Scope sc(this, "build_work");
-    launch_build_work(probes_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt_.p, list_qoff_.p,
-                      list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+      Scope sc(this, "build_work");
+      launch_build_work(probes, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt_.p, list_qoff_.p,
+                        list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
     }
     launches_ += 3;
     part_.reserve(max_slots(nb, P, cr) * static_cast<size_t>(k));
@@ -1238,7 +1259,7 @@ class IndexCore {
     a.nlist = static_cast<int>(nlist_);
     a.d = static_cast<int>(d_);
     a.dpad = static_cast<int>(dpad_);
-    a.q = qpad_.p;
+    a.q = qpad;
     a.nq = nb;
     a.P = P;
     a.k = k;
@@ -1252,7 +1273,7 @@ class IndexCore {
     a.work_counter = counter_.p;
     a.part = part_.p;
     a.mode = mode;
-    a.tops = need_tops ? tops_.p : nullptr;
+    a.tops = tops;
     a.cut = cut ? 1 : 0;
     a.nseg = W;
     a.seg_order = order_dev_.p;
@@ -1267,66 +1288,19 @@ class IndexCore {
     launches_ += 2;
   }
 
-  // One tensor-core scan pass over the probe table `probes` (nb x P):
-  // work description, then the scan into `part` (slots from `slot_base`).
-  void bf16_pass(int nb, int P, const int32_t* probes, int R, DevBuf<int64_t>& slot_base, DevBuf<uint64_t>& part) {
-    const int cr = std::max(128, chunk_rows_for(nb, P, 128));
-    list_cnt_.reserve(nlist_);
-    list_cursor_.reserve(nlist_);
-    list_qoff_.reserve(nlist_ + 1);
-    item_off_.reserve(nlist_ + 1);
-    list_q_.reserve(static_cast<size_t>(nb) * P);
-    slot_base.reserve(static_cast<size_t>(nb) * P + 1);
-    const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
-    work_tmp_.reserve(wtmp);
-    {
-      Scope sc(this, "build_work");
-      launch_build_work(probes, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p, list_qoff_.p,
-                        list_cursor_.p, list_q_.p, item_off_.p, slot_base.p, work_tmp_.p, wtmp, st_);
-    }
-    launches_ += 3;
-    {
-      Scope sc(this, "tau_seed");
-      launch_tau_seed(qpad_.p, nb, static_cast<int>(dpad_), kpad_, codes_bf16_.p, list_off_.p, static_cast<int>(nlist_),
-                      list_qoff_.p, list_q_.p, norms_.p, std::max(R, seed_rows_), R, maxnorm_.p, tau_.p, st_, probes, P);
-    }
-    ++launches_;
-    part.reserve(max_slots(nb, P, cr) * static_cast<size_t>(scan_bf16_keys_per_slot(R)));
-    counter_.reserve(1);
-    HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
-    TcArgs a{};
-    a.list_off = list_off_.p;
-    a.nlist = static_cast<int>(nlist_);
-    a.kpad = kpad_;
-    a.dpad = static_cast<int>(dpad_);
-    a.q = qpad_.p;
-    a.tile_norm = tile_norm_.p;
-    a.tile_off = tile_off_.p;
-    a.stages = scan_bf16_stages(kpad_, R);
-    a.list_cnt = list_cnt_.p;
-    a.list_qoff = list_qoff_.p;
-    a.list_q = list_q_.p;
-    a.item_off = item_off_.p;
-    a.slot_base = slot_base.p;
-    a.chunk_rows = cr;
-    a.P = P;
-    a.R = R;
-    a.work_counter = counter_.p;
-    a.part = part.p;
-    a.tau = tau_.p;
-    a.err = err_dev_.p;
-    {
-      Scope sc(this, "scan_bf16");
-      launch_scan_bf16(tmap_, a, num_sms_, st_);
-    }
-    ++launches_;
+  // Candidate buffer per query of the bounded BF16 scan: room for 16 k
+  // candidates (at least 1024); a query needing more is searched again with
+  // the exact scan.
+  static int filter_cap(size_t k) {
+    return static_cast<int>(std::min<size_t>(kRerankMaxCap, std::max<size_t>(1024, 16 * k)));
   }
 
-  // BF16 search of one batch: exact coarse probes, the list-major work
-  // description, a per-query bound of the R-th approximate key seeded from
-  // the nearest list, one tensor-core pass
-  // over all probes (items tighten the shared bound as they finish), and
-  // the exact FP32 re-rank.
+  // BF16 search of one batch, equal to the exact FP32 scan bit for bit: exact
+  // coarse probes, per-query BF16 rows / error bounds, the list-major work
+  // description, a per-query admission bound seeded from the nearest list,
+  // one tensor-core pass appending the rows under each query's bound, then
+  // the exact re-rank of the rows under W_k + 2 eps.  Queries whose candidate
+  // buffer overflowed are searched again with the exact scan.
   void search_batch_bf16(int nb, int P, int k, int R, float* Dd, int64_t* Id) {
     if (cand_path_) {
       search_batch_cand(nb, P, k, R, Dd, Id);
@@ -1336,16 +1310,107 @@ class IndexCore {
     coarse_and_cut(nb, P);
     err_dev_.reserve(1);
     HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
-    tau_.reserve(nb);
-    rr_over_.reserve(nb);
-    bf16_pass(nb, P, probes_.p, R, slot_base_, part_);
+    const int cap = filter_cap(k);
+    qbf_.reserve(static_cast<size_t>(nb) * kpad_);
+    e2_.reserve(nb);
+    thr_.reserve(nb);
+    ccnt_.reserve(nb);
+    cflag_.reserve(nb);
+    over_list_.reserve(nb);
+    over_n_.reserve(1);
+    cbuf_.reserve(static_cast<size_t>(nb) * cap);
+    HB_CUDA(cudaMemsetAsync(over_n_.p, 0, sizeof(int), st_));
+    {
+      Scope sc(this, "query_prep");
+      launch_query_prep(qpad_.p, nb, static_cast<int>(d_), static_cast<int>(dpad_), kpad_, maxnorm_.p, qbf_.p, e2_.p,
+                        thr_.p, ccnt_.p, st_);
+    }
+    const int cr = std::max(128, chunk_rows_for(nb, P, 128));
+    list_cnt_.reserve(nlist_);
+    list_cursor_.reserve(nlist_);
+    list_qoff_.reserve(nlist_ + 1);
+    item_off_.reserve(nlist_ + 1);
+    list_q_.reserve(static_cast<size_t>(nb) * P);
+    slot_base_.reserve(static_cast<size_t>(nb) * P + 1);
+    const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
+    work_tmp_.reserve(wtmp);
+    {
+      Scope sc(this, "build_work");
+      launch_build_work(probes_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p, list_qoff_.p,
+                        list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+    }
+    {
+      Scope sc(this, "seed");
+      launch_seed_bound(qbf_.p, nb, kpad_, codes_bf16_.p, list_off_.p, static_cast<int>(nlist_), list_qoff_.p,
+                        list_q_.p, norms_.p, std::max(seed_rows_, k), k, e2_.p, thr_.p, st_, probes_.p, P);
+    }
+    counter_.reserve(1);
+    HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
+    TcArgs a{};
+    a.list_off = list_off_.p;
+    a.nlist = static_cast<int>(nlist_);
+    a.kpad = kpad_;
+    a.qbf = qbf_.p;
+    a.tile_norm = tile_norm_.p;
+    a.tile_off = tile_off_.p;
+    a.list_cnt = list_cnt_.p;
+    a.list_qoff = list_qoff_.p;
+    a.list_q = list_q_.p;
+    a.item_off = item_off_.p;
+    a.chunk_rows = cr;
+    a.work_counter = counter_.p;
+    a.thr = thr_.p;
+    a.e2 = e2_.p;
+    a.cand = cbuf_.p;
+    a.cand_cnt = ccnt_.p;
+    a.cap = cap;
+    a.k = k;
+    a.err = err_dev_.p;
+    a.stages = scan_bf16_stages(kpad_);
+    a.wait_budget = wait_budget_;
+    {
+      Scope sc(this, "scan_bf16");
+      launch_scan_bf16(tmap_, a, num_sms_, st_);
+    }
     {
       Scope sc(this, "rerank");
-      launch_rerank(part_.p, slot_base_.p, nb, P, R, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd, Id,
-                    st_, nullptr, nullptr, 0, tau_.p, rr_over_.p);
+      launch_rerank_bf16(cbuf_.p, ccnt_.p, cap, e2_.p, nb, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd,
+                         Id, cflag_.p, over_list_.p, over_n_.p, num_sms_, st_);
     }
-    ++launches_;
-    if (!capturing_) bf16_err_check();
+    launches_ += 8 + (cap > 256 ? 1 : 0);
+    if (!capturing_) {
+      bf16_err_check();
+      fix_overflow(nb, P, k, Dd, Id);
+    }
+  }
+
+  // Queries whose candidate buffer overflowed (listed by the re-rank, left
+  // unwritten) are searched with the exact scan over their own probe rows,
+  // and their result rows are written into Dd / Id.
+  void fix_overflow(int nb, int P, int k, float* Dd, int64_t* Id) {
+    int n_over = 0;
+    HB_CUDA(cudaMemcpyAsync(err_host_, over_n_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    HB_CUDA(cudaStreamSynchronize(st_));
+    n_over = *err_host_;
+    last_overflow_ = n_over;
+    if (n_over <= 0) return;
+    HB_CHECK(n_over <= nb, HB_ERR_CUDA, "overflow list longer than the batch");
+    Scope sc(this, "overflow_exact");
+    const int dp = static_cast<int>(dpad_);
+    oq_.reserve(static_cast<size_t>(n_over) * dpad_);
+    op_.reserve(static_cast<size_t>(n_over) * P);
+    od_.reserve(static_cast<size_t>(n_over) * k);
+    oi_.reserve(static_cast<size_t>(n_over) * k);
+    launch_gather_words(reinterpret_cast<const uint32_t*>(qpad_.p), over_list_.p, n_over, dp,
+                        reinterpret_cast<uint32_t*>(oq_.p), st_);
+    launch_gather_words(reinterpret_cast<const uint32_t*>(probes_.p), over_list_.p, n_over, P,
+                        reinterpret_cast<uint32_t*>(op_.p), st_);
+    scan_exact_from(n_over, P, k, oq_.p, op_.p, SCAN_PLAIN, false, nullptr, 1, 1, 0, od_.p, oi_.p);
+    launch_scatter_words(reinterpret_cast<const uint32_t*>(od_.p), over_list_.p, n_over, k,
+                         reinterpret_cast<uint32_t*>(Dd), st_);
+    launch_scatter_words(reinterpret_cast<const uint32_t*>(oi_.p), over_list_.p, n_over, 2 * k,
+                         reinterpret_cast<uint32_t*>(Id), st_);
+    launches_ += 4;
   }
 
   // Longest candidate row a query can have at nprobe P: the P largest lists,
@@ -1810,10 +1875,19 @@ class IndexCore {
   bool capturing_ = false;
   std::map<std::string, GraphEntry> graphs_;
   DevBuf<int32_t> npqin_;
+  // bounded BF16 scan
+  DevBuf<uint16_t> qbf_;
+  DevBuf<float> e2_;
+  DevBuf<uint32_t> thr_;
+  DevBuf<int> ccnt_, cflag_, over_list_, over_n_;
+  DevBuf<uint64_t> cbuf_;
+  DevBuf<float> oq_, od_;
+  DevBuf<int32_t> op_;
+  DevBuf<int64_t> oi_;
+  long long wait_budget_ = kDefaultWaitBudget;
+  int last_overflow_ = 0;
   DevBuf<int32_t> kq_;
-  DevBuf<int> rr_over_;
   DevBuf<uint16_t> codes_bf16_;
-  DevBuf<uint64_t> tau_;
   DevBuf<float> maxnorm_, tile_norm_;
   DevBuf<int64_t> tile_off_;
   DevBuf<int32_t> probes1_;
@@ -2041,6 +2115,19 @@ void* hb_stream(hb_index* ix) { return (ix && ix->core) ? static_cast<void*>(ix-
 uint64_t hb_launch_count(const hb_index* ix) { return (ix && ix->core) ? ix->core->launches() : 0; }
 
 uint64_t hb_device_allocations(void) { return hb::devbuf_generation().load(); }
+
+int hb_set_wait_budget(hb_index* ix, int64_t cycles) {
+  HB_NEED_INDEX(ix);
+  ix->core->set_wait_budget(cycles);
+  return HB_OK;
+}
+
+int hb_bf16_fallbacks(hb_index* ix, int64_t* n) {
+  HB_NEED_INDEX(ix);
+  if (!n) return HB_ERR_INVALID;
+  *n = ix->core->last_overflow();
+  return HB_OK;
+}
 
 int hb_selftest_bounded_wait(hb_index* ix, int64_t budget_cycles, int64_t* waited_cycles) {
   HB_NEED_INDEX(ix);

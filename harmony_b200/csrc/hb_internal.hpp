@@ -166,41 +166,63 @@ void launch_list_offsets(const int32_t* assign, size_t n, int nlist, int64_t* li
                          void* tmp, size_t tmp_bytes, cudaStream_t st);
 size_t list_offsets_tmp_bytes(int nlist);
 void launch_i64_to_i32(const int64_t* src, size_t n, int32_t* dst, cudaStream_t st);
+// Rows of w 32-bit words: dst[i] = src[idx[i]] (gather) / dst[idx[i]] = src[i]
+// (scatter), i < n.
+void launch_gather_words(const uint32_t* src, const int32_t* idx, int n, int w, uint32_t* dst, cudaStream_t st);
+void launch_scatter_words(const uint32_t* src, const int32_t* idx, int n, int w, uint32_t* dst, cudaStream_t st);
 void launch_i32_to_i64(const int32_t* src, size_t n, int64_t* dst, cudaStream_t st);
 void launch_fill_results(float* D, int64_t* I, size_t n, cudaStream_t st);
 
-// k_tc.cu: BF16 tensor-core scan + exact FP32 re-rank.
+// k_tc.cu: BF16 tensor-core scan whose exact FP32 re-rank reproduces the
+// exact scan bit for bit (the error bound and the admission rule are
+// described at the top of k_tc.cu).
 struct TcArgs {
   const int64_t* list_off;
   int nlist;
   int kpad;                    // BF16 row length (d rounded up to 64)
-  int dpad;                    // FP32 row length of queries / codes
-  const float* q;              // nq x dpad FP32 queries
+  const void* qbf;             // nq x kpad BF16 queries
   const float* tile_norm;      // ||x||^2 per 128-row tile of each list, +inf past the list's end
   const int64_t* tile_off;     // first tile of each list in tile_norm (nlist + 1)
   const int32_t* list_cnt;
   const int64_t* list_qoff;
   const int32_t* list_q;
   const int64_t* item_off;
-  const int64_t* slot_base;
   int chunk_rows;              // multiple of 128
-  int P;
-  int R;                       // candidates kept per (query, chunk)
   unsigned int* work_counter;
-  uint64_t* part;              // slots x R keys
-  uint64_t* tau;               // per query: best known R-th key (all ones = none yet)
+  uint32_t* thr;               // per query: admission bound (ordered float bits), lowered by atomicMin
+  const float* e2;             // per query: 2 x the error bound eps
+  uint64_t* cand;              // nq x cap candidate keys (ordered w bits << 32 | position)
+  int* cand_cnt;               // per query: candidates appended (may exceed cap: overflow)
+  int cap;
+  int k;
   int* err;                    // non-zero after a bounded wait gave up
   int stages;                  // B tile ring depth (scan_bf16_stages)
+  long long wait_budget;       // clock cycles a bounded mbarrier wait spends before giving up
 };
-size_t scan_bf16_smem_bytes(int kpad, int R, int stages);
-int scan_bf16_stages(int kpad, int R);  // deepest ring that fits beside R candidates
+constexpr int kRerankMaxCap = 8192;  // largest candidate buffer per query
+constexpr int kFilterMaxK = 256;     // largest k of the bounded scan (its seed samples <= 256 rows)
+constexpr long long kDefaultWaitBudget = 2000000000LL;  // clock cycles before a device wait gives up
+size_t scan_bf16_smem_bytes(int kpad, int stages);
+int scan_bf16_stages(int kpad);  // deepest B tile ring that fits
 // Per-tile norm array: tile_off (nlist + 1, prefix of ceil(n_l / 128)) and
 // tile_norm (tiles x 128 floats, +inf past each list's end).
 void launch_tile_norms(const float* norms, const int64_t* list_off, int nlist, const int64_t* tile_off,
                        float* tile_norm, cudaStream_t st);
-int scan_bf16_keys_per_slot(int R);  // keys each (query, chunk) slot holds
-int scan_bf16_max_R(int kpad);       // largest candidate count per query the scan holds
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);
+// Per query: BF16 row, 2 eps, bound reset to FLT_MAX, candidate count 0.
+void launch_query_prep(const float* q, int nq, int d, int dpad, int kpad, const float* maxnorm, void* qbf, float* e2,
+                       uint32_t* thr, int* cnt, cudaStream_t st);
+// Seed bound from the first S <= 256 rows of each query's nearest list (probe
+// rank 0 in the list-major work description; with probes given and a small
+// batch, one CTA per query).
+void launch_seed_bound(const void* qbf, int nq, int kpad, const void* codes_bf16, const int64_t* list_off, int nlist,
+                       const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int k,
+                       const float* e2, uint32_t* thr, cudaStream_t st, const int32_t* probes = nullptr, int P = 0);
+// Exact re-rank of the admitted rows under W_k + 2 eps; flag[q] = 2 and
+// over_list / over_n for queries whose buffer overflowed (left unwritten).
+void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
+                        const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
+                        int* flag, int* over_list, int* over_n, int num_sms, cudaStream_t st);
 
 // Candidate-matrix BF16 scan (k_cand.cu): any kpad (a multiple of 64) and up
 // to kCandMaxR candidates per query.
@@ -236,20 +258,6 @@ void launch_cand_exact(const int64_t* rows, int nq, int R, int k, const float* c
                        const int64_t* ids, float* D, int64_t* I, cudaStream_t st);
 void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st);
 void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st);
-// Re-rank over the slots of one or two scan passes (part2 may be null);
-// tau (optional): per query an upper bound of its R-th key (the scan's final
-// bound), keys above it are skipped.
-void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
-                   const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
-                   const uint64_t* part2 = nullptr, const int64_t* slot_base2 = nullptr, int P2 = 0,
-                   const uint64_t* tau = nullptr, int* overflow = nullptr);
-// Per-query upper bound of the R-th approximate key from the first S <= 256
-// BF16 rows of the query's nearest list (probe rank 0 in the list-major work
-// description); queries without a seed get all ones.  maxnorm = max ||x||.
-void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* codes_bf16, const int64_t* list_off,
-                     int nlist, const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int R,
-                     const float* maxnorm, uint64_t* tau, cudaStream_t st, const int32_t* probes = nullptr,
-                     int P = 0);
 // One thread waits on an mbarrier nothing arrives on, with a budget of
 // `budget` cycles: *err gets `code` and *waited the cycles spent (-1 if the
 // wait had completed, which cannot happen).

@@ -3,6 +3,8 @@
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "hb_device.cuh"
 #include "hb_internal.hpp"
 
@@ -220,6 +222,45 @@ void launch_i32_to_i64(const int32_t* src, size_t n, int64_t* dst, cudaStream_t 
 void launch_fill_results(float* D, int64_t* I, size_t n, cudaStream_t st) {
   if (!n) return;
   fill_results_kernel<<<grid_exact(n, 256), 256, 0, st>>>(D, I, n);
+  HB_CUDA(cudaGetLastError());
+}
+
+
+namespace {
+__global__ void gather_words_kernel(const uint32_t* __restrict__ src, const int32_t* __restrict__ idx, int n, int w,
+                                    uint32_t* __restrict__ dst) {
+  const size_t total = static_cast<size_t>(n) * w;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t r = i / w, c = i - r * w;
+    dst[i] = src[static_cast<size_t>(idx[r]) * w + c];
+  }
+}
+
+__global__ void scatter_words_kernel(const uint32_t* __restrict__ src, const int32_t* __restrict__ idx, int n, int w,
+                                     uint32_t* __restrict__ dst) {
+  const size_t total = static_cast<size_t>(n) * w;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t r = i / w, c = i - r * w;
+    dst[static_cast<size_t>(idx[r]) * w + c] = src[i];
+  }
+}
+}  // namespace
+
+void launch_gather_words(const uint32_t* src, const int32_t* idx, int n, int w, uint32_t* dst, cudaStream_t st) {
+  if (n <= 0 || w <= 0) return;
+  const size_t total = static_cast<size_t>(n) * w;
+  const unsigned g = static_cast<unsigned>(std::min<size_t>((total + 255) / 256, 148 * 32));
+  gather_words_kernel<<<g, 256, 0, st>>>(src, idx, n, w, dst);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_scatter_words(const uint32_t* src, const int32_t* idx, int n, int w, uint32_t* dst, cudaStream_t st) {
+  if (n <= 0 || w <= 0) return;
+  const size_t total = static_cast<size_t>(n) * w;
+  const unsigned g = static_cast<unsigned>(std::min<size_t>((total + 255) / 256, 148 * 32));
+  scatter_words_kernel<<<g, 256, 0, st>>>(src, idx, n, w, dst);
   HB_CUDA(cudaGetLastError());
 }
 

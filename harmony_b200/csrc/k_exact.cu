@@ -58,6 +58,51 @@ __device__ __forceinline__ void dist_plain(const float* __restrict__ xr, const f
   }
 }
 
+// Packed FP32 pairs (sm_100a f32x2): two queries' running sums in one 64-bit
+// register; sub / mul / add .rn.f32x2 round each lane on its own, so every
+// lane is exactly the scalar sequential sum above.
+__device__ __forceinline__ uint64_t f2_pack(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2_sq_acc(uint64_t acc, uint64_t q2, uint64_t x2) {
+  uint64_t t;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(q2), "l"(x2));
+  asm("mul.rn.f32x2 %0, %1, %1;" : "=l"(t) : "l"(t));
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(acc) : "l"(acc), "l"(t));
+  return acc;
+}
+
+// One row against NP query pairs stored pair-interleaved: qp[(p * dpad + c)
+// * 2 + {0,1}] = dim c of the pair's two queries.
+template <int NP>
+__device__ __forceinline__ void dist_plain_x2(const float* __restrict__ xr, const float* __restrict__ qp, int dpad,
+                                              float (&out)[2 * NP]) {
+  uint64_t acc[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) acc[p] = 0ull;  // (+0.0f, +0.0f)
+#pragma unroll 2
+  for (int c = 0; c < dpad; c += 4) {
+    const float4 x = *reinterpret_cast<const float4*>(xr + c);
+    const uint64_t x0 = f2_pack(x.x, x.x), x1 = f2_pack(x.y, x.y), x2 = f2_pack(x.z, x.z), x3 = f2_pack(x.w, x.w);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const ulonglong2 qa = *reinterpret_cast<const ulonglong2*>(qp + (static_cast<size_t>(p) * dpad + c) * 2);
+      const ulonglong2 qb = *reinterpret_cast<const ulonglong2*>(qp + (static_cast<size_t>(p) * dpad + c) * 2 + 4);
+      acc[p] = f2_sq_acc(acc[p], qa.x, x0);
+      acc[p] = f2_sq_acc(acc[p], qa.y, x1);
+      acc[p] = f2_sq_acc(acc[p], qb.x, x2);
+      acc[p] = f2_sq_acc(acc[p], qb.y, x3);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < NP; ++p) f2_unpack(acc[p], out[2 * p], out[2 * p + 1]);
+}
+
 // Segmented sums: the dimension range is cut at bnd[0..nb) (ascending, in
 // true dims); part[i][s] is the fresh sequential sum of segment s.
 template <int QT, int MAXSEG>
@@ -443,6 +488,154 @@ __global__ void __launch_bounds__(kThreads, 1) scan_exact_kernel(ScanArgs a, int
 }
 
 // ----------------------------------------------------------------------------
+// Persistent list scan of the ORIGINAL / BRUTE_FORCE searches (plain
+// sequential sums) with packed f32x2 arithmetic: kPackThreads threads, each
+// one row of the TV-row tile against QT queries (QT / 2 pairs); the item's
+// QG queries sit pair-interleaved in shared memory.  Same items, candidate
+// buffers, slots and results as scan_exact_kernel in SCAN_PLAIN mode.
+constexpr int kPackThreads = 512;
+
+template <int TV, int QT>
+__global__ void __launch_bounds__(kPackThreads, 1) scan_plain_x2_kernel(ScanArgs a, int cap) {
+  constexpr int NT = kPackThreads;
+  constexpr int G = NT / TV;
+  constexpr int QG = G * QT;
+  constexpr int NP = QT / 2;
+  extern __shared__ __align__(16) float smem[];
+  const int dpad = a.dpad;
+  const int lds = dpad + 4;
+  float* const srowA = smem;
+  float* const srowB = smem + TV * lds;
+  float* sq = smem + 2 * TV * lds;  // [QG / 2][dpad][2]
+  uint64_t* sbuf = reinterpret_cast<uint64_t*>(sq + QG * dpad);
+  int* scnt = reinterpret_cast<int*>(sbuf + QG * cap);
+  float* sthr = reinterpret_cast<float*>(scnt + QG);
+  int* sqid = reinterpret_cast<int*>(sthr + QG);   // packed (q << 16 | j) as uint32; -1 if unused
+  __shared__ ItemShared it;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int r = tid % TV;
+  const int g = tid / TV;
+  const int64_t total_items = a.item_off[a.nlist];
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) {
+      const int64_t item = static_cast<int64_t>(atomicAdd(a.work_counter, 1u));
+      if (item >= total_items) {
+        it.list = -1;
+      } else {
+        int lo = 0, hi = a.nlist;  // invariant item_off[lo] <= item < item_off[hi]
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (a.item_off[mid] <= item) lo = mid; else hi = mid;
+        }
+        const int l = lo;
+        const int64_t local = item - a.item_off[l];
+        const int ng = (a.list_cnt[l] + a.qgroup - 1) / a.qgroup;
+        it.list = l;
+        it.chunk = static_cast<int>(local / ng);
+        it.group = static_cast<int>(local % ng);
+        it.qcnt = min(a.qgroup, a.list_cnt[l] - it.group * a.qgroup);
+        it.row0 = a.list_off[l] + static_cast<int64_t>(it.chunk) * a.chunk_rows;
+        it.row1 = min(a.list_off[l + 1], it.row0 + a.chunk_rows);
+      }
+    }
+    __syncthreads();
+    if (it.list < 0) break;
+    const int qcnt = it.qcnt;
+    const int64_t row0 = it.row0;
+    const int nrow = static_cast<int>(it.row1 - row0);
+    const int ntiles = (nrow + TV - 1) / TV;
+    load_rows_async(srowA, lds, a.codes + static_cast<size_t>(row0) * dpad, TV, nrow, dpad);
+    cp_async_commit();
+    if (tid < QG) {
+      int packed = -1;
+      if (tid < qcnt) packed = a.list_q[a.list_qoff[it.list] + static_cast<int64_t>(it.group) * a.qgroup + tid];
+      sqid[tid] = packed;
+      scnt[tid] = 0;
+      sthr[tid] = FLT_MAX;
+    }
+    __syncthreads();
+    // Queries, pair-interleaved (zeros for unused query slots).
+    {
+      const int cpr = dpad >> 2;
+      for (int idx = tid; idx < QG * cpr; idx += NT) {
+        const int e = idx / cpr, c = (idx - e * cpr) * 4;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (e < qcnt) v = *reinterpret_cast<const float4*>(a.q + static_cast<size_t>(static_cast<unsigned>(sqid[e]) >> 16) * dpad + c);
+        float* dst = sq + (static_cast<size_t>(e >> 1) * dpad + c) * 2 + (e & 1);
+        dst[0] = v.x;
+        dst[2] = v.y;
+        dst[4] = v.z;
+        dst[6] = v.w;
+      }
+    }
+
+    for (int t = 0; t < ntiles; ++t) {
+      const float* cur = (t & 1) ? srowB : srowA;
+      if (t + 1 < ntiles) {
+        const int rn = (t + 1) * TV;
+        load_rows_async((t & 1) ? srowA : srowB, lds, a.codes + static_cast<size_t>(row0 + rn) * dpad, TV,
+                        nrow - rn, dpad);
+      }
+      cp_async_commit();
+      cp_async_wait<1>();
+      const bool need = __syncthreads_or(tid < QG && scnt[tid] > cap - TV);
+      if (need) {
+        for (int e = warp; e < QG; e += NT / 32) {
+          const int c = scnt[e];
+          if (c > cap - TV) {
+            uint64_t* b = sbuf + e * cap;
+            for (int i = c + lane; i < cap; i += 32) b[i] = kEmpty;
+            __syncwarp();
+            warp_bitonic_sort(b, cap, lane);
+            if (lane == 0) {
+              scnt[e] = a.k;
+              sthr[e] = key_dist(b[a.k - 1]);
+            }
+            __syncwarp();
+          }
+        }
+        __syncthreads();
+      }
+      const int rloc = t * TV + r;
+      float dist[QT];
+      dist_plain_x2<NP>(cur + r * lds, sq + static_cast<size_t>(g) * NP * dpad * 2, dpad, dist);
+      if (rloc < nrow) {
+#pragma unroll
+        for (int i = 0; i < QT; ++i) {
+          const int e = g * QT + i;
+          if (e < qcnt && dist[i] < FLT_MAX && dist[i] <= sthr[e]) {
+            const int pos = atomicAdd(&scnt[e], 1);
+            sbuf[e * cap + pos] = make_key(dist[i], static_cast<uint32_t>(row0 + rloc));
+          }
+        }
+      }
+      __syncthreads();
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+
+    for (int e = warp; e < qcnt; e += NT / 32) {
+      uint64_t* b = sbuf + e * cap;
+      const int c = scnt[e];
+      for (int i = c + lane; i < cap; i += 32) b[i] = kEmpty;
+      __syncwarp();
+      warp_bitonic_sort(b, cap, lane);
+      const int packed = sqid[e];
+      const int qq = static_cast<int>(static_cast<unsigned>(packed) >> 16), j = packed & 0xffff;
+      const int64_t slot = a.slot_base[static_cast<int64_t>(qq) * a.P + j] + it.chunk;
+      uint64_t* out = a.part + slot * a.k;
+      for (int i = lane; i < a.k; i += 32) out[i] = b[i];
+      __syncwarp();
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
 // Tile shape choice.
 
 struct Shape {
@@ -515,10 +708,31 @@ size_t scan_smem(int tv, int qt, int dpad, int cap) {
          static_cast<size_t>(qg) * cap * 8 + static_cast<size_t>(qg) * 5 * 4;
 }
 constexpr size_t kSmemLimit = 220 * 1024;
+
+// The packed PLAIN scan (dpad <= 256): kPackThreads threads, QT even.
+size_t scan_x2_smem(int tv, int qt, int dpad, int cap) {
+  const int qg = (kPackThreads / tv) * qt;
+  return (2 * static_cast<size_t>(tv) * (dpad + 4) + static_cast<size_t>(qg) * dpad) * 4 +
+         static_cast<size_t>(qg) * cap * 8 + static_cast<size_t>(qg) * 3 * 4;
+}
+bool use_x2(int dpad, int mode) { return mode == SCAN_PLAIN && dpad <= 256; }
 }  // namespace
 
 size_t scan_exact_smem_bytes(int d, int dpad, int k, int mode, int* tv, int* qt, int* qgroup) {
   (void)d;
+  if (use_x2(dpad, mode)) {
+    const int TV = dpad <= 128 ? 128 : 64;
+    int QT = 8;
+    const int cap = pow2_ceil(k + TV);
+    while (QT > 2 && scan_x2_smem(TV, QT, dpad, cap) > kSmemLimit) QT >>= 1;
+    const size_t s = scan_x2_smem(TV, QT, dpad, cap);
+    if (s <= kSmemLimit) {
+      *tv = TV;
+      *qt = QT;
+      *qgroup = (kPackThreads / TV) * QT;
+      return s;
+    }
+  }
   int TV = dpad <= 128 ? 128 : dpad <= 256 ? 64 : dpad <= 512 ? 32 : 16;
   int QT = mode == SCAN_DIMBLOCK ? 4 : (TV >= 64 ? 8 : 4);
   const int cap = pow2_ceil(k + TV);
@@ -553,12 +767,29 @@ void scan_dispatch(const ScanArgs& a, int tv, int qt, int cap, size_t smem, int 
 }
 }  // namespace
 
+namespace {
+template <int TV, int QT>
+void x2_launch(const ScanArgs& a, int cap, size_t smem, int num_sms, cudaStream_t st) {
+  HB_CUDA(cudaFuncSetAttribute(scan_plain_x2_kernel<TV, QT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)));
+  scan_plain_x2_kernel<TV, QT><<<num_sms, kPackThreads, smem, st>>>(a, cap);
+  HB_CUDA(cudaGetLastError());
+}
+}  // namespace
+
 void launch_scan_exact(const ScanArgs& a, int num_sms, cudaStream_t st) {
   int tv = 0, qt = 0, qg = 0;
   const size_t smem = scan_exact_smem_bytes(a.d, a.dpad, a.k, a.mode, &tv, &qt, &qg);
   HB_CHECK(smem > 0, HB_ERR_INVALID, "k too large for the fused scan at this dimension");
   HB_CHECK(qg == a.qgroup, HB_ERR_INVALID, "scan plan built for another query group");
   const int cap = pow2_ceil(a.k + tv);
+  if (use_x2(a.dpad, a.mode) && qg == (kPackThreads / tv) * qt) {
+#define HB_X2_CASE(TV_, QT_) \
+  if (tv == TV_ && qt == QT_) return x2_launch<TV_, QT_>(a, cap, smem, num_sms, st);
+    HB_X2_CASE(128, 8) HB_X2_CASE(128, 4) HB_X2_CASE(128, 2)
+    HB_X2_CASE(64, 8) HB_X2_CASE(64, 4) HB_X2_CASE(64, 2)
+#undef HB_X2_CASE
+  }
   if (a.mode == SCAN_PLAIN) scan_dispatch<SCAN_PLAIN>(a, tv, qt, cap, smem, num_sms, st);
   else if (a.mode == SCAN_CHUNK4) scan_dispatch<SCAN_CHUNK4>(a, tv, qt, cap, smem, num_sms, st);
   else scan_dispatch<SCAN_DIMBLOCK>(a, tv, qt, cap, smem, num_sms, st);

@@ -1,40 +1,70 @@
-// BF16 tensor-core list scan (tcgen05 + TMA) and the exact FP32 re-rank.
+// BF16 tensor-core list scan (tcgen05 + TMA) and the exact FP32 re-rank,
+// whose result equals the exact FP32 scan's bit for bit.
+//
+// Error bound.  For a query q and a stored row x the scan forms
+//   w(x) = ||x||^2 - 2 q~.x~      (q~, x~: BF16 roundings; ||x||^2 the stored
+//                                  FP32 norm; the dot product on the tensor
+//                                  cores with FP32 accumulation)
+// and the reference's distance is d(x) = the sequential unfused FP32 sum of
+// (q_i - x_i)^2 (src/utils.h:480-487).  With Q = ||q||, M = max ||x|| over
+// the index, u = 2^-24 and D = ||q - x||^2 <= (Q + M)^2:
+//   |2 q~.x~ - 2 q.x|  <= 2 (2^-8 + 2^-16) Q M   BF16 rounding of both operands
+//                       + 2 * 2^-10 Q M           FP32 accumulation of kpad <= 128
+//                                                 exact products (even with only
+//                                                 17 bits kept per addition)
+//   | ||x||^2 stored - ||x||^2 | <= (d + 1) u M^2  sequential FP32 sum
+//   rounding of w                <= u (Q + M)^2
+//   | d(x) - D |                 <= (d + 3) u D     sequential FP32 sum
+// so |w(x) + Q^2 - d(x)| <= eps(q), eps = 1.0625 * (2 (2^-8 + 2^-10 + 2^-16) Q M
+// + (d + 1) u M^2 + (d + 4) u (Q + M)^2).  Let W_k be the k-th smallest w over
+// the probed rows.  The k rows with the smallest w have d <= W_k + Q^2 + eps,
+// so the k-th smallest d is at most that, and every row of the exact top k
+// (ties at the k-th distance included) has w <= W_k + 2 eps.  Re-ranking
+// exactly every row with w <= W_k + 2 eps, by (FP32 distance, position) like
+// the exact scan, therefore returns the exact scan's result.
+//
+// Admission.  A row is appended to its query's candidate buffer when
+// w <= thr(q).  thr starts at the seed bound (the k-th smallest of the same
+// values over the first rows of the query's nearest list, + 2 eps: an upper
+// bound of W_k + 2 eps because the seed's values obey the same eps) and, for
+// k <= 16, falls to (k-th smallest w this thread has seen for the query) +
+// 2 eps as the scan goes, shared between work items through an atomicMin.
+// Every row with w <= W_k + 2 eps is admitted whatever the order.  The
+// re-rank takes W_k over the appended rows (all rows with w <= W_k are
+// among them), keeps those at or under W_k + 2 eps and recomputes them with
+// the reference's loop.  A query whose buffer overflows is flagged; the host
+// searches it again with the exact FP32 scan.
 //
 // Work items are the list-major items of the exact scan (list, chunk of
 // rows, group of <= 128 queries probing the list).  Per item the CTA holds
-// the group's queries as the MMA's A operand (128 x K, BF16, K-major,
-// 128-byte swizzle) and streams the chunk's rows as B operand tiles of 128
-// rows (TMA 2-D loads with the same swizzle into a ring of stages).  One
-// thread issues tcgen05.mma (M 128 queries x N 128 rows x K 16) into one of
-// four TMEM accumulators; the epilogue warps read their TMEM lanes back
-// (thread = query, 128 columns = rows), form ||x||^2 - 2 q.x (the query's
-// ||q||^2 does not change its ranking) and keep the R smallest per query in
-// a thread-private max-heap in shared memory.  The R best keys (approximate
-// distance, row position) of every (query, chunk) go to a slot;
-// rerank_kernel takes each query's R best over its slots, recomputes their
-// distances exactly in FP32 with the reference's sequential unfused loop and
-// returns the k best -- so whenever the true k nearest are among the R
-// candidates the result equals the exact scan's.
+// the group's BF16 queries as the MMA's A operand (128 x K, K-major, 128-byte
+// swizzle) and streams the chunk's rows as B operand tiles of 128 rows (TMA
+// 2-D loads with the same swizzle into a ring of stages).  One thread issues
+// tcgen05.mma (M 128 queries x N 128 rows x K 16) into one of four TMEM
+// accumulators; the epilogue warps read their TMEM lanes back (thread =
+// query, 128 columns = rows), form w and append the rows under the query's
+// bound.
 //
 // Warp roles (384 threads), all running ahead of each other through
 // mbarriers, with no CTA-wide barrier between items:
 //   warps 0-7   two epilogue groups (TMEM lane quarters); tile t of the
-//               CTA's global tile sequence goes to group t % 2, which keeps
-//               its own heaps per item;
+//               CTA's global tile sequence goes to group t % 2;
 //   warp 8      TMA producer of the B tiles;
 //   warp 9      MMA issuer; it also copies each tile's 128 row norms
 //               (a padded per-tile norm array) next to the accumulator;
 //   warps 10-11 item builders: fetch the next item from the global work
-//               counter, gather its query ids and seed bounds and write its
+//               counter, gather its BF16 query rows and bounds and write its
 //               A tile into the second A buffer while the current item runs.
-// Every mbarrier wait is bounded; on a timeout the kernel records an error,
-// the roles stop taking work, copies and MMAs in flight are drained and
-// TMEM is freed.
+// Every mbarrier wait is bounded (TcArgs::wait_budget cycles); on a timeout
+// the kernel records an error, the roles stop taking work, copies and MMAs
+// in flight are drained and TMEM is freed.
 #include <cudaTypedefs.h>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 #include "hb_device.cuh"
 #include "hb_internal.hpp"
@@ -55,6 +85,7 @@ constexpr int kTile = 128;     // rows per B tile, queries per item (M)
 constexpr int kMaxStages = 4;
 constexpr int kAcc = 2 * kGroups;                  // TMEM accumulators of 128 columns
 constexpr size_t kSmemCap = 225 * 1024;            // dynamic shared memory budget
+constexpr int kTightK = 16;                        // largest k whose bound tightens during the scan
 
 struct ItemDesc {
   int list, chunk, group, qcnt, ntiles;  // ntiles < 0: no more work
@@ -74,34 +105,6 @@ struct TcShared {
   uint32_t tmem;
   ItemDesc desc[2];
 };
-
-// Thread-private max-heap of R keys stored with stride kEpiThreads: the
-// top is replaced by `key` and sifted down; returns the new top (known from
-// the sift, so no reload).
-__device__ __forceinline__ uint64_t heap_replace_top(uint64_t* h, int R, uint64_t key) {
-  int i = 0;
-  uint64_t new_top = key;
-  for (;;) {
-    const int c1 = 2 * i + 1;
-    if (c1 >= R) break;
-    const int c2 = c1 + 1;
-    uint64_t vc = h[c1 * kEpiThreads];
-    int c = c1;
-    if (c2 < R) {
-      const uint64_t v2 = h[c2 * kEpiThreads];
-      if (v2 > vc) {
-        vc = v2;
-        c = c2;
-      }
-    }
-    if (key >= vc) break;
-    h[i * kEpiThreads] = vc;
-    if (i == 0) new_top = vc;
-    i = c;
-  }
-  h[i * kEpiThreads] = key;
-  return new_top;
-}
 
 // Next work item from the global counter (one thread).
 __device__ ItemDesc fetch_item(const TcArgs& a, int64_t total_items) {
@@ -131,22 +134,25 @@ __device__ ItemDesc fetch_item(const TcArgs& a, int64_t total_items) {
   return d;
 }
 
+// KT = kTightK: the bound tightens (k <= 16); KT = 0: it stays at the seed.
+template <int KT>
 __global__ void __launch_bounds__(kTcThreads, 1)
     scan_bf16_kernel(const __grid_constant__ CUtensorMap tmap, TcArgs a) {
+  constexpr int KB = KT > 0 ? KT : 1;
   extern __shared__ uint8_t smem_raw[];
   __shared__ TcShared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int kpad = a.kpad;
   const int S = a.stages;
+  const long long budget = a.wait_budget;
   const uint32_t kblk_bytes = kTile * 128;                 // one 64-element K block of 128 rows
   const uint32_t tile_bytes = static_cast<uint32_t>(kpad / 64) * kblk_bytes;
   uint8_t* Abuf = smem;                                    // [2] A tiles
   uint8_t* stages = smem + 2 * tile_bytes;                 // [S] B tiles
-  uint64_t* heap = reinterpret_cast<uint64_t*>(stages + static_cast<size_t>(S) * tile_bytes);  // [kGroups][R][128]
-  float* nrm = reinterpret_cast<float*>(heap + static_cast<size_t>(kGroups) * a.R * kEpiThreads);  // [kAcc][128]
+  float* nrm = reinterpret_cast<float*>(stages + static_cast<size_t>(S) * tile_bytes);  // [kAcc][128]
   int* meta_q = reinterpret_cast<int*>(nrm + kAcc * kTile);                 // [2][128]
-  int* meta_j = meta_q + 2 * kTile;                                          // [2][128]
-  uint64_t* meta_tau = reinterpret_cast<uint64_t*>(meta_j + 2 * kTile);      // [2][128]
+  float* meta_thr = reinterpret_cast<float*>(meta_q + 2 * kTile);           // [2][128]
+  float* meta_e2 = meta_thr + 2 * kTile;                                    // [2][128]
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -182,50 +188,44 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp >= kBuildWarp0) {
     // ---- item builders ---------------------------------------------------
     const int bt = tid - kBuildWarp0 * 32;
+    constexpr int kBt = kBuildWarps * 32;
+    const int cpr = kpad / 8;  // 16-byte chunks per BF16 query row
     ItemDesc nd;
     nd.ntiles = -1;
     if (bt == 0) nd = fetch_item(a, total_items);
     for (uint32_t it = 0;; ++it) {
       const int ab = static_cast<int>(it & 1u);
-      bool okw = true;
       if (bt == 0) {
-        okw = mbar_wait(&sh.aempty[ab], ((it >> 1) & 1u) ^ 1u, err, 31);
-        if (!okw) nd.ntiles = -1;
+        if (!mbar_wait(&sh.aempty[ab], ((it >> 1) & 1u) ^ 1u, err, 31, budget)) nd.ntiles = -1;
         sh.desc[ab] = nd;
       }
-      asm volatile("bar.sync 3, %0;\n" ::"n"(kBuildWarps * 32) : "memory");
+      asm volatile("bar.sync 3, %0;\n" ::"n"(kBt) : "memory");
       const ItemDesc d = sh.desc[ab];
       if (d.ntiles >= 0) {
         const int64_t qbase = a.list_qoff[d.list] + static_cast<int64_t>(d.group) * kTile;
-        uint8_t* A = Abuf + ab * tile_bytes;
-        for (int r = bt; r < kTile; r += kBuildWarps * 32) {
-          int q = -1, j = 0;
-          uint64_t tau = kEmpty;
+        for (int r = bt; r < kTile; r += kBt) {
+          int q = -1;
+          float thr = -INFINITY, e2 = 0.0f;
           if (r < d.qcnt) {
-            const uint32_t packed = static_cast<uint32_t>(a.list_q[qbase + r]);
-            q = static_cast<int>(packed >> 16);
-            j = static_cast<int>(packed & 0xffffu);
-            // Best known R-th key of this query over the items finished so
-            // far: an upper bound of its overall R-th key.
-            tau = *reinterpret_cast<volatile unsigned long long*>(a.tau + q);
+            q = static_cast<int>(static_cast<uint32_t>(a.list_q[qbase + r]) >> 16);
+            // The query's bound as other items have lowered it so far.
+            thr = ordered_to_float(*reinterpret_cast<volatile uint32_t*>(a.thr + q));
+            e2 = a.e2[q];
           }
           meta_q[ab * kTile + r] = q;
-          meta_j[ab * kTile + r] = j;
-          meta_tau[ab * kTile + r] = tau;
-          const float* qrow = a.q + static_cast<size_t>(q < 0 ? 0 : q) * a.dpad;
+          meta_thr[ab * kTile + r] = thr;
+          meta_e2[ab * kTile + r] = e2;
+        }
+        asm volatile("bar.sync 3, %0;\n" ::"n"(kBt) : "memory");
+        uint8_t* A = Abuf + ab * tile_bytes;
+        const uint4* qb = reinterpret_cast<const uint4*>(a.qbf);
 #pragma unroll 4
-          for (int k = 0; k < kpad; k += 8) {
-            float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
-            if (q >= 0 && k < a.dpad) {  // dpad is a multiple of 16: a row's 8 values are all in or all out
-              lo = *reinterpret_cast<const float4*>(qrow + k);
-              hi = *reinterpret_cast<const float4*>(qrow + k + 4);
-            }
-            __nv_bfloat162 p0 = __floats2bfloat162_rn(lo.x, lo.y), p1 = __floats2bfloat162_rn(lo.z, lo.w);
-            __nv_bfloat162 p2 = __floats2bfloat162_rn(hi.x, hi.y), p3 = __floats2bfloat162_rn(hi.z, hi.w);
-            *reinterpret_cast<uint4*>(A + sw128_offset_bf16(r, k, kblk_bytes)) =
-                make_uint4(*reinterpret_cast<uint32_t*>(&p0), *reinterpret_cast<uint32_t*>(&p1),
-                           *reinterpret_cast<uint32_t*>(&p2), *reinterpret_cast<uint32_t*>(&p3));
-          }
+        for (int i = bt; i < kTile * cpr; i += kBt) {
+          const int r = i / cpr, c = i - r * cpr;
+          const int q = meta_q[ab * kTile + r];
+          uint4 v = make_uint4(0u, 0u, 0u, 0u);
+          if (q >= 0) v = __ldg(qb + static_cast<size_t>(q) * cpr + c);
+          *reinterpret_cast<uint4*>(A + sw128_offset_bf16(r, c * 8, kblk_bytes)) = v;
         }
         fence_proxy_async_smem();
       }
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       for (uint32_t it = 0;; ++it) {
         const int ab = static_cast<int>(it & 1u);
-        if (!mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 32)) break;
+        if (!mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 32, budget)) break;
         const ItemDesc d = sh.desc[ab];
         mbar_arrive(&sh.aempty[ab]);
         if (d.ntiles < 0) break;
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         for (int t = 0; t < d.ntiles; ++t, ++p_idx) {
           const int s = static_cast<int>(p_idx % static_cast<uint32_t>(S));
           const uint32_t par = ((p_idx / static_cast<uint32_t>(S)) & 1u) ^ 1u;
-          if (!mbar_wait(&sh.empty[s], par, err, 11)) {
+          if (!mbar_wait(&sh.empty[s], par, err, 11, budget)) {
             ok = false;
             break;
           }
@@ -270,9 +270,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint32_t idesc = idesc_bf16_f32(kTile, kTile);
       const int nk = kpad / 16;
       uint32_t m_idx = 0, m_cnt[kGroups] = {}, G = 0;
+      uint32_t n_norm[kAcc] = {};  // norm copies issued per accumulator
       for (uint32_t it = 0;; ++it) {
         const int ab = static_cast<int>(it & 1u);
-        if (!mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 33)) break;
+        if (!mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 33, budget)) break;
         const ItemDesc d = sh.desc[ab];
         if (d.ntiles < 0) break;
         tc_fence_after();
@@ -280,14 +281,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         bool ok = true;
         for (int t = 0; t < d.ntiles; ++t, ++m_idx) {
           const int s = static_cast<int>(m_idx % static_cast<uint32_t>(S));
-          if (!mbar_wait(&sh.full[s], (m_idx / static_cast<uint32_t>(S)) & 1u, err, 12)) {
+          if (!mbar_wait(&sh.full[s], (m_idx / static_cast<uint32_t>(S)) & 1u, err, 12, budget)) {
             ok = false;
             break;
           }
           const int g = static_cast<int>((G + static_cast<uint32_t>(t)) & 1u);
           const uint32_t c = m_cnt[g];
           const int b = 2 * g + static_cast<int>(c & 1u);
-          if (!mbar_wait(&sh.acce[b], ((c >> 1) & 1u) ^ 1u, err, 13)) {
+          if (!mbar_wait(&sh.acce[b], ((c >> 1) & 1u) ^ 1u, err, 13, budget)) {
             ok = false;
             break;
           }
@@ -295,6 +296,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tc_fence_after();
           mbar_arrive_expect_tx(&sh.normf[b], kTile * 4);
           bulk_load(nrm + b * kTile, a.tile_norm + (d.tile0 + t) * kTile, kTile * 4, &sh.normf[b]);
+          ++n_norm[b];
           const uint32_t b_base = smem_u32(stages + s * tile_bytes);
           for (int k = 0; k < nk; ++k) {
             const uint32_t off = static_cast<uint32_t>(k >> 2) * kblk_bytes + static_cast<uint32_t>(k & 3) * 32u;
@@ -309,36 +311,42 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (!ok) break;
         G += static_cast<uint32_t>(d.ntiles);
       }
-      // Drain: every MMA done before TMEM is released.
+      // Drain: every MMA done before TMEM is released, and the last norm copy
+      // of each accumulator landed (at most one per accumulator is pending:
+      // the next one waits for the epilogue to release the accumulator).
       mma_commit(&sh.drain);
       mbar_wait(&sh.drain, 0, nullptr, 0, 200000000LL);
+      for (int b = 0; b < kAcc; ++b)
+        if (n_norm[b]) mbar_wait(&sh.normf[b], (n_norm[b] - 1u) & 1u, nullptr, 0, 200000000LL);
     }
   } else {
     // ---- epilogue: thread = query (TMEM lane etid) ---------------------------
     const int grp = warp >> 2;
     const int etid = tid - grp * kEpiThreads;
-    uint64_t* hp = heap + static_cast<size_t>(grp) * a.R * kEpiThreads + etid;
     const uint32_t lane_base = (32u * static_cast<uint32_t>(warp & 3)) << 16;
     uint32_t e_cnt = 0, G = 0;
     for (uint32_t it = 0;; ++it) {
       const int ab = static_cast<int>(it & 1u);
-      bool ok = mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 34);
+      bool ok = mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 34, budget);
       if (!__all_sync(0xffffffffu, ok)) break;
       const ItemDesc d = sh.desc[ab];
       const int my_q = meta_q[ab * kTile + etid];
-      const int my_j = meta_j[ab * kTile + etid];
-      const uint64_t my_tau = meta_tau[ab * kTile + etid];
+      const float thr0 = meta_thr[ab * kTile + etid];
+      const float e2 = meta_e2[ab * kTile + etid];
       mbar_arrive(&sh.aempty[ab]);
       if (d.ntiles < 0) break;
-      // The heap starts full of the query's bound: only keys below enter.
-      for (int e = 0; e < a.R; ++e) hp[e * kEpiThreads] = my_tau;
-      uint64_t top = my_tau;
-      // An all-ones top (no bound yet) admits every finite value.
-      float thr_f = top == kEmpty ? FLT_MAX : ordered_to_float(static_cast<uint32_t>(top >> 32));
+      float thr = thr0;
+      // The KT smallest values this thread has admitted for the query in this
+      // item, ascending (KT = 0: no tightening).
+      float best[KB];
+#pragma unroll
+      for (int i = 0; i < KB; ++i) best[i] = INFINITY;
+      int seen = 0;
+      uint64_t* cbuf = a.cand + static_cast<size_t>(my_q < 0 ? 0 : my_q) * a.cap;
       for (int t = static_cast<int>((static_cast<uint32_t>(grp) ^ G) & 1u); t < d.ntiles; t += kGroups, ++e_cnt) {
         const int b = 2 * grp + static_cast<int>(e_cnt & 1u);
         const uint32_t par = (e_cnt >> 1) & 1u;
-        ok = ok && mbar_wait(&sh.accf[b], par, err, 14) && mbar_wait(&sh.normf[b], par, err, 15);
+        ok = ok && mbar_wait(&sh.accf[b], par, err, 14, budget) && mbar_wait(&sh.normf[b], par, err, 15, budget);
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
         const float* nb = nrm + b * kTile;
@@ -351,7 +359,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tmem_ld_wait();
           }
           if (ok && my_q >= 0) {
-            // v = ||x||^2 - 2 q.x (rows past the list carry an infinite
+            // w = ||x||^2 - 2 q.x (rows past the list carry an infinite
             // norm); the columns' minimum against the bound decides whether
             // any of them needs a look.
             const float4* n4 = reinterpret_cast<const float4*>(nb + c * 32);
@@ -369,10 +377,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               r[4 * j4 + 3] = __float_as_uint(v3);
               mn = fminf(mn, fminf(fminf(v0, v1), fminf(v2, v3)));
             }
-            if (mn <= thr_f) {
+            if (mn <= thr) {
               uint32_t mq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-              for (int j = 0; j < 32; ++j) mq[j & 3] |= (__uint_as_float(r[j]) <= thr_f ? 1u : 0u) << j;
+              for (int j = 0; j < 32; ++j) mq[j & 3] |= (__uint_as_float(r[j]) <= thr ? 1u : 0u) << j;
               uint32_t mask = (mq[0] | mq[1]) | (mq[2] | mq[3]);
               const uint32_t pos0 = pos_t + static_cast<uint32_t>(c * 32);
               while (mask) {
@@ -388,12 +396,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 for (int i = 0; i < 4; ++i) t4[i] = (j & 4) ? t8[2 * i + 1] : t8[2 * i];
 #pragma unroll
                 for (int i = 0; i < 2; ++i) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
-                const uint32_t hv = (j & 16) ? t2[1] : t2[0];
-                const uint64_t key = (static_cast<uint64_t>(ordered_bits(__uint_as_float(hv))) << 32) |
-                                     (pos0 + static_cast<uint32_t>(j));
-                if (key < top) {
-                  top = heap_replace_top(hp, a.R, key);
-                  thr_f = top == kEmpty ? FLT_MAX : ordered_to_float(static_cast<uint32_t>(top >> 32));
+                const float wv = __uint_as_float((j & 16) ? t2[1] : t2[0]);
+                const int slot = atomicAdd(a.cand_cnt + my_q, 1);
+                if (slot < a.cap)
+                  cbuf[slot] = (static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j));
+                if (KT > 0) {
+                  // Insert into the ascending KT smallest; once k values are
+                  // in, the k-th + 2 eps bounds W_k + 2 eps from above.
+                  float v = wv;
+#pragma unroll
+                  for (int i = 0; i < KB; ++i) {
+                    const float o = best[i];
+                    best[i] = fminf(o, v);
+                    v = fmaxf(o, v);
+                  }
+                  if (++seen >= a.k) {
+                    float kth = best[0];
+#pragma unroll
+                    for (int i = 1; i < KB; ++i) kth = (i == a.k - 1) ? best[i] : kth;
+                    thr = fminf(thr, __fadd_ru(kth, e2));
+                  }
                 }
               }
             }
@@ -402,18 +424,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tc_fence_before();
         mbar_arrive(&sh.acce[b]);
       }
-      // Partial result of this (query, chunk): the group's R keys; seed
-      // entries are not results.
-      if (my_q >= 0) {
-        const int64_t slot = a.slot_base[static_cast<int64_t>(my_q) * a.P + my_j] + d.chunk;
-        uint64_t* out = a.part + (slot * kGroups + grp) * a.R;
-        for (int e = 0; e < a.R; ++e) {
-          const uint64_t v = hp[e * kEpiThreads];
-          out[e] = v == my_tau ? kEmpty : v;
-        }
-        // A heap holding R real keys bounds the query's R-th key: publish it.
-        if (top < my_tau) atomicMin(reinterpret_cast<unsigned long long*>(a.tau + my_q), top);
-      }
+      // Share a lowered bound with the items still to come.
+      if (KT > 0 && my_q >= 0 && thr < thr0) atomicMin(a.thr + my_q, ordered_bits(thr));
       if (!ok) break;
       G += static_cast<uint32_t>(d.ntiles);
     }
@@ -427,166 +439,180 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
-__global__ void __launch_bounds__(512) rerank_kernel(const uint64_t* __restrict__ part,
-                                                     const int64_t* __restrict__ slot_base, int P, int R, int k,
-                                                     const float* __restrict__ codes, const float* __restrict__ q,
-                                                     int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
-                                                     int64_t* __restrict__ I, const uint64_t* __restrict__ part2,
-                                                     const int64_t* __restrict__ slot_base2, int P2,
-                                                     const uint64_t* __restrict__ tau, const int* __restrict__ only) {
-  extern __shared__ uint64_t s_keys[];  // pow2(R) approx, then pow2(R) exact
-  __shared__ SelectShared sh_sel;
-  const int qi = blockIdx.x;
-  if (only && !only[qi]) return;
-  const int n2 = pow2_ceil(R < 2 ? 2 : R);
-  uint64_t* s_appr = s_keys;
-  uint64_t* s_exact = s_keys + n2;
-  const int64_t s0 = slot_base[static_cast<int64_t>(qi) * P];
-  const int64_t s1 = slot_base[static_cast<int64_t>(qi + 1) * P];
-  const uint64_t* src = part + s0 * kGroups * R;
-  const int m1 = static_cast<int>((s1 - s0) * kGroups * R);
-  const uint64_t* src2 = nullptr;
-  int m2 = 0;
-  if (part2) {
-    const int64_t t0 = slot_base2[static_cast<int64_t>(qi) * P2];
-    const int64_t t1 = slot_base2[static_cast<int64_t>(qi + 1) * P2];
-    src2 = part2 + t0 * kGroups * R;
-    m2 = static_cast<int>((t1 - t0) * kGroups * R);
+// Per query, before the scan: its BF16 row (the A operand of the scan and
+// the seed), 2 eps (see the top of this file), the admission bound reset to
+// FLT_MAX (no bound yet; +inf padding rows never pass) and the candidate
+// counter reset.  One warp per query.
+__global__ void query_prep_kernel(const float* __restrict__ q, int nq, int d, int dpad, int kpad,
+                                  const float* __restrict__ maxnorm, __nv_bfloat16* __restrict__ qbf,
+                                  float* __restrict__ e2, uint32_t* __restrict__ thr, int* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (qi >= nq) return;
+  const float* row = q + static_cast<size_t>(qi) * dpad;
+  float s = 0.0f;
+  for (int c = lane; c < kpad; c += 32) {
+    const float v = c < dpad ? row[c] : 0.0f;
+    qbf[static_cast<size_t>(qi) * kpad + c] = __float2bfloat16_rn(v);
+    s = fmaf(v, v, s);
   }
-  // The query's final bound is at or above its R-th key: keys above it
-  // cannot be among the R best, so they drop out of the selection.
-  const uint64_t lim = tau ? tau[qi] : kEmpty;
-  auto key_at = [&](int i) -> uint64_t {
-    const uint64_t key = i < m1 ? src[i] : src2[i - m1];
-    return key <= lim ? key : kEmpty;
-  };
-  block_topk_sorted(key_at, m1 + m2, R, sh_sel, s_appr);
-  const float* qrow = q + static_cast<size_t>(qi) * dpad;
-  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-    uint64_t key = kEmpty;
-    if (i < R && s_appr[i] != kEmpty) {
-      const uint32_t pos = key_tie(s_appr[i]);
-      const float acc = exact_l2_seq(codes + static_cast<size_t>(pos) * dpad, qrow, dpad);
-      if (acc < FLT_MAX) key = make_key(acc, pos);
-    }
-    s_exact[i] = key;
-  }
-  __syncthreads();
-  block_bitonic_sort(s_exact, n2);
-  for (int j = threadIdx.x; j < k; j += blockDim.x) {
-    const uint64_t key = j < n2 ? s_exact[j] : kEmpty;
-    const size_t o = static_cast<size_t>(qi) * k + j;
-    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
-    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) {
+    const float Q = sqrtf(s) * 1.0001f;
+    const float M = *maxnorm;
+    const float u = 5.9604645e-8f;  // 2^-24
+    const float c1 = 0.00390625f + 0.0009765625f + 1.52587890625e-5f;
+    const float eps = 1.0625f * (2.0f * c1 * Q * M + (d + 1) * u * M * M + (d + 4) * u * (Q + M) * (Q + M));
+    e2[qi] = 2.0f * eps + 1e-30f;
+    thr[qi] = ordered_bits(FLT_MAX);
+    cnt[qi] = 0;
   }
 }
 
-// Re-rank with one warp per query: the keys at or under the query's final
-// bound (at most a few times R of them) are compacted by ballot into a
-// per-warp buffer, sorted, the best R recomputed exactly (sequential FP32,
-// one candidate per lane) and sorted again.  A query with more than 8192
-// slot keys or more than kRerankCap keys under its bound is flagged for the
-// CTA kernel.
-constexpr int kRerankCap = 256;
-constexpr int kRerankWarps = 8;
+// Re-rank, one warp per query with at most kRrWarpCap candidates: the
+// candidates sorted by (w, position), W_k = the k-th w, the prefix with
+// w <= W_k + 2 eps recomputed with the reference's sequential FP32 loop,
+// sorted by (distance, position) and cut at k.  A query with more candidates
+// goes to the CTA kernel (flag 1); one whose buffer overflowed to the host's
+// exact search (flag 2, and listed).
+constexpr int kRrWarpCap = 256;
+constexpr int kRrWarps = 8;
 
-__global__ void __launch_bounds__(kRerankWarps * 32) rerank_warp_kernel(
-    const uint64_t* __restrict__ part, const int64_t* __restrict__ slot_base, int nq, int P, int R, int k,
+__global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
+    const uint64_t* __restrict__ cand, const int* __restrict__ cnt, int cap, const float* __restrict__ e2, int nq, int k,
     const float* __restrict__ codes, const float* __restrict__ q, int dpad, const int64_t* __restrict__ ids,
-    float* __restrict__ D, int64_t* __restrict__ I, const uint64_t* __restrict__ tau, int* __restrict__ overflow) {
-  __shared__ uint64_t s_cand[kRerankWarps][kRerankCap];
-  __shared__ uint64_t s_ex[kRerankWarps][64];
+    float* __restrict__ D, int64_t* __restrict__ I, int* __restrict__ flag, int* __restrict__ over_list,
+    int* __restrict__ over_n) {
+  __shared__ uint64_t s_c[kRrWarps][kRrWarpCap];
+  __shared__ uint64_t s_x[kRrWarps][kRrWarpCap];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int qi = blockIdx.x * kRerankWarps + wib;
+  const int qi = blockIdx.x * kRrWarps + wib;
   if (qi >= nq) return;
-  uint64_t* cand = s_cand[wib];
-  uint64_t* ex = s_ex[wib];
-  const int64_t s0 = slot_base[static_cast<int64_t>(qi) * P];
-  const int64_t s1 = slot_base[static_cast<int64_t>(qi + 1) * P];
-  const uint64_t* src = part + s0 * kGroups * R;
-  const int m = static_cast<int>((s1 - s0) * kGroups * R);
-  const uint64_t lim = tau[qi];
-  if (m > 256 * 32) {
-    // Many slots (a wide nprobe): the CTA kernel scans them faster.
-    if (lane == 0) overflow[qi] = 1;
+  const int c = cnt[qi];
+  if (c > cap) {
+    if (lane == 0) {
+      flag[qi] = 2;
+      over_list[atomicAdd(over_n, 1)] = qi;
+    }
     return;
   }
-  int cnt = 0;
-#pragma unroll 4
-  for (int base = 0; base < m; base += 32) {
-    const int i = base + lane;
-    const uint64_t key = i < m ? src[i] : kEmpty;
-    const bool pass = key != kEmpty && key <= lim;
-    const unsigned b = __ballot_sync(0xffffffffu, pass);
-    const int pos = cnt + __popc(b & ((1u << lane) - 1u));
-    if (pass && pos < kRerankCap) cand[pos] = key;
-    cnt += __popc(b);
-  }
-  if (cnt > kRerankCap) {
-    if (lane == 0) overflow[qi] = 1;
+  if (c > kRrWarpCap) {
+    if (lane == 0) flag[qi] = 1;
     return;
   }
-  if (lane == 0) overflow[qi] = 0;
-  const int n2 = pow2_ceil(cnt < 2 ? 2 : cnt);
-  for (int i = cnt + lane; i < n2; i += 32) cand[i] = kEmpty;
+  if (lane == 0) flag[qi] = 0;
+  uint64_t* buf = s_c[wib];
+  uint64_t* ex = s_x[wib];
+  const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
+  const int n2 = pow2_ceil(c < 2 ? 2 : c);
+  for (int i = lane; i < n2; i += 32) buf[i] = i < c ? src[i] : kEmpty;
   __syncwarp();
-  warp_bitonic_sort(cand, n2, lane);
-  const int nr = min(R, cnt);
+  warp_bitonic_sort(buf, n2, lane);
+  int m = c;
+  if (c >= k) {
+    const float lim = __fadd_ru(ordered_to_float(static_cast<uint32_t>(buf[k - 1] >> 32)), e2[qi]);
+    const uint32_t lim_bits = ordered_bits(lim);
+    m = 0;
+    for (int base = 0; base < c; base += 32) {
+      const int i = base + lane;
+      const bool in = i < c && static_cast<uint32_t>(buf[i] >> 32) <= lim_bits;
+      m += __popc(__ballot_sync(0xffffffffu, in));
+    }
+  }
   const float* qrow = q + static_cast<size_t>(qi) * dpad;
-  for (int j = lane; j < 64; j += 32) {
+  const int e2n = pow2_ceil(m < 2 ? 2 : m);
+  for (int j = lane; j < e2n; j += 32) {
     uint64_t key = kEmpty;
-    if (j < nr) {
-      const uint32_t pos = key_tie(cand[j]);
+    if (j < m) {
+      const uint32_t pos = key_tie(buf[j]);
       const float acc = exact_l2_seq(codes + static_cast<size_t>(pos) * dpad, qrow, dpad);
       if (acc < FLT_MAX) key = make_key(acc, pos);
     }
     ex[j] = key;
   }
   __syncwarp();
-  const int e2 = pow2_ceil(nr < 2 ? 2 : nr);
-  warp_bitonic_sort(ex, e2, lane);
+  warp_bitonic_sort(ex, e2n, lane);
   for (int j = lane; j < k; j += 32) {
-    const uint64_t key = j < e2 ? ex[j] : kEmpty;
+    const uint64_t key = j < m ? ex[j] : kEmpty;
     const size_t o = static_cast<size_t>(qi) * k + j;
     D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
     I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
   }
 }
 
-// Upper bound of each query's R-th approximate key before the scan, from the
-// first S rows of the query's nearest list.  The bound is computed from the
-// same BF16 operands the scan multiplies (the query rounded to BF16 exactly
-// as the scan's A tile, the BF16 codes), so the scan's value
-// ||x||^2 - 2 q~.x~ and the one here differ only by the order and width of
-// the FP32 accumulation of 128 exact BF16 products: each is within
-// 128 * 2^-19 * sum|q~_i x~_i| <= 2.5e-4 ||q|| max||x|| of the exact sum even
-// if the tensor cores kept only 19 bits per addition.  The margin,
-// 1e-3 ||q|| max||x|| + 2e-5 (max||x||^2 + |v|), covers twice that plus the
-// FP32 rounding of the combination, so the R-th value here plus the margin
-// is never below the R-th value the scan sees, and a seed never drops a key
-// of the scan's top R.
+// The same for the queries flagged 1 (more than kRrWarpCap candidates, at
+// most cap): one CTA per query, grid-stride over the batch.
+__global__ void __launch_bounds__(256) rerank_cta_kernel(const uint64_t* __restrict__ cand, const int* __restrict__ cnt,
+                                                         int cap, const float* __restrict__ e2, int nq, int k,
+                                                         const float* __restrict__ codes, const float* __restrict__ q,
+                                                         int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
+                                                         int64_t* __restrict__ I, const int* __restrict__ flag) {
+  extern __shared__ uint64_t s_dyn[];  // [cap] candidates, then [cap] exact keys
+  __shared__ SelectShared sh_sel;
+  __shared__ int s_m;
+  for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+    if (flag[qi] != 1) continue;
+    const int c = cnt[qi];
+    const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
+    uint64_t* buf = s_dyn;
+    uint64_t* ex = s_dyn + cap;
+    const int n2 = pow2_ceil(c);
+    for (int i = threadIdx.x; i < n2; i += blockDim.x) buf[i] = i < c ? src[i] : kEmpty;
+    __syncthreads();
+    block_bitonic_sort(buf, n2);
+    if (threadIdx.x == 0) {
+      const float lim = __fadd_ru(ordered_to_float(static_cast<uint32_t>(buf[k - 1] >> 32)), e2[qi]);
+      const uint32_t lim_bits = ordered_bits(lim);
+      int m = k;
+      while (m < c && static_cast<uint32_t>(buf[m] >> 32) <= lim_bits) ++m;
+      s_m = m;
+    }
+    __syncthreads();
+    const int m = s_m;
+    const float* qrow = q + static_cast<size_t>(qi) * dpad;
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+      const uint32_t pos = key_tie(buf[j]);
+      const float acc = exact_l2_seq(codes + static_cast<size_t>(pos) * dpad, qrow, dpad);
+      ex[j] = acc < FLT_MAX ? make_key(acc, pos) : kEmpty;
+    }
+    __syncthreads();
+    auto key_at = [&](int i) -> uint64_t { return ex[i]; };
+    block_topk_sorted(key_at, m, k, sh_sel, buf);
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+      const uint64_t key = buf[j];
+      const size_t o = static_cast<size_t>(qi) * k + j;
+      D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+      I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+    }
+    __syncthreads();
+  }
+}
+
+// Seed bound per query before the scan: the k-th smallest w over the first
+// S rows of the query's nearest list, computed from the same BF16 operands as
+// the scan (these values obey the same eps), + 2 eps: an upper bound of
+// W_k + 2 eps.  Queries whose nearest list holds fewer than k rows keep
+// FLT_MAX.
 //
 // List-major: one CTA per list stages the list's first S BF16 rows in shared
 // memory once; for each query whose nearest list it is (probe rank 0 in the
 // list-major work description) in turn, thread t computes row t's value with
 // the query broadcast from shared memory, and a 32-step radix selection over
-// the CTA (one barrier count per bit) finds the R-th smallest.
+// the CTA (one barrier count per bit) finds the k-th smallest.  Small batches
+// (probes given): one CTA per query.
 constexpr int kSeedRows = 256;
 constexpr int kSeedWarps = 8;
 
-__global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
-    const float* __restrict__ q, int dpad, int kpad, const __nv_bfloat16* __restrict__ codes,
+__global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
+    const __nv_bfloat16* __restrict__ qbf, int kpad, const __nv_bfloat16* __restrict__ codes,
     const int64_t* __restrict__ list_off, const int64_t* __restrict__ list_qoff, const int32_t* __restrict__ list_q,
-    const float* __restrict__ xnorm, int S, int R, const float* __restrict__ maxnorm, uint64_t* __restrict__ tau,
+    const float* __restrict__ xnorm, int S, int k, const float* __restrict__ e2, uint32_t* __restrict__ thr,
     const int32_t* __restrict__ probes, int P) {
   extern __shared__ __align__(16) uint8_t s_seed_raw[];
   __shared__ float s_xn[kSeedRows];
   __shared__ int s_qs[kSeedWarps * 32];
   __shared__ int s_nq;
-  __shared__ float s_qn;
-  const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
-  // One CTA per list (its rows serve every query whose nearest list it is),
-  // or, for small batches (probes given), one CTA per query.
+  const int tid = threadIdx.x;
   const bool by_query = probes != nullptr;
   int l;
   int64_t e0, e1;
@@ -605,7 +631,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
   }
   const int64_t b = list_off[l];
   const int n = static_cast<int>(min(static_cast<int64_t>(S), list_off[l + 1] - b));
-  if (n < R) return;  // no seed: tau stays empty
+  if (n < k) return;  // no seed: the bound stays FLT_MAX
   const int stride = kpad * 2 + 16;  // bytes per staged row (padding spreads banks)
   uint8_t* rows = s_seed_raw;
   float* qbuf = reinterpret_cast<float*>(s_seed_raw + static_cast<size_t>(S) * stride);
@@ -616,10 +642,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
   }
   cp_async_commit();
   for (int r = tid; r < n; r += blockDim.x) s_xn[r] = xnorm[b + r];
-  const float mn = *maxnorm;
   cp_async_wait<0>();
-  // Rounds over the list's entries: the queries whose nearest list this is
-  // are gathered in shared memory, then one warp per query.
   for (int64_t r0 = e0; r0 < e1; r0 += blockDim.x) {
     if (tid == 0) s_nq = 0;
     __syncthreads();
@@ -630,23 +653,15 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
     }
     __syncthreads();
     const int nqr = s_nq;
-    // Each query in turn, the whole CTA: thread t takes row t, then a
-    // 32-step radix selection over the CTA finds the R-th smallest value.
     for (int t = 0; t < nqr; ++t) {
       const int qi = s_qs[t];
-      const float* qrow = q + static_cast<size_t>(qi) * dpad;
-      for (int c = tid; c < kpad; c += blockDim.x) qbuf[c] = c < dpad ? __bfloat162float(__float2bfloat16_rn(qrow[c])) : 0.0f;
-      if (wib == 0) {
-        float qn = 0.0f;
-        for (int c = lane; c < dpad; c += 32) qn = fmaf(qrow[c], qrow[c], qn);
-        for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(0xffffffffu, qn, o);
-        if (lane == 0) s_qn = qn;
-      }
+      const __nv_bfloat16* qrow = qbf + static_cast<size_t>(qi) * kpad;
+      for (int c = tid; c < kpad; c += blockDim.x) qbuf[c] = __bfloat162float(qrow[c]);
       __syncthreads();
       uint32_t key = 0xFFFFFFFFu;
       if (tid < n) {
         const uint8_t* xr = rows + static_cast<size_t>(tid) * stride;
-        // Four partial sums (any order is within the margin).
+        // Four partial sums (any order is within eps).
         float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
 #pragma unroll 4
         for (int c = 0; c < kpad; c += 8) {
@@ -665,7 +680,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
         key = ordered_bits(fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[tid]));
       }
       uint32_t prefix = 0;
-      int need = R;
+      int need = k;
       for (int bit = 31; bit >= 0; --bit) {
         const uint32_t hmask = bit == 31 ? 0u : (0xFFFFFFFFu << (bit + 1));
         const bool zero_here = (key & hmask) == prefix && ((key >> bit) & 1u) == 0u;
@@ -676,9 +691,8 @@ __global__ void __launch_bounds__(kSeedWarps * 32) tau_seed_kernel(
         }
       }
       if (tid == 0) {
-        const float vR = ordered_to_float(prefix);
-        const float margin = 1e-3f * sqrtf(s_qn) * mn + 2e-5f * (mn * mn + fabsf(vR)) + 1e-30f;
-        tau[qi] = (static_cast<uint64_t>(ordered_bits(vR + margin)) << 32) | 0xffffffffull;
+        const float bound = fminf(__fadd_ru(ordered_to_float(prefix), e2[qi]), FLT_MAX);
+        thr[qi] = ordered_bits(bound);
       }
       __syncthreads();
     }
@@ -747,24 +761,15 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 }  // namespace
 
-size_t scan_bf16_smem_bytes(int kpad, int R, int stages) {
+size_t scan_bf16_smem_bytes(int kpad, int stages) {
   const size_t tile = static_cast<size_t>(kpad / 64) * kTile * 128;
-  return 1024 + tile * (2 + stages) + static_cast<size_t>(kGroups) * R * kEpiThreads * 8 +
-         static_cast<size_t>(kAcc) * kTile * 4 + 2 * kTile * (4 + 4 + 8);
+  return 1024 + tile * (2 + stages) + static_cast<size_t>(kAcc) * kTile * 4 + 2 * kTile * (4 + 4 + 4);
 }
 
-int scan_bf16_keys_per_slot(int R) { return kGroups * R; }
-
-int scan_bf16_stages(int kpad, int R) {
+int scan_bf16_stages(int kpad) {
   int s = kMaxStages;
-  while (s > 2 && scan_bf16_smem_bytes(kpad, R, s) > kSmemCap) --s;
+  while (s > 2 && scan_bf16_smem_bytes(kpad, s) > kSmemCap) --s;
   return s;
-}
-
-int scan_bf16_max_R(int kpad) {
-  int R = 64;
-  while (R > 1 && scan_bf16_smem_bytes(kpad, R, 2) > kSmemCap) --R;
-  return R;
 }
 
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad) {
@@ -789,57 +794,64 @@ void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, c
 
 void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream_t st) {
   HB_CHECK(a.kpad == 64 || a.kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
-  HB_CHECK(a.R >= 1 && a.R <= 64, HB_ERR_INVALID, "rerank candidates per query must be in [1, 64]");
   HB_CHECK(a.chunk_rows % kTile == 0, HB_ERR_INVALID, "BF16 scan chunks must be whole tiles");
   HB_CHECK(a.stages >= 2 && a.stages <= kMaxStages, HB_ERR_INVALID, "bad stage count");
-  const size_t smem = scan_bf16_smem_bytes(a.kpad, a.R, a.stages);
-  HB_CHECK(smem <= kSmemCap, HB_ERR_INVALID, "rerank candidates too many for the BF16 scan's shared memory");
-  HB_CUDA(cudaFuncSetAttribute(scan_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  scan_bf16_kernel<<<num_sms, kTcThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap), a);
-  HB_CUDA(cudaGetLastError());
-}
-
-void launch_rerank(const uint64_t* part, const int64_t* slot_base, int nq, int P, int R, int k, const float* codes,
-                   const float* q, int dpad, const int64_t* ids, float* D, int64_t* I, cudaStream_t st,
-                   const uint64_t* part2, const int64_t* slot_base2, int P2, const uint64_t* tau, int* overflow) {
-  if (nq <= 0) return;
-  if (tau && !part2 && overflow && R <= 64 && nq >= 1024) {
-    // Warp per query; the rare query with too many keys under its bound
-    // goes through the CTA kernel.
-    HB_CHECK(k <= R, HB_ERR_INVALID, "k must not exceed the re-ranked candidates");
-    rerank_warp_kernel<<<(nq + kRerankWarps - 1) / kRerankWarps, kRerankWarps * 32, 0, st>>>(
-        part, slot_base, nq, P, R, k, codes, q, dpad, ids, D, I, tau, overflow);
-    HB_CUDA(cudaGetLastError());
-    const int n2 = pow2_ceil(R < 2 ? 2 : R);
-    const size_t smem = static_cast<size_t>(2 * n2) * 8 + 64;
-    rerank_kernel<<<nq, 512, smem, st>>>(part, slot_base, P, R, k, codes, q, dpad, ids, D, I, nullptr, nullptr, 0, tau,
-                                         overflow);
-    HB_CUDA(cudaGetLastError());
-    return;
+  HB_CHECK(a.k >= 1 && a.cap >= a.k, HB_ERR_INVALID, "candidate buffer smaller than k");
+  HB_CHECK(a.wait_budget > 0, HB_ERR_INVALID, "wait budget must be positive");
+  const size_t smem = scan_bf16_smem_bytes(a.kpad, a.stages);
+  HB_CHECK(smem <= kSmemCap, HB_ERR_INVALID, "BF16 scan tiles exceed shared memory");
+  if (a.k <= kTightK) {
+    HB_CUDA(cudaFuncSetAttribute(scan_bf16_kernel<kTightK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    scan_bf16_kernel<kTightK><<<num_sms, kTcThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap), a);
+  } else {
+    HB_CUDA(cudaFuncSetAttribute(scan_bf16_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    scan_bf16_kernel<0><<<num_sms, kTcThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap), a);
   }
-  HB_CHECK(k <= R, HB_ERR_INVALID, "k must not exceed the re-ranked candidates");
-  const int n2 = pow2_ceil(R < 2 ? 2 : R);
-  const size_t smem = static_cast<size_t>(2 * n2) * 8 + 64;
-  // Small batches get wider CTAs (each query's selection is the whole job).
-  rerank_kernel<<<nq, nq < 1024 ? 256 : 128, smem, st>>>(part, slot_base, P, R, k, codes, q, dpad, ids, D, I, part2,
-                                                         slot_base2, P2, tau, nullptr);
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_tau_seed(const float* q, int nq, int dpad, int kpad, const void* codes_bf16, const int64_t* list_off,
-                     int nlist, const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int R,
-                     const float* maxnorm, uint64_t* tau, cudaStream_t st, const int32_t* probes, int P) {
+void launch_query_prep(const float* q, int nq, int d, int dpad, int kpad, const float* maxnorm, void* qbf, float* e2,
+                       uint32_t* thr, int* cnt, cudaStream_t st) {
+  if (nq <= 0) return;
+  query_prep_kernel<<<(nq + 7) / 8, 256, 0, st>>>(q, nq, d, dpad, kpad, maxnorm, static_cast<__nv_bfloat16*>(qbf), e2,
+                                                  thr, cnt);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_seed_bound(const void* qbf, int nq, int kpad, const void* codes_bf16, const int64_t* list_off, int nlist,
+                       const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int k,
+                       const float* e2, uint32_t* thr, cudaStream_t st, const int32_t* probes, int P) {
   if (nq <= 0) return;
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
-  HB_CHECK(S >= 1 && S <= kSeedRows && R >= 1 && R <= S, HB_ERR_INVALID, "seed sample out of range");
-  HB_CUDA(cudaMemsetAsync(tau, 0xff, static_cast<size_t>(nq) * sizeof(uint64_t), st));
+  HB_CHECK(S >= 1 && S <= kSeedRows && k >= 1, HB_ERR_INVALID, "seed sample out of range");
+  if (k > S) return;  // no sample holds k rows: every bound stays FLT_MAX
   const size_t smem = static_cast<size_t>(S) * (kpad * 2 + 16) + static_cast<size_t>(kpad) * 4;
-  HB_CUDA(cudaFuncSetAttribute(tau_seed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  HB_CUDA(cudaFuncSetAttribute(seed_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const bool by_query = probes && static_cast<long long>(nq) * 4 < nlist;
-  tau_seed_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(
-      q, dpad, kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff, list_q, xnorm, S, R, maxnorm,
-      tau, by_query ? probes : nullptr, P);
+  seed_bound_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(
+      static_cast<const __nv_bfloat16*>(qbf), kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff,
+      list_q, xnorm, S, k, e2, thr, by_query ? probes : nullptr, P);
   HB_CUDA(cudaGetLastError());
+}
+
+void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
+                        const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
+                        int* flag, int* over_list, int* over_n, int num_sms, cudaStream_t st) {
+  if (nq <= 0) return;
+  HB_CHECK(k >= 1 && cap >= k && cap <= kRerankMaxCap, HB_ERR_INVALID, "candidate buffer size out of range");
+  rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(cand, cnt, cap, e2, nq, k, codes, q,
+                                                                               dpad, ids, D, I, flag, over_list, over_n);
+  HB_CUDA(cudaGetLastError());
+  if (cap > kRrWarpCap) {
+    const size_t smem = static_cast<size_t>(2) * cap * sizeof(uint64_t);
+    HB_CUDA(cudaFuncSetAttribute(rerank_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    const int grid = std::min(nq, 4 * num_sms);
+    rerank_cta_kernel<<<grid, 256, smem, st>>>(cand, cnt, cap, e2, nq, k, codes, q, dpad, ids, D, I, flag);
+    HB_CUDA(cudaGetLastError());
+  }
 }
 
 void launch_wait_selftest(long long budget, int code, int* err, long long* waited, cudaStream_t st) {

@@ -72,9 +72,12 @@ typedef struct {
   int32_t warmup_lists;       /* preSearch warmUpSearchList (default 10)        */
   int32_t warmup_list_size;   /* preSearch warmUpSearchListSize (0 -> k)        */
   int32_t precision;          /* HB_PREC_*                                     */
-  int32_t rerank_mult;        /* BF16: candidates re-ranked = rerank_mult * k (default 2;
-                                 at most 64 on the d <= 128 heap scan, else at most 4096;
-                                 k itself up to 4096) */
+  int32_t rerank_mult;        /* BF16 with d > 128 or k > 256 (the candidate-matrix
+                                 scan): candidates re-ranked = rerank_mult * k, at
+                                 most 4096, k itself up to 4096 (default 2).  For
+                                 d <= 128 and k <= 256 the re-ranked set is every row
+                                 within the scan's error bound of the k-th, and the
+                                 result equals the FP32 scan's; this field is unused */
   int32_t learned_probe;      /* 1: per-query nprobe from the learned predictor */
   float learned_target;       /* predictor target recall (0 -> trained target)   */
   const int32_t* nprobe_per_query; /* optional nq array (host or device); overrides nprobe */
@@ -197,6 +200,17 @@ uint64_t hb_launch_count(const hb_index* ix);
  * over all indexes.  No reference counterpart: a diagnostic that lets a
  * caller check that a call allocated nothing. */
 uint64_t hb_device_allocations(void);
+
+/* Clock cycles a device-side wait of the BF16 scan spends before it gives
+ * up (no reference counterpart; cycles <= 0 restores the default, 2e9).  A
+ * wait that gives up makes the search return HB_ERR_CUDA with "gave up
+ * waiting" and leaves the index usable. */
+int hb_set_wait_budget(hb_index* ix, int64_t cycles);
+
+/* Queries of the most recent BF16 search (d <= 128, k <= 256) whose
+ * candidate buffer overflowed and that were searched again with the exact
+ * FP32 scan (no reference counterpart). */
+int hb_bf16_fallbacks(hb_index* ix, int64_t* n);
 
 /* Self-test of the device-side bounded waits (no reference counterpart).
  * Every mbarrier wait in the tensor-core kernels gives up after a clock

@@ -1,6 +1,6 @@
 """GPU tests of the candidate-matrix BF16 scan (tcgen05 over any d, up to 4096
 candidates per query) with the exact FP32 re-rank: the BF16 searches the
-shared-memory heap scan does not take (d > 128, or k above 64)."""
+bounded scan does not take (d > 128, or k above 256)."""
 import os
 import tempfile
 
@@ -96,8 +96,8 @@ def test_wide_integer_data_matches_reference(ref_lib, restated):
 
 
 def test_d128_large_k(restated):
-    """d = 128 with k = 100 (above the heap scan's 64 candidates) takes the
-    candidate-matrix route."""
+    """d = 128: k = 65 and 100 take the bounded scan (exact result); k = 300,
+    above its 256, takes the candidate-matrix route."""
     base, q = datasets.config2(seed=73, nb=120_000, nq=400, ncomp=300)
     ix = Index(128, 256, 12)
     ix.train(base.shape[0], base)
@@ -107,7 +107,7 @@ def test_d128_large_k(restated):
         D, I = search(ix, q, k, mult=mult)
         De, Ie = search(ix, q, k, precision=Precision.FP32)
         same = np.mean([np.array_equal(a, b) for a, b in zip(D.view(np.uint32), De.view(np.uint32))])
-        assert same >= 0.99, (k, same)
+        assert same >= (1.0 if k <= 256 else 0.99), (k, same)
         assert (D[:, -1] >= De[:, -1]).all()
         for qi in range(0, q.shape[0], 53):
             assert D[qi, 0] == restated.l2(q[qi], base[I[qi, 0]])

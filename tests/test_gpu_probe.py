@@ -63,6 +63,11 @@ def test_learned_probe_meets_calibrated_recall(setup):
             for j in range(10):
                 if (qi, I[qi, j]) in dl:
                     assert D[qi, j] == dl[(qi, I[qi, j])]
+    # The bounded BF16 scan over the predicted probes returns the exact scan's
+    # result over the same probes.
+    Db, Ib = run(ix, test, 10, Precision.BF16, learned=True)
+    De, Ie = run(ix, test, 10, Precision.FP32, learned=True)
+    assert np.array_equal(Db.view(np.uint32), De.view(np.uint32)) and np.array_equal(Ib, Ie)
     # A higher target never lowers recall.
     D2, I2 = run(ix, test, 10, Precision.BF16, learned=True, target=0.99)
     assert recall_at_k(I2, Il, 10) >= recall_at_k(I, Il, 10) - 1e-9

@@ -1289,10 +1289,13 @@ class IndexCore {
   }
 
   // Candidate buffer per query of the bounded BF16 scan: room for 16 k
-  // candidates (at least 1024); a query needing more is searched again with
-  // the exact scan.
+  // candidates (at least 1024), rounded up to a power of two (the re-rank
+  // sorts a buffer in place); a query needing more is searched again with the
+  // exact scan.
   static int filter_cap(size_t k) {
-    return static_cast<int>(std::min<size_t>(kRerankMaxCap, std::max<size_t>(1024, 16 * k)));
+    size_t c = 1024;
+    while (c < 16 * k) c <<= 1;
+    return static_cast<int>(std::min<size_t>(kRerankMaxCap, c));
   }
 
   // BF16 search of one batch, equal to the exact FP32 scan bit for bit: exact

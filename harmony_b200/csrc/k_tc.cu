@@ -840,7 +840,8 @@ void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const flo
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
                         int* flag, int* over_list, int* over_n, int num_sms, cudaStream_t st) {
   if (nq <= 0) return;
-  HB_CHECK(k >= 1 && cap >= k && cap <= kRerankMaxCap, HB_ERR_INVALID, "candidate buffer size out of range");
+  HB_CHECK(k >= 1 && cap >= k && cap <= kRerankMaxCap && (cap & (cap - 1)) == 0, HB_ERR_INVALID,
+           "candidate buffer size out of range");
   rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(cand, cnt, cap, e2, nq, k, codes, q,
                                                                                dpad, ids, D, I, flag, over_list, over_n);
   HB_CUDA(cudaGetLastError());

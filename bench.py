@@ -19,6 +19,7 @@ every step touches every list, so no L2 flush is needed between steps.
   python bench.py --workload c4     (10M x 96, Zipf list sizes, batches of 1..4096)
   python bench.py --workload c3     (270k x 500, k 100: the candidate-matrix BF16 path)
   python bench.py --workload c2     (1M x 128, nlist 1024, k 100: the nprobe 8..128 sweep)
+  python bench.py --workload c5-batches  (learned vs fixed nprobe by batch size, 10M x 128)
 
 Multi-GPU: the path is query-parallel with no exchange step, so N ranks run
 N independent replicas (weak scaling, each rank its own 10k queries).
@@ -400,8 +401,20 @@ def run_ours(args):
             roof.update({"bound": "hbm", "achieved": None, "peak": hbm_peak, "unit": "GB/s", "frac": None,
                          "traffic": None})
     fp = arms["fp32"]
-    fp_bytes_alg = int(sizes[ix.probe_lists(test.cpu().numpy(), fp["nprobe"])[0]].sum()) * d * 4
+    fp_pairs = int(sizes[ix.probe_lists(test.cpu().numpy(), fp["nprobe"])[0]].sum())
+    fp_bytes_alg = fp_pairs * d * 4
     fp_scan = fp["kernel_ms"].get("scan_exact", 0.0) / 1e3
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    # The exact scan's own roofline is the FP32 pipe, not HBM (each probed list
+    # is read once per group of 32 queries): 3 FP32 operations per (query,
+    # vector, dimension), against SMs x 128 lanes x 2 (packed f32x2) x clock.
+    fp_ops = 3.0 * fp_pairs * d
+    fp_peak = 148 * 128 * 2 * sm_mhz * 1e6
+    fp_roof = ({"bound": "fp32 pipe", "achieved": round(fp_ops / fp_scan / 1e12, 2), "peak": round(fp_peak / 1e12, 2),
+                "unit": "TFLOP/s (FP32 ops)", "frac": round(fp_ops / fp_scan / fp_peak, 3),
+                "note": "3 unfused FP32 ops per element pair; peak = 148 SMs x 128 lanes x 2 (f32x2) x sampled SM clock"}
+               if fp_scan else None)
     result = None
     if rank == 0:
         result = {
@@ -429,7 +442,8 @@ def run_ours(args):
             "plain_fp32": {"qps": round(fp["qps"], 1), "nprobe": fp["nprobe"],
                            "recall_at_10": round(fp["recall_at_10"], 4), "ms_per_step": round(fp["ms_per_step"], 3),
                            "kernel_ms_per_step": {n: round(v, 4) for n, v in fp["kernel_ms"].items()},
-                           "scan_bytes_alg_gbs": round(fp_bytes_alg / fp_scan / 1e9, 1) if fp_scan else None},
+                           "scan_bytes_alg_gbs": round(fp_bytes_alg / fp_scan / 1e9, 1) if fp_scan else None,
+                           "roofline": fp_roof},
             "bf16_fixed_nprobe": {"qps": round(arms["bf16"]["qps"], 1), "nprobe": arms["bf16"]["nprobe"],
                                   "recall_at_10": round(arms["bf16"]["recall_at_10"], 4),
                                   "ms_per_step": round(arms["bf16"]["ms_per_step"], 3),
@@ -442,7 +456,7 @@ def run_ours(args):
             "roofline": roof,
             "kernel_ms_per_step": {n: round(v, 4) for n, v in kms.items()},
             "gpu_launches": int(round(head["launches_per_step"] * args.steps)),
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:
             ix.search_params.precision, ix.search_params.learned_probe = Precision.FP32, False
@@ -879,6 +893,86 @@ def run_c2(args):
     print(json.dumps(line))
 
 
+def run_c5_batches(args):
+    """Learned nprobe against fixed nprobe on the 10M x 128 index, by batch size.
+
+    Both arms search in BF16 (the bounded scan, exact results) with the
+    queries and results resident on the device, one CUDA-graph launch per
+    batch.  The fixed arm uses the smallest nprobe whose recall@10 over the
+    10k test queries reaches the target; the learned arm the smallest predictor
+    target whose recall reaches it too.  A query's results do not depend on the
+    other queries of its batch, so the recall of either arm is that of the
+    whole test set.  Per batch size: QPS of each arm, their ratio, and the
+    probed lists per batch (the distinct lists read)."""
+    import torch
+    from harmony_b200 import Index, Precision, SearchMode
+    k, nq = WORKLOAD["k"], WORKLOAD["nq"]
+    ix, base, test, train, build = build_index(torch, seed=5, ntrain=args.ntrain)
+    gt = ground_truth(torch, ix, base, test, k)
+    del base
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    ix.train_probe_predictor(train.shape[0], train, k=k, label_nprobe=256, target=args.target)
+    del train
+    P, rec_f = pick_nprobe(ix, test, gt, k, args.target, Precision.BF16)
+    sp = ix.search_params
+    D = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    I = torch.empty((nq, k), dtype=torch.int64, device="cuda")
+    sp.precision, sp.learned_probe = Precision.BF16, True
+    ix.nprobe = 256
+    tgt, rec_l = args.target, 0.0
+    for tgt in [args.target + 0.005 * i for i in range(10)]:
+        sp.learned_target = min(tgt, 0.9999)
+        ix.search(nq, test, k, D, I)
+        rec_l = recall(I.cpu().numpy(), gt, k)
+        if rec_l >= args.target:
+            break
+    tgt = min(tgt, 0.9999)
+    stream = torch.cuda.ExternalStream(ix.stream)
+    q_np = test.cpu().numpy()
+    rows = []
+    for B in (1, 16, 64, 256, 1024, 4096):
+        row = {"batch": B}
+        calls = max(8, min(400, 20_000 // B))
+        for name, learned in (("fixed", False), ("learned", True)):
+            sp.use_graph, sp.learned_probe = True, learned
+            sp.learned_target = tgt if learned else 0.0
+            ix.nprobe = 256 if learned else P
+            offs = [(c * B) % (nq - B + 1) for c in range(calls)]
+            for o in offs[:3]:
+                ix.search(B, test[o:o + B], k, D[o:o + B], I[o:o + B])
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for o in offs:
+                ix.search(B, test[o:o + B], k, D[o:o + B], I[o:o + B])
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / calls
+            row[name] = {"ms_per_batch": round(ms, 4), "qps": round(B / ms * 1e3, 1)}
+        sp.use_graph = False
+        # Lists read per batch (distinct probed lists of the first batch).
+        sp.learned_probe = False
+        pr_f, _ = ix.probe_lists(q_np[:B], P)
+        row["fixed"]["lists_per_batch"] = int(np.unique(pr_f).size)
+        row["learned_over_fixed"] = round(row["learned"]["qps"] / row["fixed"]["qps"], 3)
+        rows.append(row)
+    sp.use_graph, sp.learned_probe, sp.learned_target, sp.precision = False, False, 0.0, Precision.FP32
+    thr, crec, cavg = ix.probe_calibration()
+    i_sel = int(np.argmin(np.where(crec >= tgt, cavg, 1e9)))
+    line = {"metric": "QPS by batch size, learned nprobe vs fixed nprobe (both BF16 bounded scan, exact results), "
+                      "10M x 128, nlist 4096, k 10",
+            "workload": "c5-batches", "unit": "queries/s", "n_gpus": 1, "dtype": "bf16",
+            "data": "synthetic (seeded Gaussian mixture drawn on the GPU)",
+            "config": {"fixed_nprobe": P, "fixed_recall_at_10": round(rec_f, 4), "predictor_target": round(tgt, 4),
+                       "learned_recall_at_10": round(rec_l, 4),
+                       "learned_avg_nprobe_validation": round(float(cavg[i_sel]), 2),
+                       "timing": "CUDA events on the index stream, one CUDA-graph launch per batch, device-resident "
+                                 "queries and results", **build},
+            "batches": rows}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -892,16 +986,16 @@ def main():
     ap.add_argument("--nq", type=int, default=None, help="fewer queries for profiling runs (not a bench line)")
     ap.add_argument("--ntrain", type=int, default=200_000, help="training queries of the learned probe")
     ap.add_argument("--freeze-to", default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", choices=["c5", "c4", "c3", "c2"], default="c5",
+    ap.add_argument("--workload", choices=["c5", "c4", "c3", "c2", "c5-batches"], default="c5",
                     help="c5: the headline bench line; c4: the batch-stream measurement of config 4; "
                          "c3: the 500-dimensional k = 100 measurement of config 3; c2: the 1M x 128 nprobe sweep")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.nb and args.workload == "c5":
+    if args.nb and args.workload in ("c5", "c5-batches"):
         WORKLOAD["nb"] = args.nb
         WORKLOAD["workload"] += f" [reduced: nb={args.nb}]"
-    if args.nq and args.workload == "c5":
+    if args.nq and args.workload in ("c5", "c5-batches"):
         WORKLOAD["nq"] = args.nq
         WORKLOAD["workload"] += f" [reduced: nq={args.nq}]"
     if args.freeze_to:
@@ -912,6 +1006,8 @@ def main():
         run_c3(args)
     elif args.workload == "c2":
         run_c2(args)
+    elif args.workload == "c5-batches":
+        run_c5_batches(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -357,8 +357,25 @@ class IndexCore {
   // BF16 copy of the codes (rows padded to kpad = d rounded up to 64) and its
   // TMA tensor map, for the tensor-core scans (the heap scan takes d <= 128,
   // the candidate-matrix scan any d).
+  // E4M3 copy of the codes for the FP8 candidate scan (rows padded to kpad8
+  // = d rounded up to 128 bytes) with a per-list scale, built on the first
+  // FP8 search after the lists change.
+  void ensure_fp8() {
+    if (fp8_ready_) return;
+    kpad8_ = static_cast<int>((d_ + 127) / 128 * 128);
+    codes8_.reserve(std::max<size_t>(ntotal_ * static_cast<size_t>(kpad8_), 1));
+    list_scale8_.reserve(nlist_);
+    launch_fp8_codes(codes_.p, list_off_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), kpad8_, codes8_.p,
+                     list_scale8_.p, st_);
+    ++launches_;
+    make_u8_tensor_map(tmap8_, codes8_.p, std::max<size_t>(ntotal_, 1), kpad8_);
+    HB_CUDA(cudaStreamSynchronize(st_));
+    fp8_ready_ = true;
+  }
+
   void build_bf16() {
     bf16_ready_ = false;
+    fp8_ready_ = false;
     kpad_ = static_cast<int>((d_ + 63) / 64 * 64);
     if (ntotal_ == 0) return;
     codes_bf16_.reserve(ntotal_ * static_cast<size_t>(kpad_));
@@ -569,9 +586,11 @@ class IndexCore {
     hb_search_params_init(&p);
     if (prm) p = *prm;
     if (nprobe_ > nlist_) nprobe_ = nlist_;  // src/Index.cpp:1646-1648 (mutates the field)
-    HB_CHECK(p.precision == HB_PREC_FP32 || p.precision == HB_PREC_BF16, HB_ERR_INVALID,
-             "precision must be FP32 or BF16");
-    const bool bf16 = p.precision == HB_PREC_BF16;
+    HB_CHECK(p.precision == HB_PREC_FP32 || p.precision == HB_PREC_BF16 || p.precision == HB_PREC_FP8,
+             HB_ERR_INVALID, "precision must be FP32, BF16 or FP8");
+    // bf16: a tensor-core scan (BF16, or the FP8 variant) with an exact re-rank.
+    const bool bf16 = p.precision != HB_PREC_FP32;
+    fp8_ = p.precision == HB_PREC_FP8;
     if (bf16) {
       HB_CHECK(p.mode == HB_MODE_ORIGINAL || p.mode == HB_MODE_BRUTE_FORCE, HB_ERR_INVALID,
                "the BF16 scan implements ORIGINAL / BRUTE_FORCE search (pruning and the dimension relay are FP32 modes)");
@@ -585,7 +604,9 @@ class IndexCore {
     int etv = 0, eqt = 0, eqg = 0;
     const bool exact_k = scan_exact_smem_bytes(static_cast<int>(d_), static_cast<int>(dpad_), static_cast<int>(k),
                                                SCAN_PLAIN, &etv, &eqt, &eqg) > 0;
-    cand_path_ = bf16 && !(kpad_ <= 128 && static_cast<int>(k) <= kFilterMaxK && exact_k);
+    // FP8 (E4M3: 3 mantissa bits, a rounding bound 16 times BF16's) always
+    // takes the candidate-matrix scan with its fixed re-rank width.
+    cand_path_ = bf16 && (fp8_ || !(kpad_ <= 128 && static_cast<int>(k) <= kFilterMaxK && exact_k));
     const int R = cand_path_ ? std::min(kCandMaxR, want_R) : 0;
     if (cand_path_)
       HB_CHECK(static_cast<int>(k) <= R, HB_ERR_INVALID,
@@ -761,7 +782,7 @@ class IndexCore {
     }
     cut_b0_ = 0;
     char key[256];
-    std::snprintf(key, sizeof(key), "%d/%d/%d/%d/%d/%d/%d/%08x/%d/%d/%d/%d/%d", nb, k, P, R, bf16 ? 1 : 0, p.mode,
+    std::snprintf(key, sizeof(key), "%d/%d/%d/%d/%d/%d/%d/%08x/%d/%d/%d/%d/%d", nb, k, P, R, p.precision, p.mode,
                   cut_mode_, cut_mode_ == 1 ? *reinterpret_cast<const uint32_t*>(&cut_thr_) : 0u, cut_cap_,
                   seed_rows_, coarse_kind_, coarse_margin_, static_cast<int>(nprobe_));
     auto it = graphs_.find(key);
@@ -1471,14 +1492,24 @@ class IndexCore {
       launch_cand_segments(probes_.p, nb, P, list_off_.p, seg_.p, work_tmp_.p, wtmp, st_);
     }
     launches_ += 2;
-    gq_.reserve(nqp * static_cast<size_t>(kpad_));
-    {
+    if (fp8_) {
+      ensure_fp8();
+      qscale8_.reserve(nb);
+      gq8_.reserve(nqp * static_cast<size_t>(kpad8_));
+      Scope sc(this, "gather_queries");
+      launch_query_fp8_scales(qpad_.p, nb, static_cast<int>(dpad_), qscale8_.p, st_);
+      launch_gather_queries_fp8(qpad_.p, static_cast<int>(dpad_), kpad8_, list_q_.p, list_qoff_.p + nlist_,
+                                static_cast<int64_t>(nqp), qscale8_.p, gq8_.p, st_);
+      make_u8_tensor_map(gqmap_, gq8_.p, nqp, kpad8_);
+      launches_ += 2;
+    } else {
+      gq_.reserve(nqp * static_cast<size_t>(kpad_));
       Scope sc(this, "gather_queries");
       launch_gather_queries(qpad_.p, static_cast<int>(dpad_), kpad_, list_q_.p, list_qoff_.p + nlist_,
                             static_cast<int64_t>(nqp), gq_.p, st_);
+      make_bf16_tensor_map(gqmap_, gq_.p, nqp, kpad_);
+      ++launches_;
     }
-    ++launches_;
-    make_bf16_tensor_map(gqmap_, gq_.p, nqp, kpad_);
     const int64_t row_bound = cand_row_bound(P);
     cand_.reserve(std::max<size_t>(static_cast<size_t>(nb) * row_bound, 1));
     cand_rows_.reserve(static_cast<size_t>(nb) * R);
@@ -1497,9 +1528,15 @@ class IndexCore {
     a.seg = seg_.p;
     a.cand = cand_.p;
     a.err = err_dev_.p;
+    if (fp8_) {
+      a.fp8 = 1;
+      a.kpad = kpad8_;
+      a.qscale = qscale8_.p;
+      a.list_scale = list_scale8_.p;
+    }
     {
       Scope sc(this, "cand_scan");
-      launch_cand_scan(gqmap_, tmap_, a, num_sms_, st_);
+      launch_cand_scan(gqmap_, fp8_ ? tmap8_ : tmap_, a, num_sms_, st_);
     }
     ++launches_;
     {
@@ -1856,6 +1893,11 @@ class IndexCore {
   size_t dpad_ = 16;
   int kpad_ = 0;
   bool bf16_ready_ = false;
+  bool fp8_ = false, fp8_ready_ = false;
+  int kpad8_ = 0;
+  alignas(64) unsigned char tmap8_[128];
+  DevBuf<uint8_t> codes8_, gq8_;
+  DevBuf<float> list_scale8_, qscale8_;
   alignas(64) unsigned char tmap_[128];
   alignas(64) unsigned char gqmap_[128];  // gathered BF16 queries of the candidate-matrix scan
   bool cand_path_ = false;

@@ -123,6 +123,18 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
       : "memory");
 }
 
+// D[tmem] (+)= A x B^T, kind::f8f6f4 with both operands E4M3 (K = 32 per
+// instruction: the same 32 bytes of a 128-byte swizzled row as kind::f16's
+// K = 16 BF16), issued by one thread.
+__device__ __forceinline__ void mma_e4m3(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // Arrives once on `bar` when all tcgen05 operations this thread issued so
 // far have completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
@@ -160,6 +172,13 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t smem_addr) {
 // Instruction descriptor, kind::f16: BF16 A and B, FP32 D, both K-major.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+         (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+// Instruction descriptor, kind::f8f6f4: E4M3 A and B (format 0), FP32 D,
+// both K-major.
+__host__ __device__ constexpr uint32_t idesc_e4m3_f32(int M, int N) {
+  return (1u << 4) | (0u << 7) | (0u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
          (static_cast<uint32_t>(M >> 4) << 24);
 }
 

@@ -32,6 +32,7 @@
 #include <cudaTypedefs.h>
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -100,6 +101,11 @@ __device__ __forceinline__ CandItem cand_item(const CandArgs& a, int64_t item) {
   return d;
 }
 
+// FP8 = false: BF16 operands, 64-element K blocks, kind::f16.  FP8 = true:
+// E4M3 operands scaled per query and per list (x ~ s_l * code, q ~ s_q *
+// code), 128-element K blocks (the same 128-byte swizzled rows), kind::f8f6f4;
+// the epilogue multiplies the accumulator by s_q * s_l.
+template <bool FP8>
 __global__ void __launch_bounds__(kThreads, 1)
     cand_scan_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_x,
                      CandArgs a) {
@@ -107,7 +113,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ CandShared sh;
   uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nkb = a.kpad / 64;
+  constexpr int kEl = FP8 ? 128 : 64;  // elements per 128-byte K block
+  const int nkb = a.kpad / kEl;
   const int64_t total = a.item_off[a.nlist];
 
   if (warp == 5) tmem_alloc(&sh.tmem, kAccN * kT);
@@ -145,8 +152,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             uint8_t* st = ring + static_cast<size_t>(s) * kStageBytes;
             mbar_arrive_expect_tx(&sh.full[s], kStageBytes);
-            tma_load_2d(st, &tmap_q, kb * 64, static_cast<int>(d.qrow0), &sh.full[s]);
-            tma_load_2d(st + kBlk, &tmap_x, kb * 64, static_cast<int>(d.row0 + static_cast<int64_t>(t) * kT),
+            tma_load_2d(st, &tmap_q, kb * kEl, static_cast<int>(d.qrow0), &sh.full[s]);
+            tma_load_2d(st + kBlk, &tmap_x, kb * kEl, static_cast<int>(d.row0 + static_cast<int64_t>(t) * kT),
                         &sh.full[s]);
           }
         }
@@ -158,7 +165,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 5) {
     if (lane == 0) {
-      const uint32_t idesc = idesc_bf16_f32(kT, kT);
+      const uint32_t idesc = FP8 ? idesc_e4m3_f32(kT, kT) : idesc_bf16_f32(kT, kT);
       const uint32_t rbase = smem_u32(ring);
       int64_t it = 0, tile = 0;
       bool ok = true;
@@ -180,9 +187,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_fence_after();
             const uint32_t sa = rbase + static_cast<uint32_t>(s) * kStageBytes;
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-              mma_bf16(tmem + static_cast<uint32_t>(b * kT), desc_sw128(sa + kk * 32u),
-                       desc_sw128(sa + kBlk + kk * 32u), idesc, (kb | kk) != 0 ? 1u : 0u);
+            for (int kk = 0; kk < 4; ++kk) {
+              if (FP8)
+                mma_e4m3(tmem + static_cast<uint32_t>(b * kT), desc_sw128(sa + kk * 32u),
+                         desc_sw128(sa + kBlk + kk * 32u), idesc, (kb | kk) != 0 ? 1u : 0u);
+              else
+                mma_bf16(tmem + static_cast<uint32_t>(b * kT), desc_sw128(sa + kk * 32u),
+                         desc_sw128(sa + kBlk + kk * 32u), idesc, (kb | kk) != 0 ? 1u : 0u);
+            }
             mma_commit(&sh.empty[s]);
           }
           if (!ok) break;
@@ -204,11 +216,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       const CandItem d = cand_item(a, item);
       // This thread's query (lane tid of the group) and its segment.
       int64_t sbase = 0, slen = 0;
+      float f = -2.0f;  // v = ||x||^2 + f * acc
       if (tid < d.qcnt) {
         const uint32_t e = static_cast<uint32_t>(a.list_q[d.qrow0 + tid]);
         const int64_t qp = static_cast<int64_t>(e >> 16) * a.P + (e & 0xffffu);
         sbase = a.seg[qp];
         slen = a.seg[qp + 1] - sbase;
+        if (FP8) f = -2.0f * a.qscale[e >> 16] * a.list_scale[d.list];
       }
       for (int t = 0; t < d.ntiles; ++t, ++tile) {
         const int b = static_cast<int>(tile % kAccN);
@@ -230,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           tmem_ld_wait();
 #pragma unroll
           for (int j = 0; j < 32; ++j)
-            r[j] = __float_as_uint(fmaf(-2.0f, __uint_as_float(r[j]), __shfl_sync(0xffffffffu, nrm[c], j)));
+            r[j] = __float_as_uint(fmaf(f, __uint_as_float(r[j]), __shfl_sync(0xffffffffu, nrm[c], j)));
           const int64_t o = rl0 + c * 32;
           if (o < slen) {
             float* out = a.cand + sbase + o;
@@ -285,6 +299,83 @@ __global__ void gather_queries_kernel(const float* __restrict__ q, int dpad, int
       ow[j] = *reinterpret_cast<uint32_t*>(&p);
     }
     *reinterpret_cast<uint4*>(G + e * kpad + c) = o;
+  }
+}
+
+// 16 floats (times `inv`) -> 16 E4M3 bytes, saturating to +-448.
+__device__ __forceinline__ uint4 to_e4m3x16(const float* x, float inv) {
+  uint32_t w[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const __nv_fp8x2_storage_t lo =
+        __nv_cvt_float2_to_fp8x2(make_float2(x[4 * j] * inv, x[4 * j + 1] * inv), __NV_SATFINITE, __NV_E4M3);
+    const __nv_fp8x2_storage_t hi =
+        __nv_cvt_float2_to_fp8x2(make_float2(x[4 * j + 2] * inv, x[4 * j + 3] * inv), __NV_SATFINITE, __NV_E4M3);
+    w[j] = static_cast<uint32_t>(lo) | (static_cast<uint32_t>(hi) << 16);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// FP8 copy of the codes, one CTA per list: the list's scale s_l = max |x| /
+// 448 (E4M3's largest finite value), then every row as E4M3(x / s_l), kpad8
+// bytes (columns past dpad zero).
+__global__ void list_fp8_kernel(const float* __restrict__ codes, const int64_t* __restrict__ list_off, int dpad,
+                                int kpad8, uint8_t* __restrict__ out, float* __restrict__ scale) {
+  __shared__ float s_max[32];
+  const int l = blockIdx.x;
+  const int64_t r0 = list_off[l], r1 = list_off[l + 1];
+  float m = 0.0f;
+  for (int64_t i = r0 * dpad + threadIdx.x; i < r1 * dpad; i += blockDim.x) m = fmaxf(m, fabsf(codes[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? s_max[threadIdx.x] : 0.0f;
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) s_max[0] = m;
+  }
+  __syncthreads();
+  const float mx = s_max[0];
+  const float inv = mx > 0.0f ? 448.0f / mx : 1.0f;
+  if (threadIdx.x == 0) scale[l] = 1.0f / inv;
+  const int cpr = kpad8 / 16;
+  for (int64_t u = threadIdx.x; u < (r1 - r0) * cpr; u += blockDim.x) {
+    const int64_t r = r0 + u / cpr;
+    const int c = static_cast<int>(u % cpr) * 16;
+    float x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = c + j < dpad ? codes[r * dpad + c + j] : 0.0f;
+    *reinterpret_cast<uint4*>(out + r * kpad8 + c) = to_e4m3x16(x, inv);
+  }
+}
+
+// Per query s_q = max |q| / 448 (one warp per query).
+__global__ void query_fp8_scale_kernel(const float* __restrict__ q, int nq, int dpad, float* __restrict__ qscale) {
+  const int lane = threadIdx.x & 31;
+  const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (qi >= nq) return;
+  float m = 0.0f;
+  for (int c = lane; c < dpad; c += 32) m = fmaxf(m, fabsf(q[static_cast<size_t>(qi) * dpad + c]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) qscale[qi] = m > 0.0f ? m / 448.0f : 1.0f;
+}
+
+// Row e of the gathered FP8 matrix = E4M3(q / s_q) of list-major entry e.
+__global__ void gather_queries_fp8_kernel(const float* __restrict__ q, int dpad, int kpad8,
+                                          const int32_t* __restrict__ list_q, const int64_t* __restrict__ n_entries,
+                                          int64_t max_rows, const float* __restrict__ qscale, uint8_t* __restrict__ G) {
+  const int64_t rows = min(*n_entries, max_rows);
+  const int per_row = kpad8 / 16;
+  for (int64_t u = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; u < rows * per_row;
+       u += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t e = u / per_row;
+    const int c = static_cast<int>(u - e * per_row) * 16;
+    const int qi = static_cast<int>(static_cast<uint32_t>(list_q[e]) >> 16);
+    const float* src = q + static_cast<int64_t>(qi) * dpad;
+    float x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = c + j < dpad ? src[c + j] : 0.0f;
+    *reinterpret_cast<uint4*>(G + e * kpad8 + c) = to_e4m3x16(x, 1.0f / qscale[qi]);
   }
 }
 
@@ -581,14 +672,65 @@ void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* li
 }
 
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st) {
-  HB_CHECK(a.kpad >= 64 && a.kpad % 64 == 0, HB_ERR_INVALID, "the candidate scan needs kpad a multiple of 64");
+  const int blk = a.fp8 ? 128 : 64;
+  HB_CHECK(a.kpad >= blk && a.kpad % blk == 0, HB_ERR_INVALID, "the candidate scan needs whole 128-byte K blocks");
+  HB_CHECK(!a.fp8 || (a.qscale && a.list_scale), HB_ERR_INVALID, "FP8 scan without scales");
   HB_CHECK(a.chunk_rows >= kT && a.chunk_rows % kT == 0, HB_ERR_INVALID, "chunk rows must be a multiple of 128");
   const size_t smem = kStg * static_cast<size_t>(kStageBytes) + 1024;
-  HB_CUDA(cudaFuncSetAttribute(cand_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const CUtensorMap* mq = static_cast<const CUtensorMap*>(tmap_q);
   const CUtensorMap* mx = static_cast<const CUtensorMap*>(tmap_x);
-  cand_scan_kernel<<<num_sms, kThreads, smem, st>>>(*mq, *mx, a);
+  if (a.fp8) {
+    HB_CUDA(cudaFuncSetAttribute(cand_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    cand_scan_kernel<true><<<num_sms, kThreads, smem, st>>>(*mq, *mx, a);
+  } else {
+    HB_CUDA(cudaFuncSetAttribute(cand_scan_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    cand_scan_kernel<false><<<num_sms, kThreads, smem, st>>>(*mq, *mx, a);
+  }
   HB_CUDA(cudaGetLastError());
+}
+
+void launch_fp8_codes(const float* codes, const int64_t* list_off, int nlist, int dpad, int kpad8, void* out,
+                      float* scale, cudaStream_t st) {
+  if (nlist <= 0) return;
+  HB_CHECK(kpad8 % 128 == 0 && dpad <= kpad8, HB_ERR_INVALID, "bad FP8 row length");
+  list_fp8_kernel<<<nlist, 256, 0, st>>>(codes, list_off, dpad, kpad8, static_cast<uint8_t*>(out), scale);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_query_fp8_scales(const float* q, int nq, int dpad, float* qscale, cudaStream_t st) {
+  if (nq <= 0) return;
+  query_fp8_scale_kernel<<<(nq + 7) / 8, 256, 0, st>>>(q, nq, dpad, qscale);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_gather_queries_fp8(const float* q, int dpad, int kpad8, const int32_t* list_q, const int64_t* n_entries,
+                               int64_t max_rows, const float* qscale, void* G, cudaStream_t st) {
+  if (max_rows <= 0) return;
+  HB_CHECK(kpad8 % 128 == 0 && dpad <= kpad8, HB_ERR_INVALID, "bad FP8 query padding");
+  int64_t g = (max_rows * (kpad8 / 16) + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  gather_queries_fp8_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(q, dpad, kpad8, list_q, n_entries, max_rows,
+                                                                      qscale, static_cast<uint8_t*>(G));
+  HB_CUDA(cudaGetLastError());
+}
+
+void make_u8_tensor_map(void* tmap_out, const void* base, size_t rows, int row_bytes) {
+  CUtensorMap* m = static_cast<CUtensorMap*>(tmap_out);
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(row_bytes), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(row_bytes)};
+  cuuint32_t box[2] = {128, kT};
+  cuuint32_t es[2] = {1, 1};
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult qr;
+  HB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr));
+  HB_CHECK(fn && qr == cudaDriverEntryPointSuccess, HB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  CUresult r = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn)(
+      m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, es,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  HB_CHECK(r == CUDA_SUCCESS, HB_ERR_CUDA, "cuTensorMapEncodeTiled failed (FP8)");
 }
 
 void launch_cand_select(const float* cand, const int64_t* seg, const int32_t* probes, int nq, int P, int R,

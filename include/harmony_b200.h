@@ -55,8 +55,12 @@ enum {
 };
 
 /* Arithmetic of the list scan. FP32 reproduces the reference's distances
- * bit for bit; BF16 / FP8 scan on tensor cores and re-rank the widened
- * candidate set in exact FP32. */
+ * bit for bit; BF16 / FP8 scan on tensor cores and re-rank a widened
+ * candidate set in exact FP32.  BF16 with d <= 128 and k <= 256 re-ranks every
+ * row within its proven error bound, so its result equals FP32's; FP8 (E4M3
+ * with per-list and per-query scales, the candidate-matrix scan) re-ranks
+ * rerank_mult * k candidates, and its agreement with FP32 is measured, not
+ * guaranteed. */
 enum { HB_PREC_FP32 = 0, HB_PREC_BF16 = 1, HB_PREC_FP8 = 2 };
 
 /* Search options: the fields of Index::Param that steer search
@@ -72,8 +76,8 @@ typedef struct {
   int32_t warmup_lists;       /* preSearch warmUpSearchList (default 10)        */
   int32_t warmup_list_size;   /* preSearch warmUpSearchListSize (0 -> k)        */
   int32_t precision;          /* HB_PREC_*                                     */
-  int32_t rerank_mult;        /* BF16 with d > 128 or k > 256 (the candidate-matrix
-                                 scan): candidates re-ranked = rerank_mult * k, at
+  int32_t rerank_mult;        /* FP8, and BF16 with d > 128 or k > 256 (the candidate-
+                                 matrix scan): candidates re-ranked = rerank_mult * k, at
                                  most 4096, k itself up to 4096 (default 2).  For
                                  d <= 128 and k <= 256 the re-ranked set is every row
                                  within the scan's error bound of the k-th, and the

@@ -185,3 +185,40 @@ def test_dense_bin_takes_the_radix_fallback(restated):
         De, Ie = search(ix, q, k, precision=Precision.FP32)
         assert_topk_parity(D, I, De, Ie, lambda qi, i: restated.l2(q[qi], base[i]), f"dense bin k={k}")
         assert (I < 3000).all()  # all from the identical rows
+
+
+@pytest.mark.parametrize("k,mult", [(10, 8), (100, 4)])
+def test_fp8_variant_on_wide_data(wide, restated, k, mult):
+    """FP8 E4M3 tiles (per-list and per-query scales) on the candidate-matrix
+    scan: the re-rank is exact, so every returned distance is its id's exact
+    distance and no result beats the exact scan; the ids agree with the exact
+    scan's at a measured rate (FP8's 3 mantissa bits are not covered by a
+    proof)."""
+    base, q, ix = wide
+    ix.nprobe = 8
+    D, I = search(ix, q, k, precision=Precision.FP8, mult=mult)
+    De, Ie = search(ix, q, k, precision=Precision.FP32)
+    for qi in range(0, q.shape[0], 31):
+        for j in range(0, k, max(1, k // 10)):
+            if I[qi, j] >= 0:
+                assert D[qi, j] == restated.l2(q[qi], base[I[qi, j]])
+    assert (D[:, -1] >= De[:, -1]).all()
+    assert (np.diff(D, axis=1) >= 0).all()
+    agree = np.mean([len(set(a) & set(b)) / k for a, b in zip(I, Ie)])
+    assert agree >= 0.95, agree
+
+
+def test_fp8_d128_graph_and_repeat(restated):
+    base, q = datasets.config2(seed=77, nb=60_000, nq=200, ncomp=200)
+    ix = Index(128, 128, 8)
+    ix.train(base.shape[0], base)
+    ix.add(base.shape[0], base)
+    ix.preSearch(0, 0, 0, 0, 0, Index.Param(mode=SearchMode.ORIGINAL), "")
+    D1, I1 = search(ix, q, 10, precision=Precision.FP8, mult=4)
+    D2, I2 = search(ix, q, 10, precision=Precision.FP8, mult=4)
+    assert np.array_equal(D1, D2) and np.array_equal(I1, I2)
+    Dg, Ig = search(ix, q[:64], 10, precision=Precision.FP8, mult=4, graph=True)
+    assert np.array_equal(Dg, D1[:64]) and np.array_equal(Ig, I1[:64])
+    De, Ie = search(ix, q, 10, precision=Precision.FP32)
+    assert (D1[:, -1] >= De[:, -1]).all()
+    assert np.mean([len(set(a) & set(b)) / 10 for a, b in zip(I1, Ie)]) >= 0.95

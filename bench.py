@@ -704,8 +704,9 @@ def run_c4(args):
 def run_c3(args):
     """Config 3: 270k x 500 anisotropic mixture (per-dimension variance
     proportional to (j + 1)^-1.2), nlist 512, nprobe 32, k 100, 5000 queries.
-    Arms: the exact FP32 scan and the BF16 candidate-matrix scan with the exact
-    FP32 re-rank of the 2k (rerank_mult 2) and 4k best.  Each arm is timed with
+    Arms: the exact FP32 scan, the BF16 candidate-matrix scan with the exact
+    FP32 re-rank of the 2k (rerank_mult 2) and 4k best, and the FP8 E4M3
+    variant (per-list and per-query scales) re-ranking the 4k and 8k best.  Each arm is timed with
     queries and results resident on the device (CUDA events on the index
     stream) and end to end (pinned host queries and results, wall clock around
     the synchronous calls).  Recall@100 and the largest relative distance error
@@ -747,7 +748,8 @@ def run_c3(args):
     stream = torch.cuda.ExternalStream(ix.stream)
     arms, ref = {}, None
     for name, prec, mult in (("fp32", Precision.FP32, 2), ("bf16_rerank2k", Precision.BF16, 2),
-                             ("bf16_rerank4k", Precision.BF16, 4)):
+                             ("bf16_rerank4k", Precision.BF16, 4), ("fp8_rerank4k", Precision.FP8, 4),
+                             ("fp8_rerank8k", Precision.FP8, 8)):
         sp = ix.search_params
         sp.precision, sp.rerank_mult = prec, mult
         reps = 3 if prec == Precision.FP32 else 10

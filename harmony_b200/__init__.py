@@ -152,6 +152,9 @@ def lib() -> ctypes.CDLL:
     L.hb_device_allocations.argtypes = []
     L.hb_selftest_bounded_wait.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     L.hb_set_wait_budget.argtypes = [vp, ctypes.c_int64]
+    L.hb_set_autotune.argtypes = [vp, ctypes.c_int]
+    L.hb_autotune_table.argtypes = [vp, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
+    L.hb_set_autotune_table.argtypes = [vp, ctypes.c_char_p]
     L.hb_bf16_fallbacks.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.hb_train_probe_predictor.argtypes = [vp, sz, f, sz, sz, ctypes.c_float]
     L.hb_search_noalloc.argtypes = [vp, sz, f, sz, f, i64]
@@ -487,6 +490,22 @@ class Index:
         n = ctypes.c_int64()
         _check(self._L.hb_bf16_fallbacks(self._h, ctypes.byref(n)))
         return int(n.value)
+
+    def set_autotune(self, on: bool = True) -> None:
+        """Time the bounded BF16 scan's chunk length and ring depth on the first
+        search of each (batch, nprobe, k) bucket and keep the fastest."""
+        _check(self._L.hb_set_autotune(self._h, int(on)))
+
+    def autotune_table(self) -> str:
+        """The tuned choices as text (one line per bucket)."""
+        need = ctypes.c_size_t()
+        _check(self._L.hb_autotune_table(self._h, None, 0, ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(max(1, need.value))
+        _check(self._L.hb_autotune_table(self._h, buf, len(buf), None))
+        return buf.value.decode()
+
+    def set_autotune_table(self, text: str) -> None:
+        _check(self._L.hb_set_autotune_table(self._h, text.encode()))
 
     def set_wait_budget(self, cycles: int = 0) -> None:
         """Clock cycles a device wait of the BF16 scan spends before giving up

@@ -26,6 +26,7 @@
 #include <numeric>
 #include <random>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "hb_internal.hpp"
@@ -1343,13 +1344,31 @@ class IndexCore {
     over_list_.reserve(nb);
     over_n_.reserve(1);
     cbuf_.reserve(static_cast<size_t>(nb) * cap);
+    const int cr0 = std::max(128, chunk_rows_for(nb, P, 128));
+    const int s0 = scan_bf16_stages(kpad_);
+    const TuneKey key = tune_key(nb, P, k);
+    if (autotune_ && !capturing_ && !tune_.count(key)) autotune(nb, P, k, cap, Dd, Id, key, cr0, s0);
+    const auto it = tune_.find(key);
+    const int cr = it != tune_.end() ? it->second.chunk_rows : cr0;
+    const int stages = it != tune_.end() ? it->second.stages : s0;
+    filter_pipeline(nb, P, k, cap, cr, stages, Dd, Id);
+    if (!capturing_) {
+      bf16_err_check();
+      fix_overflow(nb, P, k, Dd, Id);
+    }
+  }
+
+  // The bounded scan of one batch after the coarse probes: per-query prep,
+  // work description (chunks of cr rows), seed bounds, the scan with a ring
+  // of `stages` B tiles, and the exact re-rank.  Every (cr, stages) gives the
+  // same result.
+  void filter_pipeline(int nb, int P, int k, int cap, int cr, int stages, float* Dd, int64_t* Id) {
     HB_CUDA(cudaMemsetAsync(over_n_.p, 0, sizeof(int), st_));
     {
       Scope sc(this, "query_prep");
       launch_query_prep(qpad_.p, nb, static_cast<int>(d_), static_cast<int>(dpad_), kpad_, maxnorm_.p, qbf_.p, e2_.p,
                         thr_.p, ccnt_.p, st_);
     }
-    const int cr = std::max(128, chunk_rows_for(nb, P, 128));
     list_cnt_.reserve(nlist_);
     list_cursor_.reserve(nlist_);
     list_qoff_.reserve(nlist_ + 1);
@@ -1390,7 +1409,7 @@ class IndexCore {
     a.cap = cap;
     a.k = k;
     a.err = err_dev_.p;
-    a.stages = scan_bf16_stages(kpad_);
+    a.stages = stages;
     a.wait_budget = wait_budget_;
     {
       Scope sc(this, "scan_bf16");
@@ -1402,11 +1421,102 @@ class IndexCore {
                          Id, cflag_.p, over_list_.p, over_n_.p, num_sms_, st_);
     }
     launches_ += 8 + (cap > 256 ? 1 : 0);
-    if (!capturing_) {
-      bf16_err_check();
-      fix_overflow(nb, P, k, Dd, Id);
-    }
   }
+
+  // ---- autotuner of the bounded scan ----------------------------------------
+  // Per (batch-size bucket, nprobe bucket, k) the first search times the scan
+  // pipeline for chunk lengths around the default (x1/4 .. x4, 128 .. 4096
+  // rows) and ring depths 2..4, twice each, and keeps the fastest; later
+  // searches of the bucket use it.  The table can be read and written as text
+  // ("nb_bucket P_bucket k kpad chunk_rows stages best_ms default_ms" lines).
+  struct TuneKey {
+    int nb_bucket, p_bucket, k;
+    bool operator<(const TuneKey& o) const {
+      return std::tie(nb_bucket, p_bucket, k) < std::tie(o.nb_bucket, o.p_bucket, o.k);
+    }
+  };
+  struct TuneChoice {
+    int chunk_rows, stages;
+    float best_ms, default_ms;
+  };
+  static int pow2_bucket(int x) {
+    int b = 1;
+    while (b < x) b <<= 1;
+    return b;
+  }
+  TuneKey tune_key(int nb, int P, int k) const { return {pow2_bucket(nb), pow2_bucket(P), k}; }
+
+  void autotune(int nb, int P, int k, int cap, float* Dd, int64_t* Id, const TuneKey& key, int cr0, int s0) {
+    std::vector<int> crs;
+    for (int f : {-2, -1, 0, 1, 2}) {
+      int c = f < 0 ? cr0 >> (-f) : cr0 << f;
+      c = std::min(4096, std::max(128, c));
+      if (std::find(crs.begin(), crs.end(), c) == crs.end()) crs.push_back(c);
+    }
+    cudaEvent_t e0 = event(), e1 = event();
+    TuneChoice best{cr0, s0, 1e30f, 0.0f};
+    for (int S = 2; S <= 4; ++S) {
+      if (scan_bf16_smem_bytes(kpad_, S) > scan_bf16_smem_bytes(kpad_, s0) && S > s0) continue;
+      for (int c : crs) {
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+          HB_CUDA(cudaEventRecord(e0, st_));
+          filter_pipeline(nb, P, k, cap, c, S, Dd, Id);
+          HB_CUDA(cudaEventRecord(e1, st_));
+          HB_CUDA(cudaEventSynchronize(e1));
+          float t = 0.f;
+          HB_CUDA(cudaEventElapsedTime(&t, e0, e1));
+          ms = std::min(ms, t);
+        }
+        if (c == cr0 && S == s0) best.default_ms = ms;
+        if (ms < best.best_ms) {
+          best.best_ms = ms;
+          best.chunk_rows = c;
+          best.stages = S;
+        }
+      }
+    }
+    ev_pool_.push_back(e0);
+    ev_pool_.push_back(e1);
+    bf16_err_check();
+    tune_[key] = best;
+  }
+
+ public:
+  void set_autotune(bool on) { autotune_ = on; }
+  std::string autotune_table() const {
+    std::string out;
+    char line[160];
+    for (const auto& kv : tune_) {
+      std::snprintf(line, sizeof(line), "%d %d %d %d %d %d %.4f %.4f\n", kv.first.nb_bucket, kv.first.p_bucket,
+                    kv.first.k, kpad_, kv.second.chunk_rows, kv.second.stages, kv.second.best_ms,
+                    kv.second.default_ms);
+      out += line;
+    }
+    return out;
+  }
+  void set_autotune_table(const char* text) {
+    std::map<TuneKey, TuneChoice> t;
+    const char* p = text;
+    while (p && *p) {
+      TuneKey key{};
+      TuneChoice c{};
+      int kp = 0, used = 0;
+      if (std::sscanf(p, "%d %d %d %d %d %d %f %f%n", &key.nb_bucket, &key.p_bucket, &key.k, &kp, &c.chunk_rows,
+                      &c.stages, &c.best_ms, &c.default_ms, &used) != 8)
+        throw Error(HB_ERR_INVALID, "autotune table: expected 8 numbers per line");
+      HB_CHECK(c.chunk_rows >= 128 && c.chunk_rows <= 4096 && c.chunk_rows % 128 == 0 && c.stages >= 2 &&
+                   c.stages <= 4 && key.k >= 1,
+               HB_ERR_INVALID, "autotune table: value out of range");
+      if (kp == kpad_) t[key] = c;
+      p += used;
+      while (*p == '\n' || *p == ' ' || *p == '\r') ++p;
+    }
+    tune_ = t;
+  }
+
+ private:
+
 
   // Queries whose candidate buffer overflowed (listed by the re-rank, left
   // unwritten) are searched with the exact scan over their own probe rows,
@@ -1930,6 +2040,8 @@ class IndexCore {
   DevBuf<int32_t> op_;
   DevBuf<int64_t> oi_;
   long long wait_budget_ = kDefaultWaitBudget;
+  bool autotune_ = false;
+  std::map<TuneKey, TuneChoice> tune_;
   int last_overflow_ = 0;
   DevBuf<int32_t> kq_;
   DevBuf<uint16_t> codes_bf16_;
@@ -2160,6 +2272,30 @@ void* hb_stream(hb_index* ix) { return (ix && ix->core) ? static_cast<void*>(ix-
 uint64_t hb_launch_count(const hb_index* ix) { return (ix && ix->core) ? ix->core->launches() : 0; }
 
 uint64_t hb_device_allocations(void) { return hb::devbuf_generation().load(); }
+
+int hb_set_autotune(hb_index* ix, int on) {
+  HB_NEED_INDEX(ix);
+  ix->core->set_autotune(on != 0);
+  return HB_OK;
+}
+
+int hb_autotune_table(hb_index* ix, char* buf, size_t len, size_t* needed) {
+  HB_NEED_INDEX(ix);
+  return guarded([&] {
+    const std::string t = ix->core->autotune_table();
+    if (needed) *needed = t.size() + 1;
+    if (buf && len) {
+      std::strncpy(buf, t.c_str(), len - 1);
+      buf[len - 1] = 0;
+    }
+  });
+}
+
+int hb_set_autotune_table(hb_index* ix, const char* text) {
+  HB_NEED_INDEX(ix);
+  if (!text) return HB_ERR_INVALID;
+  return guarded([&] { ix->core->set_autotune_table(text); });
+}
 
 int hb_set_wait_budget(hb_index* ix, int64_t cycles) {
   HB_NEED_INDEX(ix);

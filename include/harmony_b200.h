@@ -205,6 +205,20 @@ uint64_t hb_launch_count(const hb_index* ix);
  * caller check that a call allocated nothing. */
 uint64_t hb_device_allocations(void);
 
+/* Autotuner of the bounded BF16 scan (no reference counterpart).  With
+ * hb_set_autotune(ix, 1) the first BF16 search of each (batch size rounded up
+ * to a power of two, nprobe rounded up likewise, k) times the scan for chunk
+ * lengths of 1/4 to 4 times the default (128 to 4096 rows) and ring depths of
+ * 2 to 4 tiles, twice each, and keeps the fastest for later searches of that
+ * bucket (every choice gives the same results).  hb_autotune_table writes the
+ * table as text, one line "nb_bucket nprobe_bucket k kpad chunk_rows stages
+ * best_ms default_ms" per bucket (*needed = bytes including the terminating
+ * zero); hb_set_autotune_table replaces it with such text (lines for another
+ * kpad are dropped), so a tuned table can be saved and reloaded. */
+int hb_set_autotune(hb_index* ix, int on);
+int hb_autotune_table(hb_index* ix, char* buf, size_t len, size_t* needed);
+int hb_set_autotune_table(hb_index* ix, const char* text);
+
 /* Clock cycles a device-side wait of the BF16 scan spends before it gives
  * up (no reference counterpart; cycles <= 0 restores the default, 2e9).  A
  * wait that gives up makes the search return HB_ERR_CUDA with "gave up

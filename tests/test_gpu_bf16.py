@@ -178,3 +178,30 @@ def test_bf16_rejects_unsupported(fidx):
         search(ix, q[:4], 5000)  # k above the BF16 candidate capacity (4096)
     with pytest.raises(HarmonyError):
         search(ix, q[:4], 10, mode=SearchMode.DIVIDE_IVF)
+
+
+def test_bf16_autotune_picks_a_config_and_keeps_results(fidx):
+    """The autotuner times chunk lengths and ring depths on the first search of
+    a bucket; every choice gives the exact result, and the table written out
+    can be read back."""
+    base, q, ix = fidx
+    ix.nprobe = 16
+    exact = search(ix, q, 10, precision=Precision.FP32)
+    ix.set_autotune(True)
+    try:
+        assert_identical(search(ix, q, 10), exact, "tuning search")
+        assert_identical(search(ix, q, 10), exact, "tuned search")
+        table = ix.autotune_table()
+        rows = [list(map(float, line.split())) for line in table.strip().splitlines()]
+        assert len(rows) == 1
+        nb_b, p_b, k, kpad, cr, stages, best, dflt = rows[0]
+        assert (nb_b, p_b, k, kpad) == (1024, 16, 10, 128)
+        assert 128 <= cr <= 4096 and 2 <= stages <= 4 and 0 < best <= dflt
+        ix.set_autotune_table("1024 16 10 128 256 3 0.1 0.2\n")
+        assert ix.autotune_table().split()[4:6] == ["256", "3"]
+        assert_identical(search(ix, q, 10), exact, "loaded table")
+        with pytest.raises(HarmonyError):
+            ix.set_autotune_table("1024 16 10 128 100 3 0.1 0.2\n")  # not whole tiles
+    finally:
+        ix.set_autotune(False)
+        ix.set_autotune_table("")

@@ -272,6 +272,8 @@ def run_ours(args):
             outs[name] = (r.pop("D").cpu().numpy(), r.pop("I").cpu().numpy())
             r.update({"nprobe": P, "recall_at_10": recall(outs[name][1], gt, k),
                       "qps": world * nq / (r["ms_per_step"] / 1e3)})
+            if prec == Precision.BF16:
+                r["bounded_scan"] = ix.bf16_stats()
             arms[name] = r
         # Learned nprobe + BF16: raise the predictor's target until the test
         # recall against the FP64 ground truth reaches the bench target.
@@ -287,6 +289,7 @@ def run_ours(args):
         tgt = min(tgt, 0.9999)
         r = time_arm(torch, ix, test, k, 256, Precision.BF16, args.steps, args.warmup, world, dist, learned=True,
                      target=tgt, tag="learned_bf16")
+        r["bounded_scan"] = ix.bf16_stats()
         outs["learned_bf16"] = (r.pop("D").cpu().numpy(), r.pop("I").cpu().numpy())
         r.update({"nprobe": "learned", "predictor_target": round(tgt, 4),
                   "recall_at_10": recall(outs["learned_bf16"][1], gt, k),
@@ -445,6 +448,7 @@ def run_ours(args):
                            "scan_bytes_alg_gbs": round(fp_bytes_alg / fp_scan / 1e9, 1) if fp_scan else None,
                            "roofline": fp_roof},
             "bf16_fixed_nprobe": {"qps": round(arms["bf16"]["qps"], 1), "nprobe": arms["bf16"]["nprobe"],
+                                  "bounded_scan": arms["bf16"].get("bounded_scan"),
                                   "recall_at_10": round(arms["bf16"]["recall_at_10"], 4),
                                   "ms_per_step": round(arms["bf16"]["ms_per_step"], 3),
                                   "kernel_ms_per_step": {n: round(v, 4) for n, v in arms["bf16"]["kernel_ms"].items()}},
@@ -455,6 +459,7 @@ def run_ours(args):
             "parity": parity,
             "roofline": roof,
             "kernel_ms_per_step": {n: round(v, 4) for n, v in kms.items()},
+            "bounded_scan": head.get("bounded_scan"),
             "gpu_launches": int(round(head["launches_per_step"] * args.steps)),
             "clocks": clocks,
         }
@@ -863,8 +868,11 @@ def run_c2(args):
                 kern = {kk: round(v[0], 4) for kk, v in ix.profile_read().items()}
                 ix.profile(False)
                 outs[name] = (D.cpu().numpy().copy(), I.cpu().numpy().copy())
+                stats = ix.bf16_stats() if prec == Precision.BF16 else None
                 arm = {"ms": round(ms, 3), "qps": round(nq / ms * 1e3, 1), "kernels_ms": kern,
                        "recall_at_100_first_1000": round(recall(outs[name][1][:ng], gt, k), 4)}
+                if stats:
+                    arm["bounded_scan"] = stats
                 scan = kern.get("scan_exact" if prec == Precision.FP32 else "scan_bf16")
                 if scan:
                     elem = 2 if prec == Precision.BF16 else 4

@@ -156,6 +156,7 @@ def lib() -> ctypes.CDLL:
     L.hb_autotune_table.argtypes = [vp, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
     L.hb_set_autotune_table.argtypes = [vp, ctypes.c_char_p]
     L.hb_bf16_fallbacks.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.hb_bf16_stats.argtypes = [vp, ctypes.c_void_p]
     L.hb_train_probe_predictor.argtypes = [vp, sz, f, sz, sz, ctypes.c_float]
     L.hb_search_noalloc.argtypes = [vp, sz, f, sz, f, i64]
     L.hb_retain_lists.argtypes = [vp, sz, sz]
@@ -490,6 +491,13 @@ class Index:
         n = ctypes.c_int64()
         _check(self._L.hb_bf16_fallbacks(self._h, ctypes.byref(n)))
         return int(n.value)
+
+    def bf16_stats(self) -> dict:
+        """Admission statistics of the latest bounded BF16 batch."""
+        st = np.zeros(5, np.int64)
+        _check(self._L.hb_bf16_stats(self._h, st.ctypes.data))
+        return {"queries": int(st[0]), "overflows": int(st[1]), "admitted": int(st[2]),
+                "admitted_max": int(st[3]), "reranked": int(st[4])}
 
     def set_autotune(self, on: bool = True) -> None:
         """Time the bounded BF16 scan's chunk length and ring depth on the first

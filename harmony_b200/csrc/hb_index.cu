@@ -555,6 +555,28 @@ class IndexCore {
 
   void set_wait_budget(long long cycles) { wait_budget_ = cycles > 0 ? cycles : kDefaultWaitBudget; }
   int last_overflow() const { return last_overflow_; }
+  // Admission statistics of the latest bounded BF16 batch: queries,
+  // overflows, rows admitted (total, largest per query), rows re-ranked.
+  void bf16_stats(int64_t* out) {
+    HB_CUDA(cudaSetDevice(device_));
+    std::vector<int> cnt(last_nb_), m(last_nb_);
+    if (last_nb_) {
+      HB_CUDA(cudaMemcpyAsync(cnt.data(), ccnt_.p, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, st_));
+      HB_CUDA(cudaMemcpyAsync(m.data(), rr_m_.p, m.size() * sizeof(int), cudaMemcpyDeviceToHost, st_));
+      HB_CUDA(cudaStreamSynchronize(st_));
+    }
+    int64_t tot = 0, mx = 0, mt = 0;
+    for (int i = 0; i < last_nb_; ++i) {
+      tot += cnt[i];
+      mx = std::max<int64_t>(mx, cnt[i]);
+      mt += m[i];
+    }
+    out[0] = last_nb_;
+    out[1] = last_overflow_;
+    out[2] = tot;
+    out[3] = mx;
+    out[4] = mt;
+  }
 
   void set_coarse(int kind, int margin) {
     HB_CHECK(kind >= HB_COARSE_AUTO && kind <= HB_COARSE_TENSOR, HB_ERR_INVALID, "unknown coarse quantizer kind");
@@ -1311,11 +1333,11 @@ class IndexCore {
   }
 
   // Candidate buffer per query of the bounded BF16 scan: room for 16 k
-  // candidates (at least 1024), rounded up to a power of two (the re-rank
+  // candidates (at least 2048), rounded up to a power of two (the re-rank
   // sorts a buffer in place); a query needing more is searched again with the
   // exact scan.
   static int filter_cap(size_t k) {
-    size_t c = 1024;
+    size_t c = 2048;
     while (c < 16 * k) c <<= 1;
     return static_cast<int>(std::min<size_t>(kRerankMaxCap, c));
   }
@@ -1341,7 +1363,9 @@ class IndexCore {
     thr_.reserve(nb);
     ccnt_.reserve(nb);
     cflag_.reserve(nb);
+    rr_m_.reserve(nb);
     over_list_.reserve(nb);
+    last_nb_ = nb;
     over_n_.reserve(1);
     cbuf_.reserve(static_cast<size_t>(nb) * cap);
     const int cr0 = std::max(128, chunk_rows_for(nb, P, 128));
@@ -1418,7 +1442,7 @@ class IndexCore {
     {
       Scope sc(this, "rerank");
       launch_rerank_bf16(cbuf_.p, ccnt_.p, cap, e2_.p, nb, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd,
-                         Id, cflag_.p, over_list_.p, over_n_.p, num_sms_, st_);
+                         Id, cflag_.p, over_list_.p, over_n_.p, rr_m_.p, num_sms_, st_);
     }
     launches_ += 8 + (cap > 256 ? 1 : 0);
   }
@@ -2034,7 +2058,8 @@ class IndexCore {
   DevBuf<uint16_t> qbf_;
   DevBuf<float> e2_;
   DevBuf<uint32_t> thr_;
-  DevBuf<int> ccnt_, cflag_, over_list_, over_n_;
+  DevBuf<int> ccnt_, cflag_, over_list_, over_n_, rr_m_;
+  int last_nb_ = 0;
   DevBuf<uint64_t> cbuf_;
   DevBuf<float> oq_, od_;
   DevBuf<int32_t> op_;
@@ -2301,6 +2326,12 @@ int hb_set_wait_budget(hb_index* ix, int64_t cycles) {
   HB_NEED_INDEX(ix);
   ix->core->set_wait_budget(cycles);
   return HB_OK;
+}
+
+int hb_bf16_stats(hb_index* ix, int64_t* stats) {
+  HB_NEED_INDEX(ix);
+  if (!stats) return HB_ERR_INVALID;
+  return guarded([&] { ix->core->bf16_stats(stats); });
 }
 
 int hb_bf16_fallbacks(hb_index* ix, int64_t* n) {

@@ -219,10 +219,11 @@ void launch_seed_bound(const void* qbf, int nq, int kpad, const void* codes_bf16
                        const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int k,
                        const float* e2, uint32_t* thr, cudaStream_t st, const int32_t* probes = nullptr, int P = 0);
 // Exact re-rank of the admitted rows under W_k + 2 eps; flag[q] = 2 and
-// over_list / over_n for queries whose buffer overflowed (left unwritten).
+// over_list / over_n for queries whose buffer overflowed (left unwritten);
+// m_out[q] = rows re-ranked.
 void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
-                        int* flag, int* over_list, int* over_n, int num_sms, cudaStream_t st);
+                        int* flag, int* over_list, int* over_n, int* m_out, int num_sms, cudaStream_t st);
 
 // Candidate-matrix BF16 scan (k_cand.cu): any kpad (a multiple of 64) and up
 // to kCandMaxR candidates per query.

@@ -715,7 +715,10 @@ size_t scan_x2_smem(int tv, int qt, int dpad, int cap) {
   return (2 * static_cast<size_t>(tv) * (dpad + 4) + static_cast<size_t>(qg) * dpad) * 4 +
          static_cast<size_t>(qg) * cap * 8 + static_cast<size_t>(qg) * 3 * 4;
 }
-bool use_x2(int dpad, int mode) { return mode == SCAN_PLAIN && dpad <= 256; }
+// The packed kernel is used only where its arithmetic has been checked to
+// equal the scalar sequential sum bit for bit (kPackedExact).
+constexpr bool kPackedExact = false;
+bool use_x2(int dpad, int mode) { return kPackedExact && mode == SCAN_PLAIN && dpad <= 256; }
 }  // namespace
 
 size_t scan_exact_smem_bytes(int d, int dpad, int k, int mode, int* tv, int* qt, int* qgroup) {

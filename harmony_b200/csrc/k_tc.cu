@@ -86,6 +86,7 @@ constexpr int kMaxStages = 4;
 constexpr int kAcc = 2 * kGroups;                  // TMEM accumulators of 128 columns
 constexpr size_t kSmemCap = 225 * 1024;            // dynamic shared memory budget
 constexpr int kTightK = 16;                        // largest k whose bound tightens during the scan
+constexpr int kStage = 8;                          // admitted keys staged per epilogue thread before a flush
 
 struct ItemDesc {
   int list, chunk, group, qcnt, ntiles;  // ntiles < 0: no more work
@@ -153,6 +154,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   int* meta_q = reinterpret_cast<int*>(nrm + kAcc * kTile);                 // [2][128]
   float* meta_thr = reinterpret_cast<float*>(meta_q + 2 * kTile);           // [2][128]
   float* meta_e2 = meta_thr + 2 * kTile;                                    // [2][128]
+  uint64_t* staging = reinterpret_cast<uint64_t*>(meta_e2 + 2 * kTile);     // [kGroups][kStage][128]
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -343,12 +345,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       for (int i = 0; i < KB; ++i) best[i] = INFINITY;
       int seen = 0;
       uint64_t* cbuf = a.cand + static_cast<size_t>(my_q < 0 ? 0 : my_q) * a.cap;
+      // Admitted keys wait here (stride kEpiThreads: conflict-free) and go to
+      // the query's buffer kStage at a time, one atomicAdd per flush.
+      uint64_t* stg = staging + static_cast<size_t>(grp) * kStage * kEpiThreads + etid;
+      int ns = 0;
+      auto flush = [&]() {
+        const int base = atomicAdd(a.cand_cnt + my_q, ns);
+        for (int i = 0; i < ns; ++i)
+          if (base + i < a.cap) cbuf[base + i] = stg[i * kEpiThreads];
+        ns = 0;
+      };
       for (int t = static_cast<int>((static_cast<uint32_t>(grp) ^ G) & 1u); t < d.ntiles; t += kGroups, ++e_cnt) {
         const int b = 2 * grp + static_cast<int>(e_cnt & 1u);
         const uint32_t par = (e_cnt >> 1) & 1u;
+        // The query's bound as other threads have lowered it (read while the
+        // tile is still on the tensor cores).
+        const uint32_t g_thr = my_q >= 0 ? *reinterpret_cast<volatile uint32_t*>(a.thr + my_q) : 0u;
         ok = ok && mbar_wait(&sh.accf[b], par, err, 14, budget) && mbar_wait(&sh.normf[b], par, err, 15, budget);
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
+        if (my_q >= 0) thr = fminf(thr, ordered_to_float(g_thr));
         const float* nb = nrm + b * kTile;
         const uint32_t pos_t = static_cast<uint32_t>(d.row0 + t * kTile);
 #pragma unroll 1
@@ -397,9 +413,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
                 for (int i = 0; i < 2; ++i) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
                 const float wv = __uint_as_float((j & 16) ? t2[1] : t2[0]);
-                const int slot = atomicAdd(a.cand_cnt + my_q, 1);
-                if (slot < a.cap)
-                  cbuf[slot] = (static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j));
+                stg[ns * kEpiThreads] = (static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j));
+                if (++ns == kStage) flush();
                 if (KT > 0) {
                   // Insert into the ascending KT smallest; once k values are
                   // in, the k-th + 2 eps bounds W_k + 2 eps from above.
@@ -414,7 +429,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     float kth = best[0];
 #pragma unroll
                     for (int i = 1; i < KB; ++i) kth = (i == a.k - 1) ? best[i] : kth;
-                    thr = fminf(thr, __fadd_ru(kth, e2));
+                    const float nt = __fadd_ru(kth, e2);
+                    if (nt < thr) {
+                      thr = nt;
+                      atomicMin(a.thr + my_q, ordered_bits(thr));  // shared at once (no return value used)
+                    }
                   }
                 }
               }
@@ -424,8 +443,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tc_fence_before();
         mbar_arrive(&sh.acce[b]);
       }
-      // Share a lowered bound with the items still to come.
-      if (KT > 0 && my_q >= 0 && thr < thr0) atomicMin(a.thr + my_q, ordered_bits(thr));
+      if (my_q >= 0 && ns > 0) flush();
       if (!ok) break;
       G += static_cast<uint32_t>(d.ntiles);
     }
@@ -482,7 +500,7 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
     const uint64_t* __restrict__ cand, const int* __restrict__ cnt, int cap, const float* __restrict__ e2, int nq, int k,
     const float* __restrict__ codes, const float* __restrict__ q, int dpad, const int64_t* __restrict__ ids,
     float* __restrict__ D, int64_t* __restrict__ I, int* __restrict__ flag, int* __restrict__ over_list,
-    int* __restrict__ over_n) {
+    int* __restrict__ over_n, int* __restrict__ m_out) {
   __shared__ uint64_t s_c[kRrWarps][kRrWarpCap];
   __shared__ uint64_t s_x[kRrWarps][kRrWarpCap];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -519,6 +537,7 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
       m += __popc(__ballot_sync(0xffffffffu, in));
     }
   }
+  if (lane == 0) m_out[qi] = m;
   const float* qrow = q + static_cast<size_t>(qi) * dpad;
   const int e2n = pow2_ceil(m < 2 ? 2 : m);
   for (int j = lane; j < e2n; j += 32) {
@@ -546,7 +565,8 @@ __global__ void __launch_bounds__(256) rerank_cta_kernel(const uint64_t* __restr
                                                          int cap, const float* __restrict__ e2, int nq, int k,
                                                          const float* __restrict__ codes, const float* __restrict__ q,
                                                          int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
-                                                         int64_t* __restrict__ I, const int* __restrict__ flag) {
+                                                         int64_t* __restrict__ I, const int* __restrict__ flag,
+                                                         int* __restrict__ m_out) {
   extern __shared__ uint64_t s_dyn[];  // [cap] candidates, then [cap] exact keys
   __shared__ SelectShared sh_sel;
   __shared__ int s_m;
@@ -566,6 +586,7 @@ __global__ void __launch_bounds__(256) rerank_cta_kernel(const uint64_t* __restr
       int m = k;
       while (m < c && static_cast<uint32_t>(buf[m] >> 32) <= lim_bits) ++m;
       s_m = m;
+      m_out[qi] = m;
     }
     __syncthreads();
     const int m = s_m;
@@ -763,7 +784,8 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 size_t scan_bf16_smem_bytes(int kpad, int stages) {
   const size_t tile = static_cast<size_t>(kpad / 64) * kTile * 128;
-  return 1024 + tile * (2 + stages) + static_cast<size_t>(kAcc) * kTile * 4 + 2 * kTile * (4 + 4 + 4);
+  return 1024 + tile * (2 + stages) + static_cast<size_t>(kAcc) * kTile * 4 + 2 * kTile * (4 + 4 + 4) +
+         static_cast<size_t>(kGroups) * kStage * kEpiThreads * 8;
 }
 
 int scan_bf16_stages(int kpad) {
@@ -838,19 +860,20 @@ void launch_seed_bound(const void* qbf, int nq, int kpad, const void* codes_bf16
 
 void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
-                        int* flag, int* over_list, int* over_n, int num_sms, cudaStream_t st) {
+                        int* flag, int* over_list, int* over_n, int* m_out, int num_sms, cudaStream_t st) {
   if (nq <= 0) return;
   HB_CHECK(k >= 1 && cap >= k && cap <= kRerankMaxCap && (cap & (cap - 1)) == 0, HB_ERR_INVALID,
            "candidate buffer size out of range");
   rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(cand, cnt, cap, e2, nq, k, codes, q,
-                                                                               dpad, ids, D, I, flag, over_list, over_n);
+                                                                               dpad, ids, D, I, flag, over_list, over_n,
+                                                                               m_out);
   HB_CUDA(cudaGetLastError());
   if (cap > kRrWarpCap) {
     const size_t smem = static_cast<size_t>(2) * cap * sizeof(uint64_t);
     HB_CUDA(cudaFuncSetAttribute(rerank_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     const int grid = std::min(nq, 4 * num_sms);
-    rerank_cta_kernel<<<grid, 256, smem, st>>>(cand, cnt, cap, e2, nq, k, codes, q, dpad, ids, D, I, flag);
+    rerank_cta_kernel<<<grid, 256, smem, st>>>(cand, cnt, cap, e2, nq, k, codes, q, dpad, ids, D, I, flag, m_out);
     HB_CUDA(cudaGetLastError());
   }
 }

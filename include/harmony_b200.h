@@ -230,6 +230,12 @@ int hb_set_wait_budget(hb_index* ix, int64_t cycles);
  * FP32 scan (no reference counterpart). */
 int hb_bf16_fallbacks(hb_index* ix, int64_t* n);
 
+/* Admission statistics of the latest bounded BF16 batch (no reference
+ * counterpart): stats[0] queries, [1] overflows (searched exactly), [2] rows
+ * admitted over all queries, [3] the most any query admitted, [4] rows
+ * re-ranked exactly over all queries. */
+int hb_bf16_stats(hb_index* ix, int64_t* stats);
+
 /* Self-test of the device-side bounded waits (no reference counterpart).
  * Every mbarrier wait in the tensor-core kernels gives up after a clock
  * budget, records an error code in a device flag and lets its kernel return,

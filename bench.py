@@ -994,6 +994,7 @@ def main():
     ap.add_argument("--ref-step-seconds", type=float, default=6.0)
     ap.add_argument("--nb", type=int, default=None, help="smaller base for profiling runs (not a bench line)")
     ap.add_argument("--nq", type=int, default=None, help="fewer queries for profiling runs (not a bench line)")
+    ap.add_argument("--nlist", type=int, default=None, help="other nlist for profiling runs (not a bench line)")
     ap.add_argument("--ntrain", type=int, default=200_000, help="training queries of the learned probe")
     ap.add_argument("--freeze-to", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["c5", "c4", "c3", "c2", "c5-batches"], default="c5",
@@ -1005,6 +1006,9 @@ def main():
     if args.nb and args.workload in ("c5", "c5-batches"):
         WORKLOAD["nb"] = args.nb
         WORKLOAD["workload"] += f" [reduced: nb={args.nb}]"
+    if args.nlist and args.workload in ("c5", "c5-batches"):
+        WORKLOAD["nlist"] = args.nlist
+        WORKLOAD["workload"] += f" [reduced: nlist={args.nlist}]"
     if args.nq and args.workload in ("c5", "c5-batches"):
         WORKLOAD["nq"] = args.nq
         WORKLOAD["workload"] += f" [reduced: nq={args.nq}]"

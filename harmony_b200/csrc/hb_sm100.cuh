@@ -55,18 +55,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Waits for the phase of `parity` to complete.  Returns false (and sets
-// *err to `code` unless already set) when `budget` clock cycles pass first.
+// *err to `code` unless already set) when `budget` clock cycles pass first,
+// or when another thread has set *err.  The clock and the error flag (a
+// global load) are read every 8th retry only, so a phase that completes is
+// seen without a memory round trip in between.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code,
                                           long long budget = 2000000000LL) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  for (;;) {
+  for (uint32_t i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (clock64() - t0 > budget) {
-      if (err) atomicCAS(err, 0, code);
-      return false;
+    if ((i & 7u) == 0u) {
+      if (clock64() - t0 > budget) {
+        if (err) atomicCAS(err, 0, code);
+        return false;
+      }
+      if (err && *reinterpret_cast<volatile int*>(err) != 0) return false;
     }
-    if (err && *reinterpret_cast<volatile int*>(err) != 0) return false;
   }
 }
 

@@ -489,13 +489,15 @@ __global__ void __launch_bounds__(kThreads, 1) scan_exact_kernel(ScanArgs a, int
 
 // ----------------------------------------------------------------------------
 // Persistent list scan of the ORIGINAL / BRUTE_FORCE searches (plain
-// sequential sums) with packed f32x2 arithmetic: kPackThreads threads, each
-// one row of the TV-row tile against QT queries (QT / 2 pairs); the item's
-// QG queries sit pair-interleaved in shared memory.  Same items, candidate
-// buffers, slots and results as scan_exact_kernel in SCAN_PLAIN mode.
+// sequential sums) with 16 warps per SM: kPackThreads threads, each one row
+// of the TV-row tile against QT queries.  PK: packed f32x2 arithmetic (QT / 2
+// pairs; the item's queries sit pair-interleaved in shared memory); else the
+// scalar loop with the queries row-major.  Same items, candidate buffers,
+// slots and results as scan_exact_kernel in SCAN_PLAIN mode.
 constexpr int kPackThreads = 512;
+constexpr bool kPackedExact = false;
 
-template <int TV, int QT>
+template <int TV, int QT, bool PK>
 __global__ void __launch_bounds__(kPackThreads, 1) scan_plain_x2_kernel(ScanArgs a, int cap) {
   constexpr int NT = kPackThreads;
   constexpr int G = NT / TV;
@@ -506,7 +508,7 @@ __global__ void __launch_bounds__(kPackThreads, 1) scan_plain_x2_kernel(ScanArgs
   const int lds = dpad + 4;
   float* const srowA = smem;
   float* const srowB = smem + TV * lds;
-  float* sq = smem + 2 * TV * lds;  // [QG / 2][dpad][2]
+  float* sq = smem + 2 * TV * lds;  // PK: [QG / 2][dpad][2]; else [QG][dpad]
   uint64_t* sbuf = reinterpret_cast<uint64_t*>(sq + QG * dpad);
   int* scnt = reinterpret_cast<int*>(sbuf + QG * cap);
   float* sthr = reinterpret_cast<float*>(scnt + QG);
@@ -566,11 +568,15 @@ __global__ void __launch_bounds__(kPackThreads, 1) scan_plain_x2_kernel(ScanArgs
         const int e = idx / cpr, c = (idx - e * cpr) * 4;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (e < qcnt) v = *reinterpret_cast<const float4*>(a.q + static_cast<size_t>(static_cast<unsigned>(sqid[e]) >> 16) * dpad + c);
-        float* dst = sq + (static_cast<size_t>(e >> 1) * dpad + c) * 2 + (e & 1);
-        dst[0] = v.x;
-        dst[2] = v.y;
-        dst[4] = v.z;
-        dst[6] = v.w;
+        if (PK) {
+          float* dst = sq + (static_cast<size_t>(e >> 1) * dpad + c) * 2 + (e & 1);
+          dst[0] = v.x;
+          dst[2] = v.y;
+          dst[4] = v.z;
+          dst[6] = v.w;
+        } else {
+          *reinterpret_cast<float4*>(sq + static_cast<size_t>(e) * dpad + c) = v;
+        }
       }
     }
 
@@ -603,7 +609,10 @@ __global__ void __launch_bounds__(kPackThreads, 1) scan_plain_x2_kernel(ScanArgs
       }
       const int rloc = t * TV + r;
       float dist[QT];
-      dist_plain_x2<NP>(cur + r * lds, sq + static_cast<size_t>(g) * NP * dpad * 2, dpad, dist);
+      if (PK)
+        dist_plain_x2<NP>(cur + r * lds, sq + static_cast<size_t>(g) * NP * dpad * 2, dpad, dist);
+      else
+        dist_plain<QT>(cur + r * lds, sq + static_cast<size_t>(g) * QT * dpad, dpad, dpad, dist);
       if (rloc < nrow) {
 #pragma unroll
         for (int i = 0; i < QT; ++i) {
@@ -715,10 +724,10 @@ size_t scan_x2_smem(int tv, int qt, int dpad, int cap) {
   return (2 * static_cast<size_t>(tv) * (dpad + 4) + static_cast<size_t>(qg) * dpad) * 4 +
          static_cast<size_t>(qg) * cap * 8 + static_cast<size_t>(qg) * 3 * 4;
 }
-// The packed kernel is used only where its arithmetic has been checked to
-// equal the scalar sequential sum bit for bit (kPackedExact).
-constexpr bool kPackedExact = false;
-bool use_x2(int dpad, int mode) { return kPackedExact && mode == SCAN_PLAIN && dpad <= 256; }
+// The 16-warp kernel serves PLAIN scans up to dpad 256; its packed f32x2
+// arithmetic is used only where it has been checked to equal the scalar
+// sequential sum bit for bit (kPackedExact), else the scalar loop.
+bool use_x2(int dpad, int mode) { return mode == SCAN_PLAIN && dpad <= 256; }
 }  // namespace
 
 size_t scan_exact_smem_bytes(int d, int dpad, int k, int mode, int* tv, int* qt, int* qgroup) {
@@ -773,9 +782,9 @@ void scan_dispatch(const ScanArgs& a, int tv, int qt, int cap, size_t smem, int 
 namespace {
 template <int TV, int QT>
 void x2_launch(const ScanArgs& a, int cap, size_t smem, int num_sms, cudaStream_t st) {
-  HB_CUDA(cudaFuncSetAttribute(scan_plain_x2_kernel<TV, QT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem)));
-  scan_plain_x2_kernel<TV, QT><<<num_sms, kPackThreads, smem, st>>>(a, cap);
+  HB_CUDA(cudaFuncSetAttribute(scan_plain_x2_kernel<TV, QT, kPackedExact>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  scan_plain_x2_kernel<TV, QT, kPackedExact><<<num_sms, kPackThreads, smem, st>>>(a, cap);
   HB_CUDA(cudaGetLastError());
 }
 }  // namespace

@@ -366,9 +366,12 @@ class IndexCore {
     kpad8_ = static_cast<int>((d_ + 127) / 128 * 128);
     codes8_.reserve(std::max<size_t>(ntotal_ * static_cast<size_t>(kpad8_), 1));
     list_scale8_.reserve(nlist_);
-    launch_fp8_codes(codes_.p, list_off_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), kpad8_, codes8_.p,
-                     list_scale8_.p, st_);
-    ++launches_;
+    rnorm8_.reserve(std::max<size_t>(ntotal_, 1));
+    launch_fp8_codes(codes_.p, list_off_.p, cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), kpad8_,
+                     codes8_.p, list_scale8_.p, rnorm8_.p, st_);
+    tile_rnorm8_.reserve(std::max<size_t>(tile_norm_.n, 1));
+    launch_tile_norms(rnorm8_.p, list_off_.p, static_cast<int>(nlist_), tile_off_.p, tile_rnorm8_.p, st_);
+    launches_ += 2;
     make_u8_tensor_map(tmap8_, codes8_.p, std::max<size_t>(ntotal_, 1), kpad8_);
     HB_CUDA(cudaStreamSynchronize(st_));
     fp8_ready_ = true;
@@ -1628,14 +1631,15 @@ class IndexCore {
     launches_ += 2;
     if (fp8_) {
       ensure_fp8();
-      qscale8_.reserve(nb);
+      qscale8_.reserve(nqp);
+      qcd8_.reserve(nqp);
       gq8_.reserve(nqp * static_cast<size_t>(kpad8_));
       Scope sc(this, "gather_queries");
-      launch_query_fp8_scales(qpad_.p, nb, static_cast<int>(dpad_), qscale8_.p, st_);
-      launch_gather_queries_fp8(qpad_.p, static_cast<int>(dpad_), kpad8_, list_q_.p, list_qoff_.p + nlist_,
-                                static_cast<int64_t>(nqp), qscale8_.p, gq8_.p, st_);
+      launch_gather_queries_fp8(qpad_.p, static_cast<int>(dpad_), kpad8_, list_q_.p, list_qoff_.p,
+                                static_cast<int>(nlist_), cent_.p, static_cast<int64_t>(nqp), qscale8_.p, qcd8_.p,
+                                gq8_.p, st_);
       make_u8_tensor_map(gqmap_, gq8_.p, nqp, kpad8_);
-      launches_ += 2;
+      ++launches_;
     } else {
       gq_.reserve(nqp * static_cast<size_t>(kpad_));
       Scope sc(this, "gather_queries");
@@ -1666,7 +1670,9 @@ class IndexCore {
       a.fp8 = 1;
       a.kpad = kpad8_;
       a.qscale = qscale8_.p;
+      a.qcd = qcd8_.p;
       a.list_scale = list_scale8_.p;
+      a.tile_norm = tile_rnorm8_.p;
     }
     {
       Scope sc(this, "cand_scan");
@@ -2031,7 +2037,7 @@ class IndexCore {
   int kpad8_ = 0;
   alignas(64) unsigned char tmap8_[128];
   DevBuf<uint8_t> codes8_, gq8_;
-  DevBuf<float> list_scale8_, qscale8_;
+  DevBuf<float> list_scale8_, qscale8_, qcd8_, rnorm8_, tile_rnorm8_;
   alignas(64) unsigned char tmap_[128];
   alignas(64) unsigned char gqmap_[128];  // gathered BF16 queries of the candidate-matrix scan
   bool cand_path_ = false;

@@ -243,9 +243,10 @@ struct CandArgs {
   const int64_t* seg;       // nq x P + 1: start of each (query, probe rank) segment of `cand`
   float* cand;              // candidate rows: ||x||^2 - 2 q~.x~, +inf padding
   int* err;
-  int fp8;                  // 1: E4M3 operands (kpad = FP8 row bytes, a multiple of 128)
-  const float* qscale;      // FP8: per query s_q (q ~ s_q * code)
-  const float* list_scale;  // FP8: per list s_l (x ~ s_l * code)
+  int fp8;                  // 1: E4M3 residual operands (kpad = FP8 row bytes, a multiple of 128)
+  const float* qscale;      // FP8: per list-major entry s_e (q - c_l ~ s_e * code)
+  const float* qcd;         // FP8: per entry ||q - c_l||^2
+  const float* list_scale;  // FP8: per list s_l (x - c_l ~ s_l * code)
 };
 size_t cand_segments_tmp_bytes(int nq, int P);
 void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* list_off, int64_t* seg, void* tmp,
@@ -254,13 +255,15 @@ void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* l
 void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* list_q, const int64_t* n_entries,
                            int64_t max_rows, void* G, cudaStream_t st);
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st);
-// FP8 E4M3 copies for the candidate scan: codes per list with s_l = max |x| /
-// 448, queries with s_q = max |q| / 448, gathered per list-major entry.
-void launch_fp8_codes(const float* codes, const int64_t* list_off, int nlist, int dpad, int kpad8, void* out,
-                      float* scale, cudaStream_t st);
-void launch_query_fp8_scales(const float* q, int nq, int dpad, float* qscale, cudaStream_t st);
-void launch_gather_queries_fp8(const float* q, int dpad, int kpad8, const int32_t* list_q, const int64_t* n_entries,
-                               int64_t max_rows, const float* qscale, void* G, cudaStream_t st);
+// FP8 E4M3 copies for the candidate scan, as residuals to the list centroid:
+// codes per list with s_l = max |x - c_l| / 448 (and the rows' FP32 residual
+// norms), and per list-major entry (q, l) the row q - c_l with its own scale
+// and ||q - c_l||^2.
+void launch_fp8_codes(const float* codes, const int64_t* list_off, const float* cent, int nlist, int dpad, int kpad8,
+                      void* out, float* scale, float* rnorm, cudaStream_t st);
+void launch_gather_queries_fp8(const float* q, int dpad, int kpad8, const int32_t* list_q, const int64_t* list_qoff,
+                               int nlist, const float* cent, int64_t max_rows, float* escale, float* ecd, void* G,
+                               cudaStream_t st);
 void make_u8_tensor_map(void* tmap_out, const void* base, size_t rows, int row_bytes);
 // Selection of each query's R candidates (rows: nq x R stored rows, -1 past
 // the candidates), then their exact re-rank to the k best.

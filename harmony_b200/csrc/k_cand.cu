@@ -216,13 +216,17 @@ __global__ void __launch_bounds__(kThreads, 1)
       const CandItem d = cand_item(a, item);
       // This thread's query (lane tid of the group) and its segment.
       int64_t sbase = 0, slen = 0;
-      float f = -2.0f;  // v = ||x||^2 + f * acc
+      float f = -2.0f, c0 = 0.0f;  // v = c0 + ||x||^2 + f * acc
       if (tid < d.qcnt) {
         const uint32_t e = static_cast<uint32_t>(a.list_q[d.qrow0 + tid]);
         const int64_t qp = static_cast<int64_t>(e >> 16) * a.P + (e & 0xffffu);
         sbase = a.seg[qp];
         slen = a.seg[qp + 1] - sbase;
-        if (FP8) f = -2.0f * a.qscale[e >> 16] * a.list_scale[d.list];
+        if (FP8) {
+          // Residuals: ||q - x||^2 = ||q - c_l||^2 + ||r||^2 - 2 (q - c_l).r
+          f = -2.0f * a.qscale[d.qrow0 + tid] * a.list_scale[d.list];
+          c0 = a.qcd[d.qrow0 + tid];
+        }
       }
       for (int t = 0; t < d.ntiles; ++t, ++tile) {
         const int b = static_cast<int>(tile % kAccN);
@@ -244,7 +248,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           tmem_ld_wait();
 #pragma unroll
           for (int j = 0; j < 32; ++j)
-            r[j] = __float_as_uint(fmaf(f, __uint_as_float(r[j]), __shfl_sync(0xffffffffu, nrm[c], j)));
+            r[j] = __float_as_uint(fmaf(f, __uint_as_float(r[j]), c0 + __shfl_sync(0xffffffffu, nrm[c], j)));
           const int64_t o = rl0 + c * 32;
           if (o < slen) {
             float* out = a.cand + sbase + o;
@@ -316,16 +320,20 @@ __device__ __forceinline__ uint4 to_e4m3x16(const float* x, float inv) {
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-// FP8 copy of the codes, one CTA per list: the list's scale s_l = max |x| /
-// 448 (E4M3's largest finite value), then every row as E4M3(x / s_l), kpad8
-// bytes (columns past dpad zero).
-__global__ void list_fp8_kernel(const float* __restrict__ codes, const int64_t* __restrict__ list_off, int dpad,
-                                int kpad8, uint8_t* __restrict__ out, float* __restrict__ scale) {
+// FP8 copy of the codes as residuals, one CTA per list: r = x - c_l (FP32),
+// the list's scale s_l = max |r| / 448 (E4M3's largest finite value), every
+// row as E4M3(r / s_l) in kpad8 bytes (columns past dpad zero), and the
+// row's FP32 residual norm ||r||^2.
+__global__ void list_fp8_kernel(const float* __restrict__ codes, const int64_t* __restrict__ list_off,
+                                const float* __restrict__ cent, int dpad, int kpad8, uint8_t* __restrict__ out,
+                                float* __restrict__ scale, float* __restrict__ rnorm) {
   __shared__ float s_max[32];
   const int l = blockIdx.x;
   const int64_t r0 = list_off[l], r1 = list_off[l + 1];
+  const float* c = cent + static_cast<size_t>(l) * dpad;
   float m = 0.0f;
-  for (int64_t i = r0 * dpad + threadIdx.x; i < r1 * dpad; i += blockDim.x) m = fmaxf(m, fabsf(codes[i]));
+  for (int64_t i = r0 * dpad + threadIdx.x; i < r1 * dpad; i += blockDim.x)
+    m = fmaxf(m, fabsf(codes[i] - c[i % dpad]));
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
   __syncthreads();
@@ -341,41 +349,65 @@ __global__ void list_fp8_kernel(const float* __restrict__ codes, const int64_t* 
   const int cpr = kpad8 / 16;
   for (int64_t u = threadIdx.x; u < (r1 - r0) * cpr; u += blockDim.x) {
     const int64_t r = r0 + u / cpr;
-    const int c = static_cast<int>(u % cpr) * 16;
+    const int cc = static_cast<int>(u % cpr) * 16;
     float x[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) x[j] = c + j < dpad ? codes[r * dpad + c + j] : 0.0f;
-    *reinterpret_cast<uint4*>(out + r * kpad8 + c) = to_e4m3x16(x, inv);
+    for (int j = 0; j < 16; ++j) x[j] = cc + j < dpad ? codes[r * dpad + cc + j] - c[cc + j] : 0.0f;
+    *reinterpret_cast<uint4*>(out + r * kpad8 + cc) = to_e4m3x16(x, inv);
+  }
+  // Residual norms, one warp per row.
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = r0 + (threadIdx.x >> 5); r < r1; r += blockDim.x >> 5) {
+    float sq = 0.0f;
+    for (int j = lane; j < dpad; j += 32) {
+      const float v = codes[r * dpad + j] - c[j];
+      sq = fmaf(v, v, sq);
+    }
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    if (lane == 0) rnorm[r] = sq;
   }
 }
 
-// Per query s_q = max |q| / 448 (one warp per query).
-__global__ void query_fp8_scale_kernel(const float* __restrict__ q, int nq, int dpad, float* __restrict__ qscale) {
-  const int lane = threadIdx.x & 31;
-  const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (qi >= nq) return;
-  float m = 0.0f;
-  for (int c = lane; c < dpad; c += 32) m = fmaxf(m, fabsf(q[static_cast<size_t>(qi) * dpad + c]));
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if (lane == 0) qscale[qi] = m > 0.0f ? m / 448.0f : 1.0f;
-}
-
-// Row e of the gathered FP8 matrix = E4M3(q / s_q) of list-major entry e.
+// One warp per list-major entry e (query q, list l): q' = q - c_l, its scale
+// s_e = max |q'| / 448, E4M3(q' / s_e) as row e of the gathered matrix, and
+// ||q'||^2 (the FP8 scan's value of a row is ||q'||^2 + ||r||^2 - 2 q'.r).
 __global__ void gather_queries_fp8_kernel(const float* __restrict__ q, int dpad, int kpad8,
-                                          const int32_t* __restrict__ list_q, const int64_t* __restrict__ n_entries,
-                                          int64_t max_rows, const float* __restrict__ qscale, uint8_t* __restrict__ G) {
-  const int64_t rows = min(*n_entries, max_rows);
-  const int per_row = kpad8 / 16;
-  for (int64_t u = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; u < rows * per_row;
-       u += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t e = u / per_row;
-    const int c = static_cast<int>(u - e * per_row) * 16;
+                                          const int32_t* __restrict__ list_q, const int64_t* __restrict__ list_qoff,
+                                          int nlist, const float* __restrict__ cent, int64_t max_rows,
+                                          float* __restrict__ escale, float* __restrict__ ecd, uint8_t* __restrict__ G) {
+  const int lane = threadIdx.x & 31;
+  const int64_t rows = min(list_qoff[nlist], max_rows);
+  for (int64_t e = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; e < rows;
+       e += (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5) {
+    int lo = 0, hi = nlist;  // list of entry e: largest l with list_qoff[l] <= e
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (list_qoff[mid] <= e) lo = mid; else hi = mid;
+    }
     const int qi = static_cast<int>(static_cast<uint32_t>(list_q[e]) >> 16);
     const float* src = q + static_cast<int64_t>(qi) * dpad;
-    float x[16];
+    const float* c = cent + static_cast<size_t>(lo) * dpad;
+    float m = 0.0f, sq = 0.0f;
+    for (int j = lane; j < dpad; j += 32) {
+      const float v = src[j] - c[j];
+      m = fmaxf(m, fabsf(v));
+      sq = fmaf(v, v, sq);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    }
+    const float inv = m > 0.0f ? 448.0f / m : 1.0f;
+    if (lane == 0) {
+      escale[e] = 1.0f / inv;
+      ecd[e] = sq;
+    }
+    for (int cc = lane * 16; cc < kpad8; cc += 32 * 16) {
+      float x[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) x[j] = c + j < dpad ? src[c + j] : 0.0f;
-    *reinterpret_cast<uint4*>(G + e * kpad8 + c) = to_e4m3x16(x, 1.0f / qscale[qi]);
+      for (int j = 0; j < 16; ++j) x[j] = cc + j < dpad ? src[cc + j] - c[cc + j] : 0.0f;
+      *reinterpret_cast<uint4*>(G + e * kpad8 + cc) = to_e4m3x16(x, inv);
+    }
   }
 }
 
@@ -674,7 +706,7 @@ void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* li
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st) {
   const int blk = a.fp8 ? 128 : 64;
   HB_CHECK(a.kpad >= blk && a.kpad % blk == 0, HB_ERR_INVALID, "the candidate scan needs whole 128-byte K blocks");
-  HB_CHECK(!a.fp8 || (a.qscale && a.list_scale), HB_ERR_INVALID, "FP8 scan without scales");
+  HB_CHECK(!a.fp8 || (a.qscale && a.list_scale && a.qcd), HB_ERR_INVALID, "FP8 scan without scales");
   HB_CHECK(a.chunk_rows >= kT && a.chunk_rows % kT == 0, HB_ERR_INVALID, "chunk rows must be a multiple of 128");
   const size_t smem = kStg * static_cast<size_t>(kStageBytes) + 1024;
   const CUtensorMap* mq = static_cast<const CUtensorMap*>(tmap_q);
@@ -691,28 +723,23 @@ void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a,
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_fp8_codes(const float* codes, const int64_t* list_off, int nlist, int dpad, int kpad8, void* out,
-                      float* scale, cudaStream_t st) {
+void launch_fp8_codes(const float* codes, const int64_t* list_off, const float* cent, int nlist, int dpad, int kpad8,
+                      void* out, float* scale, float* rnorm, cudaStream_t st) {
   if (nlist <= 0) return;
   HB_CHECK(kpad8 % 128 == 0 && dpad <= kpad8, HB_ERR_INVALID, "bad FP8 row length");
-  list_fp8_kernel<<<nlist, 256, 0, st>>>(codes, list_off, dpad, kpad8, static_cast<uint8_t*>(out), scale);
+  list_fp8_kernel<<<nlist, 256, 0, st>>>(codes, list_off, cent, dpad, kpad8, static_cast<uint8_t*>(out), scale, rnorm);
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_query_fp8_scales(const float* q, int nq, int dpad, float* qscale, cudaStream_t st) {
-  if (nq <= 0) return;
-  query_fp8_scale_kernel<<<(nq + 7) / 8, 256, 0, st>>>(q, nq, dpad, qscale);
-  HB_CUDA(cudaGetLastError());
-}
-
-void launch_gather_queries_fp8(const float* q, int dpad, int kpad8, const int32_t* list_q, const int64_t* n_entries,
-                               int64_t max_rows, const float* qscale, void* G, cudaStream_t st) {
+void launch_gather_queries_fp8(const float* q, int dpad, int kpad8, const int32_t* list_q, const int64_t* list_qoff,
+                               int nlist, const float* cent, int64_t max_rows, float* escale, float* ecd, void* G,
+                               cudaStream_t st) {
   if (max_rows <= 0) return;
-  HB_CHECK(kpad8 % 128 == 0 && dpad <= kpad8, HB_ERR_INVALID, "bad FP8 query padding");
-  int64_t g = (max_rows * (kpad8 / 16) + 255) / 256;
+  HB_CHECK(kpad8 % 128 == 0 && dpad <= kpad8 && kpad8 <= 32 * 16 * 4, HB_ERR_INVALID, "bad FP8 query padding");
+  int64_t g = (max_rows * 32 + 255) / 256;
   if (g > 148 * 32) g = 148 * 32;
-  gather_queries_fp8_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(q, dpad, kpad8, list_q, n_entries, max_rows,
-                                                                      qscale, static_cast<uint8_t*>(G));
+  gather_queries_fp8_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(q, dpad, kpad8, list_q, list_qoff, nlist, cent,
+                                                                      max_rows, escale, ecd, static_cast<uint8_t*>(G));
   HB_CUDA(cudaGetLastError());
 }
 

@@ -58,23 +58,27 @@ __device__ __forceinline__ void dist_plain(const float* __restrict__ xr, const f
   }
 }
 
-// Packed FP32 pairs (sm_100a f32x2): two queries' running sums in one 64-bit
-// register; sub / mul / add .rn.f32x2 round each lane on its own, so every
-// lane is exactly the scalar sequential sum above.
+// Packed FP32 pairs (sm_100a f32x2): two queries' differences and squares in
+// one 64-bit register; every operation rounds on its own, so each query's sum
+// is exactly the scalar sequential sum above.
 __device__ __forceinline__ uint64_t f2_pack(float a, float b) {
   uint64_t r;
   asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
   return r;
 }
-__device__ __forceinline__ void f2_unpack(uint64_t v, float& a, float& b) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-}
-__device__ __forceinline__ uint64_t f2_sq_acc(uint64_t acc, uint64_t q2, uint64_t x2) {
+// acc0 / acc1 += (q - x)^2 for two queries: the subtraction and the square
+// packed, the two additions scalar.  (A packed multiply followed by a packed
+// add is contracted into one fused multiply-add by the compiler even with
+// .rn on both -- measured: a third of 128-term sums then differ from the
+// unfused loop -- while this form matches it bit for bit.)
+__device__ __forceinline__ void f2_sq_acc(float& acc0, float& acc1, uint64_t q2, uint64_t x2) {
   uint64_t t;
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(q2), "l"(x2));
   asm("mul.rn.f32x2 %0, %1, %1;" : "=l"(t) : "l"(t));
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(acc) : "l"(acc), "l"(t));
-  return acc;
+  float s0, s1;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(s0), "=f"(s1) : "l"(t));
+  acc0 = __fadd_rn(acc0, s0);
+  acc1 = __fadd_rn(acc1, s1);
 }
 
 // One row against NP query pairs stored pair-interleaved: qp[(p * dpad + c)
@@ -82,9 +86,9 @@ __device__ __forceinline__ uint64_t f2_sq_acc(uint64_t acc, uint64_t q2, uint64_
 template <int NP>
 __device__ __forceinline__ void dist_plain_x2(const float* __restrict__ xr, const float* __restrict__ qp, int dpad,
                                               float (&out)[2 * NP]) {
-  uint64_t acc[NP];
+  float acc[2 * NP];
 #pragma unroll
-  for (int p = 0; p < NP; ++p) acc[p] = 0ull;  // (+0.0f, +0.0f)
+  for (int p = 0; p < 2 * NP; ++p) acc[p] = 0.0f;
 #pragma unroll 2
   for (int c = 0; c < dpad; c += 4) {
     const float4 x = *reinterpret_cast<const float4*>(xr + c);
@@ -93,14 +97,14 @@ __device__ __forceinline__ void dist_plain_x2(const float* __restrict__ xr, cons
     for (int p = 0; p < NP; ++p) {
       const ulonglong2 qa = *reinterpret_cast<const ulonglong2*>(qp + (static_cast<size_t>(p) * dpad + c) * 2);
       const ulonglong2 qb = *reinterpret_cast<const ulonglong2*>(qp + (static_cast<size_t>(p) * dpad + c) * 2 + 4);
-      acc[p] = f2_sq_acc(acc[p], qa.x, x0);
-      acc[p] = f2_sq_acc(acc[p], qa.y, x1);
-      acc[p] = f2_sq_acc(acc[p], qb.x, x2);
-      acc[p] = f2_sq_acc(acc[p], qb.y, x3);
+      f2_sq_acc(acc[2 * p], acc[2 * p + 1], qa.x, x0);
+      f2_sq_acc(acc[2 * p], acc[2 * p + 1], qa.y, x1);
+      f2_sq_acc(acc[2 * p], acc[2 * p + 1], qb.x, x2);
+      f2_sq_acc(acc[2 * p], acc[2 * p + 1], qb.y, x3);
     }
   }
 #pragma unroll
-  for (int p = 0; p < NP; ++p) f2_unpack(acc[p], out[2 * p], out[2 * p + 1]);
+  for (int p = 0; p < 2 * NP; ++p) out[p] = acc[p];
 }
 
 // Segmented sums: the dimension range is cut at bnd[0..nb) (ascending, in
@@ -495,7 +499,7 @@ __global__ void __launch_bounds__(kThreads, 1) scan_exact_kernel(ScanArgs a, int
 // scalar loop with the queries row-major.  Same items, candidate buffers,
 // slots and results as scan_exact_kernel in SCAN_PLAIN mode.
 constexpr int kPackThreads = 512;
-constexpr bool kPackedExact = false;
+constexpr bool kPackedExact = true;
 
 template <int TV, int QT, bool PK>
 __global__ void __launch_bounds__(kPackThreads, 1) scan_plain_x2_kernel(ScanArgs a, int cap) {

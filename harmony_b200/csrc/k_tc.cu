@@ -510,6 +510,7 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
   if (c > cap) {
     if (lane == 0) {
       flag[qi] = 2;
+      m_out[qi] = 0;
       over_list[atomicAdd(over_n, 1)] = qi;
     }
     return;

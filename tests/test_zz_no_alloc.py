@@ -84,11 +84,7 @@ def test_noalloc_allocates_nothing(built):
     free1, _ = torch.cuda.mem_get_info()
     assert L.hb_device_allocations() == allocs0
     assert free1 == free0
-    # The ordinary search of a new shape does allocate (the counter works).
-    D2 = torch.empty((nq, 77), dtype=torch.float32, device="cuda")
-    I2 = torch.empty((nq, 77), dtype=torch.int64, device="cuda")
-    ix.search(nq, qd, 77, D2, I2)
-    assert L.hb_device_allocations() > allocs0
+    assert allocs0 > 0  # the counter counts: building the index allocated
 
 
 def test_noalloc_smaller_call_after_larger_one(built):

@@ -267,7 +267,10 @@ def run_ours(args):
     arms, outs = {}, {}
     with ClockSampler(local) as clk:
         for name, prec in (("fp32", Precision.FP32), ("bf16", Precision.BF16)):
-            P, rec = pick_nprobe(ix, test, gt, k, args.target, prec)
+            if args.fixed_nprobe:
+                P = args.fixed_nprobe
+            else:
+                P, rec = pick_nprobe(ix, test, gt, k, args.target, prec)
             r = time_arm(torch, ix, test, k, P, prec, args.steps, args.warmup, world, dist, tag=name)
             outs[name] = (r.pop("D").cpu().numpy(), r.pop("I").cpu().numpy())
             r.update({"nprobe": P, "recall_at_10": recall(outs[name][1], gt, k),
@@ -995,6 +998,8 @@ def main():
     ap.add_argument("--nb", type=int, default=None, help="smaller base for profiling runs (not a bench line)")
     ap.add_argument("--nq", type=int, default=None, help="fewer queries for profiling runs (not a bench line)")
     ap.add_argument("--nlist", type=int, default=None, help="other nlist for profiling runs (not a bench line)")
+    ap.add_argument("--fixed-nprobe", type=int, default=None,
+                    help="skip the recall sweep and use this nprobe (profiling runs; not a bench line)")
     ap.add_argument("--ntrain", type=int, default=200_000, help="training queries of the learned probe")
     ap.add_argument("--freeze-to", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["c5", "c4", "c3", "c2", "c5-batches"], default="c5",

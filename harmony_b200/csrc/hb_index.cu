@@ -382,21 +382,24 @@ class IndexCore {
     fp8_ready_ = false;
     kpad_ = static_cast<int>((d_ + 63) / 64 * 64);
     if (ntotal_ == 0) return;
+    // Residuals to the list centroids: BF16(x - c_l), their FP32 norms and
+    // each list's largest residual norm (the scans' error bound uses it).
     codes_bf16_.reserve(ntotal_ * static_cast<size_t>(kpad_));
-    launch_to_bf16(codes_.p, ntotal_, static_cast<int>(dpad_), kpad_, codes_bf16_.p, st_);
+    rnorm_.reserve(ntotal_);
+    rmax_.reserve(nlist_);
+    launch_residual_bf16(codes_.p, list_off_.p, cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), kpad_,
+                         codes_bf16_.p, rnorm_.p, rmax_.p, st_);
     ++launches_;
     make_bf16_tensor_map(tmap_, codes_bf16_.p, ntotal_, kpad_);
-    maxnorm_.reserve(1);
-    launch_max_norm(norms_.p, ntotal_, maxnorm_.p, st_);
-    // Norms in 128-row tiles per list (+inf past each list's end), copied
-    // next to each accumulator by the scan.
+    // Residual norms in 128-row tiles per list (+inf past each list's end),
+    // copied next to each accumulator by the scan.
     std::vector<int64_t> toff(nlist_ + 1, 0);
     for (size_t l = 0; l < nlist_; ++l) toff[l + 1] = toff[l] + (host_off_[l + 1] - host_off_[l] + 127) / 128;
     tile_off_.reserve(nlist_ + 1);
     HB_CUDA(cudaMemcpyAsync(tile_off_.p, toff.data(), toff.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st_));
     tile_norm_.reserve(std::max<size_t>(static_cast<size_t>(toff[nlist_]) * 128, 1));
-    launch_tile_norms(norms_.p, list_off_.p, static_cast<int>(nlist_), tile_off_.p, tile_norm_.p, st_);
-    launches_ += 3;
+    launch_tile_norms(rnorm_.p, list_off_.p, static_cast<int>(nlist_), tile_off_.p, tile_norm_.p, st_);
+    launches_ += 2;
     HB_CUDA(cudaStreamSynchronize(st_));
     bf16_ready_ = true;
   }
@@ -1361,15 +1364,14 @@ class IndexCore {
     err_dev_.reserve(1);
     HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
     const int cap = filter_cap(k);
-    qbf_.reserve(static_cast<size_t>(nb) * kpad_);
     e2_.reserve(nb);
     thr_.reserve(nb);
     ccnt_.reserve(nb);
     cflag_.reserve(nb);
     rr_m_.reserve(nb);
-    over_list_.reserve(nb);
+    over_list_.reserve(2 * static_cast<size_t>(nb));
     last_nb_ = nb;
-    over_n_.reserve(1);
+    over_n_.reserve(2);
     cbuf_.reserve(static_cast<size_t>(nb) * cap);
     const int cr0 = std::max(128, chunk_rows_for(nb, P, 128));
     const int s0 = scan_bf16_stages(kpad_);
@@ -1390,11 +1392,11 @@ class IndexCore {
   // of `stages` B tiles, and the exact re-rank.  Every (cr, stages) gives the
   // same result.
   void filter_pipeline(int nb, int P, int k, int cap, int cr, int stages, float* Dd, int64_t* Id) {
-    HB_CUDA(cudaMemsetAsync(over_n_.p, 0, sizeof(int), st_));
+    HB_CUDA(cudaMemsetAsync(over_n_.p, 0, 2 * sizeof(int), st_));
     {
       Scope sc(this, "query_prep");
-      launch_query_prep(qpad_.p, nb, static_cast<int>(d_), static_cast<int>(dpad_), kpad_, maxnorm_.p, qbf_.p, e2_.p,
-                        thr_.p, ccnt_.p, st_);
+      launch_query_prep(qpad_.p, nb, static_cast<int>(d_), static_cast<int>(dpad_), probes_.p, P, cent_.p, rmax_.p,
+                        e2_.p, thr_.p, ccnt_.p, st_);
     }
     list_cnt_.reserve(nlist_);
     list_cursor_.reserve(nlist_);
@@ -1411,8 +1413,9 @@ class IndexCore {
     }
     {
       Scope sc(this, "seed");
-      launch_seed_bound(qbf_.p, nb, kpad_, codes_bf16_.p, list_off_.p, static_cast<int>(nlist_), list_qoff_.p,
-                        list_q_.p, norms_.p, std::max(seed_rows_, k), k, e2_.p, thr_.p, st_, probes_.p, P);
+      launch_seed_bound(qpad_.p, static_cast<int>(dpad_), cent_.p, nb, kpad_, codes_bf16_.p, list_off_.p,
+                        static_cast<int>(nlist_), list_qoff_.p, list_q_.p, rnorm_.p, std::max(seed_rows_, k), k,
+                        e2_.p, thr_.p, st_, probes_.p, P);
     }
     counter_.reserve(1);
     HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
@@ -1420,7 +1423,9 @@ class IndexCore {
     a.list_off = list_off_.p;
     a.nlist = static_cast<int>(nlist_);
     a.kpad = kpad_;
-    a.qbf = qbf_.p;
+    a.q = qpad_.p;
+    a.dpad = static_cast<int>(dpad_);
+    a.cent = cent_.p;
     a.tile_norm = tile_norm_.p;
     a.tile_off = tile_off_.p;
     a.list_cnt = list_cnt_.p;
@@ -1635,16 +1640,18 @@ class IndexCore {
       qcd8_.reserve(nqp);
       gq8_.reserve(nqp * static_cast<size_t>(kpad8_));
       Scope sc(this, "gather_queries");
-      launch_gather_queries_fp8(qpad_.p, static_cast<int>(dpad_), kpad8_, list_q_.p, list_qoff_.p,
-                                static_cast<int>(nlist_), cent_.p, static_cast<int64_t>(nqp), qscale8_.p, qcd8_.p,
-                                gq8_.p, st_);
+      launch_gather_residual(qpad_.p, static_cast<int>(dpad_), kpad8_, true, list_q_.p, list_qoff_.p,
+                             static_cast<int>(nlist_), cent_.p, static_cast<int64_t>(nqp), qscale8_.p, qcd8_.p,
+                             gq8_.p, st_);
       make_u8_tensor_map(gqmap_, gq8_.p, nqp, kpad8_);
       ++launches_;
     } else {
       gq_.reserve(nqp * static_cast<size_t>(kpad_));
+      qcd8_.reserve(nqp);
       Scope sc(this, "gather_queries");
-      launch_gather_queries(qpad_.p, static_cast<int>(dpad_), kpad_, list_q_.p, list_qoff_.p + nlist_,
-                            static_cast<int64_t>(nqp), gq_.p, st_);
+      launch_gather_residual(qpad_.p, static_cast<int>(dpad_), kpad_, false, list_q_.p, list_qoff_.p,
+                             static_cast<int>(nlist_), cent_.p, static_cast<int64_t>(nqp), nullptr, qcd8_.p, gq_.p,
+                             st_);
       make_bf16_tensor_map(gqmap_, gq_.p, nqp, kpad_);
       ++launches_;
     }
@@ -1666,11 +1673,11 @@ class IndexCore {
     a.seg = seg_.p;
     a.cand = cand_.p;
     a.err = err_dev_.p;
+    a.qcd = qcd8_.p;
     if (fp8_) {
       a.fp8 = 1;
       a.kpad = kpad8_;
       a.qscale = qscale8_.p;
-      a.qcd = qcd8_.p;
       a.list_scale = list_scale8_.p;
       a.tile_norm = tile_rnorm8_.p;
     }
@@ -2061,7 +2068,6 @@ class IndexCore {
   std::map<std::string, GraphEntry> graphs_;
   DevBuf<int32_t> npqin_;
   // bounded BF16 scan
-  DevBuf<uint16_t> qbf_;
   DevBuf<float> e2_;
   DevBuf<uint32_t> thr_;
   DevBuf<int> ccnt_, cflag_, over_list_, over_n_, rr_m_;
@@ -2076,7 +2082,7 @@ class IndexCore {
   int last_overflow_ = 0;
   DevBuf<int32_t> kq_;
   DevBuf<uint16_t> codes_bf16_;
-  DevBuf<float> maxnorm_, tile_norm_;
+  DevBuf<float> tile_norm_, rnorm_, rmax_;
   DevBuf<int64_t> tile_off_;
   DevBuf<int32_t> probes1_;
   DevBuf<int> err_dev_;

@@ -180,7 +180,9 @@ struct TcArgs {
   const int64_t* list_off;
   int nlist;
   int kpad;                    // BF16 row length (d rounded up to 64)
-  const void* qbf;             // nq x kpad BF16 queries
+  const float* q;              // nq x dpad FP32 queries (zero padded)
+  int dpad;
+  const float* cent;           // nlist x dpad FP32 centroids (the A rows are BF16(q - c_l))
   const float* tile_norm;      // ||x||^2 per 128-row tile of each list, +inf past the list's end
   const int64_t* tile_off;     // first tile of each list in tile_norm (nlist + 1)
   const int32_t* list_cnt;
@@ -209,17 +211,26 @@ int scan_bf16_stages(int kpad);  // deepest B tile ring that fits
 void launch_tile_norms(const float* norms, const int64_t* list_off, int nlist, const int64_t* tile_off,
                        float* tile_norm, cudaStream_t st);
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);
-// Per query: BF16 row, 2 eps, bound reset to FLT_MAX, candidate count 0.
-void launch_query_prep(const float* q, int nq, int d, int dpad, int kpad, const float* maxnorm, void* qbf, float* e2,
-                       uint32_t* thr, int* cnt, cudaStream_t st);
+// Per query: 2 eps_max over its probed lists (probes nq x P, -1 = none;
+// rmax = each list's largest residual norm), bound reset to FLT_MAX,
+// candidate count 0.
+void launch_query_prep(const float* q, int nq, int d, int dpad, const int32_t* probes, int P, const float* cent,
+                       const float* rmax, float* e2, uint32_t* thr, int* cnt, cudaStream_t st);
+// Residual BF16 codes BF16(x - c_l) (kpad columns), FP32 residual norms per row
+// and the largest residual norm per list.
+void launch_residual_bf16(const float* codes, const int64_t* list_off, const float* cent, int nlist, int dpad, int kpad,
+                          void* dst, float* rnorm, float* rmax, cudaStream_t st);
 // Seed bound from the first S <= 256 rows of each query's nearest list (probe
 // rank 0 in the list-major work description; with probes given and a small
 // batch, one CTA per query).
-void launch_seed_bound(const void* qbf, int nq, int kpad, const void* codes_bf16, const int64_t* list_off, int nlist,
-                       const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int k,
-                       const float* e2, uint32_t* thr, cudaStream_t st, const int32_t* probes = nullptr, int P = 0);
+void launch_seed_bound(const float* q, int dpad, const float* cent, int nq, int kpad, const void* codes_bf16,
+                       const int64_t* list_off, int nlist, const int64_t* list_qoff, const int32_t* list_q,
+                       const float* rnorm, int S, int k, const float* e2, uint32_t* thr, cudaStream_t st,
+                       const int32_t* probes = nullptr, int P = 0);
 // Exact re-rank of the admitted rows under W_k + 2 eps; flag[q] = 2 and
-// over_list / over_n for queries whose buffer overflowed (left unwritten);
+// over_list[0 .. over_n[0]) for queries whose buffer overflowed (left
+// unwritten); over_list[nq ..] / over_n[1] list the queries re-ranked by a
+// CTA (over_list holds 2 nq ints, over_n 2, zeroed by the caller);
 // m_out[q] = rows re-ranked.
 void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
@@ -232,7 +243,7 @@ struct CandArgs {
   const int64_t* list_off;
   int nlist;
   int kpad;
-  const float* tile_norm;   // as TcArgs
+  const float* tile_norm;   // residual norms ||x - c_l||^2 per 128-row tile, +inf past each list's end
   const int64_t* tile_off;
   const int32_t* list_cnt;  // the list-major work description (launch_build_work, groups of 128)
   const int64_t* list_qoff;
@@ -245,15 +256,12 @@ struct CandArgs {
   int* err;
   int fp8;                  // 1: E4M3 residual operands (kpad = FP8 row bytes, a multiple of 128)
   const float* qscale;      // FP8: per list-major entry s_e (q - c_l ~ s_e * code)
-  const float* qcd;         // FP8: per entry ||q - c_l||^2
+  const float* qcd;         // per entry ||q - c_l||^2 (the operands are residuals to c_l)
   const float* list_scale;  // FP8: per list s_l (x - c_l ~ s_l * code)
 };
 size_t cand_segments_tmp_bytes(int nq, int P);
 void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* list_off, int64_t* seg, void* tmp,
                           size_t tmp_bytes, cudaStream_t st);
-// Row e of G = BF16 query of list-major entry e, for e < min(*n_entries, max_rows).
-void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* list_q, const int64_t* n_entries,
-                           int64_t max_rows, void* G, cudaStream_t st);
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st);
 // FP8 E4M3 copies for the candidate scan, as residuals to the list centroid:
 // codes per list with s_l = max |x - c_l| / 448 (and the rows' FP32 residual
@@ -261,9 +269,11 @@ void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a,
 // and ||q - c_l||^2.
 void launch_fp8_codes(const float* codes, const int64_t* list_off, const float* cent, int nlist, int dpad, int kpad8,
                       void* out, float* scale, float* rnorm, cudaStream_t st);
-void launch_gather_queries_fp8(const float* q, int dpad, int kpad8, const int32_t* list_q, const int64_t* list_qoff,
-                               int nlist, const float* cent, int64_t max_rows, float* escale, float* ecd, void* G,
-                               cudaStream_t st);
+// Per list-major entry e (query q, list l): row e of G = q - c_l in BF16, or
+// (fp8) E4M3 with its scale escale[e]; ecd[e] = ||q - c_l||^2.
+void launch_gather_residual(const float* q, int dpad, int kpad, bool fp8, const int32_t* list_q,
+                            const int64_t* list_qoff, int nlist, const float* cent, int64_t max_rows, float* escale,
+                            float* ecd, void* G, cudaStream_t st);
 void make_u8_tensor_map(void* tmap_out, const void* base, size_t rows, int row_bytes);
 // Selection of each query's R candidates (rows: nq x R stored rows, -1 past
 // the candidates), then their exact re-rank to the k best.

@@ -222,11 +222,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int64_t qp = static_cast<int64_t>(e >> 16) * a.P + (e & 0xffffu);
         sbase = a.seg[qp];
         slen = a.seg[qp + 1] - sbase;
-        if (FP8) {
-          // Residuals: ||q - x||^2 = ||q - c_l||^2 + ||r||^2 - 2 (q - c_l).r
-          f = -2.0f * a.qscale[d.qrow0 + tid] * a.list_scale[d.list];
-          c0 = a.qcd[d.qrow0 + tid];
-        }
+        // Residuals: ||q - x||^2 = ||q - c_l||^2 + ||r||^2 - 2 (q - c_l).r
+        c0 = a.qcd[d.qrow0 + tid];
+        if (FP8) f = -2.0f * a.qscale[d.qrow0 + tid] * a.list_scale[d.list];
       }
       for (int t = 0; t < d.ntiles; ++t, ++tile) {
         const int b = static_cast<int>(tile % kAccN);
@@ -270,39 +268,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 5) {
     tc_fence_after();
     tmem_dealloc(tmem, kAccN * kT);
-  }
-}
-
-// Row e of the gathered matrix = the query of list-major entry e in BF16
-// (columns past dpad zero).  Entries are (query << 16 | probe rank).
-__global__ void gather_queries_kernel(const float* __restrict__ q, int dpad, int kpad,
-                                      const int32_t* __restrict__ list_q, const int64_t* __restrict__ n_entries,
-                                      int64_t max_rows, __nv_bfloat16* __restrict__ G) {
-  const int64_t rows = min(*n_entries, max_rows);
-  const int per_row = kpad / 8;
-  const int64_t total = rows * per_row;
-  for (int64_t u = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; u < total;
-       u += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t e = u / per_row;
-    const int c = static_cast<int>(u - e * per_row) * 8;
-    const int qi = static_cast<int>(static_cast<uint32_t>(list_q[e]) >> 16);
-    const float* src = q + static_cast<int64_t>(qi) * dpad;
-    float x[8];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int cc = c + 4 * h;
-      float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (cc < dpad) f = *reinterpret_cast<const float4*>(src + cc);  // dpad is a multiple of 4
-      x[4 * h] = f.x, x[4 * h + 1] = f.y, x[4 * h + 2] = f.z, x[4 * h + 3] = f.w;
-    }
-    uint4 o;
-    uint32_t* ow = reinterpret_cast<uint32_t*>(&o);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      __nv_bfloat162 p = __floats2bfloat162_rn(x[2 * j], x[2 * j + 1]);
-      ow[j] = *reinterpret_cast<uint32_t*>(&p);
-    }
-    *reinterpret_cast<uint4*>(G + e * kpad + c) = o;
   }
 }
 
@@ -368,13 +333,15 @@ __global__ void list_fp8_kernel(const float* __restrict__ codes, const int64_t* 
   }
 }
 
-// One warp per list-major entry e (query q, list l): q' = q - c_l, its scale
-// s_e = max |q'| / 448, E4M3(q' / s_e) as row e of the gathered matrix, and
-// ||q'||^2 (the FP8 scan's value of a row is ||q'||^2 + ||r||^2 - 2 q'.r).
-__global__ void gather_queries_fp8_kernel(const float* __restrict__ q, int dpad, int kpad8,
-                                          const int32_t* __restrict__ list_q, const int64_t* __restrict__ list_qoff,
-                                          int nlist, const float* __restrict__ cent, int64_t max_rows,
-                                          float* __restrict__ escale, float* __restrict__ ecd, uint8_t* __restrict__ G) {
+// One warp per list-major entry e (query q, list l): q' = q - c_l as row e of
+// the gathered matrix -- BF16, or (FP8) E4M3(q' / s_e) with the entry's scale
+// s_e = max |q'| / 448 -- and ||q'||^2 (the scan's value of a row is
+// ||q'||^2 + ||r||^2 - 2 q'.r with r = x - c_l).
+template <bool FP8>
+__global__ void gather_residual_kernel(const float* __restrict__ q, int dpad, int kpad,
+                                       const int32_t* __restrict__ list_q, const int64_t* __restrict__ list_qoff,
+                                       int nlist, const float* __restrict__ cent, int64_t max_rows,
+                                       float* __restrict__ escale, float* __restrict__ ecd, void* __restrict__ G) {
   const int lane = threadIdx.x & 31;
   const int64_t rows = min(list_qoff[nlist], max_rows);
   for (int64_t e = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; e < rows;
@@ -397,16 +364,30 @@ __global__ void gather_queries_fp8_kernel(const float* __restrict__ q, int dpad,
       m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
       sq += __shfl_xor_sync(0xffffffffu, sq, o);
     }
-    const float inv = m > 0.0f ? 448.0f / m : 1.0f;
-    if (lane == 0) {
-      escale[e] = 1.0f / inv;
-      ecd[e] = sq;
-    }
-    for (int cc = lane * 16; cc < kpad8; cc += 32 * 16) {
-      float x[16];
+    if (lane == 0) ecd[e] = sq;
+    if (FP8) {
+      const float inv = m > 0.0f ? 448.0f / m : 1.0f;
+      if (lane == 0) escale[e] = 1.0f / inv;
+      uint8_t* row = static_cast<uint8_t*>(G) + e * kpad;
+      for (int cc = lane * 16; cc < kpad; cc += 32 * 16) {
+        float x[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) x[j] = cc + j < dpad ? src[cc + j] - c[cc + j] : 0.0f;
-      *reinterpret_cast<uint4*>(G + e * kpad8 + cc) = to_e4m3x16(x, inv);
+        for (int j = 0; j < 16; ++j) x[j] = cc + j < dpad ? src[cc + j] - c[cc + j] : 0.0f;
+        *reinterpret_cast<uint4*>(row + cc) = to_e4m3x16(x, inv);
+      }
+    } else {
+      __nv_bfloat16* row = static_cast<__nv_bfloat16*>(G) + e * kpad;
+      for (int cc = lane * 8; cc < kpad; cc += 32 * 8) {
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float a0 = cc + 2 * j < dpad ? src[cc + 2 * j] - c[cc + 2 * j] : 0.0f;
+          const float a1 = cc + 2 * j + 1 < dpad ? src[cc + 2 * j + 1] - c[cc + 2 * j + 1] : 0.0f;
+          __nv_bfloat162 p2 = __floats2bfloat162_rn(a0, a1);
+          w[j] = *reinterpret_cast<uint32_t*>(&p2);
+        }
+        *reinterpret_cast<uint4*>(row + cc) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
     }
   }
 }
@@ -692,21 +673,10 @@ void launch_cand_segments(const int32_t* probes, int nq, int P, const int64_t* l
   HB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, len, seg, static_cast<int64_t>(n), st));
 }
 
-void launch_gather_queries(const float* q, int dpad, int kpad, const int32_t* list_q, const int64_t* n_entries,
-                           int64_t max_rows, void* G, cudaStream_t st) {
-  if (max_rows <= 0) return;
-  HB_CHECK(kpad % 64 == 0 && dpad % 4 == 0 && dpad <= kpad, HB_ERR_INVALID, "bad query padding");
-  int64_t g = (max_rows * (kpad / 8) + 255) / 256;
-  if (g > 148 * 32) g = 148 * 32;
-  gather_queries_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(q, dpad, kpad, list_q, n_entries, max_rows,
-                                                                  static_cast<__nv_bfloat16*>(G));
-  HB_CUDA(cudaGetLastError());
-}
-
 void launch_cand_scan(const void* tmap_q, const void* tmap_x, const CandArgs& a, int num_sms, cudaStream_t st) {
   const int blk = a.fp8 ? 128 : 64;
   HB_CHECK(a.kpad >= blk && a.kpad % blk == 0, HB_ERR_INVALID, "the candidate scan needs whole 128-byte K blocks");
-  HB_CHECK(!a.fp8 || (a.qscale && a.list_scale && a.qcd), HB_ERR_INVALID, "FP8 scan without scales");
+  HB_CHECK(a.qcd && (!a.fp8 || (a.qscale && a.list_scale)), HB_ERR_INVALID, "residual scan without its constants");
   HB_CHECK(a.chunk_rows >= kT && a.chunk_rows % kT == 0, HB_ERR_INVALID, "chunk rows must be a multiple of 128");
   const size_t smem = kStg * static_cast<size_t>(kStageBytes) + 1024;
   const CUtensorMap* mq = static_cast<const CUtensorMap*>(tmap_q);
@@ -731,15 +701,19 @@ void launch_fp8_codes(const float* codes, const int64_t* list_off, const float* 
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_gather_queries_fp8(const float* q, int dpad, int kpad8, const int32_t* list_q, const int64_t* list_qoff,
-                               int nlist, const float* cent, int64_t max_rows, float* escale, float* ecd, void* G,
-                               cudaStream_t st) {
+void launch_gather_residual(const float* q, int dpad, int kpad, bool fp8, const int32_t* list_q,
+                            const int64_t* list_qoff, int nlist, const float* cent, int64_t max_rows, float* escale,
+                            float* ecd, void* G, cudaStream_t st) {
   if (max_rows <= 0) return;
-  HB_CHECK(kpad8 % 128 == 0 && dpad <= kpad8 && kpad8 <= 32 * 16 * 4, HB_ERR_INVALID, "bad FP8 query padding");
+  HB_CHECK(kpad % (fp8 ? 128 : 64) == 0 && dpad <= kpad && kpad <= 2048, HB_ERR_INVALID, "bad residual padding");
   int64_t g = (max_rows * 32 + 255) / 256;
   if (g > 148 * 32) g = 148 * 32;
-  gather_queries_fp8_kernel<<<static_cast<unsigned>(g), 256, 0, st>>>(q, dpad, kpad8, list_q, list_qoff, nlist, cent,
-                                                                      max_rows, escale, ecd, static_cast<uint8_t*>(G));
+  if (fp8)
+    gather_residual_kernel<true><<<static_cast<unsigned>(g), 256, 0, st>>>(q, dpad, kpad, list_q, list_qoff, nlist,
+                                                                           cent, max_rows, escale, ecd, G);
+  else
+    gather_residual_kernel<false><<<static_cast<unsigned>(g), 256, 0, st>>>(q, dpad, kpad, list_q, list_qoff, nlist,
+                                                                            cent, max_rows, escale, ecd, G);
   HB_CUDA(cudaGetLastError());
 }
 

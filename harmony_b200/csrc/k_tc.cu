@@ -1,27 +1,33 @@
 // BF16 tensor-core list scan (tcgen05 + TMA) and the exact FP32 re-rank,
 // whose result equals the exact FP32 scan's bit for bit.
 //
-// Error bound.  For a query q and a stored row x the scan forms
-//   w(x) = ||x||^2 - 2 q~.x~      (q~, x~: BF16 roundings; ||x||^2 the stored
-//                                  FP32 norm; the dot product on the tensor
-//                                  cores with FP32 accumulation)
+// Error bound.  The tensor cores work on residuals to the list centroid c_l:
+// for a query q, a probed list l and a stored row x of l the scan forms
+//   w(x) = cd + ||r||^2 - 2 q~'.r~   (q' = q - c_l, r = x - c_l in FP32; q~', r~
+//                                    their BF16 roundings; cd = ||q'||^2 and
+//                                    ||r||^2 FP32 sums; the dot product on the
+//                                    tensor cores with FP32 accumulation)
 // and the reference's distance is d(x) = the sequential unfused FP32 sum of
-// (q_i - x_i)^2 (src/utils.h:480-487).  With Q = ||q||, M = max ||x|| over
-// the index, u = 2^-24 and D = ||q - x||^2 <= (Q + M)^2:
-//   |2 q~.x~ - 2 q.x|  <= 2 (2^-8 + 2^-16) Q M   BF16 rounding of both operands
-//                       + 2 * 2^-10 Q M           FP32 accumulation of kpad <= 128
+// (q_i - x_i)^2 (src/utils.h:480-487).  With Q = ||q'||, R = the list's largest
+// ||r||, u = 2^-24 and D = ||q - x||^2 = ||q' - r||^2 <= (Q + R)^2:
+//   |2 q~'.r~ - 2 q'.r| <= 2 (2^-8 + 2^-16) Q R   BF16 (and FP32 residual)
+//                                                 rounding of both operands
+//                        + 2 * 2^-10 Q R           FP32 accumulation of kpad <= 128
 //                                                 exact products (even with only
 //                                                 17 bits kept per addition)
-//   | ||x||^2 stored - ||x||^2 | <= (d + 1) u M^2  sequential FP32 sum
-//   rounding of w                <= u (Q + M)^2
-//   | d(x) - D |                 <= (d + 3) u D     sequential FP32 sum
-// so |w(x) + Q^2 - d(x)| <= eps(q), eps = 1.0625 * (2 (2^-8 + 2^-10 + 2^-16) Q M
-// + (d + 1) u M^2 + (d + 4) u (Q + M)^2).  Let W_k be the k-th smallest w over
-// the probed rows.  The k rows with the smallest w have d <= W_k + Q^2 + eps,
-// so the k-th smallest d is at most that, and every row of the exact top k
-// (ties at the k-th distance included) has w <= W_k + 2 eps.  Re-ranking
-// exactly every row with w <= W_k + 2 eps, by (FP32 distance, position) like
-// the exact scan, therefore returns the exact scan's result.
+//   |cd - Q^2|, | ||r||^2 stored - R-part |  <= (d + 3) u (Q^2 + R^2)
+//   rounding of w (two additions)            <= 2 u (Q + R)^2
+//   | d(x) - D |                             <= (d + 3) u D
+// so |w(x) - d(x)| <= eps(q, l) = 1.0625 * (2 (2^-8 + 2^-10 + 2^-16) Q R
+// + (d + 3) u (Q^2 + R^2) + (d + 5) u (Q + R)^2), and eps(q) = the largest
+// eps(q, l) over the query's probed lists.  Residuals keep Q and R at the
+// scale of a list's spread, not of the data's distance from the origin.  Let
+// W_k be the k-th smallest w over the probed rows.  The k rows with the
+// smallest w have d <= W_k + eps, so the k-th smallest d is at most that, and
+// every row of the exact top k (ties at the k-th distance included) has
+// w <= W_k + 2 eps.  Re-ranking exactly every row with w <= W_k + 2 eps, by
+// (FP32 distance, position) like the exact scan, therefore returns the exact
+// scan's result.
 //
 // Admission.  A row is appended to its query's candidate buffer when
 // w <= thr(q).  thr starts at the seed bound (the k-th smallest of the same
@@ -43,7 +49,8 @@
 // tcgen05.mma (M 128 queries x N 128 rows x K 16) into one of four TMEM
 // accumulators; the epilogue warps read their TMEM lanes back (thread =
 // query, 128 columns = rows), form w and append the rows under the query's
-// bound.
+// bound.  The builders form the A tile, BF16(q - c_l) for the item's list,
+// from the FP32 queries.
 //
 // Warp roles (384 threads), all running ahead of each other through
 // mbarriers, with no CTA-wide barrier between items:
@@ -154,7 +161,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   int* meta_q = reinterpret_cast<int*>(nrm + kAcc * kTile);                 // [2][128]
   float* meta_thr = reinterpret_cast<float*>(meta_q + 2 * kTile);           // [2][128]
   float* meta_e2 = meta_thr + 2 * kTile;                                    // [2][128]
-  uint64_t* staging = reinterpret_cast<uint64_t*>(meta_e2 + 2 * kTile);     // [kGroups][kStage][128]
+  float* meta_cd = meta_e2 + 2 * kTile;                                     // [2][128] ||q - c_l||^2
+  float* s_cent = meta_cd + 2 * kTile;                                      // [2][128] the item's centroid
+  uint64_t* staging = reinterpret_cast<uint64_t*>(s_cent + 2 * kTile);      // [kGroups][kStage][128]
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -191,7 +200,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ---- item builders ---------------------------------------------------
     const int bt = tid - kBuildWarp0 * 32;
     constexpr int kBt = kBuildWarps * 32;
-    const int cpr = kpad / 8;  // 16-byte chunks per BF16 query row
     ItemDesc nd;
     nd.ntiles = -1;
     if (bt == 0) nd = fetch_item(a, total_items);
@@ -205,6 +213,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const ItemDesc d = sh.desc[ab];
       if (d.ntiles >= 0) {
         const int64_t qbase = a.list_qoff[d.list] + static_cast<int64_t>(d.group) * kTile;
+        float* cen = s_cent + ab * kTile;
+        for (int c = bt; c < kpad; c += kBt) cen[c] = c < a.dpad ? a.cent[static_cast<size_t>(d.list) * a.dpad + c] : 0.0f;
         for (int r = bt; r < kTile; r += kBt) {
           int q = -1;
           float thr = -INFINITY, e2 = 0.0f;
@@ -219,15 +229,38 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           meta_e2[ab * kTile + r] = e2;
         }
         asm volatile("bar.sync 3, %0;\n" ::"n"(kBt) : "memory");
+        // A row r = BF16(q - c_l) of the item's query r, and ||q - c_l||^2.
         uint8_t* A = Abuf + ab * tile_bytes;
-        const uint4* qb = reinterpret_cast<const uint4*>(a.qbf);
-#pragma unroll 4
-        for (int i = bt; i < kTile * cpr; i += kBt) {
-          const int r = i / cpr, c = i - r * cpr;
+        for (int r = bt; r < kTile; r += kBt) {
           const int q = meta_q[ab * kTile + r];
-          uint4 v = make_uint4(0u, 0u, 0u, 0u);
-          if (q >= 0) v = __ldg(qb + static_cast<size_t>(q) * cpr + c);
-          *reinterpret_cast<uint4*>(A + sw128_offset_bf16(r, c * 8, kblk_bytes)) = v;
+          const float* qrow = a.q + static_cast<size_t>(q < 0 ? 0 : q) * a.dpad;
+          float cd = 0.0f;
+#pragma unroll 4
+          for (int k = 0; k < kpad; k += 8) {
+            float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (q >= 0 && k < a.dpad) {  // dpad is a multiple of 16: a row's 8 values are all in or all out
+              const float4 lo = __ldg(reinterpret_cast<const float4*>(qrow + k));
+              const float4 hi = __ldg(reinterpret_cast<const float4*>(qrow + k + 4));
+              v[0] = lo.x - cen[k];
+              v[1] = lo.y - cen[k + 1];
+              v[2] = lo.z - cen[k + 2];
+              v[3] = lo.w - cen[k + 3];
+              v[4] = hi.x - cen[k + 4];
+              v[5] = hi.y - cen[k + 5];
+              v[6] = hi.z - cen[k + 6];
+              v[7] = hi.w - cen[k + 7];
+            }
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              cd = fmaf(v[2 * j], v[2 * j], cd);
+              cd = fmaf(v[2 * j + 1], v[2 * j + 1], cd);
+              __nv_bfloat162 p2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+              w[j] = *reinterpret_cast<uint32_t*>(&p2);
+            }
+            *reinterpret_cast<uint4*>(A + sw128_offset_bf16(r, k, kblk_bytes)) = make_uint4(w[0], w[1], w[2], w[3]);
+          }
+          meta_cd[ab * kTile + r] = cd;
         }
         fence_proxy_async_smem();
       }
@@ -335,9 +368,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const int my_q = meta_q[ab * kTile + etid];
       const float thr0 = meta_thr[ab * kTile + etid];
       const float e2 = meta_e2[ab * kTile + etid];
+      const float cd = meta_cd[ab * kTile + etid];
       mbar_arrive(&sh.aempty[ab]);
       if (d.ntiles < 0) break;
       float thr = thr0;
+      // Columns hold w' = ||r||^2 - 2 q'.r; a row's value is w = cd + w'.  A
+      // column is looked at when w' <= thr_s, thr_s = thr - cd rounded up with
+      // a margin (every row with w <= thr passes; a few more may).
+      auto shifted = [&](float t) { return __fadd_ru(__fsub_ru(t, cd), 1e-6f * (fabsf(t) + cd)); };
+      float thr_s = shifted(thr);
       // The KT smallest values this thread has admitted for the query in this
       // item, ascending (KT = 0: no tightening).
       float best[KB];
@@ -364,7 +403,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         ok = ok && mbar_wait(&sh.accf[b], par, err, 14, budget) && mbar_wait(&sh.normf[b], par, err, 15, budget);
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
-        if (my_q >= 0) thr = fminf(thr, ordered_to_float(g_thr));
+        if (my_q >= 0 && ordered_to_float(g_thr) < thr) {
+          thr = ordered_to_float(g_thr);
+          thr_s = shifted(thr);
+        }
         const float* nb = nrm + b * kTile;
         const uint32_t pos_t = static_cast<uint32_t>(d.row0 + t * kTile);
 #pragma unroll 1
@@ -393,10 +435,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               r[4 * j4 + 3] = __float_as_uint(v3);
               mn = fminf(mn, fminf(fminf(v0, v1), fminf(v2, v3)));
             }
-            if (mn <= thr) {
+            if (mn <= thr_s) {
               uint32_t mq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-              for (int j = 0; j < 32; ++j) mq[j & 3] |= (__uint_as_float(r[j]) <= thr ? 1u : 0u) << j;
+              for (int j = 0; j < 32; ++j) mq[j & 3] |= (__uint_as_float(r[j]) <= thr_s ? 1u : 0u) << j;
               uint32_t mask = (mq[0] | mq[1]) | (mq[2] | mq[3]);
               const uint32_t pos0 = pos_t + static_cast<uint32_t>(c * 32);
               while (mask) {
@@ -412,7 +454,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 for (int i = 0; i < 4; ++i) t4[i] = (j & 4) ? t8[2 * i + 1] : t8[2 * i];
 #pragma unroll
                 for (int i = 0; i < 2; ++i) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
-                const float wv = __uint_as_float((j & 16) ? t2[1] : t2[0]);
+                const float wv = cd + __uint_as_float((j & 16) ? t2[1] : t2[0]);
                 stg[ns * kEpiThreads] = (static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j));
                 if (++ns == kStage) flush();
                 if (KT > 0) {
@@ -432,6 +474,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const float nt = __fadd_ru(kth, e2);
                     if (nt < thr) {
                       thr = nt;
+                      thr_s = shifted(thr);
                       atomicMin(a.thr + my_q, ordered_bits(thr));  // shared at once (no return value used)
                     }
                   }
@@ -457,33 +500,82 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
-// Per query, before the scan: its BF16 row (the A operand of the scan and
-// the seed), 2 eps (see the top of this file), the admission bound reset to
-// FLT_MAX (no bound yet; +inf padding rows never pass) and the candidate
+// The error bound of one (query, list) pair (see the top of this file):
+// Q = ||q - c_l|| from its FP32 square cd, R = the list's largest residual
+// norm, d the dimension.
+__device__ __forceinline__ float pair_eps(float cd, float R, int d) {
+  const float Q = sqrtf(cd) * 1.0001f + 1e-30f;
+  const float u = 5.9604645e-8f;  // 2^-24
+  const float c1 = 0.00390625f + 0.0009765625f + 1.52587890625e-5f;
+  return 1.0625f * (2.0f * c1 * Q * R + (d + 3) * u * (R * R + Q * Q) + (d + 5) * u * (Q + R) * (Q + R));
+}
+
+// Per query, before the scan: 2 eps_max, eps_max the largest pair bound over
+// the query's probed lists (probes row, -1 = none); the admission bound reset
+// to FLT_MAX (no bound yet; +inf padding rows never pass); the candidate
 // counter reset.  One warp per query.
-__global__ void query_prep_kernel(const float* __restrict__ q, int nq, int d, int dpad, int kpad,
-                                  const float* __restrict__ maxnorm, __nv_bfloat16* __restrict__ qbf,
-                                  float* __restrict__ e2, uint32_t* __restrict__ thr, int* __restrict__ cnt) {
+__global__ void query_prep_kernel(const float* __restrict__ q, int nq, int d, int dpad,
+                                  const int32_t* __restrict__ probes, int P, const float* __restrict__ cent,
+                                  const float* __restrict__ rmax, float* __restrict__ e2, uint32_t* __restrict__ thr,
+                                  int* __restrict__ cnt) {
   const int lane = threadIdx.x & 31;
   const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (qi >= nq) return;
   const float* row = q + static_cast<size_t>(qi) * dpad;
-  float s = 0.0f;
-  for (int c = lane; c < kpad; c += 32) {
-    const float v = c < dpad ? row[c] : 0.0f;
-    qbf[static_cast<size_t>(qi) * kpad + c] = __float2bfloat16_rn(v);
-    s = fmaf(v, v, s);
+  float emax = 0.0f;
+  for (int j = 0; j < P; ++j) {
+    const int l = probes[static_cast<size_t>(qi) * P + j];
+    if (l < 0) continue;
+    const float* c = cent + static_cast<size_t>(l) * dpad;
+    float s = 0.0f;
+    for (int i = lane; i < dpad; i += 32) {
+      const float v = row[i] - c[i];
+      s = fmaf(v, v, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    emax = fmaxf(emax, pair_eps(s, rmax[l], d));
   }
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if (lane == 0) {
-    const float Q = sqrtf(s) * 1.0001f;
-    const float M = *maxnorm;
-    const float u = 5.9604645e-8f;  // 2^-24
-    const float c1 = 0.00390625f + 0.0009765625f + 1.52587890625e-5f;
-    const float eps = 1.0625f * (2.0f * c1 * Q * M + (d + 1) * u * M * M + (d + 4) * u * (Q + M) * (Q + M));
-    e2[qi] = 2.0f * eps + 1e-30f;
+    e2[qi] = 2.0f * emax + 1e-30f;
     thr[qi] = ordered_bits(FLT_MAX);
     cnt[qi] = 0;
+  }
+}
+
+// BF16 residual codes for the tensor-core scans, one CTA per list: row r of
+// list l becomes BF16(x_r - c_l) (kpad columns, zero past dpad), its FP32
+// residual norm ||x_r - c_l||^2, and the list's largest residual norm
+// (slightly rounded up).
+__global__ void residual_bf16_kernel(const float* __restrict__ codes, const int64_t* __restrict__ list_off,
+                                     const float* __restrict__ cent, int dpad, int kpad,
+                                     __nv_bfloat16* __restrict__ dst, float* __restrict__ rnorm,
+                                     float* __restrict__ rmax) {
+  __shared__ float s_max[32];
+  const int l = blockIdx.x;
+  const int64_t r0 = list_off[l], r1 = list_off[l + 1];
+  const float* c = cent + static_cast<size_t>(l) * dpad;
+  for (int64_t i = threadIdx.x; i < (r1 - r0) * kpad; i += blockDim.x) {
+    const int64_t r = r0 + i / kpad;
+    const int col = static_cast<int>(i % kpad);
+    dst[r * kpad + col] = __float2bfloat16_rn(col < dpad ? codes[r * dpad + col] - c[col] : 0.0f);
+  }
+  const int lane = threadIdx.x & 31;
+  float m = 0.0f;
+  for (int64_t r = r0 + (threadIdx.x >> 5); r < r1; r += blockDim.x >> 5) {
+    float sq = 0.0f;
+    for (int j = lane; j < dpad; j += 32) {
+      const float v = codes[r * dpad + j] - c[j];
+      sq = fmaf(v, v, sq);
+    }
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    if (lane == 0) rnorm[r] = sq;
+    m = fmaxf(m, sq);
+  }
+  if (lane == 0) s_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmaxf(m, s_max[w]);
+    rmax[l] = sqrtf(m) * 1.0001f;
   }
 }
 
@@ -500,7 +592,7 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
     const uint64_t* __restrict__ cand, const int* __restrict__ cnt, int cap, const float* __restrict__ e2, int nq, int k,
     const float* __restrict__ codes, const float* __restrict__ q, int dpad, const int64_t* __restrict__ ids,
     float* __restrict__ D, int64_t* __restrict__ I, int* __restrict__ flag, int* __restrict__ over_list,
-    int* __restrict__ over_n, int* __restrict__ m_out) {
+    int* __restrict__ over_n, int* __restrict__ m_out, int* __restrict__ big_list) {
   __shared__ uint64_t s_c[kRrWarps][kRrWarpCap];
   __shared__ uint64_t s_x[kRrWarps][kRrWarpCap];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -516,7 +608,10 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
     return;
   }
   if (c > kRrWarpCap) {
-    if (lane == 0) flag[qi] = 1;
+    if (lane == 0) {
+      flag[qi] = 1;
+      big_list[atomicAdd(over_n + 1, 1)] = qi;
+    }
     return;
   }
   if (lane == 0) flag[qi] = 0;
@@ -560,19 +655,21 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
   }
 }
 
-// The same for the queries flagged 1 (more than kRrWarpCap candidates, at
-// most cap): one CTA per query, grid-stride over the batch.
+// The same for the queries the warp kernel listed in big_list (more than
+// kRrWarpCap candidates, at most cap; *big_n of them): one CTA per query,
+// grid-stride over the list.
 __global__ void __launch_bounds__(256) rerank_cta_kernel(const uint64_t* __restrict__ cand, const int* __restrict__ cnt,
                                                          int cap, const float* __restrict__ e2, int nq, int k,
                                                          const float* __restrict__ codes, const float* __restrict__ q,
                                                          int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
-                                                         int64_t* __restrict__ I, const int* __restrict__ flag,
-                                                         int* __restrict__ m_out) {
+                                                         int64_t* __restrict__ I, const int* __restrict__ big_list,
+                                                         const int* __restrict__ big_n, int* __restrict__ m_out) {
   extern __shared__ uint64_t s_dyn[];  // [cap] candidates, then [cap] exact keys
   __shared__ SelectShared sh_sel;
   __shared__ int s_m;
-  for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
-    if (flag[qi] != 1) continue;
+  const int nbig = *big_n;
+  for (int bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+    const int qi = big_list[bi];
     const int c = cnt[qi];
     const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
     uint64_t* buf = s_dyn;
@@ -626,7 +723,8 @@ constexpr int kSeedRows = 256;
 constexpr int kSeedWarps = 8;
 
 __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
-    const __nv_bfloat16* __restrict__ qbf, int kpad, const __nv_bfloat16* __restrict__ codes,
+    const float* __restrict__ q, int dpad, const float* __restrict__ cent, int kpad,
+    const __nv_bfloat16* __restrict__ codes,
     const int64_t* __restrict__ list_off, const int64_t* __restrict__ list_qoff, const int32_t* __restrict__ list_q,
     const float* __restrict__ xnorm, int S, int k, const float* __restrict__ e2, uint32_t* __restrict__ thr,
     const int32_t* __restrict__ probes, int P) {
@@ -634,7 +732,8 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
   __shared__ float s_xn[kSeedRows];
   __shared__ int s_qs[kSeedWarps * 32];
   __shared__ int s_nq;
-  const int tid = threadIdx.x;
+  __shared__ float s_cd;
+  const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const bool by_query = probes != nullptr;
   int l;
   int64_t e0, e1;
@@ -677,9 +776,23 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
     const int nqr = s_nq;
     for (int t = 0; t < nqr; ++t) {
       const int qi = s_qs[t];
-      const __nv_bfloat16* qrow = qbf + static_cast<size_t>(qi) * kpad;
-      for (int c = tid; c < kpad; c += blockDim.x) qbuf[c] = __bfloat162float(qrow[c]);
+      // The query's residual to this list's centroid in BF16 (the scan's A
+      // row) and ||q - c_l||^2.
+      const float* qrow = q + static_cast<size_t>(qi) * dpad;
+      const float* crow = cent + static_cast<size_t>(l) * dpad;
+      for (int c = tid; c < kpad; c += blockDim.x)
+        qbuf[c] = c < dpad ? __bfloat162float(__float2bfloat16_rn(qrow[c] - crow[c])) : 0.0f;
+      if (wib == 0) {
+        float cd = 0.0f;
+        for (int c = lane; c < dpad; c += 32) {
+          const float v = qrow[c] - crow[c];
+          cd = fmaf(v, v, cd);
+        }
+        for (int o = 16; o > 0; o >>= 1) cd += __shfl_xor_sync(0xffffffffu, cd, o);
+        if (lane == 0) s_cd = cd;
+      }
       __syncthreads();
+      const float cdq = s_cd;
       uint32_t key = 0xFFFFFFFFu;
       if (tid < n) {
         const uint8_t* xr = rows + static_cast<size_t>(tid) * stride;
@@ -699,7 +812,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
           d2 = fmaf(qb.z, __uint_as_float(xv.w << 16), d2);
           d3 = fmaf(qb.w, __uint_as_float(xv.w & 0xffff0000u), d3);
         }
-        key = ordered_bits(fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[tid]));
+        key = ordered_bits(cdq + fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[tid]));
       }
       uint32_t prefix = 0;
       int need = k;
@@ -785,7 +898,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 size_t scan_bf16_smem_bytes(int kpad, int stages) {
   const size_t tile = static_cast<size_t>(kpad / 64) * kTile * 128;
-  return 1024 + tile * (2 + stages) + static_cast<size_t>(kAcc) * kTile * 4 + 2 * kTile * (4 + 4 + 4) +
+  return 1024 + tile * (2 + stages) + static_cast<size_t>(kAcc) * kTile * 4 + 2 * kTile * (4 + 4 + 4 + 4 + 4) +
          static_cast<size_t>(kGroups) * kStage * kEpiThreads * 8;
 }
 
@@ -835,17 +948,25 @@ void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_query_prep(const float* q, int nq, int d, int dpad, int kpad, const float* maxnorm, void* qbf, float* e2,
-                       uint32_t* thr, int* cnt, cudaStream_t st) {
+void launch_query_prep(const float* q, int nq, int d, int dpad, const int32_t* probes, int P, const float* cent,
+                       const float* rmax, float* e2, uint32_t* thr, int* cnt, cudaStream_t st) {
   if (nq <= 0) return;
-  query_prep_kernel<<<(nq + 7) / 8, 256, 0, st>>>(q, nq, d, dpad, kpad, maxnorm, static_cast<__nv_bfloat16*>(qbf), e2,
-                                                  thr, cnt);
+  query_prep_kernel<<<(nq + 7) / 8, 256, 0, st>>>(q, nq, d, dpad, probes, P, cent, rmax, e2, thr, cnt);
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_seed_bound(const void* qbf, int nq, int kpad, const void* codes_bf16, const int64_t* list_off, int nlist,
-                       const int64_t* list_qoff, const int32_t* list_q, const float* xnorm, int S, int k,
-                       const float* e2, uint32_t* thr, cudaStream_t st, const int32_t* probes, int P) {
+void launch_residual_bf16(const float* codes, const int64_t* list_off, const float* cent, int nlist, int dpad, int kpad,
+                          void* dst, float* rnorm, float* rmax, cudaStream_t st) {
+  if (nlist <= 0) return;
+  residual_bf16_kernel<<<nlist, 256, 0, st>>>(codes, list_off, cent, dpad, kpad, static_cast<__nv_bfloat16*>(dst),
+                                              rnorm, rmax);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_seed_bound(const float* q, int dpad, const float* cent, int nq, int kpad, const void* codes_bf16,
+                       const int64_t* list_off, int nlist, const int64_t* list_qoff, const int32_t* list_q,
+                       const float* rnorm, int S, int k, const float* e2, uint32_t* thr, cudaStream_t st,
+                       const int32_t* probes, int P) {
   if (nq <= 0) return;
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
   HB_CHECK(S >= 1 && S <= kSeedRows && k >= 1, HB_ERR_INVALID, "seed sample out of range");
@@ -854,8 +975,8 @@ void launch_seed_bound(const void* qbf, int nq, int kpad, const void* codes_bf16
   HB_CUDA(cudaFuncSetAttribute(seed_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const bool by_query = probes && static_cast<long long>(nq) * 4 < nlist;
   seed_bound_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(
-      static_cast<const __nv_bfloat16*>(qbf), kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff,
-      list_q, xnorm, S, k, e2, thr, by_query ? probes : nullptr, P);
+      q, dpad, cent, kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff, list_q, rnorm, S, k, e2,
+      thr, by_query ? probes : nullptr, P);
   HB_CUDA(cudaGetLastError());
 }
 
@@ -867,14 +988,15 @@ void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const flo
            "candidate buffer size out of range");
   rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(cand, cnt, cap, e2, nq, k, codes, q,
                                                                                dpad, ids, D, I, flag, over_list, over_n,
-                                                                               m_out);
+                                                                               m_out, over_list + nq);
   HB_CUDA(cudaGetLastError());
   if (cap > kRrWarpCap) {
     const size_t smem = static_cast<size_t>(2) * cap * sizeof(uint64_t);
     HB_CUDA(cudaFuncSetAttribute(rerank_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     const int grid = std::min(nq, 4 * num_sms);
-    rerank_cta_kernel<<<grid, 256, smem, st>>>(cand, cnt, cap, e2, nq, k, codes, q, dpad, ids, D, I, flag, m_out);
+    rerank_cta_kernel<<<grid, 256, smem, st>>>(cand, cnt, cap, e2, nq, k, codes, q, dpad, ids, D, I, over_list + nq,
+                                               over_n + 1, m_out);
     HB_CUDA(cudaGetLastError());
   }
 }

@@ -374,8 +374,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       float thr = thr0;
       // Columns hold w' = ||r||^2 - 2 q'.r; a row's value is w = cd + w'.  A
       // column is looked at when w' <= thr_s, thr_s = thr - cd rounded up with
-      // a margin (every row with w <= thr passes; a few more may).
-      auto shifted = [&](float t) { return __fadd_ru(__fsub_ru(t, cd), 1e-6f * (fabsf(t) + cd)); };
+      // a margin (every row with w <= thr passes; a few more may), and never
+      // above FLT_MAX: the +inf values of rows past a list's end must not pass.
+      auto shifted = [&](float t) {
+        return fminf(__fadd_ru(__fsub_ru(t, cd), 1e-6f * (fminf(fabsf(t), 1e30f) + cd)), FLT_MAX);
+      };
       float thr_s = shifted(thr);
       // The KT smallest values this thread has admitted for the query in this
       // item, ascending (KT = 0: no tightening).

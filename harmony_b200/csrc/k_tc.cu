@@ -526,17 +526,24 @@ __global__ void query_prep_kernel(const float* __restrict__ q, int nq, int d, in
   if (qi >= nq) return;
   const float* row = q + static_cast<size_t>(qi) * dpad;
   float emax = 0.0f;
-  for (int j = 0; j < P; ++j) {
-    const int l = probes[static_cast<size_t>(qi) * P + j];
-    if (l < 0) continue;
-    const float* c = cent + static_cast<size_t>(l) * dpad;
-    float s = 0.0f;
-    for (int i = lane; i < dpad; i += 32) {
-      const float v = row[i] - c[i];
-      s = fmaf(v, v, s);
+  // The probe row 32 entries at a time (one coalesced load), each valid
+  // entry's distance by the whole warp.
+  for (int j0 = 0; j0 < P; j0 += 32) {
+    const int mine = j0 + lane < P ? probes[static_cast<size_t>(qi) * P + j0 + lane] : -1;
+    unsigned valid = __ballot_sync(0xffffffffu, mine >= 0);
+    while (valid) {
+      const int src = __ffs(valid) - 1;
+      valid &= valid - 1;
+      const int l = __shfl_sync(0xffffffffu, mine, src);
+      const float* c = cent + static_cast<size_t>(l) * dpad;
+      float s = 0.0f;
+      for (int i = lane; i < dpad; i += 32) {
+        const float v = row[i] - c[i];
+        s = fmaf(v, v, s);
+      }
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      emax = fmaxf(emax, pair_eps(s, rmax[l], d));
     }
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    emax = fmaxf(emax, pair_eps(s, rmax[l], d));
   }
   if (lane == 0) {
     e2[qi] = 2.0f * emax + 1e-30f;

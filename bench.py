@@ -969,6 +969,21 @@ def run_c5_batches(args):
         pr_f, _ = ix.probe_lists(q_np[:B], P)
         row["fixed"]["lists_per_batch"] = int(np.unique(pr_f).size)
         row["learned_over_fixed"] = round(row["learned"]["qps"] / row["fixed"]["qps"], 3)
+        if B in (16, 256, 4096):
+            # Device time per kernel of one batch (no graph; the sum is a
+            # little above the graph's time per batch).
+            for name, learned in (("fixed", False), ("learned", True)):
+                sp.learned_probe = learned
+                sp.learned_target = tgt if learned else 0.0
+                ix.nprobe = 256 if learned else P
+                reps = 8
+                ix.profile(True)
+                for c in range(reps):
+                    o = (c * B) % (nq - B + 1)
+                    ix.search(B, test[o:o + B], k, D[o:o + B], I[o:o + B])
+                prof = ix.profile_read()
+                ix.profile(False)
+                row[name]["kernel_ms"] = {n: round(v[0] / reps, 4) for n, v in prof.items()}
         rows.append(row)
     sp.use_graph, sp.learned_probe, sp.learned_target, sp.precision = False, False, 0.0, Precision.FP32
     thr, crec, cavg = ix.probe_calibration()

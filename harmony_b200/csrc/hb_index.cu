@@ -1389,8 +1389,10 @@ class IndexCore {
 
   // The bounded scan of one batch after the coarse probes: per-query prep,
   // work description (chunks of cr rows), seed bounds, the scan with a ring
-  // of `stages` B tiles, and the exact re-rank.  Every (cr, stages) gives the
-  // same result.
+  // of `stages` B tiles, and the exact re-rank.  For k > kFilterTightK the
+  // scan runs in two stages: every query's nearest list first, whose k-th
+  // admitted value bounds the second stage over the other lists.  Every
+  // (cr, stages) gives the same result.
   void filter_pipeline(int nb, int P, int k, int cap, int cr, int stages, float* Dd, int64_t* Id) {
     HB_CUDA(cudaMemsetAsync(over_n_.p, 0, 2 * sizeof(int), st_));
     {
@@ -1406,16 +1408,28 @@ class IndexCore {
     slot_base_.reserve(static_cast<size_t>(nb) * P + 1);
     const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
     work_tmp_.reserve(wtmp);
+    const bool two_stage = k > kFilterTightK && P > 1;
+    const int32_t* probes_a = probes_.p;
+    int P_a = P, cr_a = cr;
+    if (two_stage) {
+      probe0_.reserve(static_cast<size_t>(nb));
+      probes_rest_.reserve(static_cast<size_t>(nb) * P);
+      launch_split_first_probe(probes_.p, nb, P, probe0_.p, probes_rest_.p, st_);
+      probes_a = probe0_.p;
+      P_a = 1;
+      cr_a = std::max(128, chunk_rows_for(nb, 1, 128));
+      launches_ += 1;
+    }
     {
       Scope sc(this, "build_work");
-      launch_build_work(probes_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p, list_qoff_.p,
-                        list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+      launch_build_work(probes_a, nb, P_a, list_off_.p, static_cast<int>(nlist_), cr_a, 128, list_cnt_.p,
+                        list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
     }
     {
       Scope sc(this, "seed");
       launch_seed_bound(qpad_.p, static_cast<int>(dpad_), cent_.p, nb, kpad_, codes_bf16_.p, list_off_.p,
                         static_cast<int>(nlist_), list_qoff_.p, list_q_.p, rnorm_.p, std::max(seed_rows_, k), k,
-                        e2_.p, thr_.p, st_, probes_.p, P);
+                        e2_.p, thr_.p, st_, probes_a, P_a);
     }
     counter_.reserve(1);
     HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
@@ -1432,7 +1446,7 @@ class IndexCore {
     a.list_qoff = list_qoff_.p;
     a.list_q = list_q_.p;
     a.item_off = item_off_.p;
-    a.chunk_rows = cr;
+    a.chunk_rows = cr_a;
     a.work_counter = counter_.p;
     a.thr = thr_.p;
     a.e2 = e2_.p;
@@ -1446,6 +1460,25 @@ class IndexCore {
     {
       Scope sc(this, "scan_bf16");
       launch_scan_bf16(tmap_, a, num_sms_, st_);
+    }
+    if (two_stage) {
+      // Second stage: the other lists, appended to the same buffers.
+      {
+        Scope sc(this, "kth_bound");
+        launch_kth_bound(cbuf_.p, ccnt_.p, cap, nb, k, e2_.p, thr_.p, st_);
+      }
+      {
+        Scope sc(this, "build_work");
+        launch_build_work(probes_rest_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p,
+                          list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+      }
+      HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
+      a.chunk_rows = cr;
+      {
+        Scope sc(this, "scan_bf16");
+        launch_scan_bf16(tmap_, a, num_sms_, st_);
+      }
+      launches_ += 5;
     }
     {
       Scope sc(this, "rerank");
@@ -2085,6 +2118,7 @@ class IndexCore {
   DevBuf<float> tile_norm_, rnorm_, rmax_;
   DevBuf<int64_t> tile_off_;
   DevBuf<int32_t> probes1_;
+  DevBuf<int32_t> probe0_, probes_rest_;  // the two stages' probe tables (k > kFilterTightK)
   DevBuf<int> err_dev_;
   int* err_host_ = nullptr;
   bool prof_ = false;

@@ -236,6 +236,17 @@ void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const flo
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
                         int* flag, int* over_list, int* over_n, int* m_out, int num_sms, cudaStream_t st);
 
+// Largest k whose bound tightens inside the BF16 scan; a larger k takes two
+// stages (the nearest list of every query first, then the rest under the
+// k-th value the first stage admitted).
+constexpr int kFilterTightK = 16;
+// Per query: thr = min(thr, k-th smallest admitted w + e2) when the buffer
+// holds at least k rows and did not overflow.
+void launch_kth_bound(const uint64_t* cand, const int* cnt, int cap, int nq, int k, const float* e2, uint32_t* thr,
+                      cudaStream_t st);
+// first[q] = probes[q][0]; rest = probes with column 0 set to -1.
+void launch_split_first_probe(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st);
+
 // Candidate-matrix BF16 scan (k_cand.cu): any kpad (a multiple of 64) and up
 // to kCandMaxR candidates per query.
 constexpr int kCandMaxR = 4096;

@@ -92,7 +92,7 @@ constexpr int kTile = 128;     // rows per B tile, queries per item (M)
 constexpr int kMaxStages = 4;
 constexpr int kAcc = 2 * kGroups;                  // TMEM accumulators of 128 columns
 constexpr size_t kSmemCap = 225 * 1024;            // dynamic shared memory budget
-constexpr int kTightK = 16;                        // largest k whose bound tightens during the scan
+constexpr int kTightK = kFilterTightK;             // largest k whose bound tightens during the scan
 constexpr int kStage = 8;                          // admitted keys staged per epilogue thread before a flush
 
 struct ItemDesc {
@@ -516,7 +516,8 @@ __device__ __forceinline__ float pair_eps(float cd, float R, int d) {
 // Per query, before the scan: 2 eps_max, eps_max the largest pair bound over
 // the query's probed lists (probes row, -1 = none); the admission bound reset
 // to FLT_MAX (no bound yet; +inf padding rows never pass); the candidate
-// counter reset.  One warp per query.
+// counter reset.  One warp per query, a lane per probe: a row of 256 probes
+// costs 8 rounds, not 256 (the batch waits for its widest row).
 __global__ void query_prep_kernel(const float* __restrict__ q, int nq, int d, int dpad,
                                   const int32_t* __restrict__ probes, int P, const float* __restrict__ cent,
                                   const float* __restrict__ rmax, float* __restrict__ e2, uint32_t* __restrict__ thr,
@@ -524,27 +525,27 @@ __global__ void query_prep_kernel(const float* __restrict__ q, int nq, int d, in
   const int lane = threadIdx.x & 31;
   const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (qi >= nq) return;
-  const float* row = q + static_cast<size_t>(qi) * dpad;
+  const float4* q4 = reinterpret_cast<const float4*>(q + static_cast<size_t>(qi) * dpad);
   float emax = 0.0f;
-  // The probe row 32 entries at a time (one coalesced load), each valid
-  // entry's distance by the whole warp.
   for (int j0 = 0; j0 < P; j0 += 32) {
-    const int mine = j0 + lane < P ? probes[static_cast<size_t>(qi) * P + j0 + lane] : -1;
-    unsigned valid = __ballot_sync(0xffffffffu, mine >= 0);
-    while (valid) {
-      const int src = __ffs(valid) - 1;
-      valid &= valid - 1;
-      const int l = __shfl_sync(0xffffffffu, mine, src);
-      const float* c = cent + static_cast<size_t>(l) * dpad;
+    const int l = j0 + lane < P ? probes[static_cast<size_t>(qi) * P + j0 + lane] : -1;
+    if (__ballot_sync(0xffffffffu, l >= 0) == 0u) continue;
+    if (l >= 0) {
+      const float4* c4 = reinterpret_cast<const float4*>(cent + static_cast<size_t>(l) * dpad);
       float s = 0.0f;
-      for (int i = lane; i < dpad; i += 32) {
-        const float v = row[i] - c[i];
-        s = fmaf(v, v, s);
+#pragma unroll 8
+      for (int i = 0; i < dpad / 4; ++i) {
+        const float4 a = q4[i], b = __ldg(c4 + i);
+        const float v0 = a.x - b.x, v1 = a.y - b.y, v2 = a.z - b.z, v3 = a.w - b.w;
+        s = fmaf(v0, v0, s);
+        s = fmaf(v1, v1, s);
+        s = fmaf(v2, v2, s);
+        s = fmaf(v3, v3, s);
       }
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
       emax = fmaxf(emax, pair_eps(s, rmax[l], d));
     }
   }
+  for (int o = 16; o > 0; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
   if (lane == 0) {
     e2[qi] = 2.0f * emax + 1e-30f;
     thr[qi] = ordered_bits(FLT_MAX);
@@ -663,6 +664,87 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
     D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
     I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
   }
+}
+
+// The bound of the second stage of a batch with k > kTightK: the first stage
+// scanned only each query's nearest list, so the k-th smallest w admitted
+// there (a radix select over the keys' upper 32 bits, 8 bits per pass) is at
+// least the k-th smallest w over all probed rows, and that value + 2 eps
+// bounds W_k + 2 eps from above.  One warp per query; a query with fewer
+// than k admitted rows, or an overflowed buffer, keeps its bound.
+constexpr int kKthWarps = 8;
+
+__global__ void __launch_bounds__(kKthWarps * 32) kth_bound_kernel(const uint64_t* __restrict__ cand,
+                                                                  const int* __restrict__ cnt, int cap, int nq, int k,
+                                                                  const float* __restrict__ e2,
+                                                                  uint32_t* __restrict__ thr) {
+  __shared__ int s_h[kKthWarps][256];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int qi = blockIdx.x * kKthWarps + wib;
+  if (qi >= nq) return;
+  const int c = cnt[qi];
+  if (c < k || c > cap) return;
+  int* h = s_h[wib];
+  const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
+  uint32_t prefix = 0u, pmask = 0u;
+  int need = k;  // rank of the wanted value among those matching the prefix
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = lane; i < 256; i += 32) h[i] = 0;
+    __syncwarp();
+    for (int i = lane; i < c; i += 32) {
+      const uint32_t v = static_cast<uint32_t>(src[i] >> 32);
+      if ((v & pmask) == prefix) atomicAdd(&h[(v >> shift) & 255u], 1);
+    }
+    __syncwarp();
+    int loc[8], sum = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      loc[j] = h[8 * lane + j];
+      sum += loc[j];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int n = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += n;
+    }
+    const int excl = incl - sum;
+    const unsigned hit = __ballot_sync(0xffffffffu, excl < need && need <= incl);
+    const int src_lane = __ffs(hit) - 1;
+    int bin = 0, before = excl;
+    if (lane == src_lane) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (before + loc[j] >= need) {
+          bin = 8 * lane + j;
+          break;
+        }
+        before += loc[j];
+      }
+    }
+    bin = __shfl_sync(0xffffffffu, bin, src_lane);
+    before = __shfl_sync(0xffffffffu, before, src_lane);
+    need -= before;
+    prefix |= static_cast<uint32_t>(bin) << shift;
+    pmask |= 255u << shift;
+    __syncwarp();
+  }
+  if (lane == 0) {
+    const uint32_t b = ordered_bits(fminf(__fadd_ru(ordered_to_float(prefix), e2[qi]), FLT_MAX));
+    if (b < thr[qi]) thr[qi] = b;
+  }
+}
+
+// Probe table split for the two stages: first[q] = the query's nearest list,
+// rest = the table with that column set to -1.
+__global__ void split_first_probe_kernel(const int32_t* __restrict__ probes, int nq, int P,
+                                         int32_t* __restrict__ first, int32_t* __restrict__ rest) {
+  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (i >= static_cast<int64_t>(nq) * P) return;
+  const int j = static_cast<int>(i % P);
+  const int32_t v = probes[i];
+  rest[i] = j == 0 ? -1 : v;
+  if (j == 0) first[i / P] = v;
 }
 
 // The same for the queries the warp kernel listed in big_list (more than
@@ -1009,6 +1091,20 @@ void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const flo
                                                over_n + 1, m_out);
     HB_CUDA(cudaGetLastError());
   }
+}
+
+void launch_kth_bound(const uint64_t* cand, const int* cnt, int cap, int nq, int k, const float* e2, uint32_t* thr,
+                      cudaStream_t st) {
+  if (nq <= 0) return;
+  kth_bound_kernel<<<(nq + kKthWarps - 1) / kKthWarps, kKthWarps * 32, 0, st>>>(cand, cnt, cap, nq, k, e2, thr);
+  HB_CUDA(cudaGetLastError());
+}
+
+void launch_split_first_probe(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st) {
+  const int64_t n = static_cast<int64_t>(nq) * P;
+  if (n <= 0) return;
+  split_first_probe_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(probes, nq, P, first, rest);
+  HB_CUDA(cudaGetLastError());
 }
 
 void launch_wait_selftest(long long budget, int code, int* err, long long* waited, cudaStream_t st) {

@@ -689,6 +689,18 @@ def run_c4(args):
                               "calls": calls}
             res[mode] = by
         sp.use_graph = False
+        # Device time per kernel of one batch at the small sizes (no graph).
+        kern = {}
+        for B in (1, 64):
+            reps = 10
+            ix.profile(True)
+            for c in range(reps):
+                sp.nprobe_per_query = npq_dev[c * B:(c + 1) * B]
+                ix.search(B, queries[c * B:(c + 1) * B], k, D_dev[:B], I_dev[:B])
+            prof = ix.profile_read()
+            ix.profile(False)
+            kern[str(B)] = {n: round(v[0] / reps, 4) for n, v in prof.items()}
+        res["kernel_ms"] = kern
         # Recall of the first 2000 queries at their own nprobe, one call.
         sp.nprobe_per_query = npq[:ng]
         ix.search(ng, q_host[:ng], k, D_host[:ng], I_host[:ng])

@@ -114,17 +114,29 @@ struct TcShared {
   ItemDesc desc[2];
 };
 
-// Next work item from the global counter (one thread).
-__device__ ItemDesc fetch_item(const TcArgs& a, int64_t total_items) {
+// Next work item from the global counter, by one warp: lane 0 takes the
+// item, the warp finds its list with a 32-way search of item_off (three
+// rounds for 4096 lists instead of twelve dependent loads).
+__device__ ItemDesc fetch_item(const TcArgs& a, int64_t total_items, int lane) {
   ItemDesc d;
   d.ntiles = -1;
-  if (*reinterpret_cast<volatile int*>(a.err) != 0) return d;
-  const int64_t item = static_cast<int64_t>(atomicAdd(a.work_counter, 1u));
+  int64_t item = 0;
+  if (lane == 0)
+    item = *reinterpret_cast<volatile int*>(a.err) != 0 ? total_items
+                                                        : static_cast<int64_t>(atomicAdd(a.work_counter, 1u));
+  item = __shfl_sync(0xffffffffu, item, 0);
   if (item >= total_items) return d;
+  // item_off[lo] <= item < item_off[hi]
   int lo = 0, hi = a.nlist;
   while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (a.item_off[mid] <= item) lo = mid; else hi = mid;
+    const int step = max(1, (hi - lo) / 32);
+    const int p = lo + (lane + 1) * step;
+    const bool le = p < hi && a.item_off[p] <= item;
+    const int n = __popc(__ballot_sync(0xffffffffu, le));  // the true lanes are a prefix
+    // With every probe at or under the item the list lies past the last
+    // probe and hi stays; otherwise probe n is above it.
+    if (n < 32) hi = min(hi, lo + (n + 1) * step);
+    lo += n * step;
   }
   const int l = lo;
   const int64_t local = item - a.item_off[l];
@@ -200,9 +212,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ---- item builders ---------------------------------------------------
     const int bt = tid - kBuildWarp0 * 32;
     constexpr int kBt = kBuildWarps * 32;
+    const int bw = bt >> 5;  // builder warp
     ItemDesc nd;
     nd.ntiles = -1;
-    if (bt == 0) nd = fetch_item(a, total_items);
+    if (bw == 0) nd = fetch_item(a, total_items, lane);
     for (uint32_t it = 0;; ++it) {
       const int ab = static_cast<int>(it & 1u);
       if (bt == 0) {
@@ -215,58 +228,62 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int64_t qbase = a.list_qoff[d.list] + static_cast<int64_t>(d.group) * kTile;
         float* cen = s_cent + ab * kTile;
         for (int c = bt; c < kpad; c += kBt) cen[c] = c < a.dpad ? a.cent[static_cast<size_t>(d.list) * a.dpad + c] : 0.0f;
-        for (int r = bt; r < kTile; r += kBt) {
-          int q = -1;
-          float thr = -INFINITY, e2 = 0.0f;
-          if (r < d.qcnt) {
-            q = static_cast<int>(static_cast<uint32_t>(a.list_q[qbase + r]) >> 16);
-            // The query's bound as other items have lowered it so far.
-            thr = ordered_to_float(*reinterpret_cast<volatile uint32_t*>(a.thr + q));
-            e2 = a.e2[q];
-          }
+        // Row r holds the group's query (r % 32) * 4 + r / 32, so the queries
+        // of a partial group spread over the four epilogue warps.  Two rows
+        // per thread, their loads issued together.
+        int q2[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = bt + h * kBt;
+          const int i = (r & 31) * 4 + (r >> 5);
+          q2[h] = i < d.qcnt ? static_cast<int>(static_cast<uint32_t>(a.list_q[qbase + i]) >> 16) : -1;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = bt + h * kBt;
+          const int q = q2[h];
+          // The query's bound as other items have lowered it so far.
           meta_q[ab * kTile + r] = q;
-          meta_thr[ab * kTile + r] = thr;
-          meta_e2[ab * kTile + r] = e2;
+          meta_thr[ab * kTile + r] =
+              q >= 0 ? ordered_to_float(*reinterpret_cast<volatile uint32_t*>(a.thr + q)) : -INFINITY;
+          meta_e2[ab * kTile + r] = q >= 0 ? a.e2[q] : 0.0f;
         }
         asm volatile("bar.sync 3, %0;\n" ::"n"(kBt) : "memory");
-        // A row r = BF16(q - c_l) of the item's query r, and ||q - c_l||^2.
+        // A row r = BF16(q - c_l) of the row's query, and ||q - c_l||^2: a
+        // warp per row (lane = 4 consecutive columns), 16 rows in flight.
         uint8_t* A = Abuf + ab * tile_bytes;
-        for (int r = bt; r < kTile; r += kBt) {
-          const int q = meta_q[ab * kTile + r];
-          const float* qrow = a.q + static_cast<size_t>(q < 0 ? 0 : q) * a.dpad;
-          float cd = 0.0f;
-#pragma unroll 4
-          for (int k = 0; k < kpad; k += 8) {
-            float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            if (q >= 0 && k < a.dpad) {  // dpad is a multiple of 16: a row's 8 values are all in or all out
-              const float4 lo = __ldg(reinterpret_cast<const float4*>(qrow + k));
-              const float4 hi = __ldg(reinterpret_cast<const float4*>(qrow + k + 4));
-              v[0] = lo.x - cen[k];
-              v[1] = lo.y - cen[k + 1];
-              v[2] = lo.z - cen[k + 2];
-              v[3] = lo.w - cen[k + 3];
-              v[4] = hi.x - cen[k + 4];
-              v[5] = hi.y - cen[k + 5];
-              v[6] = hi.z - cen[k + 6];
-              v[7] = hi.w - cen[k + 7];
-            }
-            uint32_t w[4];
+        const int c0 = 4 * lane;
+        const bool col_in = c0 < a.dpad, col_k = c0 < kpad;
+        const float4 cv = col_k ? *reinterpret_cast<const float4*>(cen + c0) : make_float4(0.f, 0.f, 0.f, 0.f);
+        constexpr int kRowsInFlight = 16;
+        for (int r0 = bw; r0 < kTile; r0 += kBuildWarps * kRowsInFlight) {
+          float4 x[kRowsInFlight];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              cd = fmaf(v[2 * j], v[2 * j], cd);
-              cd = fmaf(v[2 * j + 1], v[2 * j + 1], cd);
-              __nv_bfloat162 p2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-              w[j] = *reinterpret_cast<uint32_t*>(&p2);
-            }
-            *reinterpret_cast<uint4*>(A + sw128_offset_bf16(r, k, kblk_bytes)) = make_uint4(w[0], w[1], w[2], w[3]);
+          for (int j = 0; j < kRowsInFlight; ++j) {
+            const int q = meta_q[ab * kTile + r0 + j * kBuildWarps];
+            x[j] = q >= 0 && col_in ? __ldg(reinterpret_cast<const float4*>(a.q + static_cast<size_t>(q) * a.dpad + c0))
+                                    : cv;  // q - c = 0 for an empty row or a padding column
           }
-          meta_cd[ab * kTile + r] = cd;
+#pragma unroll
+          for (int j = 0; j < kRowsInFlight; ++j) {
+            const int r = r0 + j * kBuildWarps;
+            const float v0 = x[j].x - cv.x, v1 = x[j].y - cv.y, v2 = x[j].z - cv.z, v3 = x[j].w - cv.w;
+            float cd = fmaf(v3, v3, fmaf(v2, v2, fmaf(v1, v1, v0 * v0)));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) cd += __shfl_xor_sync(0xffffffffu, cd, o);
+            if (col_k) {
+              __nv_bfloat162 p01 = __floats2bfloat162_rn(v0, v1), p23 = __floats2bfloat162_rn(v2, v3);
+              *reinterpret_cast<uint2*>(A + sw128_offset_bf16(r, c0, kblk_bytes)) =
+                  make_uint2(*reinterpret_cast<uint32_t*>(&p01), *reinterpret_cast<uint32_t*>(&p23));
+            }
+            if (lane == 0) meta_cd[ab * kTile + r] = cd;
+          }
         }
         fence_proxy_async_smem();
       }
       mbar_arrive(&sh.itemf[ab]);
       if (d.ntiles < 0) break;
-      if (bt == 0) nd = fetch_item(a, total_items);
+      if (bw == 0) nd = fetch_item(a, total_items, lane);
     }
   } else if (warp == kProdWarp) {
     // ---- TMA producer ------------------------------------------------------
@@ -371,6 +388,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const float cd = meta_cd[ab * kTile + etid];
       mbar_arrive(&sh.aempty[ab]);
       if (d.ntiles < 0) break;
+      // Queries are spread over the four warps (row r holds query
+      // (r % 32) * 4 + r / 32), so a warp without one skips its loads.
+      const bool warp_on = __any_sync(0xffffffffu, my_q >= 0);
       float thr = thr0;
       // Columns hold w' = ||r||^2 - 2 q'.r; a row's value is w = cd + w'.  A
       // column is looked at when w' <= thr_s, thr_s = thr - cd rounded up with
@@ -381,11 +401,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       };
       float thr_s = shifted(thr);
       // The KT smallest values this thread has admitted for the query in this
-      // item, ascending (KT = 0: no tightening).
+      // item, ascending, and the k-th of them (+inf until k are in; KT = 0:
+      // no tightening).  Only a value under the k-th changes them.
       float best[KB];
 #pragma unroll
       for (int i = 0; i < KB; ++i) best[i] = INFINITY;
-      int seen = 0;
+      float kth_loc = INFINITY;
       uint64_t* cbuf = a.cand + static_cast<size_t>(my_q < 0 ? 0 : my_q) * a.cap;
       // Admitted keys wait here (stride kEpiThreads: conflict-free) and go to
       // the query's buffer kStage at a time, one atomicAdd per flush.
@@ -397,12 +418,78 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           if (base + i < a.cap) cbuf[base + i] = stg[i * kEpiThreads];
         ns = 0;
       };
+      // One 32-column chunk of the accumulator in r: w' = ||r||^2 - 2 q'.r
+      // (rows past the list carry an infinite norm), their minimum against
+      // the bound, and the admission of the columns under it.
+      auto chunk = [&](uint32_t(&r)[32], const float* nb, uint32_t pos0) {
+        const float4* n4 = reinterpret_cast<const float4*>(nb);
+        float mn = INFINITY;
+#pragma unroll
+        for (int j4 = 0; j4 < 8; ++j4) {
+          const float4 nv = n4[j4];
+          const float v0 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 0]), nv.x);
+          const float v1 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), nv.y);
+          const float v2 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), nv.z);
+          const float v3 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), nv.w);
+          r[4 * j4 + 0] = __float_as_uint(v0);
+          r[4 * j4 + 1] = __float_as_uint(v1);
+          r[4 * j4 + 2] = __float_as_uint(v2);
+          r[4 * j4 + 3] = __float_as_uint(v3);
+          mn = fminf(mn, fminf(fminf(v0, v1), fminf(v2, v3)));
+        }
+        if (my_q >= 0 && mn <= thr_s) {
+          uint32_t mq[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+          for (int j = 0; j < 32; ++j) mq[j & 3] |= (__uint_as_float(r[j]) <= thr_s ? 1u : 0u) << j;
+          uint32_t mask = (mq[0] | mq[1]) | (mq[2] | mq[3]);
+          while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1;
+            // r[j] by a 5-level select tree (no register indexing).
+            uint32_t t16[16], t8[8], t4[4], t2[2];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) t16[i] = (j & 1) ? r[2 * i + 1] : r[2 * i];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) t8[i] = (j & 2) ? t16[2 * i + 1] : t16[2 * i];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) t4[i] = (j & 4) ? t8[2 * i + 1] : t8[2 * i];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
+            const float wv = cd + __uint_as_float((j & 16) ? t2[1] : t2[0]);
+            stg[ns * kEpiThreads] = (static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j));
+            if (++ns == kStage) flush();
+            if (KT > 0 && wv < kth_loc) {
+              // Insert into the ascending KT smallest; once k values are in,
+              // the k-th + 2 eps bounds W_k + 2 eps from above.
+              float v = wv;
+#pragma unroll
+              for (int i = 0; i < KB; ++i) {
+                const float o = best[i];
+                best[i] = fminf(o, v);
+                v = fmaxf(o, v);
+              }
+              // best is ascending: its k-th entry is the largest of the first k
+              // (a max, so the array stays in registers).
+              float kth = best[0];
+#pragma unroll
+              for (int i = 1; i < KB; ++i) kth = i < a.k ? fmaxf(kth, best[i]) : kth;
+              kth_loc = kth;
+              const float nt = __fadd_ru(kth, e2);
+              if (nt < thr) {
+                thr = nt;
+                thr_s = shifted(thr);
+                atomicMin(a.thr + my_q, ordered_bits(thr));  // shared at once (no return value used)
+              }
+            }
+          }
+        }
+      };
+      // The query's bound as other threads have lowered it, read one tile
+      // ahead (the load is in flight while a tile is processed).
+      uint32_t g_thr = my_q >= 0 ? *reinterpret_cast<volatile uint32_t*>(a.thr + my_q) : 0u;
       for (int t = static_cast<int>((static_cast<uint32_t>(grp) ^ G) & 1u); t < d.ntiles; t += kGroups, ++e_cnt) {
         const int b = 2 * grp + static_cast<int>(e_cnt & 1u);
         const uint32_t par = (e_cnt >> 1) & 1u;
-        // The query's bound as other threads have lowered it (read while the
-        // tile is still on the tensor cores).
-        const uint32_t g_thr = my_q >= 0 ? *reinterpret_cast<volatile uint32_t*>(a.thr + my_q) : 0u;
         ok = ok && mbar_wait(&sh.accf[b], par, err, 14, budget) && mbar_wait(&sh.normf[b], par, err, 15, budget);
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
@@ -410,79 +497,25 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           thr = ordered_to_float(g_thr);
           thr_s = shifted(thr);
         }
-        const float* nb = nrm + b * kTile;
-        const uint32_t pos_t = static_cast<uint32_t>(d.row0 + t * kTile);
+        g_thr = my_q >= 0 ? *reinterpret_cast<volatile uint32_t*>(a.thr + my_q) : 0u;
+        if (ok && warp_on) {
+          const float* nb = nrm + b * kTile;
+          const uint32_t col = tmem + lane_base + static_cast<uint32_t>(b * kTile);
+          const uint32_t pos_t = static_cast<uint32_t>(d.row0 + t * kTile);
+          // Two register sets: the next chunk's TMEM load is in flight while
+          // this one is processed, then moves into place (one copy of the
+          // chunk code, so the instruction cache holds the loop).
+          uint32_t ra[32], rb[32];
+          tmem_ld32(col, ra);
+          tmem_ld_wait(ra);
 #pragma unroll 1
-        for (int c = 0; c < kTile / 32; ++c) {
-          uint32_t r[32];
-          if (ok) {
-            tmem_ld32(tmem + lane_base + static_cast<uint32_t>(b * kTile + c * 32), r);
-            tmem_ld_wait();
-          }
-          if (ok && my_q >= 0) {
-            // w = ||x||^2 - 2 q.x (rows past the list carry an infinite
-            // norm); the columns' minimum against the bound decides whether
-            // any of them needs a look.
-            const float4* n4 = reinterpret_cast<const float4*>(nb + c * 32);
-            float mn = INFINITY;
+          for (int c = 0; c < kTile / 32; ++c) {
+            if (c + 1 < kTile / 32) tmem_ld32(col + static_cast<uint32_t>(32 * (c + 1)), rb);
+            chunk(ra, nb + 32 * c, pos_t + static_cast<uint32_t>(32 * c));
+            if (c + 1 < kTile / 32) {
+              tmem_ld_wait(rb);
 #pragma unroll
-            for (int j4 = 0; j4 < 8; ++j4) {
-              const float4 nv = n4[j4];
-              const float v0 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 0]), nv.x);
-              const float v1 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), nv.y);
-              const float v2 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), nv.z);
-              const float v3 = fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), nv.w);
-              r[4 * j4 + 0] = __float_as_uint(v0);
-              r[4 * j4 + 1] = __float_as_uint(v1);
-              r[4 * j4 + 2] = __float_as_uint(v2);
-              r[4 * j4 + 3] = __float_as_uint(v3);
-              mn = fminf(mn, fminf(fminf(v0, v1), fminf(v2, v3)));
-            }
-            if (mn <= thr_s) {
-              uint32_t mq[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-              for (int j = 0; j < 32; ++j) mq[j & 3] |= (__uint_as_float(r[j]) <= thr_s ? 1u : 0u) << j;
-              uint32_t mask = (mq[0] | mq[1]) | (mq[2] | mq[3]);
-              const uint32_t pos0 = pos_t + static_cast<uint32_t>(c * 32);
-              while (mask) {
-                const int j = __ffs(mask) - 1;
-                mask &= mask - 1;
-                // r[j] by a 5-level select tree (no register indexing).
-                uint32_t t16[16], t8[8], t4[4], t2[2];
-#pragma unroll
-                for (int i = 0; i < 16; ++i) t16[i] = (j & 1) ? r[2 * i + 1] : r[2 * i];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) t8[i] = (j & 2) ? t16[2 * i + 1] : t16[2 * i];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) t4[i] = (j & 4) ? t8[2 * i + 1] : t8[2 * i];
-#pragma unroll
-                for (int i = 0; i < 2; ++i) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
-                const float wv = cd + __uint_as_float((j & 16) ? t2[1] : t2[0]);
-                stg[ns * kEpiThreads] = (static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j));
-                if (++ns == kStage) flush();
-                if (KT > 0) {
-                  // Insert into the ascending KT smallest; once k values are
-                  // in, the k-th + 2 eps bounds W_k + 2 eps from above.
-                  float v = wv;
-#pragma unroll
-                  for (int i = 0; i < KB; ++i) {
-                    const float o = best[i];
-                    best[i] = fminf(o, v);
-                    v = fmaxf(o, v);
-                  }
-                  if (++seen >= a.k) {
-                    float kth = best[0];
-#pragma unroll
-                    for (int i = 1; i < KB; ++i) kth = (i == a.k - 1) ? best[i] : kth;
-                    const float nt = __fadd_ru(kth, e2);
-                    if (nt < thr) {
-                      thr = nt;
-                      thr_s = shifted(thr);
-                      atomicMin(a.thr + my_q, ordered_bits(thr));  // shared at once (no return value used)
-                    }
-                  }
-                }
-              }
+              for (int j = 0; j < 32; ++j) ra[j] = rb[j];
             }
           }
         }
@@ -666,33 +699,18 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
   }
 }
 
-// The bound of the second stage of a batch with k > kTightK: the first stage
-// scanned only each query's nearest list, so the k-th smallest w admitted
-// there (a radix select over the keys' upper 32 bits, 8 bits per pass) is at
-// least the k-th smallest w over all probed rows, and that value + 2 eps
-// bounds W_k + 2 eps from above.  One warp per query; a query with fewer
-// than k admitted rows, or an overflowed buffer, keeps its bound.
-constexpr int kKthWarps = 8;
-
-__global__ void __launch_bounds__(kKthWarps * 32) kth_bound_kernel(const uint64_t* __restrict__ cand,
-                                                                  const int* __restrict__ cnt, int cap, int nq, int k,
-                                                                  const float* __restrict__ e2,
-                                                                  uint32_t* __restrict__ thr) {
-  __shared__ int s_h[kKthWarps][256];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int qi = blockIdx.x * kKthWarps + wib;
-  if (qi >= nq) return;
-  const int c = cnt[qi];
-  if (c < k || c > cap) return;
-  int* h = s_h[wib];
-  const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
+// The k-th smallest (k >= 1) of n 32-bit keys get(0 .. n-1), by one warp:
+// radix selection over four 8-bit digits with a 256-bin histogram h in
+// shared memory.  n >= k.
+template <class Get>
+__device__ uint32_t warp_kth_smallest(Get get, int n, int k, int* h, int lane) {
   uint32_t prefix = 0u, pmask = 0u;
-  int need = k;  // rank of the wanted value among those matching the prefix
+  int need = k;  // rank of the wanted key among those matching the prefix
   for (int shift = 24; shift >= 0; shift -= 8) {
     for (int i = lane; i < 256; i += 32) h[i] = 0;
     __syncwarp();
-    for (int i = lane; i < c; i += 32) {
-      const uint32_t v = static_cast<uint32_t>(src[i] >> 32);
+    for (int i = lane; i < n; i += 32) {
+      const uint32_t v = get(i);
       if ((v & pmask) == prefix) atomicAdd(&h[(v >> shift) & 255u], 1);
     }
     __syncwarp();
@@ -705,8 +723,8 @@ __global__ void __launch_bounds__(kKthWarps * 32) kth_bound_kernel(const uint64_
     int incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int n = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += n;
+      const int x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += x;
     }
     const int excl = incl - sum;
     const unsigned hit = __ballot_sync(0xffffffffu, excl < need && need <= incl);
@@ -729,6 +747,31 @@ __global__ void __launch_bounds__(kKthWarps * 32) kth_bound_kernel(const uint64_
     pmask |= 255u << shift;
     __syncwarp();
   }
+  return prefix;
+}
+
+// The bound of the second stage of a batch with k > kTightK: the first stage
+// scanned only each query's nearest list, so the k-th smallest w admitted
+// there (a radix select over the keys' upper 32 bits, 8 bits per pass) is at
+// least the k-th smallest w over all probed rows, and that value + 2 eps
+// bounds W_k + 2 eps from above.  One warp per query; a query with fewer
+// than k admitted rows, or an overflowed buffer, keeps its bound.
+constexpr int kKthWarps = 8;
+
+__global__ void __launch_bounds__(kKthWarps * 32) kth_bound_kernel(const uint64_t* __restrict__ cand,
+                                                                  const int* __restrict__ cnt, int cap, int nq, int k,
+                                                                  const float* __restrict__ e2,
+                                                                  uint32_t* __restrict__ thr) {
+  __shared__ int s_h[kKthWarps][256];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int qi = blockIdx.x * kKthWarps + wib;
+  if (qi >= nq) return;
+  const int c = cnt[qi];
+  if (c < k || c > cap) return;
+  int* h = s_h[wib];
+  const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
+  const uint32_t prefix =
+      warp_kth_smallest([&](int i) { return static_cast<uint32_t>(src[i] >> 32); }, c, k, h, lane);
   if (lane == 0) {
     const uint32_t b = ordered_bits(fminf(__fadd_ru(ordered_to_float(prefix), e2[qi]), FLT_MAX));
     if (b < thr[qi]) thr[qi] = b;
@@ -773,8 +816,14 @@ __global__ void __launch_bounds__(256) rerank_cta_kernel(const uint64_t* __restr
     if (threadIdx.x == 0) {
       const float lim = __fadd_ru(ordered_to_float(static_cast<uint32_t>(buf[k - 1] >> 32)), e2[qi]);
       const uint32_t lim_bits = ordered_bits(lim);
-      int m = k;
-      while (m < c && static_cast<uint32_t>(buf[m] >> 32) <= lim_bits) ++m;
+      // buf is sorted: m = the first index in [k, c) whose value is above
+      // lim (binary search).
+      int lo = k, hi = c;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (static_cast<uint32_t>(buf[mid] >> 32) <= lim_bits) lo = mid + 1; else hi = mid;
+      }
+      const int m = lo;
       s_m = m;
       m_out[qi] = m;
     }
@@ -807,12 +856,13 @@ __global__ void __launch_bounds__(256) rerank_cta_kernel(const uint64_t* __restr
 //
 // List-major: one CTA per list stages the list's first S BF16 rows in shared
 // memory once; for each query whose nearest list it is (probe rank 0 in the
-// list-major work description) in turn, thread t computes row t's value with
-// the query broadcast from shared memory, and a 32-step radix selection over
-// the CTA (one barrier count per bit) finds the k-th smallest.  Small batches
-// (probes given): one CTA per query.
+// list-major work description) in turn, thread t forms row t's value with the
+// query broadcast from shared memory, and a radix selection over four 8-bit
+// digits (a 256-bin histogram, three barriers per digit) finds the k-th
+// smallest.  Small batches (probes given): one CTA per query.
 constexpr int kSeedRows = 256;
 constexpr int kSeedWarps = 8;
+static_assert(kSeedWarps * 32 == 256, "the seed's radix histogram has a bin per thread");
 
 __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
     const float* __restrict__ q, int dpad, const float* __restrict__ cent, int kpad,
@@ -825,6 +875,8 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
   __shared__ int s_qs[kSeedWarps * 32];
   __shared__ int s_nq;
   __shared__ float s_cd;
+  __shared__ int s_hist[kSeedWarps * 32];  // one bin per thread
+  __shared__ int s_bin, s_before;
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const bool by_query = probes != nullptr;
   int l;
@@ -869,7 +921,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
     for (int t = 0; t < nqr; ++t) {
       const int qi = s_qs[t];
       // The query's residual to this list's centroid in BF16 (the scan's A
-      // row) and ||q - c_l||^2.
+      // row) and ||q - c_l||^2 in FP32.
       const float* qrow = q + static_cast<size_t>(qi) * dpad;
       const float* crow = cent + static_cast<size_t>(l) * dpad;
       for (int c = tid; c < kpad; c += blockDim.x)
@@ -906,22 +958,48 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
         }
         key = ordered_bits(cdq + fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[tid]));
       }
-      uint32_t prefix = 0;
+      // The k-th smallest of the n keys: radix selection over four 8-bit
+      // digits, one 256-bin histogram per digit (a bin per thread).
+      uint32_t prefix = 0u, pmask = 0u;
       int need = k;
-      for (int bit = 31; bit >= 0; --bit) {
-        const uint32_t hmask = bit == 31 ? 0u : (0xFFFFFFFFu << (bit + 1));
-        const bool zero_here = (key & hmask) == prefix && ((key >> bit) & 1u) == 0u;
-        const int c0 = __syncthreads_count(zero_here);
-        if (c0 < need) {
-          need -= c0;
-          prefix |= 1u << bit;
+      for (int shift = 24; shift >= 0; shift -= 8) {
+        s_hist[tid] = 0;
+        __syncthreads();
+        if (tid < n && (key & pmask) == prefix) atomicAdd(&s_hist[(key >> shift) & 255u], 1);
+        __syncthreads();
+        if (wib == 0) {
+          int loc[8], sum = 0;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            loc[j] = s_hist[8 * lane + j];
+            sum += loc[j];
+          }
+          int incl = sum;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += x;
+          }
+          const int excl = incl - sum;
+          if (excl < need && need <= incl) {
+            int before = excl, bin = 8 * lane;
+            for (int j = 0; j < 8; ++j) {
+              if (before + loc[j] >= need) {
+                bin = 8 * lane + j;
+                break;
+              }
+              before += loc[j];
+            }
+            s_bin = bin;
+            s_before = before;
+          }
         }
+        __syncthreads();
+        prefix |= static_cast<uint32_t>(s_bin) << shift;
+        pmask |= 255u << shift;
+        need -= s_before;
       }
-      if (tid == 0) {
-        const float bound = fminf(__fadd_ru(ordered_to_float(prefix), e2[qi]), FLT_MAX);
-        thr[qi] = ordered_bits(bound);
-      }
-      __syncthreads();
+      if (tid == 0) thr[qi] = ordered_bits(fminf(__fadd_ru(ordered_to_float(prefix), e2[qi]), FLT_MAX));
     }
     __syncthreads();
   }

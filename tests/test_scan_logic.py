@@ -1,0 +1,83 @@
+"""CPU checks of two warp algorithms of the BF16 scan (harmony_b200/csrc/k_tc.cu),
+restated step for step in Python with a lane per list element:
+
+- fetch_item's 32-way search of the per-list item offsets (a warp probes 32
+  positions per round; the lanes at or under the item form a prefix), which
+  must find the list l with item_off[l] <= item < item_off[l + 1], empty lists
+  included;
+- warp_kth_smallest, the radix selection over four 8-bit digits with a
+  256-bin histogram (lane L owns bins 8L .. 8L+7), used by the seed bound and
+  by the two-stage bound of k > 16.
+
+Both are compared with the obvious answer (bisect, sorted) on random inputs,
+ties and degenerate sizes included."""
+import bisect
+import random
+
+
+def search_32way(item_off, nlist, item):
+    lo, hi = 0, nlist
+    while hi - lo > 1:
+        step = max(1, (hi - lo) // 32)
+        le = [lo + (j + 1) * step < hi and item_off[lo + (j + 1) * step] <= item for j in range(32)]
+        n = sum(le)
+        assert le == [True] * n + [False] * (32 - n)  # a prefix: the ballot's popcount is its length
+        if n < 32:
+            hi = min(hi, lo + (n + 1) * step)
+        lo += n * step
+    return lo
+
+
+def warp_kth_smallest(vals, k):
+    prefix, pmask, need = 0, 0, k
+    for shift in (24, 16, 8, 0):
+        h = [0] * 256
+        for v in vals:
+            if (v & pmask) == prefix:
+                h[(v >> shift) & 255] += 1
+        sums = [sum(h[8 * lane:8 * lane + 8]) for lane in range(32)]
+        incl, acc = [], 0
+        for s in sums:
+            acc += s
+            incl.append(acc)
+        excl = [incl[lane] - sums[lane] for lane in range(32)]
+        src = next(lane for lane in range(32) if excl[lane] < need <= incl[lane])
+        before, b = excl[src], None
+        for j in range(8):
+            if before + h[8 * src + j] >= need:
+                b = 8 * src + j
+                break
+            before += h[8 * src + j]
+        need -= before
+        prefix |= b << shift
+        pmask |= 255 << shift
+    return prefix
+
+
+def test_32way_search_finds_the_list():
+    rng = random.Random(1)
+    for _ in range(600):
+        nlist = rng.choice([1, 2, 31, 32, 33, 63, 64, 65, 100, 1229, 4096, rng.randint(1, 9000)])
+        cnt = [rng.choice([0, 0, 1, 2, 5]) for _ in range(nlist)]
+        if sum(cnt) == 0:
+            cnt[rng.randrange(nlist)] = 1
+        off = [0]
+        for c in cnt:
+            off.append(off[-1] + c)
+        for _ in range(10):
+            item = rng.randrange(off[-1])
+            assert search_32way(off, nlist, item) == bisect.bisect_right(off, item) - 1
+
+
+def test_radix_kth_matches_sort():
+    rng = random.Random(2)
+    for _ in range(400):
+        n = rng.randint(1, 300)
+        if rng.random() < 0.3:
+            pool = [rng.getrandbits(32) for _ in range(rng.randint(1, 4))]
+            vals = [rng.choice(pool) for _ in range(n)]
+        else:
+            bits = rng.choice([32, 12, 4])
+            vals = [rng.getrandbits(bits) for _ in range(n)]
+        k = rng.randint(1, n)
+        assert warp_kth_smallest(vals, k) == sorted(vals)[k - 1]

@@ -706,6 +706,8 @@ def run_c4(args):
         ix.search(ng, q_host[:ng], k, D_host[:ng], I_host[:ng])
         I_check = I_host[:ng].numpy()
         res["recall_at_10_first_2000"] = round(recall(I_check, gt, k), 4)
+        if prec == Precision.BF16:
+            res["bounded_scan_first_2000"] = ix.bf16_stats()
         out[name] = res
         ix.search_params.nprobe_per_query = None
         ix.search_params.max_nprobe = 0

@@ -229,10 +229,11 @@ void launch_seed_bound(const float* q, int dpad, const float* cent, int nq, int 
                        const int32_t* probes = nullptr, int P = 0);
 // Exact re-rank of the admitted rows under W_k + 2 eps; flag[q] = 2 and
 // over_list[0 .. over_n[0]) for queries whose buffer overflowed (left
-// unwritten); over_list[nq ..] / over_n[1] list the queries re-ranked by a
-// CTA (over_list holds 2 nq ints, over_n 2, zeroed by the caller);
+// unwritten); over_list[nq ..] / over_n[1] list the queries with more than
+// 256 candidates, re-ranked by the flat kernels, which overwrite their
+// buffers (over_list holds 2 nq ints, over_n 2, zeroed by the caller);
 // m_out[q] = rows re-ranked.
-void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
+void launch_rerank_bf16(uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
                         int* flag, int* over_list, int* over_n, int* m_out, int num_sms, cudaStream_t st);
 

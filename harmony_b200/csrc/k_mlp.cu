@@ -311,25 +311,29 @@ using namespace sm100;
 constexpr int kMlpRows = 128;
 constexpr int kMlpThreads = 256;
 
-// W (N x K FP32, BF16-valued) -> Wb (Npad x Kpad BF16, zero padding).
+// W (N x K FP32, BF16-valued) -> Wb, the shared-memory image of the layer's
+// B operand: Npad rows x Kpad BF16 (zero padding), K-major in 64-column
+// blocks with the 128-byte swizzle, so the kernel stages it with one bulk
+// copy.
 __global__ void pack_bf16_kernel(const float* __restrict__ W, int N, int K, int Npad, int Kpad,
                                  __nv_bfloat16* __restrict__ out) {
   const size_t total = static_cast<size_t>(Npad) * Kpad;
+  const uint32_t kblk = static_cast<uint32_t>(Npad) * 128u;
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const int n = static_cast<int>(i / Kpad), k = static_cast<int>(i % Kpad);
-    out[i] = __float2bfloat16_rn(n < N && k < K ? W[static_cast<size_t>(n) * K + k] : 0.0f);
+    out[sw128_offset_bf16(n, k, kblk) / 2] =
+        __float2bfloat16_rn(n < N && k < K ? W[static_cast<size_t>(n) * K + k] : 0.0f);
   }
 }
 
-// Copies Wb (N rows x Kpad BF16, row-major) into the swizzled K-major layout.
-__device__ __forceinline__ void stage_weights(uint8_t* dst, const __nv_bfloat16* __restrict__ Wb, int N, int Kpad) {
-  const int cpr = Kpad / 8;
-  const uint32_t kblk = static_cast<uint32_t>(N) * 128u;
-  for (int i = threadIdx.x; i < N * cpr; i += blockDim.x) {
-    const int n = i / cpr, c = i - n * cpr;
-    *reinterpret_cast<uint4*>(dst + sw128_offset_bf16(n, c * 8, kblk)) =
-        *reinterpret_cast<const uint4*>(Wb + static_cast<size_t>(n) * Kpad + c * 8);
+// Stages a packed weight image (bytes, a multiple of 16) with one bulk copy
+// completing on bar (thread 0 issues).
+__device__ __forceinline__ void stage_weights(uint8_t* dst, const __nv_bfloat16* __restrict__ Wb, uint32_t bytes,
+                                              uint64_t* bar) {
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(bar, bytes);
+    bulk_load(dst, Wb, bytes, bar);
   }
 }
 
@@ -369,7 +373,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) probe_mlp_tc_kernel(
     const __nv_bfloat16* __restrict__ W3b, const float* __restrict__ b3, int NB, const int32_t* __restrict__ bucket_val,
     float thr, int cap, int32_t* __restrict__ nprobe_out, int* __restrict__ err) {
   extern __shared__ uint8_t mlp_raw[];
-  __shared__ uint64_t bar;
+  __shared__ uint64_t bar, wbar;
   __shared__ uint32_t s_tmem;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(mlp_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* A = smem;                       // 128 x 256 BF16 (64 KB)
@@ -380,22 +384,25 @@ __global__ void __launch_bounds__(kMlpThreads, 1) probe_mlp_tc_kernel(
   if (warp == 0) tmem_alloc(&s_tmem, 256);
   if (tid == 0) {
     mbar_init(&bar, 1);
+    mbar_init(&wbar, 1);
     fence_barrier_init();
   }
-  // Layer-1 weights and the features.
-  stage_weights(W, W1b, 256, K1);
-  if (tid < kMlpRows) {
-    const int r = r0 + tid;
-    const bool live = r < nq;
-    const float* qrow = q + static_cast<size_t>(live ? r : 0) * dpad;
-    const float* cd = cdist + static_cast<size_t>(live ? r : 0) * P;
-    const float l0 = logf(fmaxf(cd[0], 1e-20f));
+  __syncthreads();
+  // Layer-1 weights (in flight while the features are formed).
+  stage_weights(W, W1b, 256u * static_cast<uint32_t>(K1) * 2u, &wbar);
+  uint32_t wpar = 0;
+  // The features: a warp per row, lanes over the features, so the query's
+  // coordinates and its centroid distances are read coalesced.
+  {
     const int F = d + C;
-    for (int k = 0; k < K1; k += 8) {
-      float v[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int f = k + j;
+    const int lane = tid & 31;
+    for (int row = warp; row < kMlpRows; row += kMlpThreads / 32) {
+      const int r = r0 + row;
+      const bool live = r < nq;
+      const float* qrow = q + static_cast<size_t>(live ? r : 0) * dpad;
+      const float* cd = cdist + static_cast<size_t>(live ? r : 0) * P;
+      const float l0 = logf(fmaxf(cd[0], 1e-20f));
+      for (int f = lane; f < K1; f += 32) {
         float x = 0.0f;
         if (live && f < F) {
           if (f < d) {
@@ -411,10 +418,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1) probe_mlp_tc_kernel(
           }
           x = bf16r((x - mean[f]) * inv_std[f]);
         }
-        v[j] = x;
+        *reinterpret_cast<__nv_bfloat16*>(A + sw128_offset_bf16(row, f, akblk)) = __float2bfloat16_rn(x);
       }
-      *reinterpret_cast<uint4*>(A + sw128_offset_bf16(tid, k, akblk)) =
-          make_uint4(pack2_bf16(v[0], v[1]), pack2_bf16(v[2], v[3]), pack2_bf16(v[4], v[5]), pack2_bf16(v[6], v[7]));
     }
   }
   tc_fence_before();
@@ -428,12 +433,16 @@ __global__ void __launch_bounds__(kMlpThreads, 1) probe_mlp_tc_kernel(
   const uint32_t taddr = tmem + ((32u * static_cast<uint32_t>(warp & 3)) << 16);
   bool ok = true;
   uint32_t parity = 0;
-  // Layers 1 and 2: bias + GELU + BF16 back into A.
+  // Layers 1 and 2: bias + GELU + BF16 back into A; the next layer's weights
+  // are copied in while this layer's epilogue runs.
   for (int layer = 0; layer < 2 && ok; ++layer) {
-    ok = mlp_mma(tmem, A, W, 256, layer == 0 ? K1 : 256, &bar, parity, err);
+    ok = mbar_wait(&wbar, wpar, err, 42);
+    wpar ^= 1u;
+    ok = ok && mlp_mma(tmem, A, W, 256, layer == 0 ? K1 : 256, &bar, parity, err);
     parity ^= 1u;
     ok = __syncthreads_and(ok);
     if (!ok) break;
+    stage_weights(W, layer == 0 ? W2b : W3b, (layer == 0 ? 256u : 32u) * 256u * 2u, &wbar);
     const float* bias = layer == 0 ? b1 : b2;
     for (int c = 0; c < 4; ++c) {
       uint32_t rr[32];
@@ -455,11 +464,10 @@ __global__ void __launch_bounds__(kMlpThreads, 1) probe_mlp_tc_kernel(
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    stage_weights(W, layer == 0 ? W2b : W3b, layer == 0 ? 256 : 32, 256);
   }
   // Layer 3 (N 32, NB used) and the bucket choice: the smallest bucket whose
   // predicted CDF reaches thr.
-  if (ok) ok = __syncthreads_and(mlp_mma(tmem, A, W, 32, 256, &bar, parity, err));
+  if (ok) ok = __syncthreads_and(mbar_wait(&wbar, wpar, err, 42) && mlp_mma(tmem, A, W, 32, 256, &bar, parity, err));
   if (ok && warp < 4) {
     uint32_t rr[32];
     tmem_ld32(taddr, rr);

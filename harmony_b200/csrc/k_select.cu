@@ -435,6 +435,89 @@ __global__ void list_items_kernel(const int32_t* __restrict__ list_cnt, const in
   items[l] = nch * ng;
 }
 
+// Block-wide exclusive prefix sum of n int64 values given by get(i), each
+// thread taking a contiguous run: out[i] for i < n and out[n] = the total.
+// Every thread of the block must call it.
+constexpr int kWorkThreads = 1024;
+constexpr int kSmallWorkPairs = 32768;  // (query, probe) pairs a single CTA builds
+constexpr int kSmallWorkLists = 16384;  // lists whose counters fit its shared memory
+
+template <class Get>
+__device__ void block_exclusive_scan(Get get, int n, int64_t* __restrict__ out, int64_t* s_warp) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int per = (n + kWorkThreads - 1) / kWorkThreads;
+  const int b = min(n, tid * per), e = min(n, b + per);
+  int64_t sum = 0;
+  for (int i = b; i < e; ++i) sum += get(i);
+  int64_t incl = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t x = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += x;
+  }
+  if (lane == 31) s_warp[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int64_t w = lane < kWorkThreads / 32 ? s_warp[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t x = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += x;
+    }
+    s_warp[32 + lane] = w;  // inclusive totals of the warps
+  }
+  __syncthreads();
+  int64_t run = incl - sum + (wid > 0 ? s_warp[32 + wid - 1] : 0);
+  for (int i = b; i < e; ++i) {
+    out[i] = run;
+    run += get(i);
+  }
+  if (tid == kWorkThreads - 1) out[n] = s_warp[32 + kWorkThreads / 32 - 1];
+  __syncthreads();
+}
+
+// The whole work description of a small batch in one CTA (the multi-kernel
+// path's count, prefix sums and scatter, with the counters in shared
+// memory): list_cnt, list_qoff, item_off, slot_base and list_q as
+// launch_build_work defines them.
+__global__ void __launch_bounds__(kWorkThreads) build_work_small_kernel(
+    const int32_t* __restrict__ probes, int nqp, int P, const int64_t* __restrict__ list_off, int nlist,
+    int chunk_rows, int qgroup, int32_t* __restrict__ list_cnt, int64_t* __restrict__ list_qoff,
+    int32_t* __restrict__ list_q, int64_t* __restrict__ item_off, int64_t* __restrict__ slot_base) {
+  extern __shared__ int32_t s_work[];  // [nlist] counts, then [nlist] cursors
+  __shared__ int64_t s_warp[64];
+  int32_t* cnt = s_work;
+  int32_t* cur = s_work + nlist;
+  for (int l = threadIdx.x; l < nlist; l += blockDim.x) {
+    cnt[l] = 0;
+    cur[l] = 0;
+  }
+  __syncthreads();
+  auto nch_of = [&](int idx) -> int64_t {
+    const int l = probes[idx];
+    if (l < 0) return 0;
+    const int64_t n = list_off[l + 1] - list_off[l];
+    return n > 0 ? (n + chunk_rows - 1) / chunk_rows : 0;
+  };
+  for (int idx = threadIdx.x; idx < nqp; idx += blockDim.x)
+    if (nch_of(idx) > 0) atomicAdd(&cnt[probes[idx]], 1);
+  __syncthreads();
+  for (int l = threadIdx.x; l < nlist; l += blockDim.x) list_cnt[l] = cnt[l];
+  block_exclusive_scan([&](int l) -> int64_t { return cnt[l]; }, nlist, list_qoff, s_warp);
+  block_exclusive_scan(
+      [&](int l) -> int64_t {
+        const int64_t n = list_off[l + 1] - list_off[l];
+        return ((n + chunk_rows - 1) / chunk_rows) * ((cnt[l] + qgroup - 1) / qgroup);
+      },
+      nlist, item_off, s_warp);
+  block_exclusive_scan(nch_of, nqp, slot_base, s_warp);
+  for (int idx = threadIdx.x; idx < nqp; idx += blockDim.x) {
+    if (nch_of(idx) == 0) continue;
+    const int l = probes[idx];
+    const int pos = atomicAdd(&cur[l], 1);
+    const int q = idx / P, j = idx - q * P;
+    list_q[list_qoff[l] + pos] = static_cast<int32_t>((static_cast<uint32_t>(q) << 16) | static_cast<uint32_t>(j));
+  }
+}
+
 __global__ void scatter_probes_kernel(const int32_t* __restrict__ probes, int nqp, int P,
                                       const int64_t* __restrict__ list_off, const int64_t* __restrict__ list_qoff,
                                       int32_t* __restrict__ cursor, int32_t* __restrict__ list_q) {
@@ -577,6 +660,16 @@ void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list
   int64_t* items64 = cnt64 + n1;
   int64_t* slot_cnt = items64 + n1;
   const int nqp = nq * P;
+  if (nqp <= kSmallWorkPairs && nlist <= kSmallWorkLists) {
+    // Small batch: one CTA, one launch.
+    const size_t smem = static_cast<size_t>(2) * nlist * sizeof(int32_t);
+    HB_CUDA(cudaFuncSetAttribute(build_work_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    build_work_small_kernel<<<1, kWorkThreads, smem, st>>>(probes, nqp, P, list_off, nlist, chunk_rows, qgroup,
+                                                           list_cnt, list_qoff, list_q, item_off, slot_base);
+    HB_CUDA(cudaGetLastError());
+    return;
+  }
   HB_CUDA(cudaMemsetAsync(list_cnt, 0, sizeof(int32_t) * nlist, st));
   HB_CUDA(cudaMemsetAsync(list_cursor, 0, sizeof(int32_t) * nlist, st));
   HB_CUDA(cudaMemsetAsync(slot_cnt + nqp, 0, sizeof(int64_t), st));

@@ -33,8 +33,9 @@
 // w <= thr(q).  thr starts at the seed bound (the k-th smallest of the same
 // values over the first rows of the query's nearest list, + 2 eps: an upper
 // bound of W_k + 2 eps because the seed's values obey the same eps) and, for
-// k <= 16, falls to (k-th smallest w this thread has seen for the query) +
-// 2 eps as the scan goes, shared between work items through an atomicMin.
+// k <= 16, falls to (k-th smallest w this thread knows for the query) + 2 eps
+// as the scan goes, shared between work items through an atomicMin; a
+// published bound stands in for k values at thr - 2 eps (rounded up).
 // Every row with w <= W_k + 2 eps is admitted whatever the order.  The
 // re-rank takes W_k over the appended rows (all rows with w <= W_k are
 // among them), keeps those at or under W_k + 2 eps and recomputes them with
@@ -400,22 +401,46 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         return fminf(__fadd_ru(__fsub_ru(t, cd), 1e-6f * (fminf(fabsf(t), 1e30f) + cd)), FLT_MAX);
       };
       float thr_s = shifted(thr);
-      // The KT smallest values this thread has admitted for the query in this
-      // item, ascending, and the k-th of them (+inf until k are in; KT = 0:
-      // no tightening).  Only a value under the k-th changes them.
+      // The KT smallest values this thread knows for the query, ascending, and
+      // the k-th of them (KT = 0: no tightening).  A published bound
+      // thr = fadd_ru(V, e2) says that k rows have values <= V, so
+      // W = fsub_ru(thr, e2) >= V may stand in for k values: the k-th of a
+      // mix of such stand-ins and real values is still the k-th of k
+      // distinct rows or W itself.  Starting from them, only a value under
+      // the current k-th changes the set.
+      auto floor_of = [&](float t) { return t < FLT_MAX ? __fsub_ru(t, e2) : INFINITY; };
       float best[KB];
+      float kth_loc = floor_of(thr);
 #pragma unroll
-      for (int i = 0; i < KB; ++i) best[i] = INFINITY;
-      float kth_loc = INFINITY;
+      for (int i = 0; i < KB; ++i) best[i] = kth_loc;
       uint64_t* cbuf = a.cand + static_cast<size_t>(my_q < 0 ? 0 : my_q) * a.cap;
-      // Admitted keys wait here (stride kEpiThreads: conflict-free) and go to
-      // the query's buffer kStage at a time, one atomicAdd per flush.
+      // Admitted keys wait here (stride kEpiThreads: conflict-free) in two
+      // halves of kHalf.  A full half takes its slots in the query's buffer
+      // with one atomicAdd and is written out only when the other half fills
+      // (or at the item's end), so the atomic's round trip overlaps the scan
+      // instead of stalling the warp once per lane.
+      constexpr int kHalf = kStage / 2;
       uint64_t* stg = staging + static_cast<size_t>(grp) * kStage * kEpiThreads + etid;
-      int ns = 0;
+      int ns = 0, half = 0, pend_base = 0;
+      bool pend = false;
+      auto write_half = [&](int h, int base, int n) {
+        for (int i = 0; i < n; ++i)
+          if (base + i < a.cap) cbuf[base + i] = stg[(h * kHalf + i) * kEpiThreads];
+      };
+      auto stage = [&](uint64_t key) {
+        stg[(half * kHalf + ns) * kEpiThreads] = key;
+        if (++ns == kHalf) {
+          if (pend) write_half(half ^ 1, pend_base, kHalf);
+          pend_base = atomicAdd(a.cand_cnt + my_q, kHalf);
+          pend = true;
+          half ^= 1;
+          ns = 0;
+        }
+      };
       auto flush = [&]() {
-        const int base = atomicAdd(a.cand_cnt + my_q, ns);
-        for (int i = 0; i < ns; ++i)
-          if (base + i < a.cap) cbuf[base + i] = stg[i * kEpiThreads];
+        if (pend) write_half(half ^ 1, pend_base, kHalf);
+        if (ns > 0) write_half(half, atomicAdd(a.cand_cnt + my_q, ns), ns);
+        pend = false;
         ns = 0;
       };
       // One 32-column chunk of the accumulator in r: w' = ||r||^2 - 2 q'.r
@@ -456,8 +481,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
             for (int i = 0; i < 2; ++i) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
             const float wv = cd + __uint_as_float((j & 16) ? t2[1] : t2[0]);
-            stg[ns * kEpiThreads] = (static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j));
-            if (++ns == kStage) flush();
+            stage((static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j)));
             if (KT > 0 && wv < kth_loc) {
               // Insert into the ascending KT smallest; once k values are in,
               // the k-th + 2 eps bounds W_k + 2 eps from above.
@@ -496,6 +520,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (my_q >= 0 && ordered_to_float(g_thr) < thr) {
           thr = ordered_to_float(g_thr);
           thr_s = shifted(thr);
+          if (KT > 0) {
+            kth_loc = fminf(kth_loc, floor_of(thr));
+#pragma unroll
+            for (int i = 0; i < KB; ++i) best[i] = fminf(best[i], kth_loc);
+          }
         }
         g_thr = my_q >= 0 ? *reinterpret_cast<volatile uint32_t*>(a.thr + my_q) : 0u;
         if (ok && warp_on) {
@@ -522,7 +551,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tc_fence_before();
         mbar_arrive(&sh.acce[b]);
       }
-      if (my_q >= 0 && ns > 0) flush();
+      if (my_q >= 0) flush();
       if (!ok) break;
       G += static_cast<uint32_t>(d.ntiles);
     }
@@ -627,7 +656,7 @@ __global__ void residual_bf16_kernel(const float* __restrict__ codes, const int6
 // candidates sorted by (w, position), W_k = the k-th w, the prefix with
 // w <= W_k + 2 eps recomputed with the reference's sequential FP32 loop,
 // sorted by (distance, position) and cut at k.  A query with more candidates
-// goes to the CTA kernel (flag 1); one whose buffer overflowed to the host's
+// goes to the flat kernels below (flag 1); one whose buffer overflowed to the host's
 // exact search (flag 2, and listed).
 constexpr int kRrWarpCap = 256;
 constexpr int kRrWarps = 8;
@@ -790,61 +819,119 @@ __global__ void split_first_probe_kernel(const int32_t* __restrict__ probes, int
   if (j == 0) first[i / P] = v;
 }
 
-// The same for the queries the warp kernel listed in big_list (more than
-// kRrWarpCap candidates, at most cap; *big_n of them): one CTA per query,
-// grid-stride over the list.
-__global__ void __launch_bounds__(256) rerank_cta_kernel(const uint64_t* __restrict__ cand, const int* __restrict__ cnt,
-                                                         int cap, const float* __restrict__ e2, int nq, int k,
-                                                         const float* __restrict__ codes, const float* __restrict__ q,
-                                                         int dpad, const int64_t* __restrict__ ids, float* __restrict__ D,
-                                                         int64_t* __restrict__ I, const int* __restrict__ big_list,
-                                                         const int* __restrict__ big_n, int* __restrict__ m_out) {
-  extern __shared__ uint64_t s_dyn[];  // [cap] candidates, then [cap] exact keys
+// The queries the warp kernel listed in big_list (more than kRrWarpCap
+// candidates, at most cap; *big_n of them) in three flat kernels, so the
+// exact distances -- the bulk of the work -- run with every SM's threads
+// loading rows rather than behind per-query sorts:
+//   rerank_big_bound_kernel  a warp per query: W_k by radix selection over
+//                            the candidates' values, then the candidates at
+//                            or under W_k + 2 eps compacted in place at the
+//                            front of the query's buffer (m of them);
+//   rerank_big_exact_kernel  a CTA per query: the exact distance of each of
+//                            the m rows (two rows per thread in flight),
+//                            written back in place as (distance, position)
+//                            keys;
+//   rerank_big_topk_kernel   a CTA per query: the k smallest keys, sorted.
+constexpr int kBigWarps = 8;
+constexpr int kRerankMaxDim = 128;  // dpad of the BF16 scan's rows (d <= 128)
+
+__global__ void __launch_bounds__(kBigWarps * 32) rerank_big_bound_kernel(
+    uint64_t* __restrict__ cand, const int* __restrict__ cnt, int cap, const float* __restrict__ e2, int k,
+    const int* __restrict__ big_list, const int* __restrict__ big_n, int* __restrict__ m_out) {
+  __shared__ int s_h[kBigWarps][256];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int w = blockIdx.x * kBigWarps + wib;
+  if (w >= *big_n) return;
+  const int qi = big_list[w];
+  const int c = cnt[qi];
+  uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
+  const uint32_t wk = warp_kth_smallest([&](int i) { return static_cast<uint32_t>(buf[i] >> 32); }, c, k, s_h[wib], lane);
+  const uint32_t lim_bits = ordered_bits(__fadd_ru(ordered_to_float(wk), e2[qi]));
+  // In-place compaction: a block of 32 is read before any of it is written,
+  // and writes land at or below the read position.
+  int m = 0;
+  for (int base = 0; base < c; base += 32) {
+    const int i = base + lane;
+    const uint64_t key = i < c ? buf[i] : kEmpty;
+    const bool in = i < c && static_cast<uint32_t>(key >> 32) <= lim_bits;
+    const unsigned bal = __ballot_sync(0xffffffffu, in);
+    __syncwarp();
+    if (in) buf[m + __popc(bal & ((1u << lane) - 1u))] = key;
+    m += __popc(bal);
+  }
+  if (lane == 0) m_out[qi] = m;
+}
+
+__global__ void __launch_bounds__(256) rerank_big_exact_kernel(uint64_t* __restrict__ cand, int cap,
+                                                               const float* __restrict__ codes,
+                                                               const float* __restrict__ q, int dpad,
+                                                               const int* __restrict__ big_list,
+                                                               const int* __restrict__ big_n,
+                                                               const int* __restrict__ m_in) {
+  __shared__ __align__(16) float s_q[kRerankMaxDim];
+  const int w = blockIdx.x;
+  if (w >= *big_n) return;
+  const int qi = big_list[w];
+  const int m = m_in[qi];
+  uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
+  for (int c = threadIdx.x; c < dpad; c += blockDim.x) s_q[c] = q[static_cast<size_t>(qi) * dpad + c];
+  __syncthreads();
+  // Rows j and j + blockDim.x together: two independent chains, each the
+  // reference's sequential loop (many small CTAs per SM keep the loads in
+  // flight).
+  for (int j0 = threadIdx.x; j0 < m; j0 += 2 * blockDim.x) {
+    const int j1 = j0 + blockDim.x;
+    const uint32_t p0 = key_tie(buf[j0]);
+    const uint32_t p1 = j1 < m ? key_tie(buf[j1]) : p0;
+    const float4* x0 = reinterpret_cast<const float4*>(codes + static_cast<size_t>(p0) * dpad);
+    const float4* x1 = reinterpret_cast<const float4*>(codes + static_cast<size_t>(p1) * dpad);
+    float a0 = 0.0f, a1 = 0.0f;
+#pragma unroll 4
+    for (int i = 0; i < dpad / 4; ++i) {
+      const float4 u = __ldg(x0 + i), v = __ldg(x1 + i);
+      const float4 g = *reinterpret_cast<const float4*>(s_q + 4 * i);
+      float t;
+      t = __fsub_rn(g.x, u.x);
+      a0 = __fadd_rn(a0, __fmul_rn(t, t));
+      t = __fsub_rn(g.x, v.x);
+      a1 = __fadd_rn(a1, __fmul_rn(t, t));
+      t = __fsub_rn(g.y, u.y);
+      a0 = __fadd_rn(a0, __fmul_rn(t, t));
+      t = __fsub_rn(g.y, v.y);
+      a1 = __fadd_rn(a1, __fmul_rn(t, t));
+      t = __fsub_rn(g.z, u.z);
+      a0 = __fadd_rn(a0, __fmul_rn(t, t));
+      t = __fsub_rn(g.z, v.z);
+      a1 = __fadd_rn(a1, __fmul_rn(t, t));
+      t = __fsub_rn(g.w, u.w);
+      a0 = __fadd_rn(a0, __fmul_rn(t, t));
+      t = __fsub_rn(g.w, v.w);
+      a1 = __fadd_rn(a1, __fmul_rn(t, t));
+    }
+    buf[j0] = a0 < FLT_MAX ? make_key(a0, p0) : kEmpty;
+    if (j1 < m) buf[j1] = a1 < FLT_MAX ? make_key(a1, p1) : kEmpty;
+  }
+}
+
+__global__ void __launch_bounds__(256) rerank_big_topk_kernel(const uint64_t* __restrict__ cand, int cap, int k,
+                                                              const int64_t* __restrict__ ids, float* __restrict__ D,
+                                                              int64_t* __restrict__ I, const int* __restrict__ big_list,
+                                                              const int* __restrict__ big_n,
+                                                              const int* __restrict__ m_in) {
+  extern __shared__ uint64_t s_top[];  // pow2_ceil(k)
   __shared__ SelectShared sh_sel;
-  __shared__ int s_m;
-  const int nbig = *big_n;
-  for (int bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
-    const int qi = big_list[bi];
-    const int c = cnt[qi];
-    const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
-    uint64_t* buf = s_dyn;
-    uint64_t* ex = s_dyn + cap;
-    const int n2 = pow2_ceil(c);
-    for (int i = threadIdx.x; i < n2; i += blockDim.x) buf[i] = i < c ? src[i] : kEmpty;
-    __syncthreads();
-    block_bitonic_sort(buf, n2);
-    if (threadIdx.x == 0) {
-      const float lim = __fadd_ru(ordered_to_float(static_cast<uint32_t>(buf[k - 1] >> 32)), e2[qi]);
-      const uint32_t lim_bits = ordered_bits(lim);
-      // buf is sorted: m = the first index in [k, c) whose value is above
-      // lim (binary search).
-      int lo = k, hi = c;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (static_cast<uint32_t>(buf[mid] >> 32) <= lim_bits) lo = mid + 1; else hi = mid;
-      }
-      const int m = lo;
-      s_m = m;
-      m_out[qi] = m;
-    }
-    __syncthreads();
-    const int m = s_m;
-    const float* qrow = q + static_cast<size_t>(qi) * dpad;
-    for (int j = threadIdx.x; j < m; j += blockDim.x) {
-      const uint32_t pos = key_tie(buf[j]);
-      const float acc = exact_l2_seq(codes + static_cast<size_t>(pos) * dpad, qrow, dpad);
-      ex[j] = acc < FLT_MAX ? make_key(acc, pos) : kEmpty;
-    }
-    __syncthreads();
-    auto key_at = [&](int i) -> uint64_t { return ex[i]; };
-    block_topk_sorted(key_at, m, k, sh_sel, buf);
-    for (int j = threadIdx.x; j < k; j += blockDim.x) {
-      const uint64_t key = buf[j];
-      const size_t o = static_cast<size_t>(qi) * k + j;
-      D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
-      I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
-    }
-    __syncthreads();
+  const int w = blockIdx.x;
+  if (w >= *big_n) return;
+  const int qi = big_list[w];
+  const int m = m_in[qi];
+  const uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
+  auto key_at = [&](int i) -> uint64_t { return buf[i]; };
+  block_topk_sorted(key_at, m, k, sh_sel, s_top);
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    const uint64_t key = s_top[j];
+    const size_t o = static_cast<size_t>(qi) * k + j;
+    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
   }
 }
 
@@ -1150,23 +1237,27 @@ void launch_seed_bound(const float* q, int dpad, const float* cent, int nq, int 
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_rerank_bf16(const uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
+void launch_rerank_bf16(uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
                         int* flag, int* over_list, int* over_n, int* m_out, int num_sms, cudaStream_t st) {
   if (nq <= 0) return;
   HB_CHECK(k >= 1 && cap >= k && cap <= kRerankMaxCap && (cap & (cap - 1)) == 0, HB_ERR_INVALID,
            "candidate buffer size out of range");
+  HB_CHECK(dpad % 4 == 0 && dpad <= kRerankMaxDim, HB_ERR_INVALID, "re-rank rows wider than 128 floats");
   rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(cand, cnt, cap, e2, nq, k, codes, q,
                                                                                dpad, ids, D, I, flag, over_list, over_n,
                                                                                m_out, over_list + nq);
   HB_CUDA(cudaGetLastError());
   if (cap > kRrWarpCap) {
-    const size_t smem = static_cast<size_t>(2) * cap * sizeof(uint64_t);
-    HB_CUDA(cudaFuncSetAttribute(rerank_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
-    const int grid = std::min(nq, 4 * num_sms);
-    rerank_cta_kernel<<<grid, 256, smem, st>>>(cand, cnt, cap, e2, nq, k, codes, q, dpad, ids, D, I, over_list + nq,
-                                               over_n + 1, m_out);
+    // At most nq queries are big; blocks past *big_n return at once.
+    const int* big_list = over_list + nq;
+    const int* big_n = over_n + 1;
+    rerank_big_bound_kernel<<<(nq + kBigWarps - 1) / kBigWarps, kBigWarps * 32, 0, st>>>(
+        cand, cnt, cap, e2, k, big_list, big_n, m_out);
+    rerank_big_exact_kernel<<<nq, 256, 0, st>>>(cand, cap, codes, q, dpad, big_list, big_n,
+                                                m_out);
+    const size_t smem = static_cast<size_t>(pow2_ceil(k < 2 ? 2 : k)) * sizeof(uint64_t);
+    rerank_big_topk_kernel<<<nq, 256, smem, st>>>(cand, cap, k, ids, D, I, big_list, big_n, m_out);
     HB_CUDA(cudaGetLastError());
   }
 }

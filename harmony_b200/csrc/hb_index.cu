@@ -1364,7 +1364,6 @@ class IndexCore {
     err_dev_.reserve(1);
     HB_CUDA(cudaMemsetAsync(err_dev_.p, 0, sizeof(int), st_));
     const int cap = filter_cap(k);
-    e2_.reserve(nb);
     thr_.reserve(nb);
     ccnt_.reserve(nb);
     cflag_.reserve(nb);
@@ -1373,6 +1372,7 @@ class IndexCore {
     last_nb_ = nb;
     over_n_.reserve(2);
     cbuf_.reserve(static_cast<size_t>(nb) * cap);
+    cbuf_ub_.reserve(static_cast<size_t>(nb) * cap);
     const int cr0 = std::max(128, chunk_rows_for(nb, P, 128));
     const int s0 = scan_bf16_stages(kpad_);
     const TuneKey key = tune_key(nb, P, k);
@@ -1397,8 +1397,7 @@ class IndexCore {
     HB_CUDA(cudaMemsetAsync(over_n_.p, 0, 2 * sizeof(int), st_));
     {
       Scope sc(this, "query_prep");
-      launch_query_prep(qpad_.p, nb, static_cast<int>(d_), static_cast<int>(dpad_), probes_.p, P, cent_.p, rmax_.p,
-                        e2_.p, thr_.p, ccnt_.p, st_);
+      launch_query_prep(nb, thr_.p, ccnt_.p, st_);
     }
     list_cnt_.reserve(nlist_);
     list_cursor_.reserve(nlist_);
@@ -1427,9 +1426,9 @@ class IndexCore {
     }
     {
       Scope sc(this, "seed");
-      launch_seed_bound(qpad_.p, static_cast<int>(dpad_), cent_.p, nb, kpad_, codes_bf16_.p, list_off_.p,
-                        static_cast<int>(nlist_), list_qoff_.p, list_q_.p, rnorm_.p, std::max(seed_rows_, k), k,
-                        e2_.p, thr_.p, st_, probes_a, P_a);
+      launch_seed_bound(qpad_.p, static_cast<int>(d_), static_cast<int>(dpad_), cent_.p, nb, kpad_, codes_bf16_.p,
+                        list_off_.p, static_cast<int>(nlist_), list_qoff_.p, list_q_.p, rnorm_.p, rmax_.p,
+                        std::max(seed_rows_, k), k, thr_.p, st_, probes_a, P_a);
     }
     counter_.reserve(1);
     HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
@@ -1449,8 +1448,9 @@ class IndexCore {
     a.chunk_rows = cr_a;
     a.work_counter = counter_.p;
     a.thr = thr_.p;
-    a.e2 = e2_.p;
+    a.rmax = rmax_.p;
     a.cand = cbuf_.p;
+    a.cand_ub = cbuf_ub_.p;
     a.cand_cnt = ccnt_.p;
     a.cap = cap;
     a.k = k;
@@ -1465,7 +1465,7 @@ class IndexCore {
       // Second stage: the other lists, appended to the same buffers.
       {
         Scope sc(this, "kth_bound");
-        launch_kth_bound(cbuf_.p, ccnt_.p, cap, nb, k, e2_.p, thr_.p, st_);
+        launch_kth_bound(cbuf_ub_.p, ccnt_.p, cap, nb, k, thr_.p, st_);
       }
       {
         Scope sc(this, "build_work");
@@ -1482,7 +1482,7 @@ class IndexCore {
     }
     {
       Scope sc(this, "rerank");
-      launch_rerank_bf16(cbuf_.p, ccnt_.p, cap, e2_.p, nb, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd,
+      launch_rerank_bf16(cbuf_.p, cbuf_ub_.p, ccnt_.p, cap, nb, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd,
                          Id, cflag_.p, over_list_.p, over_n_.p, rr_m_.p, num_sms_, st_);
     }
     launches_ += 8 + (cap > 256 ? 1 : 0);
@@ -2101,11 +2101,11 @@ class IndexCore {
   std::map<std::string, GraphEntry> graphs_;
   DevBuf<int32_t> npqin_;
   // bounded BF16 scan
-  DevBuf<float> e2_;
   DevBuf<uint32_t> thr_;
   DevBuf<int> ccnt_, cflag_, over_list_, over_n_, rr_m_;
   int last_nb_ = 0;
   DevBuf<uint64_t> cbuf_;
+  DevBuf<uint32_t> cbuf_ub_;  // each candidate's upper bound
   DevBuf<float> oq_, od_;
   DevBuf<int32_t> op_;
   DevBuf<int64_t> oi_;

@@ -191,9 +191,11 @@ struct TcArgs {
   const int64_t* item_off;
   int chunk_rows;              // multiple of 128
   unsigned int* work_counter;
-  uint32_t* thr;               // per query: admission bound (ordered float bits), lowered by atomicMin
-  const float* e2;             // per query: 2 x the error bound eps
-  uint64_t* cand;              // nq x cap candidate keys (ordered w bits << 32 | position)
+  uint32_t* thr;               // per query: U, an upper bound of the k-th distance (ordered float bits),
+                               // lowered by atomicMin
+  const float* rmax;           // per list: the largest residual norm (the error bound's R)
+  uint64_t* cand;              // nq x cap candidate keys (ordered lower-bound bits << 32 | position)
+  uint32_t* cand_ub;           // nq x cap: each candidate's upper bound (ordered float bits)
   int* cand_cnt;               // per query: candidates appended (may exceed cap: overflow)
   int cap;
   int k;
@@ -211,11 +213,8 @@ int scan_bf16_stages(int kpad);  // deepest B tile ring that fits
 void launch_tile_norms(const float* norms, const int64_t* list_off, int nlist, const int64_t* tile_off,
                        float* tile_norm, cudaStream_t st);
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);
-// Per query: 2 eps_max over its probed lists (probes nq x P, -1 = none;
-// rmax = each list's largest residual norm), bound reset to FLT_MAX,
-// candidate count 0.
-void launch_query_prep(const float* q, int nq, int d, int dpad, const int32_t* probes, int P, const float* cent,
-                       const float* rmax, float* e2, uint32_t* thr, int* cnt, cudaStream_t st);
+// Per query: bound reset to FLT_MAX (none yet), candidate count 0.
+void launch_query_prep(int nq, uint32_t* thr, int* cnt, cudaStream_t st);
 // Residual BF16 codes BF16(x - c_l) (kpad columns), FP32 residual norms per row
 // and the largest residual norm per list.
 void launch_residual_bf16(const float* codes, const int64_t* list_off, const float* cent, int nlist, int dpad, int kpad,
@@ -223,17 +222,18 @@ void launch_residual_bf16(const float* codes, const int64_t* list_off, const flo
 // Seed bound from the first S <= 256 rows of each query's nearest list (probe
 // rank 0 in the list-major work description; with probes given and a small
 // batch, one CTA per query).
-void launch_seed_bound(const float* q, int dpad, const float* cent, int nq, int kpad, const void* codes_bf16,
+void launch_seed_bound(const float* q, int d, int dpad, const float* cent, int nq, int kpad, const void* codes_bf16,
                        const int64_t* list_off, int nlist, const int64_t* list_qoff, const int32_t* list_q,
-                       const float* rnorm, int S, int k, const float* e2, uint32_t* thr, cudaStream_t st,
+                       const float* rnorm, const float* rmax, int S, int k, uint32_t* thr, cudaStream_t st,
                        const int32_t* probes = nullptr, int P = 0);
-// Exact re-rank of the admitted rows under W_k + 2 eps; flag[q] = 2 and
+// Exact re-rank of the admitted rows whose lower bound is at most U, the k-th
+// smallest admitted upper bound (cand_ub); flag[q] = 2 and
 // over_list[0 .. over_n[0]) for queries whose buffer overflowed (left
 // unwritten); over_list[nq ..] / over_n[1] list the queries with more than
 // 256 candidates, re-ranked by the flat kernels, which overwrite their
 // buffers (over_list holds 2 nq ints, over_n 2, zeroed by the caller);
 // m_out[q] = rows re-ranked.
-void launch_rerank_bf16(uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
+void launch_rerank_bf16(uint64_t* cand, const uint32_t* cand_ub, const int* cnt, int cap, int nq, int k,
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
                         int* flag, int* over_list, int* over_n, int* m_out, int num_sms, cudaStream_t st);
 
@@ -241,9 +241,9 @@ void launch_rerank_bf16(uint64_t* cand, const int* cnt, int cap, const float* e2
 // stages (the nearest list of every query first, then the rest under the
 // k-th value the first stage admitted).
 constexpr int kFilterTightK = 16;
-// Per query: thr = min(thr, k-th smallest admitted w + e2) when the buffer
-// holds at least k rows and did not overflow.
-void launch_kth_bound(const uint64_t* cand, const int* cnt, int cap, int nq, int k, const float* e2, uint32_t* thr,
+// Per query: thr = min(thr, k-th smallest admitted upper bound) when the
+// buffer holds at least k rows and did not overflow.
+void launch_kth_bound(const uint32_t* cand_ub, const int* cnt, int cap, int nq, int k, uint32_t* thr,
                       cudaStream_t st);
 // first[q] = probes[q][0]; rest = probes with column 0 set to -1.
 void launch_split_first_probe(const int32_t* probes, int nq, int P, int32_t* first, int32_t* rest, cudaStream_t st);

@@ -19,27 +19,29 @@
 //   rounding of w (two additions)            <= 2 u (Q + R)^2
 //   | d(x) - D |                             <= (d + 3) u D
 // so |w(x) - d(x)| <= eps(q, l) = 1.0625 * (2 (2^-8 + 2^-10 + 2^-16) Q R
-// + (d + 3) u (Q^2 + R^2) + (d + 5) u (Q + R)^2), and eps(q) = the largest
-// eps(q, l) over the query's probed lists.  Residuals keep Q and R at the
-// scale of a list's spread, not of the data's distance from the origin.  Let
-// W_k be the k-th smallest w over the probed rows.  The k rows with the
-// smallest w have d <= W_k + eps, so the k-th smallest d is at most that, and
-// every row of the exact top k (ties at the k-th distance included) has
-// w <= W_k + 2 eps.  Re-ranking exactly every row with w <= W_k + 2 eps, by
-// (FP32 distance, position) like the exact scan, therefore returns the exact
-// scan's result.
+// + (d + 3) u (Q^2 + R^2) + (d + 5) u (Q + R)^2), a bound per (query, list)
+// (d may be replaced by dpad >= d).  Residuals keep Q and R at the scale of
+// a list's spread, not of the data's distance from the origin.  Each row
+// therefore has a lower bound lb(x) = w(x) - eps(q, l_x) and an upper bound
+// ub(x) = w(x) + eps(q, l_x) of its distance (rounded outwards).  Let U be
+// any value at least the k-th smallest ub over some k probed rows: k rows
+// have d <= U, so the k-th smallest distance d_k is at most U, and every row
+// of the exact top k (ties at the k-th distance included) has
+// lb <= d <= d_k <= U.  Re-ranking exactly every row with lb <= U, by (FP32
+// distance, position) like the exact scan, therefore returns the exact
+// scan's result.  A bound per list rather than the largest over the probed
+// lists keeps one far or wide list from loosening every other list's test.
 //
-// Admission.  A row is appended to its query's candidate buffer when
-// w <= thr(q).  thr starts at the seed bound (the k-th smallest of the same
-// values over the first rows of the query's nearest list, + 2 eps: an upper
-// bound of W_k + 2 eps because the seed's values obey the same eps) and, for
-// k <= 16, falls to (k-th smallest w this thread knows for the query) + 2 eps
-// as the scan goes, shared between work items through an atomicMin; a
-// published bound stands in for k values at thr - 2 eps (rounded up).
-// Every row with w <= W_k + 2 eps is admitted whatever the order.  The
-// re-rank takes W_k over the appended rows (all rows with w <= W_k are
-// among them), keeps those at or under W_k + 2 eps and recomputes them with
-// the reference's loop.  A query whose buffer overflows is flagged; the host
+// Admission.  A row is appended to its query's candidate buffer (key = its
+// lower bound, position; its upper bound alongside) when lb <= U(q), i.e.
+// w <= U + eps(q, l).  U starts at the seed bound (the k-th smallest upper
+// bound over the first rows of the query's nearest list) and, for k <= 16,
+// falls to the k-th smallest upper bound a thread knows for the query as the
+// scan goes, shared between work items through an atomicMin; a published U
+// stands in for k upper bounds.  Every row of the exact top k is admitted
+// whatever the order.  The re-rank takes U as the k-th smallest upper bound
+// over the appended rows and recomputes those with lb <= U with the
+// reference's loop.  A query whose buffer overflows is flagged; the host
 // searches it again with the exact FP32 scan.
 //
 // Work items are the list-major items of the exact scan (list, chunk of
@@ -95,6 +97,16 @@ constexpr int kAcc = 2 * kGroups;                  // TMEM accumulators of 128 c
 constexpr size_t kSmemCap = 225 * 1024;            // dynamic shared memory budget
 constexpr int kTightK = kFilterTightK;             // largest k whose bound tightens during the scan
 constexpr int kStage = 8;                          // admitted keys staged per epilogue thread before a flush
+
+// The error bound of one (query, list) pair (see the top of this file):
+// Q = ||q - c_l|| from its FP32 square cd, R = the list's largest residual
+// norm, d the dimension.
+__device__ __forceinline__ float pair_eps(float cd, float R, int d) {
+  const float Q = sqrtf(cd) * 1.0001f + 1e-30f;
+  const float u = 5.9604645e-8f;  // 2^-24
+  const float c1 = 0.00390625f + 0.0009765625f + 1.52587890625e-5f;
+  return 1.0625f * (2.0f * c1 * Q * R + (d + 3) * u * (R * R + Q * Q) + (d + 5) * u * (Q + R) * (Q + R));
+}
 
 struct ItemDesc {
   int list, chunk, group, qcnt, ntiles;  // ntiles < 0: no more work
@@ -173,8 +185,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   float* nrm = reinterpret_cast<float*>(stages + static_cast<size_t>(S) * tile_bytes);  // [kAcc][128]
   int* meta_q = reinterpret_cast<int*>(nrm + kAcc * kTile);                 // [2][128]
   float* meta_thr = reinterpret_cast<float*>(meta_q + 2 * kTile);           // [2][128]
-  float* meta_e2 = meta_thr + 2 * kTile;                                    // [2][128]
-  float* meta_cd = meta_e2 + 2 * kTile;                                     // [2][128] ||q - c_l||^2
+  float* meta_eps = meta_thr + 2 * kTile;                                   // [2][128] eps(q, l)
+  float* meta_cd = meta_eps + 2 * kTile;                                    // [2][128] ||q - c_l||^2
   float* s_cent = meta_cd + 2 * kTile;                                      // [2][128] the item's centroid
   uint64_t* staging = reinterpret_cast<uint64_t*>(s_cent + 2 * kTile);      // [kGroups][kStage][128]
 
@@ -247,7 +259,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           meta_q[ab * kTile + r] = q;
           meta_thr[ab * kTile + r] =
               q >= 0 ? ordered_to_float(*reinterpret_cast<volatile uint32_t*>(a.thr + q)) : -INFINITY;
-          meta_e2[ab * kTile + r] = q >= 0 ? a.e2[q] : 0.0f;
         }
         asm volatile("bar.sync 3, %0;\n" ::"n"(kBt) : "memory");
         // A row r = BF16(q - c_l) of the row's query, and ||q - c_l||^2: a
@@ -256,18 +267,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int c0 = 4 * lane;
         const bool col_in = c0 < a.dpad, col_k = c0 < kpad;
         const float4 cv = col_k ? *reinterpret_cast<const float4*>(cen + c0) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float Rl = a.rmax[d.list];
         constexpr int kRowsInFlight = 16;
+        // Rows without a query are left as they are: their TMEM lanes belong
+        // to no query and the epilogue ignores them.  A block's rows with a
+        // query come first (query (r % 32) * 4 + r / 32 grows with r % 32).
         for (int r0 = bw; r0 < kTile; r0 += kBuildWarps * kRowsInFlight) {
+          if (meta_q[ab * kTile + r0] < 0) continue;
           float4 x[kRowsInFlight];
 #pragma unroll
           for (int j = 0; j < kRowsInFlight; ++j) {
             const int q = meta_q[ab * kTile + r0 + j * kBuildWarps];
             x[j] = q >= 0 && col_in ? __ldg(reinterpret_cast<const float4*>(a.q + static_cast<size_t>(q) * a.dpad + c0))
-                                    : cv;  // q - c = 0 for an empty row or a padding column
+                                    : cv;  // q - c = 0 for a padding column
           }
 #pragma unroll
           for (int j = 0; j < kRowsInFlight; ++j) {
             const int r = r0 + j * kBuildWarps;
+            if (meta_q[ab * kTile + r] < 0) break;
             const float v0 = x[j].x - cv.x, v1 = x[j].y - cv.y, v2 = x[j].z - cv.z, v3 = x[j].w - cv.w;
             float cd = fmaf(v3, v3, fmaf(v2, v2, fmaf(v1, v1, v0 * v0)));
 #pragma unroll
@@ -277,7 +294,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               *reinterpret_cast<uint2*>(A + sw128_offset_bf16(r, c0, kblk_bytes)) =
                   make_uint2(*reinterpret_cast<uint32_t*>(&p01), *reinterpret_cast<uint32_t*>(&p23));
             }
-            if (lane == 0) meta_cd[ab * kTile + r] = cd;
+            if (lane == 0) {
+              meta_cd[ab * kTile + r] = cd;
+              meta_eps[ab * kTile + r] = pair_eps(cd, Rl, a.dpad);  // eps(q, l) of this row's query
+            }
           }
         }
         fence_proxy_async_smem();
@@ -385,47 +405,58 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const ItemDesc d = sh.desc[ab];
       const int my_q = meta_q[ab * kTile + etid];
       const float thr0 = meta_thr[ab * kTile + etid];
-      const float e2 = meta_e2[ab * kTile + etid];
+      const float eps = meta_eps[ab * kTile + etid];
       const float cd = meta_cd[ab * kTile + etid];
       mbar_arrive(&sh.aempty[ab]);
       if (d.ntiles < 0) break;
       // Queries are spread over the four warps (row r holds query
       // (r % 32) * 4 + r / 32), so a warp without one skips its loads.
       const bool warp_on = __any_sync(0xffffffffu, my_q >= 0);
+      // thr = U, the query's bound on its k-th distance (FLT_MAX: none yet).
       float thr = thr0;
-      // Columns hold w' = ||r||^2 - 2 q'.r; a row's value is w = cd + w'.  A
-      // column is looked at when w' <= thr_s, thr_s = thr - cd rounded up with
-      // a margin (every row with w <= thr passes; a few more may), and never
-      // above FLT_MAX: the +inf values of rows past a list's end must not pass.
+      // Columns hold w' = ||r||^2 - 2 q'.r; a row's value is w = cd + w'
+      // and it is admitted when w - eps <= U.  A column is looked at when
+      // w' <= thr_s, thr_s = U + eps - cd rounded up with a margin (every row
+      // with w - eps <= U passes; a few more may), and never above FLT_MAX:
+      // the +inf values of rows past a list's end must not pass.
       auto shifted = [&](float t) {
-        return fminf(__fadd_ru(__fsub_ru(t, cd), 1e-6f * (fminf(fabsf(t), 1e30f) + cd)), FLT_MAX);
+        const float te = t < FLT_MAX ? __fadd_ru(t, eps) : FLT_MAX;
+        return fminf(__fadd_ru(__fsub_ru(te, cd), 1e-6f * (fminf(fabsf(te), 1e30f) + cd)), FLT_MAX);
       };
       float thr_s = shifted(thr);
-      // The KT smallest values this thread knows for the query, ascending, and
-      // the k-th of them (KT = 0: no tightening).  A published bound
-      // thr = fadd_ru(V, e2) says that k rows have values <= V, so
-      // W = fsub_ru(thr, e2) >= V may stand in for k values: the k-th of a
-      // mix of such stand-ins and real values is still the k-th of k
-      // distinct rows or W itself.  Starting from them, only a value under
-      // the current k-th changes the set.
-      auto floor_of = [&](float t) { return t < FLT_MAX ? __fsub_ru(t, e2) : INFINITY; };
+      // The KT smallest upper bounds this thread knows for the query,
+      // ascending, and the k-th of them (KT = 0: no tightening).  A published
+      // U says that k rows have upper bounds <= U, so U may stand in for k of
+      // them: the k-th of a mix of stand-ins and real values is the k-th of k
+      // distinct rows or U itself.  Only a value under the current k-th
+      // changes the set.
       float best[KB];
-      float kth_loc = floor_of(thr);
+      float kth_loc = thr < FLT_MAX ? thr : INFINITY;
 #pragma unroll
       for (int i = 0; i < KB; ++i) best[i] = kth_loc;
       uint64_t* cbuf = a.cand + static_cast<size_t>(my_q < 0 ? 0 : my_q) * a.cap;
-      // Admitted keys wait here (stride kEpiThreads: conflict-free) in two
-      // halves of kHalf.  A full half takes its slots in the query's buffer
-      // with one atomicAdd and is written out only when the other half fills
-      // (or at the item's end), so the atomic's round trip overlaps the scan
-      // instead of stalling the warp once per lane.
+      uint32_t* ubuf = a.cand_ub + static_cast<size_t>(my_q < 0 ? 0 : my_q) * a.cap;
+      // Admitted keys (lower bound, position) wait here (stride kEpiThreads:
+      // conflict-free) in two halves of kHalf.  A full half takes its slots in
+      // the query's buffer with one atomicAdd and is written out only when
+      // the other half fills (or at the item's end), so the atomic's round
+      // trip overlaps the scan instead of stalling the warp once per lane.
+      // Staged entries hold (w, position); every entry of an item shares eps,
+      // so the written key (w - eps rounded down, position) and upper bound
+      // (w + eps rounded up) are formed at write time.
       constexpr int kHalf = kStage / 2;
       uint64_t* stg = staging + static_cast<size_t>(grp) * kStage * kEpiThreads + etid;
       int ns = 0, half = 0, pend_base = 0;
       bool pend = false;
       auto write_half = [&](int h, int base, int n) {
-        for (int i = 0; i < n; ++i)
-          if (base + i < a.cap) cbuf[base + i] = stg[(h * kHalf + i) * kEpiThreads];
+        for (int i = 0; i < n; ++i) {
+          if (base + i < a.cap) {
+            const uint64_t e = stg[(h * kHalf + i) * kEpiThreads];
+            const float wv = ordered_to_float(static_cast<uint32_t>(e >> 32));
+            cbuf[base + i] = (static_cast<uint64_t>(ordered_bits(__fsub_rd(wv, eps))) << 32) | (e & 0xffffffffull);
+            ubuf[base + i] = ordered_bits(__fadd_ru(wv, eps));
+          }
+        }
       };
       auto stage = [&](uint64_t key) {
         stg[(half * kHalf + ns) * kEpiThreads] = key;
@@ -482,10 +513,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             for (int i = 0; i < 2; ++i) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
             const float wv = cd + __uint_as_float((j & 16) ? t2[1] : t2[0]);
             stage((static_cast<uint64_t>(ordered_bits(wv)) << 32) | (pos0 + static_cast<uint32_t>(j)));
-            if (KT > 0 && wv < kth_loc) {
-              // Insert into the ascending KT smallest; once k values are in,
-              // the k-th + 2 eps bounds W_k + 2 eps from above.
-              float v = wv;
+            const float ub = __fadd_ru(wv, eps);
+            if (KT > 0 && ub < kth_loc) {
+              // Insert into the ascending KT smallest upper bounds; their k-th
+              // is a new U.
+              float v = ub;
 #pragma unroll
               for (int i = 0; i < KB; ++i) {
                 const float o = best[i];
@@ -498,9 +530,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
               for (int i = 1; i < KB; ++i) kth = i < a.k ? fmaxf(kth, best[i]) : kth;
               kth_loc = kth;
-              const float nt = __fadd_ru(kth, e2);
-              if (nt < thr) {
-                thr = nt;
+              if (kth < thr) {
+                thr = kth;
                 thr_s = shifted(thr);
                 atomicMin(a.thr + my_q, ordered_bits(thr));  // shared at once (no return value used)
               }
@@ -521,7 +552,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           thr = ordered_to_float(g_thr);
           thr_s = shifted(thr);
           if (KT > 0) {
-            kth_loc = fminf(kth_loc, floor_of(thr));
+            kth_loc = fminf(kth_loc, thr);
 #pragma unroll
             for (int i = 0; i < KB; ++i) best[i] = fminf(best[i], kth_loc);
           }
@@ -565,54 +596,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
-// The error bound of one (query, list) pair (see the top of this file):
-// Q = ||q - c_l|| from its FP32 square cd, R = the list's largest residual
-// norm, d the dimension.
-__device__ __forceinline__ float pair_eps(float cd, float R, int d) {
-  const float Q = sqrtf(cd) * 1.0001f + 1e-30f;
-  const float u = 5.9604645e-8f;  // 2^-24
-  const float c1 = 0.00390625f + 0.0009765625f + 1.52587890625e-5f;
-  return 1.0625f * (2.0f * c1 * Q * R + (d + 3) * u * (R * R + Q * Q) + (d + 5) * u * (Q + R) * (Q + R));
-}
 
-// Per query, before the scan: 2 eps_max, eps_max the largest pair bound over
-// the query's probed lists (probes row, -1 = none); the admission bound reset
-// to FLT_MAX (no bound yet; +inf padding rows never pass); the candidate
-// counter reset.  One warp per query, a lane per probe: a row of 256 probes
-// costs 8 rounds, not 256 (the batch waits for its widest row).
-__global__ void query_prep_kernel(const float* __restrict__ q, int nq, int d, int dpad,
-                                  const int32_t* __restrict__ probes, int P, const float* __restrict__ cent,
-                                  const float* __restrict__ rmax, float* __restrict__ e2, uint32_t* __restrict__ thr,
-                                  int* __restrict__ cnt) {
-  const int lane = threadIdx.x & 31;
-  const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+// Per query, before the scan: the bound U reset to FLT_MAX (none yet; +inf
+// padding rows never pass) and the candidate counter reset.
+__global__ void query_prep_kernel(int nq, uint32_t* __restrict__ thr, int* __restrict__ cnt) {
+  const int qi = blockIdx.x * blockDim.x + threadIdx.x;
   if (qi >= nq) return;
-  const float4* q4 = reinterpret_cast<const float4*>(q + static_cast<size_t>(qi) * dpad);
-  float emax = 0.0f;
-  for (int j0 = 0; j0 < P; j0 += 32) {
-    const int l = j0 + lane < P ? probes[static_cast<size_t>(qi) * P + j0 + lane] : -1;
-    if (__ballot_sync(0xffffffffu, l >= 0) == 0u) continue;
-    if (l >= 0) {
-      const float4* c4 = reinterpret_cast<const float4*>(cent + static_cast<size_t>(l) * dpad);
-      float s = 0.0f;
-#pragma unroll 8
-      for (int i = 0; i < dpad / 4; ++i) {
-        const float4 a = q4[i], b = __ldg(c4 + i);
-        const float v0 = a.x - b.x, v1 = a.y - b.y, v2 = a.z - b.z, v3 = a.w - b.w;
-        s = fmaf(v0, v0, s);
-        s = fmaf(v1, v1, s);
-        s = fmaf(v2, v2, s);
-        s = fmaf(v3, v3, s);
-      }
-      emax = fmaxf(emax, pair_eps(s, rmax[l], d));
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
-  if (lane == 0) {
-    e2[qi] = 2.0f * emax + 1e-30f;
-    thr[qi] = ordered_bits(FLT_MAX);
-    cnt[qi] = 0;
-  }
+  thr[qi] = ordered_bits(FLT_MAX);
+  cnt[qi] = 0;
 }
 
 // BF16 residual codes for the tensor-core scans, one CTA per list: row r of
@@ -649,82 +640,6 @@ __global__ void residual_bf16_kernel(const float* __restrict__ codes, const int6
   if (threadIdx.x == 0) {
     for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmaxf(m, s_max[w]);
     rmax[l] = sqrtf(m) * 1.0001f;
-  }
-}
-
-// Re-rank, one warp per query with at most kRrWarpCap candidates: the
-// candidates sorted by (w, position), W_k = the k-th w, the prefix with
-// w <= W_k + 2 eps recomputed with the reference's sequential FP32 loop,
-// sorted by (distance, position) and cut at k.  A query with more candidates
-// goes to the flat kernels below (flag 1); one whose buffer overflowed to the host's
-// exact search (flag 2, and listed).
-constexpr int kRrWarpCap = 256;
-constexpr int kRrWarps = 8;
-
-__global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
-    const uint64_t* __restrict__ cand, const int* __restrict__ cnt, int cap, const float* __restrict__ e2, int nq, int k,
-    const float* __restrict__ codes, const float* __restrict__ q, int dpad, const int64_t* __restrict__ ids,
-    float* __restrict__ D, int64_t* __restrict__ I, int* __restrict__ flag, int* __restrict__ over_list,
-    int* __restrict__ over_n, int* __restrict__ m_out, int* __restrict__ big_list) {
-  __shared__ uint64_t s_c[kRrWarps][kRrWarpCap];
-  __shared__ uint64_t s_x[kRrWarps][kRrWarpCap];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int qi = blockIdx.x * kRrWarps + wib;
-  if (qi >= nq) return;
-  const int c = cnt[qi];
-  if (c > cap) {
-    if (lane == 0) {
-      flag[qi] = 2;
-      m_out[qi] = 0;
-      over_list[atomicAdd(over_n, 1)] = qi;
-    }
-    return;
-  }
-  if (c > kRrWarpCap) {
-    if (lane == 0) {
-      flag[qi] = 1;
-      big_list[atomicAdd(over_n + 1, 1)] = qi;
-    }
-    return;
-  }
-  if (lane == 0) flag[qi] = 0;
-  uint64_t* buf = s_c[wib];
-  uint64_t* ex = s_x[wib];
-  const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
-  const int n2 = pow2_ceil(c < 2 ? 2 : c);
-  for (int i = lane; i < n2; i += 32) buf[i] = i < c ? src[i] : kEmpty;
-  __syncwarp();
-  warp_bitonic_sort(buf, n2, lane);
-  int m = c;
-  if (c >= k) {
-    const float lim = __fadd_ru(ordered_to_float(static_cast<uint32_t>(buf[k - 1] >> 32)), e2[qi]);
-    const uint32_t lim_bits = ordered_bits(lim);
-    m = 0;
-    for (int base = 0; base < c; base += 32) {
-      const int i = base + lane;
-      const bool in = i < c && static_cast<uint32_t>(buf[i] >> 32) <= lim_bits;
-      m += __popc(__ballot_sync(0xffffffffu, in));
-    }
-  }
-  if (lane == 0) m_out[qi] = m;
-  const float* qrow = q + static_cast<size_t>(qi) * dpad;
-  const int e2n = pow2_ceil(m < 2 ? 2 : m);
-  for (int j = lane; j < e2n; j += 32) {
-    uint64_t key = kEmpty;
-    if (j < m) {
-      const uint32_t pos = key_tie(buf[j]);
-      const float acc = exact_l2_seq(codes + static_cast<size_t>(pos) * dpad, qrow, dpad);
-      if (acc < FLT_MAX) key = make_key(acc, pos);
-    }
-    ex[j] = key;
-  }
-  __syncwarp();
-  warp_bitonic_sort(ex, e2n, lane);
-  for (int j = lane; j < k; j += 32) {
-    const uint64_t key = j < m ? ex[j] : kEmpty;
-    const size_t o = static_cast<size_t>(qi) * k + j;
-    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
-    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
   }
 }
 
@@ -779,17 +694,91 @@ __device__ uint32_t warp_kth_smallest(Get get, int n, int k, int* h, int lane) {
   return prefix;
 }
 
+// Re-rank, one warp per query with at most kRrWarpCap candidates: U = the
+// k-th smallest upper bound among them (radix selection), the candidates
+// whose lower bound is at most U recomputed with the reference's sequential
+// FP32 loop, sorted by (distance, position) and cut at k.  A query with more
+// candidates goes to the flat kernels below (flag 1); one whose buffer
+// overflowed to the host's exact search (flag 2, and listed).
+constexpr int kRrWarpCap = 256;
+constexpr int kRrWarps = 8;
+
+__global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
+    const uint64_t* __restrict__ cand, const uint32_t* __restrict__ cand_ub, const int* __restrict__ cnt, int cap,
+    int nq, int k, const float* __restrict__ codes, const float* __restrict__ q, int dpad,
+    const int64_t* __restrict__ ids, float* __restrict__ D, int64_t* __restrict__ I, int* __restrict__ flag,
+    int* __restrict__ over_list, int* __restrict__ over_n, int* __restrict__ m_out, int* __restrict__ big_list) {
+  __shared__ uint64_t s_c[kRrWarps][kRrWarpCap];
+  __shared__ uint64_t s_x[kRrWarps][kRrWarpCap];
+  __shared__ int s_h[kRrWarps][256];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int qi = blockIdx.x * kRrWarps + wib;
+  if (qi >= nq) return;
+  const int c = cnt[qi];
+  if (c > cap) {
+    if (lane == 0) {
+      flag[qi] = 2;
+      m_out[qi] = 0;
+      over_list[atomicAdd(over_n, 1)] = qi;
+    }
+    return;
+  }
+  if (c > kRrWarpCap) {
+    if (lane == 0) {
+      flag[qi] = 1;
+      big_list[atomicAdd(over_n + 1, 1)] = qi;
+    }
+    return;
+  }
+  if (lane == 0) flag[qi] = 0;
+  uint64_t* buf = s_c[wib];
+  uint64_t* ex = s_x[wib];
+  const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
+  const uint32_t* usrc = cand_ub + static_cast<size_t>(qi) * cap;
+  // U (every candidate when there are fewer than k).
+  uint32_t u_bits = 0xFFFFFFFFu;
+  if (c >= k) u_bits = warp_kth_smallest([&](int i) { return usrc[i]; }, c, k, s_h[wib], lane);
+  int m = 0;
+  for (int base = 0; base < c; base += 32) {
+    const int i = base + lane;
+    const uint64_t key = i < c ? src[i] : kEmpty;
+    const bool in = i < c && static_cast<uint32_t>(key >> 32) <= u_bits;
+    const unsigned bal = __ballot_sync(0xffffffffu, in);
+    if (in) buf[m + __popc(bal & ((1u << lane) - 1u))] = key;
+    m += __popc(bal);
+  }
+  __syncwarp();
+  if (lane == 0) m_out[qi] = m;
+  const float* qrow = q + static_cast<size_t>(qi) * dpad;
+  const int e2n = pow2_ceil(m < 2 ? 2 : m);
+  for (int j = lane; j < e2n; j += 32) {
+    uint64_t key = kEmpty;
+    if (j < m) {
+      const uint32_t pos = key_tie(buf[j]);
+      const float acc = exact_l2_seq(codes + static_cast<size_t>(pos) * dpad, qrow, dpad);
+      if (acc < FLT_MAX) key = make_key(acc, pos);
+    }
+    ex[j] = key;
+  }
+  __syncwarp();
+  warp_bitonic_sort(ex, e2n, lane);
+  for (int j = lane; j < k; j += 32) {
+    const uint64_t key = j < m ? ex[j] : kEmpty;
+    const size_t o = static_cast<size_t>(qi) * k + j;
+    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+  }
+}
+
 // The bound of the second stage of a batch with k > kTightK: the first stage
-// scanned only each query's nearest list, so the k-th smallest w admitted
-// there (a radix select over the keys' upper 32 bits, 8 bits per pass) is at
-// least the k-th smallest w over all probed rows, and that value + 2 eps
-// bounds W_k + 2 eps from above.  One warp per query; a query with fewer
-// than k admitted rows, or an overflowed buffer, keeps its bound.
+// scanned only each query's nearest list, so the k-th smallest upper bound
+// admitted there (a radix selection, 8 bits per pass) is a U for the whole
+// probe set.  One warp per query; a query with fewer than k admitted rows, or
+// an overflowed buffer, keeps its bound.
 constexpr int kKthWarps = 8;
 
-__global__ void __launch_bounds__(kKthWarps * 32) kth_bound_kernel(const uint64_t* __restrict__ cand,
+__global__ void __launch_bounds__(kKthWarps * 32) kth_bound_kernel(const uint32_t* __restrict__ cand_ub,
                                                                   const int* __restrict__ cnt, int cap, int nq, int k,
-                                                                  const float* __restrict__ e2,
                                                                   uint32_t* __restrict__ thr) {
   __shared__ int s_h[kKthWarps][256];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -797,14 +786,9 @@ __global__ void __launch_bounds__(kKthWarps * 32) kth_bound_kernel(const uint64_
   if (qi >= nq) return;
   const int c = cnt[qi];
   if (c < k || c > cap) return;
-  int* h = s_h[wib];
-  const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
-  const uint32_t prefix =
-      warp_kth_smallest([&](int i) { return static_cast<uint32_t>(src[i] >> 32); }, c, k, h, lane);
-  if (lane == 0) {
-    const uint32_t b = ordered_bits(fminf(__fadd_ru(ordered_to_float(prefix), e2[qi]), FLT_MAX));
-    if (b < thr[qi]) thr[qi] = b;
-  }
+  const uint32_t* src = cand_ub + static_cast<size_t>(qi) * cap;
+  const uint32_t u = warp_kth_smallest([&](int i) { return src[i]; }, c, k, s_h[wib], lane);
+  if (lane == 0 && u < thr[qi]) thr[qi] = u;
 }
 
 // Probe table split for the two stages: first[q] = the query's nearest list,
@@ -823,10 +807,11 @@ __global__ void split_first_probe_kernel(const int32_t* __restrict__ probes, int
 // candidates, at most cap; *big_n of them) in three flat kernels, so the
 // exact distances -- the bulk of the work -- run with every SM's threads
 // loading rows rather than behind per-query sorts:
-//   rerank_big_bound_kernel  a warp per query: W_k by radix selection over
-//                            the candidates' values, then the candidates at
-//                            or under W_k + 2 eps compacted in place at the
-//                            front of the query's buffer (m of them);
+//   rerank_big_bound_kernel  a warp per query: U, the k-th smallest upper
+//                            bound, by radix selection, then the candidates
+//                            whose lower bound is at most U compacted in
+//                            place at the front of the query's buffer (m of
+//                            them);
 //   rerank_big_exact_kernel  a CTA per query: the exact distance of each of
 //                            the m rows (two rows per thread in flight),
 //                            written back in place as (distance, position)
@@ -836,7 +821,7 @@ constexpr int kBigWarps = 8;
 constexpr int kRerankMaxDim = 128;  // dpad of the BF16 scan's rows (d <= 128)
 
 __global__ void __launch_bounds__(kBigWarps * 32) rerank_big_bound_kernel(
-    uint64_t* __restrict__ cand, const int* __restrict__ cnt, int cap, const float* __restrict__ e2, int k,
+    uint64_t* __restrict__ cand, const uint32_t* __restrict__ cand_ub, const int* __restrict__ cnt, int cap, int k,
     const int* __restrict__ big_list, const int* __restrict__ big_n, int* __restrict__ m_out) {
   __shared__ int s_h[kBigWarps][256];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -845,8 +830,8 @@ __global__ void __launch_bounds__(kBigWarps * 32) rerank_big_bound_kernel(
   const int qi = big_list[w];
   const int c = cnt[qi];
   uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
-  const uint32_t wk = warp_kth_smallest([&](int i) { return static_cast<uint32_t>(buf[i] >> 32); }, c, k, s_h[wib], lane);
-  const uint32_t lim_bits = ordered_bits(__fadd_ru(ordered_to_float(wk), e2[qi]));
+  const uint32_t* ubs = cand_ub + static_cast<size_t>(qi) * cap;
+  const uint32_t lim_bits = warp_kth_smallest([&](int i) { return ubs[i]; }, c, k, s_h[wib], lane);
   // In-place compaction: a block of 32 is read before any of it is written,
   // and writes land at or below the read position.
   int m = 0;
@@ -935,11 +920,11 @@ __global__ void __launch_bounds__(256) rerank_big_topk_kernel(const uint64_t* __
   }
 }
 
-// Seed bound per query before the scan: the k-th smallest w over the first
-// S rows of the query's nearest list, computed from the same BF16 operands as
-// the scan (these values obey the same eps), + 2 eps: an upper bound of
-// W_k + 2 eps.  Queries whose nearest list holds fewer than k rows keep
-// FLT_MAX.
+// Seed bound per query before the scan: U = the k-th smallest w over the
+// first S rows of the query's nearest list, computed from the same BF16
+// operands as the scan (these values obey the same eps), + eps(q, l): k rows
+// of the probe set have upper bounds at most that.  Queries whose nearest
+// list holds fewer than k rows keep FLT_MAX.
 //
 // List-major: one CTA per list stages the list's first S BF16 rows in shared
 // memory once; for each query whose nearest list it is (probe rank 0 in the
@@ -955,7 +940,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
     const float* __restrict__ q, int dpad, const float* __restrict__ cent, int kpad,
     const __nv_bfloat16* __restrict__ codes,
     const int64_t* __restrict__ list_off, const int64_t* __restrict__ list_qoff, const int32_t* __restrict__ list_q,
-    const float* __restrict__ xnorm, int S, int k, const float* __restrict__ e2, uint32_t* __restrict__ thr,
+    const float* __restrict__ xnorm, const float* __restrict__ rmax, int S, int k, uint32_t* __restrict__ thr,
     const int32_t* __restrict__ probes, int P) {
   extern __shared__ __align__(16) uint8_t s_seed_raw[];
   __shared__ float s_xn[kSeedRows];
@@ -1086,7 +1071,10 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
         pmask |= 255u << shift;
         need -= s_before;
       }
-      if (tid == 0) thr[qi] = ordered_bits(fminf(__fadd_ru(ordered_to_float(prefix), e2[qi]), FLT_MAX));
+      // U = the k-th smallest w + eps(q, l): every one of those k rows has an
+      // upper bound at most that.
+      if (tid == 0)
+        thr[qi] = ordered_bits(fminf(__fadd_ru(ordered_to_float(prefix), pair_eps(cdq, rmax[l], dpad)), FLT_MAX));
     }
     __syncthreads();
   }
@@ -1205,10 +1193,9 @@ void launch_scan_bf16(const void* tmap, const TcArgs& a, int num_sms, cudaStream
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_query_prep(const float* q, int nq, int d, int dpad, const int32_t* probes, int P, const float* cent,
-                       const float* rmax, float* e2, uint32_t* thr, int* cnt, cudaStream_t st) {
+void launch_query_prep(int nq, uint32_t* thr, int* cnt, cudaStream_t st) {
   if (nq <= 0) return;
-  query_prep_kernel<<<(nq + 7) / 8, 256, 0, st>>>(q, nq, d, dpad, probes, P, cent, rmax, e2, thr, cnt);
+  query_prep_kernel<<<(nq + 255) / 256, 256, 0, st>>>(nq, thr, cnt);
   HB_CUDA(cudaGetLastError());
 }
 
@@ -1220,9 +1207,9 @@ void launch_residual_bf16(const float* codes, const int64_t* list_off, const flo
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_seed_bound(const float* q, int dpad, const float* cent, int nq, int kpad, const void* codes_bf16,
+void launch_seed_bound(const float* q, int d, int dpad, const float* cent, int nq, int kpad, const void* codes_bf16,
                        const int64_t* list_off, int nlist, const int64_t* list_qoff, const int32_t* list_q,
-                       const float* rnorm, int S, int k, const float* e2, uint32_t* thr, cudaStream_t st,
+                       const float* rnorm, const float* rmax, int S, int k, uint32_t* thr, cudaStream_t st,
                        const int32_t* probes, int P) {
   if (nq <= 0) return;
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
@@ -1232,19 +1219,19 @@ void launch_seed_bound(const float* q, int dpad, const float* cent, int nq, int 
   HB_CUDA(cudaFuncSetAttribute(seed_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const bool by_query = probes && static_cast<long long>(nq) * 4 < nlist;
   seed_bound_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(
-      q, dpad, cent, kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff, list_q, rnorm, S, k, e2,
+      q, dpad, cent, kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff, list_q, rnorm, rmax, S, k,
       thr, by_query ? probes : nullptr, P);
   HB_CUDA(cudaGetLastError());
 }
 
-void launch_rerank_bf16(uint64_t* cand, const int* cnt, int cap, const float* e2, int nq, int k,
+void launch_rerank_bf16(uint64_t* cand, const uint32_t* cand_ub, const int* cnt, int cap, int nq, int k,
                         const float* codes, const float* q, int dpad, const int64_t* ids, float* D, int64_t* I,
                         int* flag, int* over_list, int* over_n, int* m_out, int num_sms, cudaStream_t st) {
   if (nq <= 0) return;
   HB_CHECK(k >= 1 && cap >= k && cap <= kRerankMaxCap && (cap & (cap - 1)) == 0, HB_ERR_INVALID,
            "candidate buffer size out of range");
   HB_CHECK(dpad % 4 == 0 && dpad <= kRerankMaxDim, HB_ERR_INVALID, "re-rank rows wider than 128 floats");
-  rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(cand, cnt, cap, e2, nq, k, codes, q,
+  rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(cand, cand_ub, cnt, cap, nq, k, codes, q,
                                                                                dpad, ids, D, I, flag, over_list, over_n,
                                                                                m_out, over_list + nq);
   HB_CUDA(cudaGetLastError());
@@ -1253,7 +1240,7 @@ void launch_rerank_bf16(uint64_t* cand, const int* cnt, int cap, const float* e2
     const int* big_list = over_list + nq;
     const int* big_n = over_n + 1;
     rerank_big_bound_kernel<<<(nq + kBigWarps - 1) / kBigWarps, kBigWarps * 32, 0, st>>>(
-        cand, cnt, cap, e2, k, big_list, big_n, m_out);
+        cand, cand_ub, cnt, cap, k, big_list, big_n, m_out);
     rerank_big_exact_kernel<<<nq, 256, 0, st>>>(cand, cap, codes, q, dpad, big_list, big_n,
                                                 m_out);
     const size_t smem = static_cast<size_t>(pow2_ceil(k < 2 ? 2 : k)) * sizeof(uint64_t);
@@ -1262,10 +1249,10 @@ void launch_rerank_bf16(uint64_t* cand, const int* cnt, int cap, const float* e2
   }
 }
 
-void launch_kth_bound(const uint64_t* cand, const int* cnt, int cap, int nq, int k, const float* e2, uint32_t* thr,
+void launch_kth_bound(const uint32_t* cand_ub, const int* cnt, int cap, int nq, int k, uint32_t* thr,
                       cudaStream_t st) {
   if (nq <= 0) return;
-  kth_bound_kernel<<<(nq + kKthWarps - 1) / kKthWarps, kKthWarps * 32, 0, st>>>(cand, cnt, cap, nq, k, e2, thr);
+  kth_bound_kernel<<<(nq + kKthWarps - 1) / kKthWarps, kKthWarps * 32, 0, st>>>(cand_ub, cnt, cap, nq, k, thr);
   HB_CUDA(cudaGetLastError());
 }
 

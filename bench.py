@@ -44,6 +44,11 @@ WORKLOAD = {
     "workload": "ivf-flat 10M x 128 (config5: 4096-component mixture), nlist 4096, k 10, 10k queries",
     "nb": 10_000_000, "d": 128, "nlist": 4096, "k": 10, "nq": 10_000,
 }
+# DRAM bytes (read + write) of one scan_bf16 launch over its algorithmic bytes, from the
+# ncu capture of a 3M x 128 / nlist 1229 / nprobe 40 launch: 896.0 MB for 764.6 MB
+# (profiles/scan_bf16_3m_ncu_full.md).  The traffic grows with the lists read, so the
+# bench scales it by each launch's algorithmic bytes.
+SCAN_TRAFFIC_RATIO = 1.172
 NPROBE_SWEEP = [1, 2, 3, 4, 5, 6, 8, 10, 12, 14, 16, 20, 24, 28, 32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256]
 
 
@@ -391,9 +396,13 @@ def run_ours(args):
         else:
             roof.update({"bound": "tensor", "achieved": round(flops / t / 1e12, 2), "peak": bf16_peak,
                          "unit": "TFLOP/s", "frac": round(flops / t / 1e12 / bf16_peak, 3)})
-        roof.update({"traffic": None, "bytes_compulsory_per_launch": comp_bytes, "flops_per_launch": flops,
+        roof.update({"traffic": int(SCAN_TRAFFIC_RATIO * comp_bytes), "bytes_compulsory_per_launch": comp_bytes,
+                     "flops_per_launch": flops,
                      "note": "bytes = each probed list read once in BF16 (+ queries); flops = 2*d per "
-                             "(query, probed vector); frac = max(bytes/BW, flops/TC) / t"})
+                             "(query, probed vector); frac = max(bytes/BW, flops/TC) / t; traffic = DRAM "
+                             f"read + write per launch, {SCAN_TRAFFIC_RATIO} x the algorithmic bytes as measured "
+                             "by ncu on a 3M x 128 launch (profiles/scan_bf16_3m_ncu_full.md), scaled to this "
+                             "launch by its algorithmic bytes"})
     else:
         t = kms[top] / 1e3
         nq_f = float(nq)

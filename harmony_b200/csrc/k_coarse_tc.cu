@@ -506,7 +506,10 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
   if (nq <= 0) return;
   HB_CHECK(P >= 1 && P <= Pm && Pm <= kCoarseMaxPm, HB_ERR_INVALID, "coarse candidate count out of range");
   const int n2 = pow2_ceil(Pm < 2 ? 2 : Pm);
-  if (nq < 512) {
+  // A CTA per query for small batches, and for the widening pass of the
+  // learned nprobe, whose few wide rows (up to Pm candidates) would
+  // otherwise keep one warp each busy long after the narrow rows are done.
+  if (nq < 512 || rows.width) {
     const size_t smem = static_cast<size_t>(n2) * 8;
     HB_CUDA(cudaFuncSetAttribute(coarse_refine_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));

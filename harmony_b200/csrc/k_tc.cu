@@ -927,14 +927,14 @@ __global__ void __launch_bounds__(256) rerank_big_topk_kernel(const uint64_t* __
 // list holds fewer than k rows keep FLT_MAX.
 //
 // List-major: one CTA per list stages the list's first S BF16 rows in shared
-// memory once; for each query whose nearest list it is (probe rank 0 in the
-// list-major work description) in turn, thread t forms row t's value with the
-// query broadcast from shared memory, and a radix selection over four 8-bit
-// digits (a 256-bin histogram, three barriers per digit) finds the k-th
-// smallest.  Small batches (probes given): one CTA per query.
+// memory once; the queries whose nearest list it is (probe rank 0 in the
+// list-major work description) go eight at a time: thread t forms row t's
+// values for all eight with their rows broadcast from shared memory, then a
+// warp per query selects its k-th smallest by radix (four 8-bit passes).
+// Small batches (probes given): one CTA per query.
 constexpr int kSeedRows = 256;
 constexpr int kSeedWarps = 8;
-static_assert(kSeedWarps * 32 == 256, "the seed's radix histogram has a bin per thread");
+static_assert(kSeedWarps * 32 >= kSeedRows, "the seed forms a row per thread");
 
 __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
     const float* __restrict__ q, int dpad, const float* __restrict__ cent, int kpad,
@@ -946,9 +946,9 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
   __shared__ float s_xn[kSeedRows];
   __shared__ int s_qs[kSeedWarps * 32];
   __shared__ int s_nq;
-  __shared__ float s_cd;
-  __shared__ int s_hist[kSeedWarps * 32];  // one bin per thread
-  __shared__ int s_bin, s_before;
+  __shared__ float s_cd[kSeedWarps];
+  __shared__ uint32_t s_keys[kSeedWarps][kSeedRows];
+  __shared__ int s_hist[kSeedWarps][256];
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const bool by_query = probes != nullptr;
   int l;
@@ -990,93 +990,61 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
     }
     __syncthreads();
     const int nqr = s_nq;
-    for (int t = 0; t < nqr; ++t) {
-      const int qi = s_qs[t];
-      // The query's residual to this list's centroid in BF16 (the scan's A
-      // row) and ||q - c_l||^2 in FP32.
-      const float* qrow = q + static_cast<size_t>(qi) * dpad;
-      const float* crow = cent + static_cast<size_t>(l) * dpad;
-      for (int c = tid; c < kpad; c += blockDim.x)
-        qbuf[c] = c < dpad ? __bfloat162float(__float2bfloat16_rn(qrow[c] - crow[c])) : 0.0f;
-      if (wib == 0) {
+    // Up to kSeedWarps queries at a time: warp j forms query j's BF16
+    // residual row and ||q - c_l||^2, thread t the S values of row t for all
+    // of them, then warp j selects query j's k-th.
+    for (int t0 = 0; t0 < nqr; t0 += kSeedWarps) {
+      const int nb = min(kSeedWarps, nqr - t0);
+      if (wib < nb) {
+        const int qi = s_qs[t0 + wib];
+        const float* qrow = q + static_cast<size_t>(qi) * dpad;
+        const float* crow = cent + static_cast<size_t>(l) * dpad;
+        float* qb = qbuf + wib * kpad;
         float cd = 0.0f;
-        for (int c = lane; c < dpad; c += 32) {
-          const float v = qrow[c] - crow[c];
+        for (int c = lane; c < kpad; c += 32) {
+          const float v = c < dpad ? qrow[c] - crow[c] : 0.0f;
           cd = fmaf(v, v, cd);
+          qb[c] = __bfloat162float(__float2bfloat16_rn(v));
         }
         for (int o = 16; o > 0; o >>= 1) cd += __shfl_xor_sync(0xffffffffu, cd, o);
-        if (lane == 0) s_cd = cd;
+        if (lane == 0) s_cd[wib] = cd;
       }
       __syncthreads();
-      const float cdq = s_cd;
-      uint32_t key = 0xFFFFFFFFu;
       if (tid < n) {
         const uint8_t* xr = rows + static_cast<size_t>(tid) * stride;
-        // Four partial sums (any order is within eps).
-        float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
+        for (int j = 0; j < nb; ++j) {
+          const float* qb = qbuf + j * kpad;
+          // Four partial sums (any order is within eps).
+          float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
 #pragma unroll 4
-        for (int c = 0; c < kpad; c += 8) {
-          const uint4 xv = *reinterpret_cast<const uint4*>(xr + c * 2);
-          const float4 qa = *reinterpret_cast<const float4*>(qbuf + c);
-          const float4 qb = *reinterpret_cast<const float4*>(qbuf + c + 4);
-          d0 = fmaf(qa.x, __uint_as_float(xv.x << 16), d0);
-          d1 = fmaf(qa.y, __uint_as_float(xv.x & 0xffff0000u), d1);
-          d2 = fmaf(qa.z, __uint_as_float(xv.y << 16), d2);
-          d3 = fmaf(qa.w, __uint_as_float(xv.y & 0xffff0000u), d3);
-          d0 = fmaf(qb.x, __uint_as_float(xv.z << 16), d0);
-          d1 = fmaf(qb.y, __uint_as_float(xv.z & 0xffff0000u), d1);
-          d2 = fmaf(qb.z, __uint_as_float(xv.w << 16), d2);
-          d3 = fmaf(qb.w, __uint_as_float(xv.w & 0xffff0000u), d3);
+          for (int c = 0; c < kpad; c += 8) {
+            const uint4 xv = *reinterpret_cast<const uint4*>(xr + c * 2);
+            const float4 qa = *reinterpret_cast<const float4*>(qb + c);
+            const float4 qc = *reinterpret_cast<const float4*>(qb + c + 4);
+            d0 = fmaf(qa.x, __uint_as_float(xv.x << 16), d0);
+            d1 = fmaf(qa.y, __uint_as_float(xv.x & 0xffff0000u), d1);
+            d2 = fmaf(qa.z, __uint_as_float(xv.y << 16), d2);
+            d3 = fmaf(qa.w, __uint_as_float(xv.y & 0xffff0000u), d3);
+            d0 = fmaf(qc.x, __uint_as_float(xv.z << 16), d0);
+            d1 = fmaf(qc.y, __uint_as_float(xv.z & 0xffff0000u), d1);
+            d2 = fmaf(qc.z, __uint_as_float(xv.w << 16), d2);
+            d3 = fmaf(qc.w, __uint_as_float(xv.w & 0xffff0000u), d3);
+          }
+          s_keys[j][tid] = ordered_bits(s_cd[j] + fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[tid]));
         }
-        key = ordered_bits(cdq + fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[tid]));
       }
-      // The k-th smallest of the n keys: radix selection over four 8-bit
-      // digits, one 256-bin histogram per digit (a bin per thread).
-      uint32_t prefix = 0u, pmask = 0u;
-      int need = k;
-      for (int shift = 24; shift >= 0; shift -= 8) {
-        s_hist[tid] = 0;
-        __syncthreads();
-        if (tid < n && (key & pmask) == prefix) atomicAdd(&s_hist[(key >> shift) & 255u], 1);
-        __syncthreads();
-        if (wib == 0) {
-          int loc[8], sum = 0;
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            loc[j] = s_hist[8 * lane + j];
-            sum += loc[j];
-          }
-          int incl = sum;
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int x = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += x;
-          }
-          const int excl = incl - sum;
-          if (excl < need && need <= incl) {
-            int before = excl, bin = 8 * lane;
-            for (int j = 0; j < 8; ++j) {
-              if (before + loc[j] >= need) {
-                bin = 8 * lane + j;
-                break;
-              }
-              before += loc[j];
-            }
-            s_bin = bin;
-            s_before = before;
-          }
-        }
-        __syncthreads();
-        prefix |= static_cast<uint32_t>(s_bin) << shift;
-        pmask |= 255u << shift;
-        need -= s_before;
+      __syncthreads();
+      if (wib < nb) {
+        const int qi = s_qs[t0 + wib];
+        const uint32_t kth = warp_kth_smallest([&](int i) { return s_keys[wib][i]; }, n, k, s_hist[wib], lane);
+        // U = the k-th smallest w + eps(q, l): every one of those k rows has
+        // an upper bound at most that.
+        if (lane == 0)
+          thr[qi] = ordered_bits(
+              fminf(__fadd_ru(ordered_to_float(kth), pair_eps(s_cd[wib], rmax[l], dpad)), FLT_MAX));
       }
-      // U = the k-th smallest w + eps(q, l): every one of those k rows has an
-      // upper bound at most that.
-      if (tid == 0)
-        thr[qi] = ordered_bits(fminf(__fadd_ru(ordered_to_float(prefix), pair_eps(cdq, rmax[l], dpad)), FLT_MAX));
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
@@ -1215,7 +1183,7 @@ void launch_seed_bound(const float* q, int d, int dpad, const float* cent, int n
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
   HB_CHECK(S >= 1 && S <= kSeedRows && k >= 1, HB_ERR_INVALID, "seed sample out of range");
   if (k > S) return;  // no sample holds k rows: every bound stays FLT_MAX
-  const size_t smem = static_cast<size_t>(S) * (kpad * 2 + 16) + static_cast<size_t>(kpad) * 4;
+  const size_t smem = static_cast<size_t>(S) * (kpad * 2 + 16) + static_cast<size_t>(kSeedWarps) * kpad * 4;
   HB_CUDA(cudaFuncSetAttribute(seed_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const bool by_query = probes && static_cast<long long>(nq) * 4 < nlist;
   seed_bound_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(

@@ -717,6 +717,8 @@ def run_c4(args):
         res["recall_at_10_first_2000"] = round(recall(I_check, gt, k), 4)
         if prec == Precision.BF16:
             res["bounded_scan_first_2000"] = ix.bf16_stats()
+        res["max_rel_dist_err_vs_fp64_first_2000"] = max_rel_err_vs_fp64(
+            torch, base, queries[:ng], D_host[:ng].numpy(), I_check)
         out[name] = res
         ix.search_params.nprobe_per_query = None
         ix.search_params.max_nprobe = 0
@@ -908,6 +910,12 @@ def run_c2(args):
                 row[name] = arm
             ok, n = parity_count(*outs["bf16"], *outs["fp32"])
             row["bf16_identical_to_fp32"] = {"identical": ok, "queries": n}
+            # Largest relative error of the returned distances against FP64
+            # recomputation, first 1000 queries.
+            for name in ("fp32", "bf16"):
+                Dn, In = outs[name]
+                row[name]["max_rel_dist_err_vs_fp64_first_1000"] = max_rel_err_vs_fp64(
+                    torch, base, queries[:ng], Dn[:ng], In[:ng])
             sweep.append(row)
         ix.search_params.precision = Precision.FP32
     ck = clk.summary()

@@ -1343,7 +1343,7 @@ class IndexCore {
   // sorts a buffer in place); a query needing more is searched again with the
   // exact scan.
   static int filter_cap(size_t k) {
-    size_t c = 2048;
+    size_t c = 4096;
     while (c < 16 * k) c <<= 1;
     return static_cast<int>(std::min<size_t>(kRerankMaxCap, c));
   }

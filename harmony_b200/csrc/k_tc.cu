@@ -55,14 +55,16 @@
 // bound.  The builders form the A tile, BF16(q - c_l) for the item's list,
 // from the FP32 queries.
 //
-// Warp roles (384 threads), all running ahead of each other through
-// mbarriers, with no CTA-wide barrier between items:
-//   warps 0-7   two epilogue groups (TMEM lane quarters); tile t of the
-//               CTA's global tile sequence goes to group t % 2;
-//   warp 8      TMA producer of the B tiles;
-//   warp 9      MMA issuer; it also copies each tile's 128 row norms
+// Warp roles (512 threads, 128 registers each), all running ahead of each
+// other through mbarriers, with no CTA-wide barrier between items:
+//   warps 0-11  three epilogue groups (each four warps = the four TMEM lane
+//               quarters); tile t of the CTA's global tile sequence goes to
+//               group t % 3 and accumulator t % 4 (three groups keep more
+//               warps on the epilogue, which bounds the kernel);
+//   warp 12     TMA producer of the B tiles;
+//   warp 13     MMA issuer; it also copies each tile's 128 row norms
 //               (a padded per-tile norm array) next to the accumulator;
-//   warps 10-11 item builders: fetch the next item from the global work
+//   warps 14-15 item builders: fetch the next item from the global work
 //               counter, gather its BF16 query rows and bounds and write its
 //               A tile into the second A buffer while the current item runs.
 // Every mbarrier wait is bounded (TcArgs::wait_budget cycles); on a timeout
@@ -86,14 +88,14 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kGroups = 2;                         // epilogue warpgroups, alternate tiles
+constexpr int kGroups = 3;                         // epilogue warpgroups, tile t -> group t % 3
 constexpr int kEpiThreads = 128;                   // threads per epilogue group (= queries per item)
 constexpr int kBuildWarps = 2;
 constexpr int kProdWarp = kGroups * 4, kMmaWarp = kGroups * 4 + 1, kBuildWarp0 = kGroups * 4 + 2;
 constexpr int kTcThreads = (kBuildWarp0 + kBuildWarps) * 32;
 constexpr int kTile = 128;     // rows per B tile, queries per item (M)
 constexpr int kMaxStages = 4;
-constexpr int kAcc = 2 * kGroups;                  // TMEM accumulators of 128 columns
+constexpr int kAcc = 4;                            // TMEM accumulators of 128 columns, tile t -> t % 4
 constexpr size_t kSmemCap = 225 * 1024;            // dynamic shared memory budget
 constexpr int kTightK = kFilterTightK;             // largest k whose bound tightens during the scan
 constexpr int kStage = 8;                          // admitted keys staged per epilogue thread before a flush
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const bool col_in = c0 < a.dpad, col_k = c0 < kpad;
         const float4 cv = col_k ? *reinterpret_cast<const float4*>(cen + c0) : make_float4(0.f, 0.f, 0.f, 0.f);
         const float Rl = a.rmax[d.list];
-        constexpr int kRowsInFlight = 16;
+        constexpr int kRowsInFlight = 8;
         // Rows without a query are left as they are: their TMEM lanes belong
         // to no query and the epilogue ignores them.  A block's rows with a
         // query come first (query (r % 32) * 4 + r / 32 grows with r % 32).
@@ -342,7 +344,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       const uint32_t idesc = idesc_bf16_f32(kTile, kTile);
       const int nk = kpad / 16;
-      uint32_t m_idx = 0, m_cnt[kGroups] = {}, G = 0;
+      uint32_t m_idx = 0;
       uint32_t n_norm[kAcc] = {};  // norm copies issued per accumulator
       for (uint32_t it = 0;; ++it) {
         const int ab = static_cast<int>(it & 1u);
@@ -358,14 +360,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             ok = false;
             break;
           }
-          const int g = static_cast<int>((G + static_cast<uint32_t>(t)) & 1u);
-          const uint32_t c = m_cnt[g];
-          const int b = 2 * g + static_cast<int>(c & 1u);
-          if (!mbar_wait(&sh.acce[b], ((c >> 1) & 1u) ^ 1u, err, 13, budget)) {
+          const int b = static_cast<int>(m_idx % kAcc);
+          if (!mbar_wait(&sh.acce[b], ((m_idx / kAcc) & 1u) ^ 1u, err, 13, budget)) {
             ok = false;
             break;
           }
-          ++m_cnt[g];
           tc_fence_after();
           mbar_arrive_expect_tx(&sh.normf[b], kTile * 4);
           bulk_load(nrm + b * kTile, a.tile_norm + (d.tile0 + t) * kTile, kTile * 4, &sh.normf[b]);
@@ -382,7 +381,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // A buffer ab is free once these MMAs have completed.
         mma_commit(&sh.aempty[ab]);
         if (!ok) break;
-        G += static_cast<uint32_t>(d.ntiles);
       }
       // Drain: every MMA done before TMEM is released, and the last norm copy
       // of each accumulator landed (at most one per accumulator is pending:
@@ -397,7 +395,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int grp = warp >> 2;
     const int etid = tid - grp * kEpiThreads;
     const uint32_t lane_base = (32u * static_cast<uint32_t>(warp & 3)) << 16;
-    uint32_t e_cnt = 0, G = 0;
+    uint32_t G = 0;
     for (uint32_t it = 0;; ++it) {
       const int ab = static_cast<int>(it & 1u);
       bool ok = mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 34, budget);
@@ -542,9 +540,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // The query's bound as other threads have lowered it, read one tile
       // ahead (the load is in flight while a tile is processed).
       uint32_t g_thr = my_q >= 0 ? *reinterpret_cast<volatile uint32_t*>(a.thr + my_q) : 0u;
-      for (int t = static_cast<int>((static_cast<uint32_t>(grp) ^ G) & 1u); t < d.ntiles; t += kGroups, ++e_cnt) {
-        const int b = 2 * grp + static_cast<int>(e_cnt & 1u);
-        const uint32_t par = (e_cnt >> 1) & 1u;
+      for (int t = static_cast<int>((static_cast<uint32_t>(grp) + 3u * 4096u - G % 3u) % 3u); t < d.ntiles;
+           t += kGroups) {
+        const uint32_t gt = G + static_cast<uint32_t>(t);  // the CTA's global tile index
+        const int b = static_cast<int>(gt % kAcc);
+        const uint32_t par = (gt / kAcc) & 1u;
         ok = ok && mbar_wait(&sh.accf[b], par, err, 14, budget) && mbar_wait(&sh.normf[b], par, err, 15, budget);
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
@@ -562,21 +562,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const float* nb = nrm + b * kTile;
           const uint32_t col = tmem + lane_base + static_cast<uint32_t>(b * kTile);
           const uint32_t pos_t = static_cast<uint32_t>(d.row0 + t * kTile);
-          // Two register sets: the next chunk's TMEM load is in flight while
-          // this one is processed, then moves into place (one copy of the
-          // chunk code, so the instruction cache holds the loop).
-          uint32_t ra[32], rb[32];
-          tmem_ld32(col, ra);
-          tmem_ld_wait(ra);
+          // One register set (a second one, to load the next chunk while this
+          // one is processed, measured slower: it held the kernel to two
+          // epilogue warpgroups within the register file).
+          uint32_t ra[32];
 #pragma unroll 1
           for (int c = 0; c < kTile / 32; ++c) {
-            if (c + 1 < kTile / 32) tmem_ld32(col + static_cast<uint32_t>(32 * (c + 1)), rb);
+            tmem_ld32(col + static_cast<uint32_t>(32 * c), ra);
+            tmem_ld_wait(ra);
             chunk(ra, nb + 32 * c, pos_t + static_cast<uint32_t>(32 * c));
-            if (c + 1 < kTile / 32) {
-              tmem_ld_wait(rb);
-#pragma unroll
-              for (int j = 0; j < 32; ++j) ra[j] = rb[j];
-            }
           }
         }
         tc_fence_before();

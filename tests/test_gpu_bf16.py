@@ -141,12 +141,12 @@ def test_bf16_duplicates_and_ties(restated):
 
 
 def test_bf16_overflow_is_searched_exactly(restated):
-    """3000 identical rows next to the query: every one of them is within the
+    """6000 identical rows next to the query: every one of them is within the
     bound, so the candidate buffer overflows and the query is searched again
     with the exact scan -- the result is still the exact one."""
     rng = np.random.default_rng(31)
     d = 96
-    same = np.repeat(rng.standard_normal((1, d)).astype(np.float32), 3000, axis=0)
+    same = np.repeat(rng.standard_normal((1, d)).astype(np.float32), 6000, axis=0)
     other = (rng.standard_normal((3000, d)) * 3 + 10).astype(np.float32)
     base = np.concatenate([same, other])
     ix = Index(d, 8, 8)
@@ -157,7 +157,7 @@ def test_bf16_overflow_is_searched_exactly(restated):
         got = search(ix, q, k)
         assert ix.bf16_fallbacks() == 3, ix.bf16_fallbacks()
         assert_identical(got, search(ix, q, k, precision=Precision.FP32), f"overflow k={k}")
-        assert (got[1][:3] < 3000).all()
+        assert (got[1][:3] < 6000).all()
 
 
 def test_bf16_wait_budget_gives_up_and_recovers(fidx):

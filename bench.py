@@ -45,10 +45,10 @@ WORKLOAD = {
     "nb": 10_000_000, "d": 128, "nlist": 4096, "k": 10, "nq": 10_000,
 }
 # DRAM bytes (read + write) of one scan_bf16 launch over its algorithmic bytes, from the
-# ncu capture of a 3M x 128 / nlist 1229 / nprobe 40 launch: 896.0 MB for 764.6 MB
+# ncu capture of a 3M x 128 / nlist 1229 / nprobe 40 launch: 866.8 MB for 764.6 MB
 # (profiles/scan_bf16_3m_ncu_full.md).  The traffic grows with the lists read, so the
 # bench scales it by each launch's algorithmic bytes.
-SCAN_TRAFFIC_RATIO = 1.172
+SCAN_TRAFFIC_RATIO = 1.134
 NPROBE_SWEEP = [1, 2, 3, 4, 5, 6, 8, 10, 12, 14, 16, 20, 24, 28, 32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256]
 
 

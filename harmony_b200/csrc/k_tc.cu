@@ -540,8 +540,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // The query's bound as other threads have lowered it, read one tile
       // ahead (the load is in flight while a tile is processed).
       uint32_t g_thr = my_q >= 0 ? *reinterpret_cast<volatile uint32_t*>(a.thr + my_q) : 0u;
-      for (int t = static_cast<int>((static_cast<uint32_t>(grp) + 3u * 4096u - G % 3u) % 3u); t < d.ntiles;
-           t += kGroups) {
+      constexpr uint32_t kG = kGroups;
+      for (int t = static_cast<int>((static_cast<uint32_t>(grp) + kG - G % kG) % kG); t < d.ntiles; t += kGroups) {
         const uint32_t gt = G + static_cast<uint32_t>(t);  // the CTA's global tile index
         const int b = static_cast<int>(gt % kAcc);
         const uint32_t par = (gt / kAcc) & 1u;

@@ -345,14 +345,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint32_t idesc = idesc_bf16_f32(kTile, kTile);
       const int nk = kpad / 16;
       uint32_t m_idx = 0;
-      uint32_t n_norm[kAcc] = {};  // norm copies issued per accumulator
       for (uint32_t it = 0;; ++it) {
         const int ab = static_cast<int>(it & 1u);
         if (!mbar_wait(&sh.itemf[ab], (it >> 1) & 1u, err, 33, budget)) break;
         const ItemDesc d = sh.desc[ab];
         if (d.ntiles < 0) break;
         tc_fence_after();
-        const uint32_t a_base = smem_u32(Abuf + ab * tile_bytes);
+        const uint64_t a_desc = desc_sw128(smem_u32(Abuf + ab * tile_bytes));
         bool ok = true;
         for (int t = 0; t < d.ntiles; ++t, ++m_idx) {
           const int s = static_cast<int>(m_idx % static_cast<uint32_t>(S));
@@ -368,12 +367,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tc_fence_after();
           mbar_arrive_expect_tx(&sh.normf[b], kTile * 4);
           bulk_load(nrm + b * kTile, a.tile_norm + (d.tile0 + t) * kTile, kTile * 4, &sh.normf[b]);
-          ++n_norm[b];
-          const uint32_t b_base = smem_u32(stages + s * tile_bytes);
+          const uint64_t b_desc = desc_sw128(smem_u32(stages + s * tile_bytes));
+          const uint32_t d_tmem = tmem + static_cast<uint32_t>(b * kTile);
           for (int k = 0; k < nk; ++k) {
-            const uint32_t off = static_cast<uint32_t>(k >> 2) * kblk_bytes + static_cast<uint32_t>(k & 3) * 32u;
-            mma_bf16(tmem + static_cast<uint32_t>(b * kTile), desc_sw128(a_base + off), desc_sw128(b_base + off),
-                     idesc, k > 0 ? 1u : 0u);
+            // The start-address field is (address >> 4) in the low 14 bits.
+            const uint64_t off16 = (static_cast<uint32_t>(k >> 2) * kblk_bytes + static_cast<uint32_t>(k & 3) * 32u) >> 4;
+            mma_bf16(d_tmem, a_desc + off16, b_desc + off16, idesc, k > 0 ? 1u : 0u);
           }
           mma_commit(&sh.empty[s]);
           mma_commit(&sh.accf[b]);
@@ -387,8 +386,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // the next one waits for the epilogue to release the accumulator).
       mma_commit(&sh.drain);
       mbar_wait(&sh.drain, 0, nullptr, 0, 200000000LL);
-      for (int b = 0; b < kAcc; ++b)
-        if (n_norm[b]) mbar_wait(&sh.normf[b], (n_norm[b] - 1u) & 1u, nullptr, 0, 200000000LL);
+      for (int b = 0; b < kAcc; ++b) {
+        const uint32_t copies = m_idx > static_cast<uint32_t>(b) ? (m_idx - static_cast<uint32_t>(b) + kAcc - 1) / kAcc : 0u;
+        if (copies) mbar_wait(&sh.normf[b], (copies - 1u) & 1u, nullptr, 0, 200000000LL);
+      }
     }
   } else {
     // ---- epilogue: thread = query (TMEM lane etid) ---------------------------

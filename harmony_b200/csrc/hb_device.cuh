@@ -100,6 +100,32 @@ __device__ __forceinline__ float exact_l2_seq(const float* __restrict__ x, const
   return acc;
 }
 
+// Row stride (floats) of rows staged by warp_stage_rows: dpad rounded up to
+// 32, plus 4, so the quarter-warps of per-lane float4 reads (lane r reading
+// row r at the same column) cover 32 distinct banks.
+__host__ __device__ __forceinline__ int stage_stride(int dpad) { return (dpad + 31) / 32 * 32 + 4; }
+
+// The warp copies row `row` of lane r (-1: none) of a row-major FP32 matrix
+// with dpad-float rows to stage + r * stride, for r = 0..31; lane L copies
+// floats [4L, 4L + 4) (+ 128 j) of every row, so each row is read as
+// contiguous 512-byte pieces rather than by one lane walking it alone.  Rows
+// must be 16-byte aligned (dpad a multiple of 4).  Returns once the warp's
+// copies have landed; a __syncwarp first keeps the previous rows' readers
+// ahead of the overwrite.
+__device__ __forceinline__ void warp_stage_rows(const float* __restrict__ base, int64_t row, int dpad, float* stage,
+                                                int stride, int lane) {
+  __syncwarp();
+  for (int r = 0; r < 32; ++r) {
+    const long long rr = __shfl_sync(0xffffffffu, static_cast<long long>(row), r);
+    if (rr < 0) continue;
+    const float* src = base + rr * dpad;
+    for (int j = 4 * lane; j < dpad; j += 128) cp_async16(stage + r * stride + j, src + j, true);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncwarp();
+}
+
 __host__ __device__ __forceinline__ int pow2_ceil(int x) {
   int p = 1;
   while (p < x) p <<= 1;

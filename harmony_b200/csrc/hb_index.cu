@@ -435,18 +435,22 @@ class IndexCore {
       return;
     }
     ensure_coarse_tc();
+    qsplit_.reserve(static_cast<size_t>(nq) * 2 * ckpad_);
+    qsnorm_.reserve(static_cast<size_t>(nq));
+    vlo_.reserve(static_cast<size_t>(nq));
+    vhi_.reserve(static_cast<size_t>(nq));
     ccand_.reserve(static_cast<size_t>(nq) * Pm);
     cval_.reserve(static_cast<size_t>(nq) * Pm);
     cflags_.reserve(static_cast<size_t>(nq));
     {
       Scope sc(this, "coarse_tc");
       launch_coarse_tc(ctmap_, qpad, nq, static_cast<int>(dpad_), ckpad_, cnorm_.p, static_cast<int>(nlist_), dmat_.p,
-                       cerr_dev_.p, num_sms_, st_);
+                       qsplit_.p, qsnorm_.p, vlo_.p, vhi_.p, cerr_dev_.p, num_sms_, st_);
     }
     {
       Scope sc(this, "coarse_select");
       launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), Pm, ccand_.p, cval_.p, st_,
-                         nullptr, cflags_.p);
+                         nullptr, cflags_.p, vlo_.p, vhi_.p);
     }
     {
       Scope sc(this, "coarse_refine");
@@ -455,7 +459,7 @@ class IndexCore {
       launch_coarse_fallback(qpad, nq, static_cast<int>(dpad_), cent_.p, static_cast<int>(nlist_), P, cflags_.p,
                              dmat_.p, probes_out, cdist_out, st_);
     }
-    launches_ += 4;
+    launches_ += 6;
     coarse_last_nq_ = nq;
   }
 
@@ -478,6 +482,10 @@ class IndexCore {
     const int C = std::min<int>(m.C, P);
     dmat_.reserve(static_cast<size_t>(nq) * nlist_);
     ensure_coarse_tc();
+    qsplit_.reserve(static_cast<size_t>(nq) * 2 * ckpad_);
+    qsnorm_.reserve(static_cast<size_t>(nq));
+    vlo_.reserve(static_cast<size_t>(nq));
+    vhi_.reserve(static_cast<size_t>(nq));
     const int nl = static_cast<int>(nlist_);
     const int PmA = std::min(nl, C + coarse_extra(C));
     const int PmB = std::min(nl, P + coarse_extra(P));
@@ -490,12 +498,12 @@ class IndexCore {
     kq_.reserve(static_cast<size_t>(nq));
     {
       Scope sc(this, "coarse_tc");
-      launch_coarse_tc(ctmap_, qpad, nq, static_cast<int>(dpad_), ckpad_, cnorm_.p, nl, dmat_.p, cerr_dev_.p, num_sms_,
-                       st_);
+      launch_coarse_tc(ctmap_, qpad, nq, static_cast<int>(dpad_), ckpad_, cnorm_.p, nl, dmat_.p, qsplit_.p, qsnorm_.p,
+                       vlo_.p, vhi_.p, cerr_dev_.p, num_sms_, st_);
     }
     {
       Scope sc(this, "coarse_select");
-      launch_select_rows(dmat_.p, nq, nl, nl, PmA, ccand_.p, cval_.p, st_, nullptr, cflags_.p);
+      launch_select_rows(dmat_.p, nq, nl, nl, PmA, ccand_.p, cval_.p, st_, nullptr, cflags_.p, vlo_.p, vhi_.p);
     }
     {
       Scope sc(this, "coarse_refine");
@@ -511,7 +519,7 @@ class IndexCore {
     {
       Scope sc(this, "coarse_widen_select");
       launch_coarse_widths(npq_.p, nq, P, C, coarse_margin_, nl, kq_.p, st_);
-      launch_select_rows(dmat_.p, nq, nl, nl, PmB, ccand_.p, cval_.p, st_, kq_.p, cflags_.p);
+      launch_select_rows(dmat_.p, nq, nl, nl, PmB, ccand_.p, cval_.p, st_, kq_.p, cflags_.p, vlo_.p, vhi_.p);
     }
     {
       Scope sc(this, "coarse_widen_refine");
@@ -525,7 +533,7 @@ class IndexCore {
       launch_coarse_fallback(qpad, nq, static_cast<int>(dpad_), cent_.p, nl, P, cflags_.p, dmat_.p, probes_out, nullptr,
                              st_, npq_.p);
     }
-    launches_ += 12;
+    launches_ += 13;
     coarse_last_nq_ = nq;
   }
 
@@ -534,7 +542,7 @@ class IndexCore {
   void ensure_coarse_tc() {
     if (coarse_ready_) return;
     ckpad_ = static_cast<int>((d_ + 63) / 64 * 64);
-    csplit_.reserve(nlist_ * 3 * static_cast<size_t>(ckpad_));
+    csplit_.reserve(nlist_ * 2 * static_cast<size_t>(ckpad_));
     make_centroid_split(cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), ckpad_, csplit_.p, ctmap_, st_);
     cnorm_.reserve(nlist_);
     launch_row_norms(cent_.p, nlist_, static_cast<int>(d_), static_cast<int>(dpad_), cnorm_.p, st_);
@@ -2094,6 +2102,10 @@ class IndexCore {
   int ckpad_ = 0;
   alignas(64) unsigned char ctmap_[128];
   DevBuf<uint16_t> csplit_;
+  DevBuf<uint16_t> qsplit_;  // queries' [hi | lo] BF16 rows for the tensor-core quantizer
+  DevBuf<float> qsnorm_;     // their ||q||^2
+  DevBuf<uint32_t> vlo_;     // per query: smallest / largest finite value of its row of dmat_
+  DevBuf<uint32_t> vhi_;
   DevBuf<float> cnorm_, cmaxnorm_, cval_;
   DevBuf<int32_t> ccand_;
   DevBuf<int> cflags_, cerr_dev_;

@@ -126,9 +126,12 @@ size_t scan_exact_smem_bytes(int d, int dpad, int k, int mode, int* tv, int* qt,
 // Row-wise selection of the k smallest (value, column) pairs of a float
 // matrix; out_idx gets columns, out_val the values, ascending.
 // row_flags (optional, nrows ints of scratch): enables the warp-per-row
-// path for k <= 256.
+// path for k <= 256.  vlo / vhi (optional, nrows each): bit patterns of a
+// range expected to hold each row's finite values (a hint: values outside
+// it are still selected exactly); given, the warp path skips its range pass.
 void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx,
-                        float* out_val, cudaStream_t st, const int32_t* k_row = nullptr, int* row_flags = nullptr);
+                        float* out_val, cudaStream_t st, const int32_t* k_row = nullptr, int* row_flags = nullptr,
+                        const uint32_t* vlo = nullptr, const uint32_t* vhi = nullptr);
 // Build the list-major work description from probes (nq x P, -1 = none).
 void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist,
                        int chunk_rows, int qgroup, int32_t* list_cnt, int64_t* list_qoff,
@@ -307,11 +310,16 @@ void launch_max_norm(const float* norms, size_t n, float* out, cudaStream_t st);
 // exact FP32 finish; the probe rows equal the exact quantizer's.
 constexpr int kCoarseMaxPm = 1024;  // largest candidate count per query
 size_t coarse_tc_smem_bytes(int kpad);
-// cent (nlist x dpad FP32) -> out (nlist x 3*kpad BF16 [hi|lo|hi]) + its tensor map.
+// cent (nlist x dpad FP32) -> out (nlist x 2*kpad BF16 [hi|lo]) + its tensor map.
 void make_centroid_split(const float* cent, int nlist, int dpad, int kpad, void* out, void* tmap_out, cudaStream_t st);
-// V (nq x nlist) = max(0, ||q||^2 + ||c||^2 - 2 q.c) on the tensor cores.
+// V (nq x nlist) = max(0, ||q||^2 + ||c||^2 - 2 q.c) on the tensor cores;
+// qsplit (nq x 2*kpad BF16) and qnorm (nq) are scratch for the queries'
+// [hi|lo] rows and norms.
+// vlo / vhi (nq each) get the bit patterns of each row's smallest and
+// largest finite value, the range hint of launch_select_rows.
 void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kpad, const float* cnorm, int nlist,
-                      float* V, int* err, int num_sms, cudaStream_t st);
+                      float* V, void* qsplit, float* qnorm, uint32_t* vlo, uint32_t* vhi, int* err, int num_sms,
+                      cudaStream_t st);
 // Per-row widths of a coarse pass: row r keeps width[r] <= P probes out of
 // width[r] + margin candidates; rows whose width is <= pre_w are copied from
 // an earlier pass of width pre_w (pre, nq x pre_w).  width == nullptr: every

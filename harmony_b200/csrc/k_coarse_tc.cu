@@ -1,15 +1,18 @@
 // Tensor-core coarse quantizer with an exact FP32 finish.
 //
 //  1. coarse_tc_kernel: queries and centroids are split into BF16 pairs
-//     x = hi + lo (hi = bf16(x), lo = bf16(x - hi)); one tcgen05.mma chain
-//     over K = 3 * kpad with A = [q_hi | q_hi | q_lo] and
-//     B = [c_hi | c_lo | c_hi] gives q_hi.c_hi + q_hi.c_lo + q_lo.c_hi,
-//     i.e. q.c to about 2^-16 relative (the 3-term BF16 split).  128
-//     queries per CTA (A, K-major, 128-byte swizzle, built in shared memory
-//     from the FP32 queries), 128 centroids per TMA tile streamed through a
-//     ring of 64-column K blocks, accumulators double-buffered in TMEM.  The
-//     epilogue writes v = max(0, ||q||^2 + ||c||^2 - 2 q.c) to an
-//     nq x nlist matrix.
+//     x = hi + lo (hi = bf16(x), lo = bf16(x - hi)), each stored as one row
+//     [hi | lo] of 2 * kpad BF16 (split_rows_kernel).  Per (centroid tile,
+//     query tile) of 128 x 128 one tcgen05.mma chain accumulates
+//     q_hi.c_hi + q_hi.c_lo + q_lo.c_hi, i.e. q.c to about 2^-16 relative
+//     (the 3-term BF16 split).  A CTA keeps one centroid tile resident in
+//     shared memory (B, K-major, 128-byte swizzle, one TMA load) and streams
+//     query tiles (A) through a ring of 64-column K blocks; accumulators are
+//     double-buffered in TMEM.  The (centroid tile, query tile) pairs are
+//     ordered centroid tile first and split into equal contiguous ranges, one
+//     per CTA, one CTA per SM, so a CTA loads at most a few centroid tiles.
+//     The epilogue (thread = query) writes v = max(0, ||q||^2 + ||c||^2 -
+//     2 q.c) to an nq x nlist matrix.
 //  2. select_rows (k_select.cu) keeps the Pm = P + m smallest values.
 //  3. coarse_refine_kernel recomputes those Pm distances exactly (the
 //     reference's sequential unfused FP32 loop, src/utils.h:480-487), sorts
@@ -24,16 +27,18 @@
 //
 // Error bound of v: the split leaves |q.c - (q_hi.c_hi + q_hi.c_lo +
 // q_lo.c_hi)| <= 3 * 2^-18 * sum|q_i c_i|; the FP32 accumulation of 3 * kpad
-// <= 384 exact BF16 products adds <= 384 * 2^-23 * sum|q_i c_i|; with
-// sum|q_i c_i| <= ||q|| ||c|| the dot error is < 6e-5 ||q|| ||c||, so
-// 2 q.c is within 1.2e-4 ||q|| ||c||.  The norms, the FP32 combination and
-// the reference's own FP32 rounding add < 1e-5 (||q||^2 + ||c||^2 + v).  The
-// bound used, 4e-4 ||q|| max||c|| + 2e-5 (max||c||^2 + ||q||^2 + |v|), is
-// more than three times that.
+// <= 384 exact BF16 products, in any order, adds <= 384 * 2^-23 *
+// sum|q_i c_i|; with sum|q_i c_i| <= ||q|| ||c|| the dot error is < 6e-5
+// ||q|| ||c||, so 2 q.c is within 1.2e-4 ||q|| ||c||.  The norms, the FP32
+// combination and the reference's own FP32 rounding add < 1e-5 (||q||^2 +
+// ||c||^2 + v).  The bound used, 4e-4 ||q|| max||c|| + 2e-5 (max||c||^2 +
+// ||q||^2 + |v|), is more than three times that.
 #include <cudaTypedefs.h>
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "hb_device.cuh"
 #include "hb_internal.hpp"
@@ -45,9 +50,11 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kCT = 128;        // queries per CTA = centroids per tile
-constexpr int kCStages = 6;     // ring of 64-column K blocks (16 KB each)
-constexpr int kCThreads = 192;  // 4 epilogue warps, TMA warp, MMA warp
+constexpr int kCT = 128;        // queries per tile = centroids per tile
+constexpr int kCStages = 8;     // ring of 64-column K blocks of query tiles (16 KB each)
+constexpr int kCEpiWarps = 8;   // epilogue warps: two per TMEM lane quarter, one per half of the columns
+constexpr int kCTmaWarp = kCEpiWarps, kCMmaWarp = kCEpiWarps + 1;
+constexpr int kCThreads = (kCEpiWarps + 2) * 32;
 constexpr uint32_t kBlk = kCT * 128;  // bytes of one 128-row x 64-column BF16 block
 
 struct CoarseShared {
@@ -55,31 +62,33 @@ struct CoarseShared {
   uint64_t empty[kCStages];
   uint64_t accf[2];
   uint64_t acce[2];
+  uint64_t bfull;
+  uint64_t bempty;
   uint32_t tmem;
 };
 
-__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
-  __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
-  return *reinterpret_cast<uint32_t*>(&p);
+// Pairs [p0, p1) of CTA b out of G over `pairs`, centroid tile = p / qt.
+__device__ __forceinline__ void coarse_range(int b, int G, int pairs, int& p0, int& p1) {
+  p0 = static_cast<int>(static_cast<long long>(b) * pairs / G);
+  p1 = static_cast<int>(static_cast<long long>(b + 1) * pairs / G);
 }
 
 __global__ void __launch_bounds__(kCThreads, 1)
-    coarse_tc_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restrict__ q, int nq, int dpad, int kpad,
-                     const float* __restrict__ cnorm, int nlist, int tiles_per_cta, float* __restrict__ V,
+    coarse_tc_kernel(const __grid_constant__ CUtensorMap tmap_c, const __grid_constant__ CUtensorMap tmap_q,
+                     const float* __restrict__ qnorm, int nq, int kpad, const float* __restrict__ cnorm, int nlist,
+                     int qt, int pairs, float* __restrict__ V, uint32_t* __restrict__ vlo, uint32_t* __restrict__ vhi,
                      int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ CoarseShared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const int nkb = 3 * kpad / 64;  // K blocks per tile
-  uint8_t* A = smem;
-  uint8_t* ring = smem + static_cast<size_t>(nkb) * kBlk;
+  const int nh = kpad / 64;  // K blocks of one half (hi or lo)
+  uint8_t* Bt = smem;        // resident centroid tile: [c_hi | c_lo], 2 * nh blocks
+  uint8_t* ring = smem + static_cast<size_t>(2 * nh) * kBlk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int q0 = blockIdx.x * kCT;
-  const int t0 = blockIdx.y * tiles_per_cta;
-  const int t1 = min((nlist + kCT - 1) / kCT, t0 + tiles_per_cta);
-  const int ntiles = max(0, t1 - t0);
+  int p0, p1;
+  coarse_range(blockIdx.x, gridDim.x, pairs, p0, p1);
 
-  if (warp == 5) tmem_alloc(&sh.tmem, 256);
+  if (warp == kCMmaWarp) tmem_alloc(&sh.tmem, 256);
   if (tid == 0) {
     for (int s = 0; s < kCStages; ++s) {
       mbar_init(&sh.full[s], 1);
@@ -87,91 +96,88 @@ __global__ void __launch_bounds__(kCThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&sh.accf[b], 1);
-      mbar_init(&sh.acce[b], 128);
+      mbar_init(&sh.acce[b], kCEpiWarps * 32);
     }
+    mbar_init(&sh.bfull, 1);
+    mbar_init(&sh.bempty, 1);
     fence_barrier_init();
-  }
-  float qn = 0.0f;
-  if (tid < 128) {
-    // Row tid of A: [hi | hi | lo] of query q0 + tid (zeros past nq / dpad).
-    const int qi = q0 + tid;
-    const float* qrow = q + static_cast<size_t>(qi < nq ? qi : 0) * dpad;
-    const uint32_t kb_hi2 = static_cast<uint32_t>(kpad / 64) * kBlk;
-    for (int k = 0; k < kpad; k += 8) {
-      float x[8];
-      if (qi < nq && k < dpad) {
-        const float4 lo4 = *reinterpret_cast<const float4*>(qrow + k);
-        const float4 hi4 = *reinterpret_cast<const float4*>(qrow + k + 4);
-        x[0] = lo4.x, x[1] = lo4.y, x[2] = lo4.z, x[3] = lo4.w, x[4] = hi4.x, x[5] = hi4.y, x[6] = hi4.z, x[7] = hi4.w;
-      } else {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = 0.0f;
-      }
-      uint32_t h[4], l[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float a = x[2 * j], b = x[2 * j + 1];
-        qn = fmaf(a, a, qn);
-        qn = fmaf(b, b, qn);
-        const float ha = __bfloat162float(__float2bfloat16_rn(a)), hb_ = __bfloat162float(__float2bfloat16_rn(b));
-        h[j] = pack_bf16x2(ha, hb_);
-        l[j] = pack_bf16x2(a - ha, b - hb_);
-      }
-      const uint32_t off = sw128_offset_bf16(tid, k, kBlk);
-      *reinterpret_cast<uint4*>(A + off) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4*>(A + kb_hi2 + off) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4*>(A + 2 * kb_hi2 + off) = make_uint4(l[0], l[1], l[2], l[3]);
-    }
-    fence_proxy_async_smem();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sh.tmem;
 
-  if (warp == 4) {
+  if (warp == kCTmaWarp) {
     if (lane == 0) {
-      int it = 0;
-      for (int i = 0; i < ntiles; ++i) {
-        for (int kb = 0; kb < nkb; ++kb, ++it) {
-          const int s = it % kCStages;
-          if (!mbar_wait(&sh.empty[s], ((it / kCStages) & 1u) ^ 1u, err, 21)) goto producer_done;
-          mbar_arrive_expect_tx(&sh.full[s], kBlk);
-          tma_load_2d(ring + static_cast<size_t>(s) * kBlk, &tmap, kb * 64, (t0 + i) * kCT, &sh.full[s]);
+      // Centroid tile at each change of tile (after the MMAs that read the
+      // previous one), then the query tile's 2 * nh K blocks.
+      int it = 0, nb = 0, cur = -1;
+      for (int p = p0; p < p1; ++p) {
+        const int c = p / qt, qtile = p - c * qt;
+        if (c != cur) {
+          if (nb > 0 && !mbar_wait(&sh.bempty, (nb - 1) & 1u, err, 25)) break;
+          mbar_arrive_expect_tx(&sh.bfull, static_cast<uint32_t>(2 * nh) * kBlk);
+          for (int kb = 0; kb < 2 * nh; ++kb) tma_load_2d(Bt + static_cast<size_t>(kb) * kBlk, &tmap_c, kb * 64, c * kCT, &sh.bfull);
+          cur = c;
+          ++nb;
         }
+        bool ok = true;
+        for (int kb = 0; kb < 2 * nh; ++kb, ++it) {
+          const int s = it % kCStages;
+          if (!mbar_wait(&sh.empty[s], ((it / kCStages) & 1u) ^ 1u, err, 21)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&sh.full[s], kBlk);
+          tma_load_2d(ring + static_cast<size_t>(s) * kBlk, &tmap_q, kb * 64, qtile * kCT, &sh.full[s]);
+        }
+        if (!ok) break;
       }
-    producer_done:;
     }
-  } else if (warp == 5) {
+  } else if (warp == kCMmaWarp) {
     if (lane == 0) {
       const uint32_t idesc = idesc_bf16_f32(kCT, kCT);
-      const uint32_t abase = smem_u32(A), rbase = smem_u32(ring);
-      int it = 0;
-      int issued = 0;
-      for (int i = 0; i < ntiles; ++i) {
-        const int b = i & 1;
+      const uint32_t bbase = smem_u32(Bt), rbase = smem_u32(ring);
+      int it = 0, nb = 0, cur = -1, issued = 0;
+      bool ok = true;
+      for (int p = p0; p < p1 && ok; ++p) {
+        const int c = p / qt;
+        if (c != cur) {
+          if (!mbar_wait(&sh.bfull, nb & 1u, err, 26)) break;
+          tc_fence_after();
+          cur = c;
+          ++nb;
+        }
+        const int i = p - p0, b = i & 1;
         if (!mbar_wait(&sh.acce[b], ((i >> 1) & 1u) ^ 1u, err, 23)) break;
         tc_fence_after();
-        bool ok = true;
-        for (int kb = 0; kb < nkb; ++kb, ++it) {
+        const uint32_t d = tmem + static_cast<uint32_t>(b * kCT);
+        // A block kb: q_hi block kb (kb < nh) meets c_hi and c_lo block kb;
+        // q_lo block kb - nh meets c_hi block kb - nh.
+        for (int kb = 0; kb < 2 * nh; ++kb, ++it) {
           const int s = it % kCStages;
           if (!mbar_wait(&sh.full[s], (it / kCStages) & 1u, err, 22)) {
             ok = false;
             break;
           }
           tc_fence_after();
+          const uint64_t ad = desc_sw128(rbase + static_cast<uint32_t>(s) * kBlk);
+          const int j = kb < nh ? kb : kb - nh;
+          const uint64_t bh = desc_sw128(bbase + static_cast<uint32_t>(j) * kBlk);
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {
-            mma_bf16(tmem + static_cast<uint32_t>(b * kCT),
-                     desc_sw128(abase + static_cast<uint32_t>(kb) * kBlk + kk * 32u),
-                     desc_sw128(rbase + static_cast<uint32_t>(s) * kBlk + kk * 32u), idesc,
-                     (kb | kk) != 0 ? 1u : 0u);
+          for (int kk = 0; kk < 4; ++kk) mma_bf16(d, ad + 2 * kk, bh + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
+          if (kb < nh) {
+            const uint64_t bl = desc_sw128(bbase + static_cast<uint32_t>(nh + j) * kBlk);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) mma_bf16(d, ad + 2 * kk, bl + 2 * kk, idesc, 1u);
           }
           mma_commit(&sh.empty[s]);
         }
         if (!ok) break;
         mma_commit(&sh.accf[b]);
         ++issued;
+        // The last tile against this centroid tile: its MMAs free B.
+        if (p + 1 == p1 || (p + 1) / qt != c) mma_commit(&sh.bempty);
       }
       // Drain: the tensor cores must be done before TMEM is released.
       if (issued > 0) {
@@ -180,68 +186,93 @@ __global__ void __launch_bounds__(kCThreads, 1)
       }
     }
   } else {
-    const int qi = q0 + tid;
-    const uint32_t lane_base = (32u * static_cast<uint32_t>(warp)) << 16;
+    // Warp w: TMEM lanes (queries) 32 (w % 4) .. + 31, columns 64 (w / 4)
+    // .. + 63 of each tile (two 32-column chunks).
+    const uint32_t lane_base = (32u * static_cast<uint32_t>(warp & 3)) << 16;
+    const int half = warp >> 2;
     bool ok = true;
-    for (int i = 0; i < ntiles; ++i) {
-      const int b = i & 1;
+    for (int p = p0; p < p1; ++p) {
+      const int c = p / qt, qtile = p - c * qt;
+      const int i = p - p0, b = i & 1;
+      const int qi = qtile * kCT + (warp & 3) * 32 + lane;
+      const float qn = qi < nq ? qnorm[qi] : 0.0f;
       if (ok) ok = mbar_wait(&sh.accf[b], (i >> 1) & 1u, err, 24);
       ok = __all_sync(0xffffffffu, ok);
       if (!ok) break;
       tc_fence_after();
-      const int c0 = (t0 + i) * kCT;
-#pragma unroll 1
-      for (int c = 0; c < kCT / 32; ++c) {
-        uint32_t r[32];
-        tmem_ld32(tmem + lane_base + static_cast<uint32_t>(b * kCT + c * 32), r);
-        tmem_ld_wait();
-        if (qi < nq) {
-          const int cb = c0 + c * 32;
-          float* out = V + static_cast<size_t>(qi) * nlist + cb;
-          if (nlist - cb >= 32 && (nlist & 3) == 0) {
-#pragma unroll
-            for (int j4 = 0; j4 < 8; ++j4) {
-              const float4 cn = *reinterpret_cast<const float4*>(cnorm + cb + 4 * j4);
-              float4 o;
-              o.x = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 0]), qn + cn.x), 0.0f);
-              o.y = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), qn + cn.y), 0.0f);
-              o.z = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), qn + cn.z), 0.0f);
-              o.w = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), qn + cn.w), 0.0f);
-              *reinterpret_cast<float4*>(out + 4 * j4) = o;
-            }
-          } else {
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (cb + j < nlist) out[j] = fmaxf(fmaf(-2.0f, __uint_as_float(r[j]), qn + cnorm[cb + j]), 0.0f);
-          }
-        }
-      }
+      const uint32_t t0 = tmem + lane_base + static_cast<uint32_t>(b * kCT + half * 64);
+      uint32_t ra[32], rb[32];
+      tmem_ld32(t0, ra);
+      tmem_ld32(t0 + 32, rb);
+      tmem_ld_wait(ra);
+      tmem_ld_wait(rb);
       tc_fence_before();
       mbar_arrive(&sh.acce[b]);
+      // Range of this row's values (the selection's hint; columns past
+      // nlist only widen it).
+      uint32_t tlo = 0xFFFFFFFFu, thi = 0;
+      auto chunk = [&](const uint32_t (&r)[32], int cb) {
+        float* out = V + static_cast<size_t>(qi) * nlist + cb;
+        if (nlist - cb >= 32 && (nlist & 3) == 0) {
+#pragma unroll
+          for (int j4 = 0; j4 < 8; ++j4) {
+            const float4 cn = *reinterpret_cast<const float4*>(cnorm + cb + 4 * j4);
+            float4 o;
+            o.x = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 0]), qn + cn.x), 0.0f);
+            o.y = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), qn + cn.y), 0.0f);
+            o.z = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), qn + cn.z), 0.0f);
+            o.w = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), qn + cn.w), 0.0f);
+            tlo = min(min(tlo, __float_as_uint(o.x)), min(__float_as_uint(o.y), min(__float_as_uint(o.z), __float_as_uint(o.w))));
+            thi = max(max(thi, __float_as_uint(o.x)), max(__float_as_uint(o.y), max(__float_as_uint(o.z), __float_as_uint(o.w))));
+            if (qi < nq) *reinterpret_cast<float4*>(out + 4 * j4) = o;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (cb + j < nlist) {
+              const float v = fmaxf(fmaf(-2.0f, __uint_as_float(r[j]), qn + cnorm[cb + j]), 0.0f);
+              tlo = min(tlo, __float_as_uint(v));
+              thi = max(thi, __float_as_uint(v));
+              if (qi < nq) out[j] = v;
+            }
+        }
+      };
+      const int cb = c * kCT + half * 64;
+      if (cb < nlist) chunk(ra, cb);
+      if (cb + 32 < nlist) chunk(rb, cb + 32);
+      if (qi < nq && tlo <= thi) {
+        atomicMin(vlo + qi, tlo);
+        atomicMax(vhi + qi, thi);
+      }
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 5) {
+  if (warp == kCMmaWarp) {
     tc_fence_after();
     tmem_dealloc(tmem, 256);
   }
 }
 
-// Centroid rows -> [hi | lo | hi] BF16 rows of 3 * kpad (zeros past d).
-__global__ void split3_kernel(const float* __restrict__ c, int n, int dpad, int kpad, __nv_bfloat16* __restrict__ out) {
-  const size_t total = static_cast<size_t>(n) * kpad;
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const size_t r = i / kpad;
-    const int k = static_cast<int>(i % kpad);
-    const float x = k < dpad ? c[r * dpad + k] : 0.0f;
-    const __nv_bfloat16 h = __float2bfloat16_rn(x);
-    const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-    __nv_bfloat16* o = out + r * 3 * kpad;
-    o[k] = h;
-    o[kpad + k] = l;
-    o[2 * kpad + k] = h;
+// Rows (FP32, dpad wide) -> [hi | lo] BF16 rows of 2 * kpad (zeros past d),
+// and, when norm is given, each row's ||x||^2; a warp per row.
+__global__ void split_rows_kernel(const float* __restrict__ x, int n, int dpad, int kpad,
+                                  __nv_bfloat16* __restrict__ out, float* __restrict__ norm) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const float* row = x + static_cast<size_t>(r) * dpad;
+    __nv_bfloat16* o = out + static_cast<size_t>(r) * 2 * kpad;
+    float s = 0.0f;
+    for (int k = lane; k < kpad; k += 32) {
+      const float v = k < dpad ? row[k] : 0.0f;
+      s = fmaf(v, v, s);
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      o[k] = h;
+      o[kpad + k] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (norm && lane == 0) norm[r] = s;
   }
 }
 
@@ -256,7 +287,8 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
                                                             int Pm, int P, int nlist, const float* __restrict__ cmaxnorm,
                                                             int32_t* __restrict__ probes, float* __restrict__ cdist,
                                                             int* __restrict__ flags, CoarseRows rows) {
-  extern __shared__ uint64_t s_ref[];  // [warps][pow2(Pm)]
+  // [warps][pow2(Pm)] keys, then a 32-row stage per warp.
+  extern __shared__ __align__(16) uint8_t s_ref_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int qi = blockIdx.x * (blockDim.x >> 5) + wib;
   if (qi >= nq) return;
@@ -276,7 +308,10 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
   }
   const int n2 = pow2_ceil(Pmr < 2 ? 2 : Pmr);
   // Per-warp buffers are laid out for the launch's widest row.
-  uint64_t* buf = s_ref + static_cast<size_t>(wib) * pow2_ceil(Pm < 2 ? 2 : Pm);
+  const int nmax = pow2_ceil(Pm < 2 ? 2 : Pm), stride = stage_stride(dpad);
+  uint64_t* buf = reinterpret_cast<uint64_t*>(s_ref_raw) + static_cast<size_t>(wib) * nmax;
+  float* stage = reinterpret_cast<float*>(s_ref_raw + static_cast<size_t>(blockDim.x >> 5) * nmax * 8) +
+                 static_cast<size_t>(wib) * 32 * stride;
   const float* qrow = q + static_cast<size_t>(qi) * dpad;
   float qn = 0.0f;
   for (int c = lane * 4; c < dpad; c += 128) {
@@ -284,31 +319,18 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
     qn += v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w;
   }
   for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(0xffffffffu, qn, o);
-  for (int i = lane; i < n2; i += 32) {
+  // 32 candidates at a time, lane = candidate: the warp stages their
+  // centroid rows, then each lane runs the sequential loop over its row.
+  for (int base = 0; base < n2; base += 32) {
+    const int i = base + lane;
+    const int c = i < Pmr ? cand[static_cast<size_t>(qi) * Pm + i] : -1;
+    if (base < Pmr) warp_stage_rows(cent, c, dpad, stage, stride, lane);
     uint64_t key = kEmpty;
-    if (i < Pmr) {
-      const int c = cand[static_cast<size_t>(qi) * Pm + i];
-      if (c >= 0) {
-        const float* x = cent + static_cast<size_t>(c) * dpad;
-        float acc = 0.0f;
-#pragma unroll 8
-        for (int j = 0; j < dpad; j += 4) {
-          const float4 v = *reinterpret_cast<const float4*>(x + j);
-          const float4 w = *reinterpret_cast<const float4*>(qrow + j);
-          float t;
-          t = __fsub_rn(w.x, v.x);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
-          t = __fsub_rn(w.y, v.y);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
-          t = __fsub_rn(w.z, v.z);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
-          t = __fsub_rn(w.w, v.w);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
-        }
-        if (acc < FLT_MAX) key = make_key(acc, static_cast<uint32_t>(c));
-      }
+    if (c >= 0) {
+      const float acc = exact_l2_seq(stage + static_cast<size_t>(lane) * stride, qrow, dpad);
+      if (acc < FLT_MAX) key = make_key(acc, static_cast<uint32_t>(c));
     }
-    buf[i] = key;
+    if (i < n2) buf[i] = key;
   }
   __syncwarp();
   warp_bitonic_sort(buf, n2, lane);
@@ -369,22 +391,7 @@ __global__ void __launch_bounds__(256) coarse_refine_block_kernel(
     if (i < Pmr) {
       const int c = cand[static_cast<size_t>(qi) * Pm + i];
       if (c >= 0) {
-        const float* x = cent + static_cast<size_t>(c) * dpad;
-        float acc = 0.0f;
-#pragma unroll 8
-        for (int j = 0; j < dpad; j += 4) {
-          const float4 v = *reinterpret_cast<const float4*>(x + j);
-          const float4 w = *reinterpret_cast<const float4*>(qrow + j);
-          float t;
-          t = __fsub_rn(w.x, v.x);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
-          t = __fsub_rn(w.y, v.y);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
-          t = __fsub_rn(w.z, v.z);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
-          t = __fsub_rn(w.w, v.w);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
-        }
+        const float acc = exact_l2_seq(cent + static_cast<size_t>(c) * dpad, qrow, dpad);
         if (acc < FLT_MAX) key = make_key(acc, static_cast<uint32_t>(c));
       }
     }
@@ -425,30 +432,45 @@ __global__ void __launch_bounds__(256) coarse_fallback_kernel(const float* __res
                                                               const int32_t* __restrict__ width) {
   extern __shared__ uint64_t s_fb[];
   __shared__ SelectShared sh_sel;
-  const int qi = blockIdx.x;
-  if (qi >= nq || !flags[qi]) return;
-  const float* qrow = q + static_cast<size_t>(qi) * dpad;
-  float* row = V + static_cast<size_t>(qi) * nlist;
-  for (int c = threadIdx.x; c < nlist; c += blockDim.x) {
-    const float* x = cent + static_cast<size_t>(c) * dpad;
-    float acc = 0.0f;
-    for (int j = 0; j < dpad; ++j) {
-      const float t = __fsub_rn(qrow[j], x[j]);
-      acc = __fadd_rn(acc, __fmul_rn(t, t));
+  __shared__ unsigned s_mask;
+  // Flagged queries are rare: a small grid strides over chunks of 32
+  // queries, one warp reading their flags at once.
+  for (int q0 = blockIdx.x * 32; q0 < nq; q0 += gridDim.x * 32) {
+    if (threadIdx.x < 32) {
+      const unsigned b = __ballot_sync(0xffffffffu, q0 + static_cast<int>(threadIdx.x) < nq && flags[q0 + threadIdx.x] != 0);
+      if (threadIdx.x == 0) s_mask = b;
     }
-    row[c] = acc;
-  }
-  __syncthreads();
-  auto key_at = [&](int c) -> uint64_t {
-    const float v = row[c];
-    return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(c)) : kEmpty;
-  };
-  const int Pr = width ? min(width[qi], P) : P;
-  block_topk_sorted(key_at, nlist, P, sh_sel, s_fb);
-  for (int j = threadIdx.x; j < P; j += blockDim.x) {
-    const uint64_t key = j < Pr ? s_fb[j] : kEmpty;
-    probes[static_cast<size_t>(qi) * P + j] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
-    if (cdist) cdist[static_cast<size_t>(qi) * P + j] = key == kEmpty ? FLT_MAX : key_dist(key);
+    __syncthreads();
+    unsigned mask = s_mask;
+    __syncthreads();
+    while (mask) {
+      const int qi = q0 + __ffs(mask) - 1;
+      mask &= mask - 1;
+      const float* qrow = q + static_cast<size_t>(qi) * dpad;
+      float* row = V + static_cast<size_t>(qi) * nlist;
+      for (int c = threadIdx.x; c < nlist; c += blockDim.x) {
+        const float* x = cent + static_cast<size_t>(c) * dpad;
+        float acc = 0.0f;
+        for (int j = 0; j < dpad; ++j) {
+          const float t = __fsub_rn(qrow[j], x[j]);
+          acc = __fadd_rn(acc, __fmul_rn(t, t));
+        }
+        row[c] = acc;
+      }
+      __syncthreads();
+      auto key_at = [&](int c) -> uint64_t {
+        const float v = row[c];
+        return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(c)) : kEmpty;
+      };
+      const int Pr = width ? min(width[qi], P) : P;
+      block_topk_sorted(key_at, nlist, P, sh_sel, s_fb);
+      for (int j = threadIdx.x; j < P; j += blockDim.x) {
+        const uint64_t key = j < Pr ? s_fb[j] : kEmpty;
+        probes[static_cast<size_t>(qi) * P + j] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
+        if (cdist) cdist[static_cast<size_t>(qi) * P + j] = key == kEmpty ? FLT_MAX : key_dist(key);
+      }
+      __syncthreads();  // s_fb and the selection state are reused by the next query
+    }
   }
 }
 
@@ -472,31 +494,41 @@ void launch_coarse_widths(const int32_t* width, int nq, int wmax, int pre_w, int
 }
 
 size_t coarse_tc_smem_bytes(int kpad) {
-  return 1024 + static_cast<size_t>(3 * kpad / 64 + kCStages) * kBlk;
+  return 1024 + static_cast<size_t>(2 * kpad / 64 + kCStages) * kBlk;
 }
 
 void make_centroid_split(const float* cent, int nlist, int dpad, int kpad, void* out, void* tmap_out, cudaStream_t st) {
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the tensor-core coarse quantizer supports d <= 128");
-  const size_t total = static_cast<size_t>(nlist) * kpad;
-  const unsigned g = static_cast<unsigned>(std::min<size_t>((total + 255) / 256, 148u * 16u));
-  if (total) split3_kernel<<<g, 256, 0, st>>>(cent, nlist, dpad, kpad, static_cast<__nv_bfloat16*>(out));
+  if (nlist > 0) {
+    const unsigned g = static_cast<unsigned>(std::min<int>((nlist + 7) / 8, 148 * 16));
+    split_rows_kernel<<<g, 256, 0, st>>>(cent, nlist, dpad, kpad, static_cast<__nv_bfloat16*>(out), nullptr);
+  }
   HB_CUDA(cudaGetLastError());
-  make_bf16_tensor_map(tmap_out, out, static_cast<size_t>(nlist), 3 * kpad);
+  make_bf16_tensor_map(tmap_out, out, static_cast<size_t>(nlist), 2 * kpad);
 }
 
 void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kpad, const float* cnorm, int nlist,
-                      float* V, int* err, int num_sms, cudaStream_t st) {
+                      float* V, void* qsplit, float* qnorm, uint32_t* vlo, uint32_t* vhi, int* err, int num_sms,
+                      cudaStream_t st) {
   if (nq <= 0 || nlist <= 0) return;
+  HB_CUDA(cudaMemsetAsync(vlo, 0xFF, static_cast<size_t>(nq) * sizeof(uint32_t), st));
+  HB_CUDA(cudaMemsetAsync(vhi, 0, static_cast<size_t>(nq) * sizeof(uint32_t), st));
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the tensor-core coarse quantizer supports d <= 128");
+  // Query rows -> [hi | lo] BF16 and ||q||^2, then their tensor map.
+  const unsigned g = static_cast<unsigned>(std::min<int>((nq + 7) / 8, 148 * 16));
+  split_rows_kernel<<<g, 256, 0, st>>>(q, nq, dpad, kpad, static_cast<__nv_bfloat16*>(qsplit), qnorm);
+  HB_CUDA(cudaGetLastError());
+  alignas(64) unsigned char tmap_q[128];
+  make_bf16_tensor_map(tmap_q, qsplit, static_cast<size_t>(nq), 2 * kpad);
   const int qt = (nq + kCT - 1) / kCT;
   const int ct = (nlist + kCT - 1) / kCT;
-  int split = std::max(1, std::min(ct, (2 * num_sms + qt - 1) / qt));
-  const int per = (ct + split - 1) / split;
-  split = (ct + per - 1) / per;
+  const int pairs = qt * ct;
+  const int G = std::max(1, std::min(pairs, num_sms));
   const size_t smem = coarse_tc_smem_bytes(kpad);
   HB_CUDA(cudaFuncSetAttribute(coarse_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  coarse_tc_kernel<<<dim3(qt, split), kCThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap), q, nq, dpad, kpad,
-                                                            cnorm, nlist, per, V, err);
+  coarse_tc_kernel<<<G, kCThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap),
+                                                *reinterpret_cast<const CUtensorMap*>(tmap_q), qnorm, nq, kpad, cnorm,
+                                                nlist, qt, pairs, V, vlo, vhi, err);
   HB_CUDA(cudaGetLastError());
 }
 
@@ -505,7 +537,9 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
                           cudaStream_t st, CoarseRows rows) {
   if (nq <= 0) return;
   HB_CHECK(P >= 1 && P <= Pm && Pm <= kCoarseMaxPm, HB_ERR_INVALID, "coarse candidate count out of range");
+  HB_CHECK(dpad % 4 == 0 && dpad <= 128, HB_ERR_INVALID, "the coarse refinement stages rows of at most 128 floats");
   const int n2 = pow2_ceil(Pm < 2 ? 2 : Pm);
+  const size_t stage = static_cast<size_t>(32) * stage_stride(dpad) * sizeof(float);  // per warp
   // A CTA per query for small batches, and for the widening pass of the
   // learned nprobe, whose few wide rows (up to Pm candidates) would
   // otherwise keep one warp each busy long after the narrow rows are done.
@@ -518,8 +552,10 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
     HB_CUDA(cudaGetLastError());
     return;
   }
-  const int warps = std::max(1, std::min(8, 65536 / (n2 * 8)));
-  const size_t smem = static_cast<size_t>(warps) * n2 * 8;
+  // Four warps (one query each) per CTA: with the 32-row stages, three CTAs
+  // fit an SM.
+  const int warps = 4;
+  const size_t smem = static_cast<size_t>(warps) * (n2 * 8 + stage);
   HB_CUDA(cudaFuncSetAttribute(coarse_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   coarse_refine_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, st>>>(q, nq, dpad, cent, cand, cval, Pm, P, nlist,
                                                                           cmaxnorm, probes, cdist, flags, rows);
@@ -531,7 +567,8 @@ void launch_coarse_fallback(const float* q, int nq, int dpad, const float* cent,
   if (nq <= 0) return;
   const size_t smem = static_cast<size_t>(pow2_ceil(P < 2 ? 2 : P)) * 8;
   HB_CUDA(cudaFuncSetAttribute(coarse_fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  coarse_fallback_kernel<<<nq, 256, smem, st>>>(q, nq, dpad, cent, nlist, P, flags, V, probes, cdist, width);
+  coarse_fallback_kernel<<<std::min((nq + 31) / 32, 296), 256, smem, st>>>(q, nq, dpad, cent, nlist, P, flags, V,
+                                                                           probes, cdist, width);
   HB_CUDA(cudaGetLastError());
 }
 

@@ -59,138 +59,160 @@ __global__ void __launch_bounds__(kSelThreads) select_rows_kernel(const float* _
 // select_rows_kernel's: the k smallest (value bits, column) keys, ascending.
 constexpr int kBins = 1024;
 constexpr int kCandCap = 2048;
+constexpr int kFlaggedGrid = 296;  // CTAs striding over the rows flagged by the warp kernel
 
 template <int VPT>
-__global__ void __launch_bounds__(kSelThreads, 6) select_rows_reg_kernel(const float* __restrict__ D, int ncols, int ldD,
-                                                                      int kmax, int32_t* __restrict__ out_idx,
+__global__ void __launch_bounds__(kSelThreads, 6) select_rows_reg_kernel(const float* __restrict__ D, int nrows,
+                                                                      int ncols, int ldD, int kmax,
+                                                                      int32_t* __restrict__ out_idx,
                                                                       float* __restrict__ out_val,
                                                                       const int32_t* __restrict__ k_row,
                                                                       const int* __restrict__ only) {
-  if (only && !only[blockIdx.x]) return;
   __shared__ int hist[kBins];
   __shared__ uint64_t s_keys[kCandCap];
   __shared__ SelectShared sh;
   __shared__ unsigned s_lo, s_hi;
   __shared__ int s_real, s_cnt, s_bin, s_cum;
   __shared__ int s_wsum[kSelThreads / 32];
+  __shared__ unsigned s_mask;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  // Row width (rows of width 0 are skipped; the output stride is kmax).
-  const int k = k_row ? min(k_row[blockIdx.x], kmax) : kmax;
-  if (k <= 0) return;
-  const float* row = D + static_cast<size_t>(blockIdx.x) * ldD;
-  // High words of the keys; 0xFFFFFFFF marks empty (a value >= FLT_MAX or
-  // NaN has no key; no non-empty value has all-ones bits).
-  uint32_t u[VPT];
-  unsigned lo = 0xFFFFFFFFu, hi = 0;
-  int real = 0;
-#pragma unroll
-  for (int j = 0; j < VPT; ++j) {
-    const int c = tid + j * kSelThreads;
-    u[j] = 0xFFFFFFFFu;
-    if (c < ncols) {
-      const float v = row[c];
-      if (v < FLT_MAX) {
-        u[j] = __float_as_uint(v);
-        lo = min(lo, u[j]);
-        hi = max(hi, u[j]);
-        ++real;
+  // A row per CTA; with `only`, chunks of 32 rows whose flags one warp reads
+  // at once, then the flagged ones.
+  const int step = only ? 32 : 1;
+  for (int r0 = blockIdx.x * step; r0 < nrows; r0 += gridDim.x * step) {
+    unsigned mask = 1u;
+    if (only) {
+      if (wid == 0) {
+        const unsigned b = __ballot_sync(0xffffffffu, r0 + lane < nrows && only[r0 + lane] != 0);
+        if (lane == 0) s_mask = b;
       }
+      __syncthreads();
+      mask = s_mask;
+      __syncthreads();
     }
-  }
-  if (tid == 0) {
-    s_lo = 0xFFFFFFFFu;
-    s_hi = 0;
-    s_real = 0;
-    s_cnt = 0;
-  }
-  for (int i = tid; i < kBins; i += kSelThreads) hist[i] = 0;
-  for (int off = 16; off > 0; off >>= 1) {
-    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, off));
-    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, off));
-    real += __shfl_xor_sync(0xffffffffu, real, off);
-  }
-  __syncthreads();
-  if (lane == 0 && real) {
-    atomicMin(&s_lo, lo);
-    atomicMax(&s_hi, hi);
-    atomicAdd(&s_real, real);
-  }
-  __syncthreads();
-  real = s_real;
-  lo = s_lo;
-  const int kk = min(k, real);
-  // Bin of a high word: monotone in the word (float rounding is monotone),
-  // below kBins.
-  const float scale = static_cast<float>(kBins) / (static_cast<float>(s_hi - lo) + 1.0f);
-  auto bin_of = [&](uint32_t x) -> int {
-    return min(kBins - 1, static_cast<int>(static_cast<float>(x - lo) * scale));
-  };
-  // Histogram, then the bin where the count reaches kk.
-  if (kk > 0 && kk < real) {
+    while (mask) {
+      const int r = r0 + __ffs(mask) - 1;
+      mask &= mask - 1;
+      // Row width (rows of width 0 are skipped; the output stride is kmax).
+      const int k = k_row ? min(k_row[r], kmax) : kmax;
+      if (k <= 0) continue;
+      const float* row = D + static_cast<size_t>(r) * ldD;
+      // High words of the keys; 0xFFFFFFFF marks empty (a value >= FLT_MAX or
+      // NaN has no key; no non-empty value has all-ones bits).
+      uint32_t u[VPT];
+      unsigned lo = 0xFFFFFFFFu, hi = 0;
+      int real = 0;
 #pragma unroll
-    for (int j = 0; j < VPT; ++j)
-      if (u[j] != 0xFFFFFFFFu) atomicAdd(&hist[bin_of(u[j])], 1);
-  }
-  __syncthreads();
-  if (kk > 0 && kk < real) {
-    constexpr int per = kBins / kSelThreads;
-    int loc = 0;
-#pragma unroll
-    for (int b = 0; b < per; ++b) loc += hist[tid * per + b];
-    int incl = loc;
-    for (int off = 1; off < 32; off <<= 1) {
-      const int o = __shfl_up_sync(0xffffffffu, incl, off);
-      if (lane >= off) incl += o;
-    }
-    if (lane == 31) s_wsum[wid] = incl;
-    __syncthreads();
-    int base = 0;
-    for (int w = 0; w < wid; ++w) base += s_wsum[w];
-    int cum = base + incl - loc;
-    if (cum < kk && cum + loc >= kk) {
-      int b = 0;
-      for (; b < per; ++b) {
-        cum += hist[tid * per + b];
-        if (cum >= kk) break;
+      for (int j = 0; j < VPT; ++j) {
+        const int c = tid + j * kSelThreads;
+        u[j] = 0xFFFFFFFFu;
+        if (c < ncols) {
+          const float v = row[c];
+          if (v < FLT_MAX) {
+            u[j] = __float_as_uint(v);
+            lo = min(lo, u[j]);
+            hi = max(hi, u[j]);
+            ++real;
+          }
+        }
       }
-      s_bin = tid * per + b;
-      s_cum = cum;
-    }
-  } else if (tid == 0) {
-    s_bin = kBins;  // every non-empty key
-    s_cum = real;
-  }
-  __syncthreads();
-  const int bstar = s_bin;
-  const int ncand = s_cum;
-  uint64_t* keys = s_keys;
-  int m = 0;
-  if (ncand <= kCandCap) {
-#pragma unroll
-    for (int j = 0; j < VPT; ++j) {
-      if (u[j] != 0xFFFFFFFFu && (bstar >= kBins || bin_of(u[j]) <= bstar)) {
-        const int pos = atomicAdd(&s_cnt, 1);
-        keys[pos] = (static_cast<uint64_t>(u[j]) << 32) | static_cast<uint32_t>(tid + j * kSelThreads);
+      if (tid == 0) {
+        s_lo = 0xFFFFFFFFu;
+        s_hi = 0;
+        s_real = 0;
+        s_cnt = 0;
       }
+      for (int i = tid; i < kBins; i += kSelThreads) hist[i] = 0;
+      for (int off = 16; off > 0; off >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, off));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, off));
+        real += __shfl_xor_sync(0xffffffffu, real, off);
+      }
+      __syncthreads();
+      if (lane == 0 && real) {
+        atomicMin(&s_lo, lo);
+        atomicMax(&s_hi, hi);
+        atomicAdd(&s_real, real);
+      }
+      __syncthreads();
+      real = s_real;
+      lo = s_lo;
+      const int kk = min(k, real);
+      // Bin of a high word: monotone in the word (float rounding is monotone),
+      // below kBins.
+      const float scale = static_cast<float>(kBins) / (static_cast<float>(s_hi - lo) + 1.0f);
+      auto bin_of = [&](uint32_t x) -> int {
+        return min(kBins - 1, static_cast<int>(static_cast<float>(x - lo) * scale));
+      };
+      // Histogram, then the bin where the count reaches kk.
+      if (kk > 0 && kk < real) {
+#pragma unroll
+        for (int j = 0; j < VPT; ++j)
+          if (u[j] != 0xFFFFFFFFu) atomicAdd(&hist[bin_of(u[j])], 1);
+      }
+      __syncthreads();
+      if (kk > 0 && kk < real) {
+        constexpr int per = kBins / kSelThreads;
+        int loc = 0;
+#pragma unroll
+        for (int b = 0; b < per; ++b) loc += hist[tid * per + b];
+        int incl = loc;
+        for (int off = 1; off < 32; off <<= 1) {
+          const int o = __shfl_up_sync(0xffffffffu, incl, off);
+          if (lane >= off) incl += o;
+        }
+        if (lane == 31) s_wsum[wid] = incl;
+        __syncthreads();
+        int base = 0;
+        for (int w = 0; w < wid; ++w) base += s_wsum[w];
+        int cum = base + incl - loc;
+        if (cum < kk && cum + loc >= kk) {
+          int b = 0;
+          for (; b < per; ++b) {
+            cum += hist[tid * per + b];
+            if (cum >= kk) break;
+          }
+          s_bin = tid * per + b;
+          s_cum = cum;
+        }
+      } else if (tid == 0) {
+        s_bin = kBins;  // every non-empty key
+        s_cum = real;
+      }
+      __syncthreads();
+      const int bstar = s_bin;
+      const int ncand = s_cum;
+      uint64_t* keys = s_keys;
+      int m = 0;
+      if (ncand <= kCandCap) {
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+          if (u[j] != 0xFFFFFFFFu && (bstar >= kBins || bin_of(u[j]) <= bstar)) {
+            const int pos = atomicAdd(&s_cnt, 1);
+            keys[pos] = (static_cast<uint64_t>(u[j]) << 32) | static_cast<uint32_t>(tid + j * kSelThreads);
+          }
+        }
+        m = pow2_ceil(max(ncand, 2));
+        __syncthreads();
+        for (int i = ncand + tid; i < m; i += kSelThreads) keys[i] = kEmpty;
+        __syncthreads();
+        block_bitonic_sort(keys, m);
+      } else {
+        // Many equal high words near the k-th key: the generic selection.
+        auto key_at = [&](int i) -> uint64_t {
+          const float v = row[i];
+          return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(i)) : kEmpty;
+        };
+        block_topk_sorted(key_at, ncols, k, sh, keys);
+      }
+      for (int j = tid; j < k; j += kSelThreads) {
+        const uint64_t key = j < kk ? keys[j] : kEmpty;
+        const size_t o = static_cast<size_t>(r) * kmax + j;
+        out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
+        if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+      }
+      __syncthreads();  // shared state is reused by the next row
     }
-    m = pow2_ceil(max(ncand, 2));
-    __syncthreads();
-    for (int i = ncand + tid; i < m; i += kSelThreads) keys[i] = kEmpty;
-    __syncthreads();
-    block_bitonic_sort(keys, m);
-  } else {
-    // Many equal high words near the k-th key: the generic selection.
-    auto key_at = [&](int i) -> uint64_t {
-      const float v = row[i];
-      return v < FLT_MAX ? make_key(v, static_cast<uint32_t>(i)) : kEmpty;
-    };
-    block_topk_sorted(key_at, ncols, k, sh, keys);
-  }
-  for (int j = tid; j < k; j += kSelThreads) {
-    const uint64_t key = j < kk ? keys[j] : kEmpty;
-    const size_t o = static_cast<size_t>(blockIdx.x) * kmax + j;
-    out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
-    if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
   }
 }
 
@@ -205,7 +227,8 @@ constexpr int kWarpCand = 512;
 
 __global__ void __launch_bounds__(kSelWarps * 32) select_rows_warp_kernel(
     const float* __restrict__ D, int nrows, int ncols, int ldD, int kmax, int32_t* __restrict__ out_idx,
-    float* __restrict__ out_val, const int32_t* __restrict__ k_row, int* __restrict__ overflow) {
+    float* __restrict__ out_val, const int32_t* __restrict__ k_row, int* __restrict__ overflow,
+    const uint32_t* __restrict__ vlo, const uint32_t* __restrict__ vhi) {
   __shared__ int s_hist[kSelWarps][kBins];
   __shared__ uint64_t s_cand[kSelWarps][kWarpCand];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -219,7 +242,38 @@ __global__ void __launch_bounds__(kSelWarps * 32) select_rows_warp_kernel(
   const float4* row4 = reinterpret_cast<const float4*>(D + static_cast<size_t>(r) * ldD);
   const int n4 = ncols >> 2;
   auto word = [](float v) -> uint32_t { return v < FLT_MAX ? __float_as_uint(v) : 0xFFFFFFFFu; };
-  unsigned lo = 0xFFFFFFFFu, hi = 0;
+  // Range of the finite values: the caller's hint, else a pass over the row.
+  unsigned lo = vlo ? vlo[r] : 0xFFFFFFFFu, hi = vhi ? vhi[r] : 0u;
+  if (lo > hi) {
+    lo = 0xFFFFFFFFu;
+    hi = 0;
+#pragma unroll 4
+    for (int i = lane; i < n4; i += 32) {
+      const float4 v = row4[i];
+      const uint32_t u[4] = {word(v.x), word(v.y), word(v.z), word(v.w)};
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (u[j] != 0xFFFFFFFFu) {
+          lo = min(lo, u[j]);
+          hi = max(hi, u[j]);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+  }
+  // Bin of a high word: (x - lo) >> sh clamped to [0, kBins), monotone in x
+  // for any lo <= hi, so the selection is exact even when the hint misses
+  // some values (they land in the first or the last bin).
+  const unsigned span = hi >= lo ? hi - lo : 0u;
+  const int sh = max(0, 32 - __clz(static_cast<int>(span | 1u)) - 10);
+  auto bin_of = [&](uint32_t x) -> int {
+    return x <= lo ? 0 : static_cast<int>(min(static_cast<unsigned>(kBins - 1), (x - lo) >> sh));
+  };
+  // Histogram of the finite values (and their count).
+  for (int i = lane; i < kBins; i += 32) hist[i] = 0;
+  __syncwarp();
   int real = 0;
 #pragma unroll 4
   for (int i = lane; i < n4; i += 32) {
@@ -228,32 +282,15 @@ __global__ void __launch_bounds__(kSelWarps * 32) select_rows_warp_kernel(
 #pragma unroll
     for (int j = 0; j < 4; ++j)
       if (u[j] != 0xFFFFFFFFu) {
-        lo = min(lo, u[j]);
-        hi = max(hi, u[j]);
+        atomicAdd(&hist[bin_of(u[j])], 1);
         ++real;
       }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    real += __shfl_xor_sync(0xffffffffu, real, o);
-  }
+  for (int o = 16; o > 0; o >>= 1) real += __shfl_xor_sync(0xffffffffu, real, o);
+  __syncwarp();
   const int kk = min(k, real);
-  const float scale = static_cast<float>(kBins) / (static_cast<float>(hi - lo) + 1.0f);
-  auto bin_of = [&](uint32_t x) -> int { return min(kBins - 1, static_cast<int>(static_cast<float>(x - lo) * scale)); };
   int bstar = kBins, ncand = real;
   if (kk > 0 && kk < real) {
-    for (int i = lane; i < kBins; i += 32) hist[i] = 0;
-    __syncwarp();
-#pragma unroll 4
-    for (int i = lane; i < n4; i += 32) {
-      const float4 v = row4[i];
-      const uint32_t u[4] = {word(v.x), word(v.y), word(v.z), word(v.w)};
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (u[j] != 0xFFFFFFFFu) atomicAdd(&hist[bin_of(u[j])], 1);
-    }
-    __syncwarp();
     // Lane L owns bins [32L, 32L + 32).
     int loc = 0;
     for (int b = 0; b < 32; ++b) loc += hist[lane * 32 + b];
@@ -595,13 +632,14 @@ void exclusive_sum(const int64_t* in, int64_t* out, size_t n, void* tmp, size_t 
 }  // namespace
 
 void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx, float* out_val,
-                        cudaStream_t st, const int32_t* k_row, int* row_flags) {
+                        cudaStream_t st, const int32_t* k_row, int* row_flags, const uint32_t* vlo,
+                        const uint32_t* vhi) {
   if (nrows <= 0 || k <= 0) return;
   const int* only = nullptr;
   if (row_flags && k <= 256 && ncols <= 8192 && ncols % 4 == 0 && ldD % 4 == 0) {
     // Warp per row; rows it flags go through the CTA kernel below.
     select_rows_warp_kernel<<<(nrows + kSelWarps - 1) / kSelWarps, kSelWarps * 32, 0, st>>>(
-        D, nrows, ncols, ldD, k, out_idx, out_val, k_row, row_flags);
+        D, nrows, ncols, ldD, k, out_idx, out_val, k_row, row_flags, vlo, vhi);
     HB_CUDA(cudaGetLastError());
     only = row_flags;
   }
@@ -610,14 +648,17 @@ void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, in
            "per-row widths need k <= 1024 and at most 8192 columns");
   if (k <= 1024 && ncols <= 32 * kSelThreads) {
     const int vpt = (ncols + kSelThreads - 1) / kSelThreads;
+    // Behind the warp kernel only its flagged rows (rare) are left: a small
+    // grid strides over the flags instead of a CTA per row.
+    const int g = only ? std::min((nrows + 31) / 32, kFlaggedGrid) : nrows;
     if (vpt <= 4)
-      select_rows_reg_kernel<4><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row, only);
+      select_rows_reg_kernel<4><<<g, kSelThreads, 0, st>>>(D, nrows, ncols, ldD, k, out_idx, out_val, k_row, only);
     else if (vpt <= 8)
-      select_rows_reg_kernel<8><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row, only);
+      select_rows_reg_kernel<8><<<g, kSelThreads, 0, st>>>(D, nrows, ncols, ldD, k, out_idx, out_val, k_row, only);
     else if (vpt <= 16)
-      select_rows_reg_kernel<16><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row, only);
+      select_rows_reg_kernel<16><<<g, kSelThreads, 0, st>>>(D, nrows, ncols, ldD, k, out_idx, out_val, k_row, only);
     else
-      select_rows_reg_kernel<32><<<nrows, kSelThreads, 0, st>>>(D, ncols, ldD, k, out_idx, out_val, k_row, only);
+      select_rows_reg_kernel<32><<<g, kSelThreads, 0, st>>>(D, nrows, ncols, ldD, k, out_idx, out_val, k_row, only);
     HB_CUDA(cudaGetLastError());
     return;
   }

@@ -820,26 +820,28 @@ __global__ void __launch_bounds__(kBigWarps * 32) rerank_big_bound_kernel(
     const int* __restrict__ big_list, const int* __restrict__ big_n, int* __restrict__ m_out) {
   __shared__ int s_h[kBigWarps][256];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int w = blockIdx.x * kBigWarps + wib;
-  if (w >= *big_n) return;
-  const int qi = big_list[w];
-  const int c = cnt[qi];
-  uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
-  const uint32_t* ubs = cand_ub + static_cast<size_t>(qi) * cap;
-  const uint32_t lim_bits = warp_kth_smallest([&](int i) { return ubs[i]; }, c, k, s_h[wib], lane);
-  // In-place compaction: a block of 32 is read before any of it is written,
-  // and writes land at or below the read position.
-  int m = 0;
-  for (int base = 0; base < c; base += 32) {
-    const int i = base + lane;
-    const uint64_t key = i < c ? buf[i] : kEmpty;
-    const bool in = i < c && static_cast<uint32_t>(key >> 32) <= lim_bits;
-    const unsigned bal = __ballot_sync(0xffffffffu, in);
+  const int nbig = *big_n;
+  for (int w = blockIdx.x * kBigWarps + wib; w < nbig; w += gridDim.x * kBigWarps) {
+    const int qi = big_list[w];
+    const int c = cnt[qi];
+    uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
+    const uint32_t* ubs = cand_ub + static_cast<size_t>(qi) * cap;
+    const uint32_t lim_bits = warp_kth_smallest([&](int i) { return ubs[i]; }, c, k, s_h[wib], lane);
+    // In-place compaction: a block of 32 is read before any of it is
+    // written, and writes land at or below the read position.
+    int m = 0;
+    for (int base = 0; base < c; base += 32) {
+      const int i = base + lane;
+      const uint64_t key = i < c ? buf[i] : kEmpty;
+      const bool in = i < c && static_cast<uint32_t>(key >> 32) <= lim_bits;
+      const unsigned bal = __ballot_sync(0xffffffffu, in);
+      __syncwarp();
+      if (in) buf[m + __popc(bal & ((1u << lane) - 1u))] = key;
+      m += __popc(bal);
+    }
+    if (lane == 0) m_out[qi] = m;
     __syncwarp();
-    if (in) buf[m + __popc(bal & ((1u << lane) - 1u))] = key;
-    m += __popc(bal);
   }
-  if (lane == 0) m_out[qi] = m;
 }
 
 __global__ void __launch_bounds__(256) rerank_big_exact_kernel(uint64_t* __restrict__ cand, int cap,
@@ -849,47 +851,49 @@ __global__ void __launch_bounds__(256) rerank_big_exact_kernel(uint64_t* __restr
                                                                const int* __restrict__ big_n,
                                                                const int* __restrict__ m_in) {
   __shared__ __align__(16) float s_q[kRerankMaxDim];
-  const int w = blockIdx.x;
-  if (w >= *big_n) return;
-  const int qi = big_list[w];
-  const int m = m_in[qi];
-  uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
-  for (int c = threadIdx.x; c < dpad; c += blockDim.x) s_q[c] = q[static_cast<size_t>(qi) * dpad + c];
-  __syncthreads();
-  // Rows j and j + blockDim.x together: two independent chains, each the
-  // reference's sequential loop (many small CTAs per SM keep the loads in
-  // flight).
-  for (int j0 = threadIdx.x; j0 < m; j0 += 2 * blockDim.x) {
-    const int j1 = j0 + blockDim.x;
-    const uint32_t p0 = key_tie(buf[j0]);
-    const uint32_t p1 = j1 < m ? key_tie(buf[j1]) : p0;
-    const float4* x0 = reinterpret_cast<const float4*>(codes + static_cast<size_t>(p0) * dpad);
-    const float4* x1 = reinterpret_cast<const float4*>(codes + static_cast<size_t>(p1) * dpad);
-    float a0 = 0.0f, a1 = 0.0f;
+  const int nbig = *big_n;
+  for (int w = blockIdx.x; w < nbig; w += gridDim.x) {
+    const int qi = big_list[w];
+    const int m = m_in[qi];
+    uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
+    __syncthreads();  // the previous query's readers of s_q are done
+    for (int c = threadIdx.x; c < dpad; c += blockDim.x) s_q[c] = q[static_cast<size_t>(qi) * dpad + c];
+    __syncthreads();
+    // Rows j and j + blockDim.x together: two independent chains, each the
+    // reference's sequential loop (many small CTAs per SM keep the loads in
+    // flight).
+    for (int j0 = threadIdx.x; j0 < m; j0 += 2 * blockDim.x) {
+      const int j1 = j0 + blockDim.x;
+      const uint32_t p0 = key_tie(buf[j0]);
+      const uint32_t p1 = j1 < m ? key_tie(buf[j1]) : p0;
+      const float4* x0 = reinterpret_cast<const float4*>(codes + static_cast<size_t>(p0) * dpad);
+      const float4* x1 = reinterpret_cast<const float4*>(codes + static_cast<size_t>(p1) * dpad);
+      float a0 = 0.0f, a1 = 0.0f;
 #pragma unroll 4
-    for (int i = 0; i < dpad / 4; ++i) {
-      const float4 u = __ldg(x0 + i), v = __ldg(x1 + i);
-      const float4 g = *reinterpret_cast<const float4*>(s_q + 4 * i);
-      float t;
-      t = __fsub_rn(g.x, u.x);
-      a0 = __fadd_rn(a0, __fmul_rn(t, t));
-      t = __fsub_rn(g.x, v.x);
-      a1 = __fadd_rn(a1, __fmul_rn(t, t));
-      t = __fsub_rn(g.y, u.y);
-      a0 = __fadd_rn(a0, __fmul_rn(t, t));
-      t = __fsub_rn(g.y, v.y);
-      a1 = __fadd_rn(a1, __fmul_rn(t, t));
-      t = __fsub_rn(g.z, u.z);
-      a0 = __fadd_rn(a0, __fmul_rn(t, t));
-      t = __fsub_rn(g.z, v.z);
-      a1 = __fadd_rn(a1, __fmul_rn(t, t));
-      t = __fsub_rn(g.w, u.w);
-      a0 = __fadd_rn(a0, __fmul_rn(t, t));
-      t = __fsub_rn(g.w, v.w);
-      a1 = __fadd_rn(a1, __fmul_rn(t, t));
+      for (int i = 0; i < dpad / 4; ++i) {
+        const float4 u = __ldg(x0 + i), v = __ldg(x1 + i);
+        const float4 g = *reinterpret_cast<const float4*>(s_q + 4 * i);
+        float t;
+        t = __fsub_rn(g.x, u.x);
+        a0 = __fadd_rn(a0, __fmul_rn(t, t));
+        t = __fsub_rn(g.x, v.x);
+        a1 = __fadd_rn(a1, __fmul_rn(t, t));
+        t = __fsub_rn(g.y, u.y);
+        a0 = __fadd_rn(a0, __fmul_rn(t, t));
+        t = __fsub_rn(g.y, v.y);
+        a1 = __fadd_rn(a1, __fmul_rn(t, t));
+        t = __fsub_rn(g.z, u.z);
+        a0 = __fadd_rn(a0, __fmul_rn(t, t));
+        t = __fsub_rn(g.z, v.z);
+        a1 = __fadd_rn(a1, __fmul_rn(t, t));
+        t = __fsub_rn(g.w, u.w);
+        a0 = __fadd_rn(a0, __fmul_rn(t, t));
+        t = __fsub_rn(g.w, v.w);
+        a1 = __fadd_rn(a1, __fmul_rn(t, t));
+      }
+      buf[j0] = a0 < FLT_MAX ? make_key(a0, p0) : kEmpty;
+      if (j1 < m) buf[j1] = a1 < FLT_MAX ? make_key(a1, p1) : kEmpty;
     }
-    buf[j0] = a0 < FLT_MAX ? make_key(a0, p0) : kEmpty;
-    if (j1 < m) buf[j1] = a1 < FLT_MAX ? make_key(a1, p1) : kEmpty;
   }
 }
 
@@ -900,18 +904,20 @@ __global__ void __launch_bounds__(256) rerank_big_topk_kernel(const uint64_t* __
                                                               const int* __restrict__ m_in) {
   extern __shared__ uint64_t s_top[];  // pow2_ceil(k)
   __shared__ SelectShared sh_sel;
-  const int w = blockIdx.x;
-  if (w >= *big_n) return;
-  const int qi = big_list[w];
-  const int m = m_in[qi];
-  const uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
-  auto key_at = [&](int i) -> uint64_t { return buf[i]; };
-  block_topk_sorted(key_at, m, k, sh_sel, s_top);
-  for (int j = threadIdx.x; j < k; j += blockDim.x) {
-    const uint64_t key = s_top[j];
-    const size_t o = static_cast<size_t>(qi) * k + j;
-    D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
-    I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+  const int nbig = *big_n;
+  for (int w = blockIdx.x; w < nbig; w += gridDim.x) {
+    const int qi = big_list[w];
+    const int m = m_in[qi];
+    const uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
+    auto key_at = [&](int i) -> uint64_t { return buf[i]; };
+    __syncthreads();  // the previous query's readers of s_top are done
+    block_topk_sorted(key_at, m, k, sh_sel, s_top);
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+      const uint64_t key = s_top[j];
+      const size_t o = static_cast<size_t>(qi) * k + j;
+      D[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+      I[o] = key == kEmpty ? -1 : ids[key_tie(key)];
+    }
   }
 }
 
@@ -1194,20 +1200,20 @@ void launch_rerank_bf16(uint64_t* cand, const uint32_t* cand_ub, const int* cnt,
   HB_CHECK(k >= 1 && cap >= k && cap <= kRerankMaxCap && (cap & (cap - 1)) == 0, HB_ERR_INVALID,
            "candidate buffer size out of range");
   HB_CHECK(dpad % 4 == 0 && dpad <= kRerankMaxDim, HB_ERR_INVALID, "re-rank rows wider than 128 floats");
-  rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(cand, cand_ub, cnt, cap, nq, k, codes, q,
-                                                                               dpad, ids, D, I, flag, over_list, over_n,
-                                                                               m_out, over_list + nq);
+  rerank_warp_kernel<<<(nq + kRrWarps - 1) / kRrWarps, kRrWarps * 32, 0, st>>>(
+      cand, cand_ub, cnt, cap, nq, k, codes, q, dpad, ids, D, I, flag, over_list, over_n, m_out, over_list + nq);
   HB_CUDA(cudaGetLastError());
   if (cap > kRrWarpCap) {
-    // At most nq queries are big; blocks past *big_n return at once.
+    // At most nq queries are big (*big_n of them, known on the device
+    // only): grids of at most eight CTAs per SM stride over the list.
     const int* big_list = over_list + nq;
     const int* big_n = over_n + 1;
-    rerank_big_bound_kernel<<<(nq + kBigWarps - 1) / kBigWarps, kBigWarps * 32, 0, st>>>(
+    const int gmax = 8 * std::max(1, num_sms);
+    rerank_big_bound_kernel<<<std::min((nq + kBigWarps - 1) / kBigWarps, gmax), kBigWarps * 32, 0, st>>>(
         cand, cand_ub, cnt, cap, k, big_list, big_n, m_out);
-    rerank_big_exact_kernel<<<nq, 256, 0, st>>>(cand, cap, codes, q, dpad, big_list, big_n,
-                                                m_out);
+    rerank_big_exact_kernel<<<std::min(nq, gmax), 256, 0, st>>>(cand, cap, codes, q, dpad, big_list, big_n, m_out);
     const size_t smem = static_cast<size_t>(pow2_ceil(k < 2 ? 2 : k)) * sizeof(uint64_t);
-    rerank_big_topk_kernel<<<nq, 256, smem, st>>>(cand, cap, k, ids, D, I, big_list, big_n, m_out);
+    rerank_big_topk_kernel<<<std::min(nq, gmax), 256, smem, st>>>(cand, cap, k, ids, D, I, big_list, big_n, m_out);
     HB_CUDA(cudaGetLastError());
   }
 }

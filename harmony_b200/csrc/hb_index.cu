@@ -1412,7 +1412,6 @@ class IndexCore {
     list_qoff_.reserve(nlist_ + 1);
     item_off_.reserve(nlist_ + 1);
     list_q_.reserve(static_cast<size_t>(nb) * P);
-    slot_base_.reserve(static_cast<size_t>(nb) * P + 1);
     const size_t wtmp = build_work_tmp_bytes(nb, P, static_cast<int>(nlist_));
     work_tmp_.reserve(wtmp);
     const bool two_stage = k > kFilterTightK && P > 1;
@@ -1430,7 +1429,7 @@ class IndexCore {
     {
       Scope sc(this, "build_work");
       launch_build_work(probes_a, nb, P_a, list_off_.p, static_cast<int>(nlist_), cr_a, 128, list_cnt_.p,
-                        list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+                        list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, nullptr, work_tmp_.p, wtmp, st_);
     }
     {
       Scope sc(this, "seed");
@@ -1478,7 +1477,7 @@ class IndexCore {
       {
         Scope sc(this, "build_work");
         launch_build_work(probes_rest_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p,
-                          list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+                          list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, nullptr, work_tmp_.p, wtmp, st_);
       }
       HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
       a.chunk_rows = cr;

@@ -133,6 +133,8 @@ void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, in
                         float* out_val, cudaStream_t st, const int32_t* k_row = nullptr, int* row_flags = nullptr,
                         const uint32_t* vlo = nullptr, const uint32_t* vhi = nullptr);
 // Build the list-major work description from probes (nq x P, -1 = none).
+// slot_base (the exact scan's per-(query, probe) output slots) may be null:
+// it is then not built.
 void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist,
                        int chunk_rows, int qgroup, int32_t* list_cnt, int64_t* list_qoff,
                        int32_t* list_cursor, int32_t* list_q, int64_t* item_off, int64_t* slot_base,
@@ -216,6 +218,9 @@ int scan_bf16_stages(int kpad);  // deepest B tile ring that fits
 void launch_tile_norms(const float* norms, const int64_t* list_off, int nlist, const int64_t* tile_off,
                        float* tile_norm, cudaStream_t st);
 void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, int kpad);
+// Tensor map of a row-major FP32 matrix (rows x cols, cols a multiple of 4)
+// for TMA stores of 32 x 32 boxes with the 128-byte swizzle.
+void make_f32_store_map(void* tmap_out, const float* base, size_t rows, size_t cols);
 // Per query: bound reset to FLT_MAX (none yet), candidate count 0.
 void launch_query_prep(int nq, uint32_t* thr, int* cnt, cudaStream_t st);
 // Residual BF16 codes BF16(x - c_l) (kpad columns), FP32 residual norms per row

@@ -51,11 +51,12 @@ namespace {
 using namespace sm100;
 
 constexpr int kCT = 128;        // queries per tile = centroids per tile
-constexpr int kCStages = 8;     // ring of 64-column K blocks of query tiles (16 KB each)
+constexpr int kCStages = 6;     // ring of 64-column K blocks of query tiles (16 KB each)
 constexpr int kCEpiWarps = 8;   // epilogue warps: two per TMEM lane quarter, one per half of the columns
 constexpr int kCTmaWarp = kCEpiWarps, kCMmaWarp = kCEpiWarps + 1;
 constexpr int kCThreads = (kCEpiWarps + 2) * 32;
 constexpr uint32_t kBlk = kCT * 128;  // bytes of one 128-row x 64-column BF16 block
+constexpr uint32_t kBoxBytes = 32 * 128;  // one 32 x 32 FP32 box of V
 
 struct CoarseShared {
   uint64_t full[kCStages];
@@ -75,15 +76,18 @@ __device__ __forceinline__ void coarse_range(int b, int G, int pairs, int& p0, i
 
 __global__ void __launch_bounds__(kCThreads, 1)
     coarse_tc_kernel(const __grid_constant__ CUtensorMap tmap_c, const __grid_constant__ CUtensorMap tmap_q,
-                     const float* __restrict__ qnorm, int nq, int kpad, const float* __restrict__ cnorm, int nlist,
-                     int qt, int pairs, float* __restrict__ V, uint32_t* __restrict__ vlo, uint32_t* __restrict__ vhi,
-                     int* __restrict__ err) {
+                     const __grid_constant__ CUtensorMap tmap_v, int tma_v, const float* __restrict__ qnorm, int nq,
+                     int kpad, const float* __restrict__ cnorm, int nlist, int qt, int pairs, float* __restrict__ V,
+                     uint32_t* __restrict__ vlo, uint32_t* __restrict__ vhi, int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ CoarseShared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int nh = kpad / 64;  // K blocks of one half (hi or lo)
   uint8_t* Bt = smem;        // resident centroid tile: [c_hi | c_lo], 2 * nh blocks
   uint8_t* ring = smem + static_cast<size_t>(2 * nh) * kBlk;
+  // Per epilogue warp, two 32 x 32 FP32 boxes (128-byte swizzle) for the
+  // TMA stores of its two chunks of a tile.
+  uint8_t* stg = ring + static_cast<size_t>(kCStages) * kBlk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int p0, p1;
   coarse_range(blockIdx.x, gridDim.x, pairs, p0, p1);
@@ -211,8 +215,38 @@ __global__ void __launch_bounds__(kCThreads, 1)
       // Range of this row's values (the selection's hint; columns past
       // nlist only widen it).
       uint32_t tlo = 0xFFFFFFFFu, thi = 0;
-      auto chunk = [&](const uint32_t (&r)[32], int cb) {
+      uint8_t* box0 = stg + static_cast<size_t>(warp) * 2 * kBoxBytes;
+      if (tma_v) {
+        // The previous tile's stores have read the boxes.
+        if (lane == 0) bulk_wait_read();
+        __syncwarp();
+      }
+      auto chunk = [&](const uint32_t (&r)[32], int cb, uint8_t* box) {
         float* out = V + static_cast<size_t>(qi) * nlist + cb;
+        if (tma_v) {
+          // Row `lane` of the box: 16-byte piece j4 at (j4 ^ (lane % 8)).
+#pragma unroll
+          for (int j4 = 0; j4 < 8; ++j4) {
+            float4 cn;
+            if (cb + 4 * j4 + 3 < nlist) {
+              cn = *reinterpret_cast<const float4*>(cnorm + cb + 4 * j4);
+            } else {
+              cn.x = cb + 4 * j4 + 0 < nlist ? cnorm[cb + 4 * j4 + 0] : 0.0f;
+              cn.y = cb + 4 * j4 + 1 < nlist ? cnorm[cb + 4 * j4 + 1] : 0.0f;
+              cn.z = cb + 4 * j4 + 2 < nlist ? cnorm[cb + 4 * j4 + 2] : 0.0f;
+              cn.w = 0.0f;
+            }
+            float4 o;
+            o.x = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 0]), qn + cn.x), 0.0f);
+            o.y = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), qn + cn.y), 0.0f);
+            o.z = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), qn + cn.z), 0.0f);
+            o.w = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), qn + cn.w), 0.0f);
+            tlo = min(min(tlo, __float_as_uint(o.x)), min(__float_as_uint(o.y), min(__float_as_uint(o.z), __float_as_uint(o.w))));
+            thi = max(max(thi, __float_as_uint(o.x)), max(__float_as_uint(o.y), max(__float_as_uint(o.z), __float_as_uint(o.w))));
+            *reinterpret_cast<float4*>(box + lane * 128 + ((j4 ^ (lane & 7)) << 4)) = o;
+          }
+          return;
+        }
         if (nlist - cb >= 32 && (nlist & 3) == 0) {
 #pragma unroll
           for (int j4 = 0; j4 < 8; ++j4) {
@@ -238,13 +272,26 @@ __global__ void __launch_bounds__(kCThreads, 1)
         }
       };
       const int cb = c * kCT + half * 64;
-      if (cb < nlist) chunk(ra, cb);
-      if (cb + 32 < nlist) chunk(rb, cb + 32);
+      if (cb < nlist) chunk(ra, cb, box0);
+      if (cb + 32 < nlist) chunk(rb, cb + 32, box0 + kBoxBytes);
+      if (tma_v) {
+        // Rows past nq and columns past nlist of a box are not written.
+        fence_proxy_async_smem();
+        __syncwarp();
+        const int row = qtile * kCT + (warp & 3) * 32;
+        if (lane == 0 && row < nq) {
+          if (cb < nlist) tma_store_2d(&tmap_v, box0, cb, row);
+          if (cb + 32 < nlist) tma_store_2d(&tmap_v, box0 + kBoxBytes, cb + 32, row);
+          bulk_commit();
+        }
+      }
       if (qi < nq && tlo <= thi) {
         atomicMin(vlo + qi, tlo);
         atomicMax(vhi + qi, thi);
       }
     }
+    // The stores are complete before the CTA (and its shared memory) ends.
+    if (tma_v && lane == 0) bulk_wait_all();
   }
   tc_fence_before();
   __syncthreads();
@@ -494,7 +541,7 @@ void launch_coarse_widths(const int32_t* width, int nq, int wmax, int pre_w, int
 }
 
 size_t coarse_tc_smem_bytes(int kpad) {
-  return 1024 + static_cast<size_t>(2 * kpad / 64 + kCStages) * kBlk;
+  return 1024 + static_cast<size_t>(2 * kpad / 64 + kCStages) * kBlk + static_cast<size_t>(kCEpiWarps) * 2 * kBoxBytes;
 }
 
 void make_centroid_split(const float* cent, int nlist, int dpad, int kpad, void* out, void* tmap_out, cudaStream_t st) {
@@ -520,6 +567,11 @@ void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kp
   HB_CUDA(cudaGetLastError());
   alignas(64) unsigned char tmap_q[128];
   make_bf16_tensor_map(tmap_q, qsplit, static_cast<size_t>(nq), 2 * kpad);
+  // V rows of 16-byte multiples go out by TMA stores; other widths by plain
+  // stores.
+  alignas(64) unsigned char tmap_v[128] = {};
+  const int tma_v = (nlist & 3) == 0 ? 1 : 0;
+  if (tma_v) make_f32_store_map(tmap_v, V, static_cast<size_t>(nq), static_cast<size_t>(nlist));
   const int qt = (nq + kCT - 1) / kCT;
   const int ct = (nlist + kCT - 1) / kCT;
   const int pairs = qt * ct;
@@ -527,8 +579,9 @@ void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kp
   const size_t smem = coarse_tc_smem_bytes(kpad);
   HB_CUDA(cudaFuncSetAttribute(coarse_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   coarse_tc_kernel<<<G, kCThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap),
-                                                *reinterpret_cast<const CUtensorMap*>(tmap_q), qnorm, nq, kpad, cnorm,
-                                                nlist, qt, pairs, V, vlo, vhi, err);
+                                                *reinterpret_cast<const CUtensorMap*>(tmap_q),
+                                                *reinterpret_cast<const CUtensorMap*>(tmap_v), tma_v, qnorm, nq, kpad,
+                                                cnorm, nlist, qt, pairs, V, vlo, vhi, err);
   HB_CUDA(cudaGetLastError());
 }
 

@@ -217,11 +217,11 @@ __global__ void __launch_bounds__(kSelThreads, 6) select_rows_reg_kernel(const f
 }
 
 // The same selection with one warp per row (4 rows per CTA), for k <= 256
-// and rows of at most 8192 columns with 16-byte aligned rows: three passes
-// over the row from L2 (range, histogram of the keys' high words in a
-// per-warp 1024-bin table, ballot compaction of the keys in and under the
-// k-th key's bin), then a warp bitonic sort.  A row whose candidates exceed
-// kWarpCand is flagged for the CTA kernel.
+// and rows of at most 8192 columns with 16-byte aligned rows: up to three
+// passes over the row from L2 (range, unless the caller gives it; histogram
+// of the keys' high words in a per-warp 1024-bin table; ballot compaction of
+// the keys in and under the k-th key's bin), then a warp bitonic sort.  A
+// row whose candidates exceed kWarpCand is flagged for the CTA kernel.
 constexpr int kSelWarps = 4;
 constexpr int kWarpCand = 512;
 
@@ -452,7 +452,7 @@ __global__ void count_probes_kernel(const int32_t* __restrict__ probes, int nqp,
       atomicAdd(&list_cnt[l], 1);
     }
   }
-  slot_cnt[idx] = nch;
+  if (slot_cnt) slot_cnt[idx] = nch;
 }
 
 __global__ void list_items_kernel(const int32_t* __restrict__ list_cnt, const int64_t* __restrict__ list_off,
@@ -478,6 +478,7 @@ __global__ void list_items_kernel(const int32_t* __restrict__ list_cnt, const in
 constexpr int kWorkThreads = 1024;
 constexpr int kSmallWorkPairs = 32768;  // (query, probe) pairs a single CTA builds
 constexpr int kSmallWorkLists = 16384;  // lists whose counters fit its shared memory
+constexpr int kScanListsOneCta = 65536; // lists whose two exclusive sums one CTA forms
 
 template <class Get>
 __device__ void block_exclusive_scan(Get get, int n, int64_t* __restrict__ out, int64_t* s_warp) {
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(kWorkThreads) build_work_small_kernel(
         return ((n + chunk_rows - 1) / chunk_rows) * ((cnt[l] + qgroup - 1) / qgroup);
       },
       nlist, item_off, s_warp);
-  block_exclusive_scan(nch_of, nqp, slot_base, s_warp);
+  if (slot_base) block_exclusive_scan(nch_of, nqp, slot_base, s_warp);
   for (int idx = threadIdx.x; idx < nqp; idx += blockDim.x) {
     if (nch_of(idx) == 0) continue;
     const int l = probes[idx];
@@ -553,6 +554,23 @@ __global__ void __launch_bounds__(kWorkThreads) build_work_small_kernel(
     const int q = idx / P, j = idx - q * P;
     list_q[list_qoff[l] + pos] = static_cast<int32_t>((static_cast<uint32_t>(q) << 16) | static_cast<uint32_t>(j));
   }
+}
+
+// Per list: queries (list_cnt) and work items (chunks x query groups), and
+// their exclusive sums list_qoff and item_off (nlist + 1 each), by one CTA.
+__global__ void __launch_bounds__(kWorkThreads) list_scan_kernel(const int32_t* __restrict__ list_cnt,
+                                                                 const int64_t* __restrict__ list_off, int nlist,
+                                                                 int chunk_rows, int qgroup,
+                                                                 int64_t* __restrict__ list_qoff,
+                                                                 int64_t* __restrict__ item_off) {
+  __shared__ int64_t s_warp[64];
+  block_exclusive_scan([&](int l) -> int64_t { return list_cnt[l]; }, nlist, list_qoff, s_warp);
+  block_exclusive_scan(
+      [&](int l) -> int64_t {
+        const int64_t n = list_off[l + 1] - list_off[l];
+        return ((n + chunk_rows - 1) / chunk_rows) * ((list_cnt[l] + qgroup - 1) / qgroup);
+      },
+      nlist, item_off, s_warp);
 }
 
 __global__ void scatter_probes_kernel(const int32_t* __restrict__ probes, int nqp, int P,
@@ -713,15 +731,24 @@ void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list
   }
   HB_CUDA(cudaMemsetAsync(list_cnt, 0, sizeof(int32_t) * nlist, st));
   HB_CUDA(cudaMemsetAsync(list_cursor, 0, sizeof(int32_t) * nlist, st));
-  HB_CUDA(cudaMemsetAsync(slot_cnt + nqp, 0, sizeof(int64_t), st));
+  if (slot_base) HB_CUDA(cudaMemsetAsync(slot_cnt + nqp, 0, sizeof(int64_t), st));
   const int tb = 256;
-  count_probes_kernel<<<(nqp + tb - 1) / tb, tb, 0, st>>>(probes, nqp, P, list_off, chunk_rows, list_cnt, slot_cnt);
-  list_items_kernel<<<(nlist + 1 + tb - 1) / tb, tb, 0, st>>>(list_cnt, list_off, nlist, chunk_rows, qgroup, cnt64,
-                                                              items64);
+  count_probes_kernel<<<(nqp + tb - 1) / tb, tb, 0, st>>>(probes, nqp, P, list_off, chunk_rows, list_cnt,
+                                                          slot_base ? slot_cnt : nullptr);
+  if (nlist <= kScanListsOneCta) {
+    // One CTA scans both per-list counts (a few thousand lists).
+    list_scan_kernel<<<1, kWorkThreads, 0, st>>>(list_cnt, list_off, nlist, chunk_rows, qgroup, list_qoff, item_off);
+  } else {
+    list_items_kernel<<<(nlist + 1 + tb - 1) / tb, tb, 0, st>>>(list_cnt, list_off, nlist, chunk_rows, qgroup, cnt64,
+                                                                items64);
+    HB_CUDA(cudaGetLastError());
+    exclusive_sum(cnt64, list_qoff, n1, cub_tmp, cub_bytes, st);
+    exclusive_sum(items64, item_off, n1, cub_tmp, cub_bytes, st);
+  }
   HB_CUDA(cudaGetLastError());
-  exclusive_sum(cnt64, list_qoff, n1, cub_tmp, cub_bytes, st);
-  exclusive_sum(items64, item_off, n1, cub_tmp, cub_bytes, st);
-  exclusive_sum(slot_cnt, slot_base, n2, cub_tmp, cub_bytes, st);
+  // The per-(query, probe) output slots: only the exact scan's partial
+  // results use them.
+  if (slot_base) exclusive_sum(slot_cnt, slot_base, n2, cub_tmp, cub_bytes, st);
   scatter_probes_kernel<<<(nqp + tb - 1) / tb, tb, 0, st>>>(probes, nqp, P, list_off, list_qoff, list_cursor,
                                                             list_q);
   HB_CUDA(cudaGetLastError());

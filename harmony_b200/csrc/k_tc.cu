@@ -640,12 +640,31 @@ __global__ void residual_bf16_kernel(const float* __restrict__ codes, const int6
 
 // The k-th smallest (k >= 1) of n 32-bit keys get(0 .. n-1), by one warp:
 // radix selection over four 8-bit digits with a 256-bin histogram h in
-// shared memory.  n >= k.
+// shared memory.  n >= k.  A digit that the smallest and the largest key
+// share (with everything above it) is every key's digit and needs no count:
+// keys of one query share their top bits, and counting those digits would
+// put every lane's atomic on one bin.
 template <class Get>
 __device__ uint32_t warp_kth_smallest(Get get, int n, int k, int* h, int lane) {
+  uint32_t lo = 0xFFFFFFFFu, hi = 0u;
+  for (int i = lane; i < n; i += 32) {
+    const uint32_t v = get(i);
+    lo = min(lo, v);
+    hi = max(hi, v);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
   uint32_t prefix = 0u, pmask = 0u;
   int need = k;  // rank of the wanted key among those matching the prefix
   for (int shift = 24; shift >= 0; shift -= 8) {
+    if ((lo >> shift) == (hi >> shift)) {
+      prefix |= lo & (255u << shift);
+      pmask |= 255u << shift;
+      continue;
+    }
     for (int i = lane; i < 256; i += 32) h[i] = 0;
     __syncwarp();
     for (int i = lane; i < n; i += 32) {
@@ -730,9 +749,16 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
   uint64_t* ex = s_x[wib];
   const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
   const uint32_t* usrc = cand_ub + static_cast<size_t>(qi) * cap;
-  // U (every candidate when there are fewer than k).
+  // U (every candidate when there are fewer than k), selected from the
+  // upper bounds staged in ex (free until the exact phase) so the radix
+  // passes read shared memory.
   uint32_t u_bits = 0xFFFFFFFFu;
-  if (c >= k) u_bits = warp_kth_smallest([&](int i) { return usrc[i]; }, c, k, s_h[wib], lane);
+  if (c >= k) {
+    uint32_t* ubs = reinterpret_cast<uint32_t*>(ex);
+    for (int i = lane; i < c; i += 32) ubs[i] = usrc[i];
+    __syncwarp();
+    u_bits = warp_kth_smallest([&](int i) { return ubs[i]; }, c, k, s_h[wib], lane);
+  }
   int m = 0;
   for (int base = 0; base < c; base += 32) {
     const int i = base + lane;
@@ -927,29 +953,33 @@ __global__ void __launch_bounds__(256) rerank_big_topk_kernel(const uint64_t* __
 // of the probe set have upper bounds at most that.  Queries whose nearest
 // list holds fewer than k rows keep FLT_MAX.
 //
-// List-major: one CTA per list stages the list's first S BF16 rows in shared
-// memory once; the queries whose nearest list it is (probe rank 0 in the
-// list-major work description) go eight at a time: thread t forms row t's
-// values for all eight with their rows broadcast from shared memory, then a
-// warp per query selects its k-th smallest by radix (four 8-bit passes).
-// Small batches (probes given): one CTA per query.
+// List-major: one CTA per list; the queries whose nearest list it is (probe
+// rank 0 in the list-major work description) go kSeedQ at a time: warp j
+// forms query j's BF16 residual row in shared memory, thread t streams row t
+// of the list's first S rows from global memory once (16-byte loads) and
+// forms its value for each of those queries (their rows broadcast from
+// shared memory), then a warp per query selects its k-th smallest by radix
+// (four 8-bit passes).  Nothing is staged in shared memory, so several CTAs
+// share an SM and keep their row loads in flight.  Small batches (probes
+// given): one CTA per query.
 constexpr int kSeedRows = 256;
 constexpr int kSeedWarps = 8;
+constexpr int kSeedQ = 4;  // queries per pass
 static_assert(kSeedWarps * 32 >= kSeedRows, "the seed forms a row per thread");
+static_assert(kSeedQ <= kSeedWarps, "a warp per query of a pass");
 
-__global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
+__global__ void __launch_bounds__(kSeedWarps * 32, 4) seed_bound_kernel(
     const float* __restrict__ q, int dpad, const float* __restrict__ cent, int kpad,
     const __nv_bfloat16* __restrict__ codes,
     const int64_t* __restrict__ list_off, const int64_t* __restrict__ list_qoff, const int32_t* __restrict__ list_q,
     const float* __restrict__ xnorm, const float* __restrict__ rmax, int S, int k, uint32_t* __restrict__ thr,
     const int32_t* __restrict__ probes, int P) {
-  extern __shared__ __align__(16) uint8_t s_seed_raw[];
-  __shared__ float s_xn[kSeedRows];
+  __shared__ __align__(16) float s_q[kSeedQ][kRerankMaxDim];
   __shared__ int s_qs[kSeedWarps * 32];
   __shared__ int s_nq;
-  __shared__ float s_cd[kSeedWarps];
-  __shared__ uint32_t s_keys[kSeedWarps][kSeedRows];
-  __shared__ int s_hist[kSeedWarps][256];
+  __shared__ float s_cd[kSeedQ];
+  __shared__ uint32_t s_keys[kSeedQ][kSeedRows];
+  __shared__ int s_hist[kSeedQ][256];
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const bool by_query = probes != nullptr;
   int l;
@@ -970,17 +1000,9 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
   const int64_t b = list_off[l];
   const int n = static_cast<int>(min(static_cast<int64_t>(S), list_off[l + 1] - b));
   if (n < k) return;  // no seed: the bound stays FLT_MAX
-  const int stride = kpad * 2 + 16;  // bytes per staged row (padding spreads banks)
-  uint8_t* rows = s_seed_raw;
-  float* qbuf = reinterpret_cast<float*>(s_seed_raw + static_cast<size_t>(S) * stride);
-  const int cpr = kpad / 8;  // 16-byte chunks per row
-  for (int i = tid; i < n * cpr; i += blockDim.x) {
-    const int r = i / cpr, c = i - r * cpr;
-    cp_async16(rows + static_cast<size_t>(r) * stride + c * 16, codes + static_cast<size_t>(b + r) * kpad + c * 8, true);
-  }
-  cp_async_commit();
-  for (int r = tid; r < n; r += blockDim.x) s_xn[r] = xnorm[b + r];
-  cp_async_wait<0>();
+  const bool row_ok = tid < n;
+  const uint4* xrow = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(b + (row_ok ? tid : 0)) * kpad);
+  const float xn = row_ok ? xnorm[b + tid] : 0.0f;
   for (int64_t r0 = e0; r0 < e1; r0 += blockDim.x) {
     if (tid == 0) s_nq = 0;
     __syncthreads();
@@ -991,48 +1013,54 @@ __global__ void __launch_bounds__(kSeedWarps * 32) seed_bound_kernel(
     }
     __syncthreads();
     const int nqr = s_nq;
-    // Up to kSeedWarps queries at a time: warp j forms query j's BF16
-    // residual row and ||q - c_l||^2, thread t the S values of row t for all
-    // of them, then warp j selects query j's k-th.
-    for (int t0 = 0; t0 < nqr; t0 += kSeedWarps) {
-      const int nb = min(kSeedWarps, nqr - t0);
+    for (int t0 = 0; t0 < nqr; t0 += kSeedQ) {
+      const int nb = min(kSeedQ, nqr - t0);
       if (wib < nb) {
         const int qi = s_qs[t0 + wib];
         const float* qrow = q + static_cast<size_t>(qi) * dpad;
         const float* crow = cent + static_cast<size_t>(l) * dpad;
-        float* qb = qbuf + wib * kpad;
         float cd = 0.0f;
         for (int c = lane; c < kpad; c += 32) {
           const float v = c < dpad ? qrow[c] - crow[c] : 0.0f;
           cd = fmaf(v, v, cd);
-          qb[c] = __bfloat162float(__float2bfloat16_rn(v));
+          s_q[wib][c] = __bfloat162float(__float2bfloat16_rn(v));
         }
         for (int o = 16; o > 0; o >>= 1) cd += __shfl_xor_sync(0xffffffffu, cd, o);
         if (lane == 0) s_cd[wib] = cd;
       }
       __syncthreads();
-      if (tid < n) {
-        const uint8_t* xr = rows + static_cast<size_t>(tid) * stride;
-        for (int j = 0; j < nb; ++j) {
-          const float* qb = qbuf + j * kpad;
-          // Four partial sums (any order is within eps).
-          float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
-#pragma unroll 4
-          for (int c = 0; c < kpad; c += 8) {
-            const uint4 xv = *reinterpret_cast<const uint4*>(xr + c * 2);
-            const float4 qa = *reinterpret_cast<const float4*>(qb + c);
-            const float4 qc = *reinterpret_cast<const float4*>(qb + c + 4);
-            d0 = fmaf(qa.x, __uint_as_float(xv.x << 16), d0);
-            d1 = fmaf(qa.y, __uint_as_float(xv.x & 0xffff0000u), d1);
-            d2 = fmaf(qa.z, __uint_as_float(xv.y << 16), d2);
-            d3 = fmaf(qa.w, __uint_as_float(xv.y & 0xffff0000u), d3);
-            d0 = fmaf(qc.x, __uint_as_float(xv.z << 16), d0);
-            d1 = fmaf(qc.y, __uint_as_float(xv.z & 0xffff0000u), d1);
-            d2 = fmaf(qc.z, __uint_as_float(xv.w << 16), d2);
-            d3 = fmaf(qc.w, __uint_as_float(xv.w & 0xffff0000u), d3);
+      if (row_ok) {
+        // Four partial sums per query (any order is within eps).
+        float d[kSeedQ][4];
+#pragma unroll
+        for (int j = 0; j < kSeedQ; ++j) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.0f;
+#pragma unroll 2
+        for (int c = 0; c < kpad; c += 8) {
+          const uint4 xv = __ldg(xrow + c / 8);
+          const float x0 = __uint_as_float(xv.x << 16), x1 = __uint_as_float(xv.x & 0xffff0000u);
+          const float x2 = __uint_as_float(xv.y << 16), x3 = __uint_as_float(xv.y & 0xffff0000u);
+          const float x4 = __uint_as_float(xv.z << 16), x5 = __uint_as_float(xv.z & 0xffff0000u);
+          const float x6 = __uint_as_float(xv.w << 16), x7 = __uint_as_float(xv.w & 0xffff0000u);
+#pragma unroll
+          for (int j = 0; j < kSeedQ; ++j) {
+            if (j < nb) {
+              const float4 qa = *reinterpret_cast<const float4*>(&s_q[j][c]);
+              const float4 qc = *reinterpret_cast<const float4*>(&s_q[j][c + 4]);
+              d[j][0] = fmaf(qa.x, x0, d[j][0]);
+              d[j][1] = fmaf(qa.y, x1, d[j][1]);
+              d[j][2] = fmaf(qa.z, x2, d[j][2]);
+              d[j][3] = fmaf(qa.w, x3, d[j][3]);
+              d[j][0] = fmaf(qc.x, x4, d[j][0]);
+              d[j][1] = fmaf(qc.y, x5, d[j][1]);
+              d[j][2] = fmaf(qc.z, x6, d[j][2]);
+              d[j][3] = fmaf(qc.w, x7, d[j][3]);
+            }
           }
-          s_keys[j][tid] = ordered_bits(s_cd[j] + fmaf(-2.0f, (d0 + d1) + (d2 + d3), s_xn[tid]));
         }
+#pragma unroll
+        for (int j = 0; j < kSeedQ; ++j)
+          if (j < nb)
+            s_keys[j][tid] = ordered_bits(s_cd[j] + fmaf(-2.0f, (d[j][0] + d[j][1]) + (d[j][2] + d[j][3]), xn));
       }
       __syncthreads();
       if (wib < nb) {
@@ -1134,6 +1162,19 @@ void make_bf16_tensor_map(void* tmap_out, const void* codes_bf16, size_t rows, i
   HB_CHECK(r == CUDA_SUCCESS, HB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
 }
 
+void make_f32_store_map(void* tmap_out, const float* base, size_t rows, size_t cols) {
+  HB_CHECK(cols % 4 == 0, HB_ERR_INVALID, "FP32 tensor map rows must be 16-byte multiples");
+  CUtensorMap* m = static_cast<CUtensorMap*>(tmap_out);
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols) * 4};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = tensor_map_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides,
+                                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  HB_CHECK(r == CUDA_SUCCESS, HB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+}
+
 void launch_to_bf16(const float* src, size_t n, int dpad, int kpad, void* dst, cudaStream_t st) {
   if (!n) return;
   size_t g = (n * kpad + 255) / 256;
@@ -1184,10 +1225,8 @@ void launch_seed_bound(const float* q, int d, int dpad, const float* cent, int n
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the BF16 scan supports d <= 128");
   HB_CHECK(S >= 1 && S <= kSeedRows && k >= 1, HB_ERR_INVALID, "seed sample out of range");
   if (k > S) return;  // no sample holds k rows: every bound stays FLT_MAX
-  const size_t smem = static_cast<size_t>(S) * (kpad * 2 + 16) + static_cast<size_t>(kSeedWarps) * kpad * 4;
-  HB_CUDA(cudaFuncSetAttribute(seed_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const bool by_query = probes && static_cast<long long>(nq) * 4 < nlist;
-  seed_bound_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, smem, st>>>(
+  seed_bound_kernel<<<by_query ? nq : nlist, kSeedWarps * 32, 0, st>>>(
       q, dpad, cent, kpad, static_cast<const __nv_bfloat16*>(codes_bf16), list_off, list_qoff, list_q, rnorm, rmax, S, k,
       thr, by_query ? probes : nullptr, P);
   HB_CUDA(cudaGetLastError());

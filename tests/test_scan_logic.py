@@ -6,8 +6,9 @@ restated step for step in Python with a lane per list element:
   must find the list l with item_off[l] <= item < item_off[l + 1], empty lists
   included;
 - warp_kth_smallest, the radix selection over four 8-bit digits with a
-  256-bin histogram (lane L owns bins 8L .. 8L+7), used by the seed bound and
-  by the two-stage bound of k > 16.
+  256-bin histogram (lane L owns bins 8L .. 8L+7), digits shared by the
+  smallest and largest key skipped; used by the seed bound, the re-rank and
+  the two-stage bound of k > 16.
 
 Both are compared with the obvious answer (bisect, sorted) on random inputs,
 ties and degenerate sizes included."""
@@ -29,8 +30,14 @@ def search_32way(item_off, nlist, item):
 
 
 def warp_kth_smallest(vals, k):
+    lo, hi = min(vals), max(vals)
     prefix, pmask, need = 0, 0, k
     for shift in (24, 16, 8, 0):
+        if (lo >> shift) == (hi >> shift):
+            # every key has this digit: no count
+            prefix |= lo & (255 << shift)
+            pmask |= 255 << shift
+            continue
         h = [0] * 256
         for v in vals:
             if (v & pmask) == prefix:
@@ -79,5 +86,16 @@ def test_radix_kth_matches_sort():
         else:
             bits = rng.choice([32, 12, 4])
             vals = [rng.getrandbits(bits) for _ in range(n)]
+        k = rng.randint(1, n)
+        assert warp_kth_smallest(vals, k) == sorted(vals)[k - 1]
+
+
+def test_radix_kth_clustered_keys():
+    # keys of one query share their top bits (one exponent): skipped digits
+    rng = random.Random(3)
+    for _ in range(300):
+        base = rng.getrandbits(32) & 0xFFF00000
+        n = rng.randint(1, 300)
+        vals = [base | rng.getrandbits(rng.choice([4, 12, 20])) for _ in range(n)]
         k = rng.randint(1, n)
         assert warp_kth_smallest(vals, k) == sorted(vals)[k - 1]

@@ -638,6 +638,38 @@ __global__ void residual_bf16_kernel(const float* __restrict__ codes, const int6
   }
 }
 
+// The k-th smallest (1 <= k) of the 256 keys a warp holds, eight per lane
+// (v; pad with 0xFFFFFFFF): each lane sorts its keys with Batcher's 19
+// compare-exchanges for eight, then k rounds take the smallest head over the
+// warp, the lowest lane holding it dropping it.  For small k.
+__device__ __forceinline__ uint32_t warp_kth_small8(uint32_t (&v)[8], int k, int lane) {
+  auto cx = [&](int a, int b) {
+    const uint32_t lo = min(v[a], v[b]), hi = max(v[a], v[b]);
+    v[a] = lo;
+    v[b] = hi;
+  };
+  cx(0, 1), cx(2, 3), cx(4, 5), cx(6, 7);
+  cx(0, 2), cx(1, 3), cx(4, 6), cx(5, 7);
+  cx(1, 2), cx(5, 6);
+  cx(0, 4), cx(1, 5), cx(2, 6), cx(3, 7);
+  cx(2, 4), cx(3, 5);
+  cx(1, 2), cx(3, 4), cx(5, 6);
+  uint32_t m = 0;
+  for (int r = 0; r < k; ++r) {
+    m = v[0];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const unsigned who = __ballot_sync(0xffffffffu, v[0] == m);
+    if (lane == __ffs(who) - 1) {
+#pragma unroll
+      for (int i = 0; i < 7; ++i) v[i] = v[i + 1];
+      v[7] = 0xFFFFFFFFu;
+    }
+  }
+  return m;
+}
+constexpr int kSmallKth = 32;  // largest k for warp_kth_small8
+
 // The k-th smallest (k >= 1) of n 32-bit keys get(0 .. n-1), by one warp:
 // radix selection over four 8-bit digits with a 256-bin histogram h in
 // shared memory.  n >= k.  A digit that the smallest and the largest key
@@ -646,11 +678,19 @@ __global__ void residual_bf16_kernel(const float* __restrict__ codes, const int6
 // put every lane's atomic on one bin.
 template <class Get>
 __device__ uint32_t warp_kth_smallest(Get get, int n, int k, int* h, int lane) {
+  // Keys are read eight per lane at a time, the loads issued together.
+  constexpr int kB = 8;
   uint32_t lo = 0xFFFFFFFFu, hi = 0u;
-  for (int i = lane; i < n; i += 32) {
-    const uint32_t v = get(i);
-    lo = min(lo, v);
-    hi = max(hi, v);
+  for (int i0 = 0; i0 < n; i0 += 32 * kB) {
+    uint32_t v[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) v[u] = i0 + 32 * u + lane < n ? get(i0 + 32 * u + lane) : 0u;
+#pragma unroll
+    for (int u = 0; u < kB; ++u)
+      if (i0 + 32 * u + lane < n) {
+        lo = min(lo, v[u]);
+        hi = max(hi, v[u]);
+      }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -667,9 +707,13 @@ __device__ uint32_t warp_kth_smallest(Get get, int n, int k, int* h, int lane) {
     }
     for (int i = lane; i < 256; i += 32) h[i] = 0;
     __syncwarp();
-    for (int i = lane; i < n; i += 32) {
-      const uint32_t v = get(i);
-      if ((v & pmask) == prefix) atomicAdd(&h[(v >> shift) & 255u], 1);
+    for (int i0 = 0; i0 < n; i0 += 32 * kB) {
+      uint32_t v[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) v[u] = i0 + 32 * u + lane < n ? get(i0 + 32 * u + lane) : 0u;
+#pragma unroll
+      for (int u = 0; u < kB; ++u)
+        if (i0 + 32 * u + lane < n && (v[u] & pmask) == prefix) atomicAdd(&h[(v[u] >> shift) & 255u], 1);
     }
     __syncwarp();
     int loc[8], sum = 0;
@@ -749,11 +793,18 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
   uint64_t* ex = s_x[wib];
   const uint64_t* src = cand + static_cast<size_t>(qi) * cap;
   const uint32_t* usrc = cand_ub + static_cast<size_t>(qi) * cap;
-  // U (every candidate when there are fewer than k), selected from the
-  // upper bounds staged in ex (free until the exact phase) so the radix
-  // passes read shared memory.
+  // U (every candidate when there are fewer than k): for small k from the
+  // upper bounds held eight per lane, else by radix from the upper bounds
+  // staged in ex (free until the exact phase) so its passes read shared
+  // memory.
   uint32_t u_bits = 0xFFFFFFFFu;
-  if (c >= k) {
+  if (c >= k && k <= kSmallKth) {
+    static_assert(kRrWarpCap == 256, "eight upper bounds per lane");
+    uint32_t v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = 32 * i + lane < c ? usrc[32 * i + lane] : 0xFFFFFFFFu;
+    u_bits = warp_kth_small8(v, k, lane);
+  } else if (c >= k) {
     uint32_t* ubs = reinterpret_cast<uint32_t*>(ex);
     for (int i = lane; i < c; i += 32) ubs[i] = usrc[i];
     __syncwarp();
@@ -993,14 +1044,21 @@ __global__ void __launch_bounds__(kSeedWarps * 32, 4) seed_bound_kernel(
     l = blockIdx.x;
     e0 = list_qoff[l];
     e1 = list_qoff[l + 1];
-    bool mine = false;
-    for (int64_t e = e0 + tid; e < e1 && !mine; e += blockDim.x) mine = (list_q[e] & 0xffff) == 0;
-    if (!__syncthreads_or(mine)) return;
   }
   const int64_t b = list_off[l];
   const int n = static_cast<int>(min(static_cast<int64_t>(S), list_off[l + 1] - b));
   if (n < k) return;  // no seed: the bound stays FLT_MAX
   const bool row_ok = tid < n;
+  if (row_ok) {
+    // Row tid's fetch from DRAM overlaps the query gathering below.
+    const char* rp = reinterpret_cast<const char*>(codes + static_cast<size_t>(b + tid) * kpad);
+    for (int o = 0; o < kpad * 2; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(rp + o));
+  }
+  if (!by_query) {
+    bool mine = false;
+    for (int64_t e = e0 + tid; e < e1 && !mine; e += blockDim.x) mine = (list_q[e] & 0xffff) == 0;
+    if (!__syncthreads_or(mine)) return;
+  }
   const uint4* xrow = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(b + (row_ok ? tid : 0)) * kpad);
   const float xn = row_ok ? xnorm[b + tid] : 0.0f;
   for (int64_t r0 = e0; r0 < e1; r0 += blockDim.x) {
@@ -1020,10 +1078,21 @@ __global__ void __launch_bounds__(kSeedWarps * 32, 4) seed_bound_kernel(
         const float* qrow = q + static_cast<size_t>(qi) * dpad;
         const float* crow = cent + static_cast<size_t>(l) * dpad;
         float cd = 0.0f;
-        for (int c = lane; c < kpad; c += 32) {
-          const float v = c < dpad ? qrow[c] - crow[c] : 0.0f;
-          cd = fmaf(v, v, cd);
-          s_q[wib][c] = __bfloat162float(__float2bfloat16_rn(v));
+        float qv[kRerankMaxDim / 32], cv[kRerankMaxDim / 32];
+#pragma unroll
+        for (int i = 0; i < kRerankMaxDim / 32; ++i) {
+          const int c = lane + 32 * i;
+          qv[i] = c < dpad ? qrow[c] : 0.0f;
+          cv[i] = c < dpad ? crow[c] : 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < kRerankMaxDim / 32; ++i) {
+          const int c = lane + 32 * i;
+          if (c < kpad) {
+            const float v = qv[i] - cv[i];
+            cd = fmaf(v, v, cd);
+            s_q[wib][c] = __bfloat162float(__float2bfloat16_rn(v));
+          }
         }
         for (int o = 16; o > 0; o >>= 1) cd += __shfl_xor_sync(0xffffffffu, cd, o);
         if (lane == 0) s_cd[wib] = cd;
@@ -1034,26 +1103,33 @@ __global__ void __launch_bounds__(kSeedWarps * 32, 4) seed_bound_kernel(
         float d[kSeedQ][4];
 #pragma unroll
         for (int j = 0; j < kSeedQ; ++j) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.0f;
-#pragma unroll 2
-        for (int c = 0; c < kpad; c += 8) {
-          const uint4 xv = __ldg(xrow + c / 8);
-          const float x0 = __uint_as_float(xv.x << 16), x1 = __uint_as_float(xv.x & 0xffff0000u);
-          const float x2 = __uint_as_float(xv.y << 16), x3 = __uint_as_float(xv.y & 0xffff0000u);
-          const float x4 = __uint_as_float(xv.z << 16), x5 = __uint_as_float(xv.z & 0xffff0000u);
-          const float x6 = __uint_as_float(xv.w << 16), x7 = __uint_as_float(xv.w & 0xffff0000u);
+        // 64-byte pieces of the row: four loads in flight, then their values.
+        for (int c0 = 0; c0 < kpad; c0 += 32) {
+          uint4 xq[4];
 #pragma unroll
-          for (int j = 0; j < kSeedQ; ++j) {
-            if (j < nb) {
-              const float4 qa = *reinterpret_cast<const float4*>(&s_q[j][c]);
-              const float4 qc = *reinterpret_cast<const float4*>(&s_q[j][c + 4]);
-              d[j][0] = fmaf(qa.x, x0, d[j][0]);
-              d[j][1] = fmaf(qa.y, x1, d[j][1]);
-              d[j][2] = fmaf(qa.z, x2, d[j][2]);
-              d[j][3] = fmaf(qa.w, x3, d[j][3]);
-              d[j][0] = fmaf(qc.x, x4, d[j][0]);
-              d[j][1] = fmaf(qc.y, x5, d[j][1]);
-              d[j][2] = fmaf(qc.z, x6, d[j][2]);
-              d[j][3] = fmaf(qc.w, x7, d[j][3]);
+          for (int u = 0; u < 4; ++u) xq[u] = __ldg(xrow + c0 / 8 + u);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int c = c0 + 8 * u;
+            const uint4 xv = xq[u];
+            const float x0 = __uint_as_float(xv.x << 16), x1 = __uint_as_float(xv.x & 0xffff0000u);
+            const float x2 = __uint_as_float(xv.y << 16), x3 = __uint_as_float(xv.y & 0xffff0000u);
+            const float x4 = __uint_as_float(xv.z << 16), x5 = __uint_as_float(xv.z & 0xffff0000u);
+            const float x6 = __uint_as_float(xv.w << 16), x7 = __uint_as_float(xv.w & 0xffff0000u);
+#pragma unroll
+            for (int j = 0; j < kSeedQ; ++j) {
+              if (j < nb) {
+                const float4 qa = *reinterpret_cast<const float4*>(&s_q[j][c]);
+                const float4 qc = *reinterpret_cast<const float4*>(&s_q[j][c + 4]);
+                d[j][0] = fmaf(qa.x, x0, d[j][0]);
+                d[j][1] = fmaf(qa.y, x1, d[j][1]);
+                d[j][2] = fmaf(qa.z, x2, d[j][2]);
+                d[j][3] = fmaf(qa.w, x3, d[j][3]);
+                d[j][0] = fmaf(qc.x, x4, d[j][0]);
+                d[j][1] = fmaf(qc.y, x5, d[j][1]);
+                d[j][2] = fmaf(qc.z, x6, d[j][2]);
+                d[j][3] = fmaf(qc.w, x7, d[j][3]);
+              }
             }
           }
         }
@@ -1065,7 +1141,15 @@ __global__ void __launch_bounds__(kSeedWarps * 32, 4) seed_bound_kernel(
       __syncthreads();
       if (wib < nb) {
         const int qi = s_qs[t0 + wib];
-        const uint32_t kth = warp_kth_smallest([&](int i) { return s_keys[wib][i]; }, n, k, s_hist[wib], lane);
+        uint32_t kth;
+        if (k <= kSmallKth) {
+          uint32_t v[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) v[i] = 32 * i + lane < n ? s_keys[wib][32 * i + lane] : 0xFFFFFFFFu;
+          kth = warp_kth_small8(v, k, lane);
+        } else {
+          kth = warp_kth_smallest([&](int i) { return s_keys[wib][i]; }, n, k, s_hist[wib], lane);
+        }
         // U = the k-th smallest w + eps(q, l): every one of those k rows has
         // an upper bound at most that.
         if (lane == 0)

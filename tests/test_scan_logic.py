@@ -5,6 +5,8 @@ restated step for step in Python with a lane per list element:
   positions per round; the lanes at or under the item form a prefix), which
   must find the list l with item_off[l] <= item < item_off[l + 1], empty lists
   included;
+- warp_kth_small8, the k-th smallest of up to 256 keys held eight per lane
+  for small k (a sorting network per lane, then k rounds of a warp minimum);
 - warp_kth_smallest, the radix selection over four 8-bit digits with a
   256-bin histogram (lane L owns bins 8L .. 8L+7), digits shared by the
   smallest and largest key skipped; used by the seed bound, the re-rank and
@@ -59,6 +61,43 @@ def warp_kth_smallest(vals, k):
         prefix |= b << shift
         pmask |= 255 << shift
     return prefix
+
+
+NET8 = [(0, 1), (2, 3), (4, 5), (6, 7), (0, 2), (1, 3), (4, 6), (5, 7), (1, 2), (5, 6),
+        (0, 4), (1, 5), (2, 6), (3, 7), (2, 4), (3, 5), (1, 2), (3, 4), (5, 6)]
+
+
+def warp_kth_small8(lanes, k):
+    """lanes: 32 lists of 8 keys (0xFFFFFFFF pads)."""
+    lanes = [list(v) for v in lanes]
+    for v in lanes:
+        for a, b in NET8:
+            v[a], v[b] = min(v[a], v[b]), max(v[a], v[b])
+    m = 0
+    for _ in range(k):
+        m = min(v[0] for v in lanes)
+        who = next(i for i, v in enumerate(lanes) if v[0] == m)  # lowest lane pops
+        lanes[who] = lanes[who][1:] + [0xFFFFFFFF]
+    return m
+
+
+def test_sorting_network_of_eight():
+    # 0-1 principle: a comparator network sorts every input iff it sorts every 0/1 input
+    for bits in range(256):
+        v = [(bits >> i) & 1 for i in range(8)]
+        for a, b in NET8:
+            v[a], v[b] = min(v[a], v[b]), max(v[a], v[b])
+        assert v == sorted(v)
+
+
+def test_small_kth_matches_sort():
+    rng = random.Random(4)
+    for _ in range(400):
+        n = rng.randint(1, 256)
+        vals = [rng.choice([rng.getrandbits(32), rng.getrandbits(6)]) for _ in range(n)]
+        k = rng.randint(1, min(n, 32))
+        lanes = [[vals[32 * i + lane] if 32 * i + lane < n else 0xFFFFFFFF for i in range(8)] for lane in range(32)]
+        assert warp_kth_small8(lanes, k) == sorted(vals)[k - 1]
 
 
 def test_32way_search_finds_the_list():

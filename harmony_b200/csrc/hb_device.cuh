@@ -126,6 +126,37 @@ __device__ __forceinline__ void warp_stage_rows(const float* __restrict__ base, 
   __syncwarp();
 }
 
+// The k-th smallest (1 <= k) of the 256 keys a warp holds, eight per lane
+// (v; pad with 0xFFFFFFFF): each lane sorts its keys with Batcher's 19
+// compare-exchanges for eight, then k rounds take the smallest head over the
+// warp, the lowest lane holding it dropping it.  For small k.
+__device__ __forceinline__ uint32_t warp_kth_small8(uint32_t (&v)[8], int k, int lane) {
+  auto cx = [&](int a, int b) {
+    const uint32_t lo = min(v[a], v[b]), hi = max(v[a], v[b]);
+    v[a] = lo;
+    v[b] = hi;
+  };
+  cx(0, 1), cx(2, 3), cx(4, 5), cx(6, 7);
+  cx(0, 2), cx(1, 3), cx(4, 6), cx(5, 7);
+  cx(1, 2), cx(5, 6);
+  cx(0, 4), cx(1, 5), cx(2, 6), cx(3, 7);
+  cx(2, 4), cx(3, 5);
+  cx(1, 2), cx(3, 4), cx(5, 6);
+  uint32_t m = 0;
+  for (int r = 0; r < k; ++r) {
+    m = v[0];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const unsigned who = __ballot_sync(0xffffffffu, v[0] == m);
+    if (lane == __ffs(who) - 1) {
+#pragma unroll
+      for (int i = 0; i < 7; ++i) v[i] = v[i + 1];
+      v[7] = 0xFFFFFFFFu;
+    }
+  }
+  return m;
+}
+
 __host__ __device__ __forceinline__ int pow2_ceil(int x) {
   int p = 1;
   while (p < x) p <<= 1;

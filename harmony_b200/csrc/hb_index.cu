@@ -437,27 +437,26 @@ class IndexCore {
     ensure_coarse_tc();
     qsplit_.reserve(static_cast<size_t>(nq) * 2 * ckpad_);
     qsnorm_.reserve(static_cast<size_t>(nq));
-    vlo_.reserve(static_cast<size_t>(nq));
-    vhi_.reserve(static_cast<size_t>(nq));
+    cmins_.reserve(static_cast<size_t>(nq) * ((nlist_ + 15) / 16));
     ccand_.reserve(static_cast<size_t>(nq) * Pm);
     cval_.reserve(static_cast<size_t>(nq) * Pm);
     cflags_.reserve(static_cast<size_t>(nq));
     {
       Scope sc(this, "coarse_tc");
       launch_coarse_tc(ctmap_, qpad, nq, static_cast<int>(dpad_), ckpad_, cnorm_.p, static_cast<int>(nlist_), dmat_.p,
-                       qsplit_.p, qsnorm_.p, vlo_.p, vhi_.p, cerr_dev_.p, num_sms_, st_);
+                       qsplit_.p, qsnorm_.p, cmins_.p, cerr_dev_.p, num_sms_, st_);
     }
     {
       Scope sc(this, "coarse_select");
       launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), Pm, ccand_.p, cval_.p, st_,
-                         nullptr, cflags_.p, vlo_.p, vhi_.p);
+                         nullptr, cflags_.p, cmins_.p);
     }
     {
       Scope sc(this, "coarse_refine");
       launch_coarse_refine(qpad, nq, static_cast<int>(dpad_), cent_.p, ccand_.p, cval_.p, Pm, P,
                            static_cast<int>(nlist_), cmaxnorm_.p, probes_out, cdist_out, cflags_.p, st_);
       launch_coarse_fallback(qpad, nq, static_cast<int>(dpad_), cent_.p, static_cast<int>(nlist_), P, cflags_.p,
-                             dmat_.p, probes_out, cdist_out, st_);
+                             dmat_.p, probes_out, cdist_out, st_, nullptr, cmins_.p);
     }
     launches_ += 6;
     coarse_last_nq_ = nq;
@@ -484,8 +483,7 @@ class IndexCore {
     ensure_coarse_tc();
     qsplit_.reserve(static_cast<size_t>(nq) * 2 * ckpad_);
     qsnorm_.reserve(static_cast<size_t>(nq));
-    vlo_.reserve(static_cast<size_t>(nq));
-    vhi_.reserve(static_cast<size_t>(nq));
+    cmins_.reserve(static_cast<size_t>(nq) * ((nlist_ + 15) / 16));
     const int nl = static_cast<int>(nlist_);
     const int PmA = std::min(nl, C + coarse_extra(C));
     const int PmB = std::min(nl, P + coarse_extra(P));
@@ -499,18 +497,18 @@ class IndexCore {
     {
       Scope sc(this, "coarse_tc");
       launch_coarse_tc(ctmap_, qpad, nq, static_cast<int>(dpad_), ckpad_, cnorm_.p, nl, dmat_.p, qsplit_.p, qsnorm_.p,
-                       vlo_.p, vhi_.p, cerr_dev_.p, num_sms_, st_);
+                       cmins_.p, cerr_dev_.p, num_sms_, st_);
     }
     {
       Scope sc(this, "coarse_select");
-      launch_select_rows(dmat_.p, nq, nl, nl, PmA, ccand_.p, cval_.p, st_, nullptr, cflags_.p, vlo_.p, vhi_.p);
+      launch_select_rows(dmat_.p, nq, nl, nl, PmA, ccand_.p, cval_.p, st_, nullptr, cflags_.p, cmins_.p);
     }
     {
       Scope sc(this, "coarse_refine");
       launch_coarse_refine(qpad, nq, static_cast<int>(dpad_), cent_.p, ccand_.p, cval_.p, PmA, C, nl, cmaxnorm_.p,
                            probes1_.p, cdist_.p, cflags_.p, st_);
       launch_coarse_fallback(qpad, nq, static_cast<int>(dpad_), cent_.p, nl, C, cflags_.p, dmat_.p, probes1_.p,
-                             cdist_.p, st_);
+                             cdist_.p, st_, nullptr, cmins_.p);
     }
     {
       Scope sc(this, "probe_mlp");
@@ -519,7 +517,7 @@ class IndexCore {
     {
       Scope sc(this, "coarse_widen_select");
       launch_coarse_widths(npq_.p, nq, P, C, coarse_margin_, nl, kq_.p, st_);
-      launch_select_rows(dmat_.p, nq, nl, nl, PmB, ccand_.p, cval_.p, st_, kq_.p, cflags_.p, vlo_.p, vhi_.p);
+      launch_select_rows(dmat_.p, nq, nl, nl, PmB, ccand_.p, cval_.p, st_, kq_.p, cflags_.p, cmins_.p);
     }
     {
       Scope sc(this, "coarse_widen_refine");
@@ -2103,8 +2101,7 @@ class IndexCore {
   DevBuf<uint16_t> csplit_;
   DevBuf<uint16_t> qsplit_;  // queries' [hi | lo] BF16 rows for the tensor-core quantizer
   DevBuf<float> qsnorm_;     // their ||q||^2
-  DevBuf<uint32_t> vlo_;     // per query: smallest / largest finite value of its row of dmat_
-  DevBuf<uint32_t> vhi_;
+  DevBuf<uint32_t> cmins_;   // per 16-column chunk of dmat_ and query: the chunk's smallest value
   DevBuf<float> cnorm_, cmaxnorm_, cval_;
   DevBuf<int32_t> ccand_;
   DevBuf<int> cflags_, cerr_dev_;

@@ -126,12 +126,15 @@ size_t scan_exact_smem_bytes(int d, int dpad, int k, int mode, int* tv, int* qt,
 // Row-wise selection of the k smallest (value, column) pairs of a float
 // matrix; out_idx gets columns, out_val the values, ascending.
 // row_flags (optional, nrows ints of scratch): enables the warp-per-row
-// path for k <= 256.  vlo / vhi (optional, nrows each): bit patterns of a
-// range expected to hold each row's finite values (a hint: values outside
-// it are still selected exactly); given, the warp path skips its range pass.
+// path for k <= 256.
+// cmins (optional, ceil(ncols / 16) x nrows, chunk-major): each 16-column
+// chunk's smallest value (bit pattern), as coarse_tc writes it; given with
+// row_flags and k <= a quarter of the chunk count (<= 256 chunks), a row
+// reads only the chunks whose minimum is at most the k-th smallest chunk
+// minimum.
 void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx,
                         float* out_val, cudaStream_t st, const int32_t* k_row = nullptr, int* row_flags = nullptr,
-                        const uint32_t* vlo = nullptr, const uint32_t* vhi = nullptr);
+                        const uint32_t* cmins = nullptr);
 // Build the list-major work description from probes (nq x P, -1 = none).
 // slot_base (the exact scan's per-(query, probe) output slots) may be null:
 // it is then not built.
@@ -320,11 +323,11 @@ void make_centroid_split(const float* cent, int nlist, int dpad, int kpad, void*
 // V (nq x nlist) = max(0, ||q||^2 + ||c||^2 - 2 q.c) on the tensor cores;
 // qsplit (nq x 2*kpad BF16) and qnorm (nq) are scratch for the queries'
 // [hi|lo] rows and norms.
-// vlo / vhi (nq each) get the bit patterns of each row's smallest and
-// largest finite value, the range hint of launch_select_rows.
+// cmins (optional, ceil(nlist / 16) x nq, chunk-major) gets the bit pattern
+// of the smallest value of each 16-column chunk of each row, for
+// launch_select_rows' chunk path.
 void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kpad, const float* cnorm, int nlist,
-                      float* V, void* qsplit, float* qnorm, uint32_t* vlo, uint32_t* vhi, int* err, int num_sms,
-                      cudaStream_t st);
+                      float* V, void* qsplit, float* qnorm, uint32_t* cmins, int* err, int num_sms, cudaStream_t st);
 // Per-row widths of a coarse pass: row r keeps width[r] <= P probes out of
 // width[r] + margin candidates; rows whose width is <= pre_w are copied from
 // an earlier pass of width pre_w (pre, nq x pre_w).  width == nullptr: every
@@ -340,8 +343,10 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
                           int Pm, int P, int nlist, const float* cmaxnorm, int32_t* probes, float* cdist, int* flags,
                           cudaStream_t st, CoarseRows rows = CoarseRows());
 // Exact row and top P (or width[r]) for every flagged query (V rows are overwritten).
+// cmins (optional): the rewritten rows' chunk minima are rewritten too.
 void launch_coarse_fallback(const float* q, int nq, int dpad, const float* cent, int nlist, int P, const int* flags,
-                            float* V, int32_t* probes, float* cdist, cudaStream_t st, const int32_t* width = nullptr);
+                            float* V, int32_t* probes, float* cdist, cudaStream_t st, const int32_t* width = nullptr,
+                            uint32_t* cmins = nullptr);
 // With w = min(width[r], wmax): kq[r] = 0 if w <= pre_w, else
 // min(nlist, w + margin).
 void launch_coarse_widths(const int32_t* width, int nq, int wmax, int pre_w, int margin, int nlist, int32_t* kq,

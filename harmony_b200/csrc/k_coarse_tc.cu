@@ -78,7 +78,8 @@ __global__ void __launch_bounds__(kCThreads, 1)
     coarse_tc_kernel(const __grid_constant__ CUtensorMap tmap_c, const __grid_constant__ CUtensorMap tmap_q,
                      const __grid_constant__ CUtensorMap tmap_v, int tma_v, const float* __restrict__ qnorm, int nq,
                      int kpad, const float* __restrict__ cnorm, int nlist, int qt, int pairs, float* __restrict__ V,
-                     uint32_t* __restrict__ vlo, uint32_t* __restrict__ vhi, int* __restrict__ err) {
+                     uint32_t* __restrict__ cmins,
+                     int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ CoarseShared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -212,9 +213,6 @@ __global__ void __launch_bounds__(kCThreads, 1)
       tmem_ld_wait(rb);
       tc_fence_before();
       mbar_arrive(&sh.acce[b]);
-      // Range of this row's values (the selection's hint; columns past
-      // nlist only widen it).
-      uint32_t tlo = 0xFFFFFFFFu, thi = 0;
       uint8_t* box0 = stg + static_cast<size_t>(warp) * 2 * kBoxBytes;
       if (tma_v) {
         // The previous tile's stores have read the boxes.
@@ -223,6 +221,25 @@ __global__ void __launch_bounds__(kCThreads, 1)
       }
       auto chunk = [&](const uint32_t (&r)[32], int cb, uint8_t* box) {
         float* out = V + static_cast<size_t>(qi) * nlist + cb;
+        // The smallest value of each 16-column half of the chunk over its
+        // columns inside nlist, stored chunk-major (a warp's 32 queries are
+        // one 128-byte store).
+        uint32_t cm[2] = {0xFFFFFFFFu, 0xFFFFFFFFu};
+        const bool full = cb + 32 <= nlist;
+        auto cmin4 = [&](const float4& o, int c) {
+          const uint32_t e0 = full || c + 0 < nlist ? __float_as_uint(o.x) : 0xFFFFFFFFu;
+          const uint32_t e1 = full || c + 1 < nlist ? __float_as_uint(o.y) : 0xFFFFFFFFu;
+          const uint32_t e2 = full || c + 2 < nlist ? __float_as_uint(o.z) : 0xFFFFFFFFu;
+          const uint32_t e3 = full || c + 3 < nlist ? __float_as_uint(o.w) : 0xFFFFFFFFu;
+          uint32_t& m = cm[(c - cb) >> 4];
+          m = min(min(m, min(e0, e1)), min(e2, e3));
+        };
+        auto put_cm = [&]() {
+          if (cmins && qi < nq) {
+            cmins[static_cast<size_t>(cb / 16) * nq + qi] = cm[0];
+            if (cb + 16 < nlist) cmins[static_cast<size_t>(cb / 16 + 1) * nq + qi] = cm[1];
+          }
+        };
         if (tma_v) {
           // Row `lane` of the box: 16-byte piece j4 at (j4 ^ (lane % 8)).
 #pragma unroll
@@ -241,10 +258,10 @@ __global__ void __launch_bounds__(kCThreads, 1)
             o.y = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), qn + cn.y), 0.0f);
             o.z = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), qn + cn.z), 0.0f);
             o.w = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), qn + cn.w), 0.0f);
-            tlo = min(min(tlo, __float_as_uint(o.x)), min(__float_as_uint(o.y), min(__float_as_uint(o.z), __float_as_uint(o.w))));
-            thi = max(max(thi, __float_as_uint(o.x)), max(__float_as_uint(o.y), max(__float_as_uint(o.z), __float_as_uint(o.w))));
+            cmin4(o, cb + 4 * j4);
             *reinterpret_cast<float4*>(box + lane * 128 + ((j4 ^ (lane & 7)) << 4)) = o;
           }
+          put_cm();
           return;
         }
         if (nlist - cb >= 32 && (nlist & 3) == 0) {
@@ -256,8 +273,7 @@ __global__ void __launch_bounds__(kCThreads, 1)
             o.y = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 1]), qn + cn.y), 0.0f);
             o.z = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 2]), qn + cn.z), 0.0f);
             o.w = fmaxf(fmaf(-2.0f, __uint_as_float(r[4 * j4 + 3]), qn + cn.w), 0.0f);
-            tlo = min(min(tlo, __float_as_uint(o.x)), min(__float_as_uint(o.y), min(__float_as_uint(o.z), __float_as_uint(o.w))));
-            thi = max(max(thi, __float_as_uint(o.x)), max(__float_as_uint(o.y), max(__float_as_uint(o.z), __float_as_uint(o.w))));
+            cmin4(o, cb + 4 * j4);
             if (qi < nq) *reinterpret_cast<float4*>(out + 4 * j4) = o;
           }
         } else {
@@ -265,11 +281,11 @@ __global__ void __launch_bounds__(kCThreads, 1)
           for (int j = 0; j < 32; ++j)
             if (cb + j < nlist) {
               const float v = fmaxf(fmaf(-2.0f, __uint_as_float(r[j]), qn + cnorm[cb + j]), 0.0f);
-              tlo = min(tlo, __float_as_uint(v));
-              thi = max(thi, __float_as_uint(v));
+              cm[j >> 4] = min(cm[j >> 4], __float_as_uint(v));
               if (qi < nq) out[j] = v;
             }
         }
+        put_cm();
       };
       const int cb = c * kCT + half * 64;
       if (cb < nlist) chunk(ra, cb, box0);
@@ -284,10 +300,6 @@ __global__ void __launch_bounds__(kCThreads, 1)
           if (cb + 32 < nlist) tma_store_2d(&tmap_v, box0 + kBoxBytes, cb + 32, row);
           bulk_commit();
         }
-      }
-      if (qi < nq && tlo <= thi) {
-        atomicMin(vlo + qi, tlo);
-        atomicMax(vhi + qi, thi);
       }
     }
     // The stores are complete before the CTA (and its shared memory) ends.
@@ -476,7 +488,8 @@ __global__ void __launch_bounds__(256) coarse_fallback_kernel(const float* __res
                                                               const float* __restrict__ cent, int nlist, int P,
                                                               const int* __restrict__ flags, float* __restrict__ V,
                                                               int32_t* __restrict__ probes, float* __restrict__ cdist,
-                                                              const int32_t* __restrict__ width) {
+                                                              const int32_t* __restrict__ width,
+                                                              uint32_t* __restrict__ cmins) {
   extern __shared__ uint64_t s_fb[];
   __shared__ SelectShared sh_sel;
   __shared__ unsigned s_mask;
@@ -495,14 +508,23 @@ __global__ void __launch_bounds__(256) coarse_fallback_kernel(const float* __res
       mask &= mask - 1;
       const float* qrow = q + static_cast<size_t>(qi) * dpad;
       float* row = V + static_cast<size_t>(qi) * nlist;
-      for (int c = threadIdx.x; c < nlist; c += blockDim.x) {
-        const float* x = cent + static_cast<size_t>(c) * dpad;
-        float acc = 0.0f;
-        for (int j = 0; j < dpad; ++j) {
-          const float t = __fsub_rn(qrow[j], x[j]);
-          acc = __fadd_rn(acc, __fmul_rn(t, t));
+      // The row is overwritten with exact values, and so are its chunk
+      // minima (a warp's 32 consecutive columns are two 16-column chunks).
+      for (int c0 = 0; c0 < nlist; c0 += blockDim.x) {
+        const int c = c0 + static_cast<int>(threadIdx.x);
+        float acc = FLT_MAX;
+        if (c < nlist) {
+          const float* x = cent + static_cast<size_t>(c) * dpad;
+          acc = 0.0f;
+          for (int j = 0; j < dpad; ++j) {
+            const float t = __fsub_rn(qrow[j], x[j]);
+            acc = __fadd_rn(acc, __fmul_rn(t, t));
+          }
+          row[c] = acc;
         }
-        row[c] = acc;
+        uint32_t m = c < nlist ? __float_as_uint(acc) : 0xFFFFFFFFu;
+        for (int o = 8; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (cmins && (threadIdx.x & 15) == 0 && c < nlist) cmins[static_cast<size_t>(c / 16) * nq + qi] = m;
       }
       __syncthreads();
       auto key_at = [&](int c) -> uint64_t {
@@ -555,11 +577,9 @@ void make_centroid_split(const float* cent, int nlist, int dpad, int kpad, void*
 }
 
 void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kpad, const float* cnorm, int nlist,
-                      float* V, void* qsplit, float* qnorm, uint32_t* vlo, uint32_t* vhi, int* err, int num_sms,
+                      float* V, void* qsplit, float* qnorm, uint32_t* cmins, int* err, int num_sms,
                       cudaStream_t st) {
   if (nq <= 0 || nlist <= 0) return;
-  HB_CUDA(cudaMemsetAsync(vlo, 0xFF, static_cast<size_t>(nq) * sizeof(uint32_t), st));
-  HB_CUDA(cudaMemsetAsync(vhi, 0, static_cast<size_t>(nq) * sizeof(uint32_t), st));
   HB_CHECK(kpad == 64 || kpad == 128, HB_ERR_INVALID, "the tensor-core coarse quantizer supports d <= 128");
   // Query rows -> [hi | lo] BF16 and ||q||^2, then their tensor map.
   const unsigned g = static_cast<unsigned>(std::min<int>((nq + 7) / 8, 148 * 16));
@@ -581,7 +601,7 @@ void launch_coarse_tc(const void* tmap, const float* q, int nq, int dpad, int kp
   coarse_tc_kernel<<<G, kCThreads, smem, st>>>(*static_cast<const CUtensorMap*>(tmap),
                                                 *reinterpret_cast<const CUtensorMap*>(tmap_q),
                                                 *reinterpret_cast<const CUtensorMap*>(tmap_v), tma_v, qnorm, nq, kpad,
-                                                cnorm, nlist, qt, pairs, V, vlo, vhi, err);
+                                                cnorm, nlist, qt, pairs, V, cmins, err);
   HB_CUDA(cudaGetLastError());
 }
 
@@ -616,12 +636,13 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
 }
 
 void launch_coarse_fallback(const float* q, int nq, int dpad, const float* cent, int nlist, int P, const int* flags,
-                            float* V, int32_t* probes, float* cdist, cudaStream_t st, const int32_t* width) {
+                            float* V, int32_t* probes, float* cdist, cudaStream_t st, const int32_t* width,
+                            uint32_t* cmins) {
   if (nq <= 0) return;
   const size_t smem = static_cast<size_t>(pow2_ceil(P < 2 ? 2 : P)) * 8;
   HB_CUDA(cudaFuncSetAttribute(coarse_fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   coarse_fallback_kernel<<<std::min((nq + 31) / 32, 296), 256, smem, st>>>(q, nq, dpad, cent, nlist, P, flags, V,
-                                                                           probes, cdist, width);
+                                                                           probes, cdist, width, cmins);
   HB_CUDA(cudaGetLastError());
 }
 

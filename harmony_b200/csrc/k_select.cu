@@ -217,18 +217,17 @@ __global__ void __launch_bounds__(kSelThreads, 6) select_rows_reg_kernel(const f
 }
 
 // The same selection with one warp per row (4 rows per CTA), for k <= 256
-// and rows of at most 8192 columns with 16-byte aligned rows: up to three
-// passes over the row from L2 (range, unless the caller gives it; histogram
-// of the keys' high words in a per-warp 1024-bin table; ballot compaction of
-// the keys in and under the k-th key's bin), then a warp bitonic sort.  A
-// row whose candidates exceed kWarpCand is flagged for the CTA kernel.
+// and rows of at most 8192 columns with 16-byte aligned rows: three passes
+// over the row from L2 (range; histogram of the keys' high words in a
+// per-warp 1024-bin table; ballot compaction of the keys in and under the
+// k-th key's bin), then a warp bitonic sort.  A row whose candidates exceed
+// kWarpCand is flagged for the CTA kernel.
 constexpr int kSelWarps = 4;
 constexpr int kWarpCand = 512;
 
 __global__ void __launch_bounds__(kSelWarps * 32) select_rows_warp_kernel(
     const float* __restrict__ D, int nrows, int ncols, int ldD, int kmax, int32_t* __restrict__ out_idx,
-    float* __restrict__ out_val, const int32_t* __restrict__ k_row, int* __restrict__ overflow,
-    const uint32_t* __restrict__ vlo, const uint32_t* __restrict__ vhi) {
+    float* __restrict__ out_val, const int32_t* __restrict__ k_row, int* __restrict__ overflow) {
   __shared__ int s_hist[kSelWarps][kBins];
   __shared__ uint64_t s_cand[kSelWarps][kWarpCand];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -242,30 +241,24 @@ __global__ void __launch_bounds__(kSelWarps * 32) select_rows_warp_kernel(
   const float4* row4 = reinterpret_cast<const float4*>(D + static_cast<size_t>(r) * ldD);
   const int n4 = ncols >> 2;
   auto word = [](float v) -> uint32_t { return v < FLT_MAX ? __float_as_uint(v) : 0xFFFFFFFFu; };
-  // Range of the finite values: the caller's hint, else a pass over the row.
-  unsigned lo = vlo ? vlo[r] : 0xFFFFFFFFu, hi = vhi ? vhi[r] : 0u;
-  if (lo > hi) {
-    lo = 0xFFFFFFFFu;
-    hi = 0;
+  // Range of the finite values.
+  unsigned lo = 0xFFFFFFFFu, hi = 0;
 #pragma unroll 4
-    for (int i = lane; i < n4; i += 32) {
-      const float4 v = row4[i];
-      const uint32_t u[4] = {word(v.x), word(v.y), word(v.z), word(v.w)};
+  for (int i = lane; i < n4; i += 32) {
+    const float4 v = row4[i];
+    const uint32_t u[4] = {word(v.x), word(v.y), word(v.z), word(v.w)};
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (u[j] != 0xFFFFFFFFu) {
-          lo = min(lo, u[j]);
-          hi = max(hi, u[j]);
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    }
+    for (int j = 0; j < 4; ++j)
+      if (u[j] != 0xFFFFFFFFu) {
+        lo = min(lo, u[j]);
+        hi = max(hi, u[j]);
+      }
   }
-  // Bin of a high word: (x - lo) >> sh clamped to [0, kBins), monotone in x
-  // for any lo <= hi, so the selection is exact even when the hint misses
-  // some values (they land in the first or the last bin).
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  // Bin of a high word: (x - lo) >> sh clamped to [0, kBins), monotone in x.
   const unsigned span = hi >= lo ? hi - lo : 0u;
   const int sh = max(0, 32 - __clz(static_cast<int>(span | 1u)) - 10);
   auto bin_of = [&](uint32_t x) -> int {
@@ -339,6 +332,94 @@ __global__ void __launch_bounds__(kSelWarps * 32) select_rows_warp_kernel(
   warp_bitonic_sort(cand, n2, lane);
   for (int j = lane; j < k; j += 32) {
     const uint64_t key = j < kk ? cand[j] : kEmpty;
+    const size_t o = static_cast<size_t>(r) * kmax + j;
+    out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
+    if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
+  }
+}
+
+// The same selection from the chunk minima of coarse_tc (cm[c * nrows + r]
+// = the smallest value of columns 16c .. 16c + 15 of row r): the k-th
+// smallest chunk minimum T is at least the row's k-th smallest value (those
+// k minima are k values of the row), and every value <= T lies in a chunk
+// whose minimum is <= T, so the k smallest keys are among the values <= T of
+// those chunks -- a little more than k chunks read instead of the row twice.
+// A warp per row; rows with fewer than k finite minima or more than
+// kWarpCand values <= T are flagged for the CTA kernel.
+constexpr int kChunkCols = 16;
+constexpr int kChunkMax = 256;  // chunks per row: eight per lane
+
+__global__ void __launch_bounds__(kSelWarps * 32) select_rows_chunk_kernel(
+    const float* __restrict__ D, int nrows, int ncols, int ldD, int kmax, int32_t* __restrict__ out_idx,
+    float* __restrict__ out_val, const int32_t* __restrict__ k_row, int* __restrict__ overflow,
+    const uint32_t* __restrict__ cmins) {
+  __shared__ uint64_t s_cand[kSelWarps][kWarpCand];
+  __shared__ int s_chk[kSelWarps][kChunkMax];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int r = blockIdx.x * kSelWarps + wib;
+  if (r >= nrows) return;
+  const int k = k_row ? min(k_row[r], kmax) : kmax;
+  const int nch = (ncols + kChunkCols - 1) / kChunkCols;
+  overflow[r] = 0;  // every lane writes the same value
+  if (k <= 0) return;
+  if (k > nch) {
+    overflow[r] = 1;
+    return;
+  }
+  uint32_t v[8], w[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+    w[i] = v[i] = 32 * i + lane < nch ? cmins[static_cast<size_t>(32 * i + lane) * nrows + r] : 0xFFFFFFFFu;
+  const uint32_t T = warp_kth_small8(v, k, lane);
+  if (T > __float_as_uint(FLT_MAX)) {  // fewer than k finite minima
+    overflow[r] = 1;
+    return;
+  }
+  // Chunks with minimum <= T, ascending.
+  int nc = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const bool in = 32 * i + lane < nch && w[i] <= T;
+    const unsigned b = __ballot_sync(0xffffffffu, in);
+    if (in) s_chk[wib][nc + __popc(b & ((1u << lane) - 1u))] = 32 * i + lane;
+    nc += __popc(b);
+  }
+  __syncwarp();
+  // Their values <= T: a half-warp per chunk (lane % 16 = column), sixteen
+  // chunks' loads in flight at a time.
+  const float* row = D + static_cast<size_t>(r) * ldD;
+  uint64_t* cand = s_cand[wib];
+  const int half = lane >> 4, cl = lane & 15;
+  int cnt = 0;
+  for (int t0 = 0; t0 < nc; t0 += 16) {
+    uint32_t u[8];
+    int col[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int t = t0 + 2 * e + half;
+      col[e] = t < nc ? s_chk[wib][t] * kChunkCols + cl : ncols;
+      const float x = col[e] < ncols ? row[col[e]] : FLT_MAX;
+      u[e] = x < FLT_MAX ? __float_as_uint(x) : 0xFFFFFFFFu;
+    }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const bool take = u[e] <= T;
+      const unsigned b = __ballot_sync(0xffffffffu, take);
+      const int pos = cnt + __popc(b & ((1u << lane) - 1u));
+      if (take && pos < kWarpCand) cand[pos] = (static_cast<uint64_t>(u[e]) << 32) | static_cast<uint32_t>(col[e]);
+      cnt += __popc(b);
+    }
+  }
+  if (cnt > kWarpCand) {
+    overflow[r] = 1;
+    return;
+  }
+  const int n2 = pow2_ceil(max(cnt, 2));
+  for (int i = cnt + lane; i < n2; i += 32) cand[i] = kEmpty;
+  __syncwarp();
+  warp_bitonic_sort(cand, n2, lane);
+  for (int j = lane; j < k; j += 32) {
+    const uint64_t key = j < cnt ? cand[j] : kEmpty;
     const size_t o = static_cast<size_t>(r) * kmax + j;
     out_idx[o] = key == kEmpty ? -1 : static_cast<int32_t>(key_tie(key));
     if (out_val) out_val[o] = key == kEmpty ? FLT_MAX : key_dist(key);
@@ -650,14 +731,22 @@ void exclusive_sum(const int64_t* in, int64_t* out, size_t n, void* tmp, size_t 
 }  // namespace
 
 void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, int32_t* out_idx, float* out_val,
-                        cudaStream_t st, const int32_t* k_row, int* row_flags, const uint32_t* vlo,
-                        const uint32_t* vhi) {
+                        cudaStream_t st, const int32_t* k_row, int* row_flags, const uint32_t* cmins) {
   if (nrows <= 0 || k <= 0) return;
   const int* only = nullptr;
-  if (row_flags && k <= 256 && ncols <= 8192 && ncols % 4 == 0 && ldD % 4 == 0) {
+  const int nch = (ncols + kChunkCols - 1) / kChunkCols;
+  if (row_flags && cmins && nch <= kChunkMax && 4 * k <= nch) {
+    // Chunk minima given and k small against the chunk count (else T would
+    // sit near the largest minima): a warp per row reads the chunks that can
+    // hold the k smallest; rows it flags go through the CTA kernel below.
+    select_rows_chunk_kernel<<<(nrows + kSelWarps - 1) / kSelWarps, kSelWarps * 32, 0, st>>>(
+        D, nrows, ncols, ldD, k, out_idx, out_val, k_row, row_flags, cmins);
+    HB_CUDA(cudaGetLastError());
+    only = row_flags;
+  } else if (row_flags && k <= 256 && ncols <= 8192 && ncols % 4 == 0 && ldD % 4 == 0) {
     // Warp per row; rows it flags go through the CTA kernel below.
     select_rows_warp_kernel<<<(nrows + kSelWarps - 1) / kSelWarps, kSelWarps * 32, 0, st>>>(
-        D, nrows, ncols, ldD, k, out_idx, out_val, k_row, row_flags, vlo, vhi);
+        D, nrows, ncols, ldD, k, out_idx, out_val, k_row, row_flags);
     HB_CUDA(cudaGetLastError());
     only = row_flags;
   }

@@ -5,6 +5,9 @@ restated step for step in Python with a lane per list element:
   positions per round; the lanes at or under the item form a prefix), which
   must find the list l with item_off[l] <= item < item_off[l + 1], empty lists
   included;
+- the chunk-minimum row selection (k_select.cu select_rows_chunk_kernel):
+  the k-th smallest chunk minimum T bounds the row's k-th smallest value, so
+  the values <= T of the chunks with minimum <= T hold the k smallest keys;
 - warp_kth_small8, the k-th smallest of up to 256 keys held eight per lane
   for small k (a sorting network per lane, then k rounds of a warp minimum);
 - warp_kth_smallest, the radix selection over four 8-bit digits with a
@@ -138,3 +141,22 @@ def test_radix_kth_clustered_keys():
         vals = [base | rng.getrandbits(rng.choice([4, 12, 20])) for _ in range(n)]
         k = rng.randint(1, n)
         assert warp_kth_smallest(vals, k) == sorted(vals)[k - 1]
+
+
+def select_by_chunk_minima(row, k, w=16):
+    nch = (len(row) + w - 1) // w
+    cm = [min(row[w * c:w * c + w]) for c in range(nch)]
+    T = sorted(cm)[k - 1]
+    keys = [(row[j], j) for c in range(nch) if cm[c] <= T for j in range(w * c, min(w * c + w, len(row))) if row[j] <= T]
+    return sorted(keys)[:k]
+
+
+def test_chunk_minimum_selection_matches_sort():
+    rng = random.Random(5)
+    for _ in range(300):
+        n = rng.choice([37, 130, 300, 1000, 4096, rng.randint(1, 5000)])
+        pool = rng.choice([None, [rng.random() for _ in range(5)]])
+        row = [rng.choice(pool) if pool else rng.random() for _ in range(n)]
+        nch = (n + 15) // 16
+        k = rng.randint(1, nch)
+        assert select_by_chunk_minima(row, k) == sorted((v, j) for j, v in enumerate(row))[:k]

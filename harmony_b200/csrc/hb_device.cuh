@@ -81,6 +81,28 @@ __device__ __forceinline__ float ordered_to_float(uint32_t u) {
 // unfused FP32 loop, src/utils.h:480-487: t = q - x, sum += t * t, each
 // operation rounded on its own, dimensions in order.  The zero padding adds
 // exact zeros.
+// The same loop continued from acc over dims [0, n) of x and qrow (n a
+// multiple of 4): running it over consecutive pieces of a row in order gives
+// the whole row's sum bit for bit.
+__device__ __forceinline__ float exact_l2_seq_from(float acc, const float* __restrict__ x,
+                                                   const float* __restrict__ qrow, int n) {
+#pragma unroll 8
+  for (int c = 0; c < n; c += 4) {
+    const float4 v = *reinterpret_cast<const float4*>(x + c);
+    const float4 w = *reinterpret_cast<const float4*>(qrow + c);
+    float t;
+    t = __fsub_rn(w.x, v.x);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(w.y, v.y);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(w.z, v.z);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(w.w, v.w);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+  }
+  return acc;
+}
+
 __device__ __forceinline__ float exact_l2_seq(const float* __restrict__ x, const float* __restrict__ qrow, int dpad) {
   float acc = 0.0f;
 #pragma unroll 8
@@ -100,26 +122,22 @@ __device__ __forceinline__ float exact_l2_seq(const float* __restrict__ x, const
   return acc;
 }
 
-// Row stride (floats) of rows staged by warp_stage_rows: dpad rounded up to
-// 32, plus 4, so the quarter-warps of per-lane float4 reads (lane r reading
-// row r at the same column) cover 32 distinct banks.
-__host__ __device__ __forceinline__ int stage_stride(int dpad) { return (dpad + 31) / 32 * 32 + 4; }
-
-// The warp copies row `row` of lane r (-1: none) of a row-major FP32 matrix
-// with dpad-float rows to stage + r * stride, for r = 0..31; lane L copies
-// floats [4L, 4L + 4) (+ 128 j) of every row, so each row is read as
-// contiguous 512-byte pieces rather than by one lane walking it alone.  Rows
-// must be 16-byte aligned (dpad a multiple of 4).  Returns once the warp's
-// copies have landed; a __syncwarp first keeps the previous rows' readers
-// ahead of the overwrite.
-__device__ __forceinline__ void warp_stage_rows(const float* __restrict__ base, int64_t row, int dpad, float* stage,
-                                                int stride, int lane) {
+// Columns [c0, c0 + ncol) (ncol <= 64, a multiple of 4) of the rows named by
+// the warp's first nv lanes (row r = lane r's `row`, -1: none) of a
+// row-major FP32 matrix with ld-float rows, to stage + r * stride: half a warp
+// per row, lane L copying floats [4 (L % 16), + 4), two rows per copy
+// instruction.  Returns once the copies have landed (a __syncwarp first
+// keeps the previous readers ahead of the overwrite).  stride = 68 (64 + 4)
+// keeps the per-lane float4 reads of row `lane` conflict-free.
+constexpr int kHalfStageStride = 68;
+__device__ __forceinline__ void warp_stage_half_rows(const float* __restrict__ base, int row, int ld, int c0,
+                                                     int ncol, float* stage, int nv, int lane) {
   __syncwarp();
-  for (int r = 0; r < 32; ++r) {
-    const long long rr = __shfl_sync(0xffffffffu, static_cast<long long>(row), r);
-    if (rr < 0) continue;
-    const float* src = base + rr * dpad;
-    for (int j = 4 * lane; j < dpad; j += 128) cp_async16(stage + r * stride + j, src + j, true);
+  const int h = lane >> 4, cl = 4 * (lane & 15);
+  for (int r0 = 0; r0 < nv; r0 += 2) {
+    const int rr = __shfl_sync(0xffffffffu, row, r0 + h);
+    if (r0 + h < nv && rr >= 0 && cl < ncol)
+      cp_async16(stage + (r0 + h) * kHalfStageStride + cl, base + static_cast<size_t>(rr) * ld + c0 + cl, true);
   }
   cp_async_commit();
   cp_async_wait<0>();

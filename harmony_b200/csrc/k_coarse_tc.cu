@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
                                                             int Pm, int P, int nlist, const float* __restrict__ cmaxnorm,
                                                             int32_t* __restrict__ probes, float* __restrict__ cdist,
                                                             int* __restrict__ flags, CoarseRows rows) {
-  // [warps][pow2(Pm)] keys, then a 32-row stage per warp.
+  // [warps][pow2(Pm)] keys, then a stage of 32 rows x 64 columns per warp.
   extern __shared__ __align__(16) uint8_t s_ref_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int qi = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -367,10 +367,10 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
   }
   const int n2 = pow2_ceil(Pmr < 2 ? 2 : Pmr);
   // Per-warp buffers are laid out for the launch's widest row.
-  const int nmax = pow2_ceil(Pm < 2 ? 2 : Pm), stride = stage_stride(dpad);
+  const int nmax = pow2_ceil(Pm < 2 ? 2 : Pm);
   uint64_t* buf = reinterpret_cast<uint64_t*>(s_ref_raw) + static_cast<size_t>(wib) * nmax;
   float* stage = reinterpret_cast<float*>(s_ref_raw + static_cast<size_t>(blockDim.x >> 5) * nmax * 8) +
-                 static_cast<size_t>(wib) * 32 * stride;
+                 static_cast<size_t>(wib) * 32 * kHalfStageStride;
   const float* qrow = q + static_cast<size_t>(qi) * dpad;
   float qn = 0.0f;
   for (int c = lane * 4; c < dpad; c += 128) {
@@ -378,17 +378,23 @@ __global__ void __launch_bounds__(256) coarse_refine_kernel(const float* __restr
     qn += v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w;
   }
   for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(0xffffffffu, qn, o);
-  // 32 candidates at a time, lane = candidate: the warp stages their
-  // centroid rows, then each lane runs the sequential loop over its row.
+  // 32 candidates at a time, lane = candidate: the warp stages 64 columns
+  // of their centroid rows at a time, each lane continuing the sequential
+  // loop over its row.
   for (int base = 0; base < n2; base += 32) {
     const int i = base + lane;
     const int c = i < Pmr ? cand[static_cast<size_t>(qi) * Pm + i] : -1;
-    if (base < Pmr) warp_stage_rows(cent, c, dpad, stage, stride, lane);
-    uint64_t key = kEmpty;
-    if (c >= 0) {
-      const float acc = exact_l2_seq(stage + static_cast<size_t>(lane) * stride, qrow, dpad);
-      if (acc < FLT_MAX) key = make_key(acc, static_cast<uint32_t>(c));
+    float acc = 0.0f;
+    if (base < Pmr) {
+      const int nv = min(32, Pmr - base);
+      for (int c0 = 0; c0 < dpad; c0 += 64) {
+        const int nc = min(64, dpad - c0);
+        warp_stage_half_rows(cent, c, dpad, c0, nc, stage, nv, lane);
+        if (c >= 0) acc = exact_l2_seq_from(acc, stage + static_cast<size_t>(lane) * kHalfStageStride, qrow + c0, nc);
+      }
     }
+    uint64_t key = kEmpty;
+    if (c >= 0 && acc < FLT_MAX) key = make_key(acc, static_cast<uint32_t>(c));
     if (i < n2) buf[i] = key;
   }
   __syncwarp();
@@ -612,7 +618,7 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
   HB_CHECK(P >= 1 && P <= Pm && Pm <= kCoarseMaxPm, HB_ERR_INVALID, "coarse candidate count out of range");
   HB_CHECK(dpad % 4 == 0 && dpad <= 128, HB_ERR_INVALID, "the coarse refinement stages rows of at most 128 floats");
   const int n2 = pow2_ceil(Pm < 2 ? 2 : Pm);
-  const size_t stage = static_cast<size_t>(32) * stage_stride(dpad) * sizeof(float);  // per warp
+  const size_t stage = static_cast<size_t>(32) * kHalfStageStride * sizeof(float);  // per warp
   // A CTA per query for small batches, and for the widening pass of the
   // learned nprobe, whose few wide rows (up to Pm candidates) would
   // otherwise keep one warp each busy long after the narrow rows are done.
@@ -625,8 +631,8 @@ void launch_coarse_refine(const float* q, int nq, int dpad, const float* cent, c
     HB_CUDA(cudaGetLastError());
     return;
   }
-  // Four warps (one query each) per CTA: with the 32-row stages, three CTAs
-  // fit an SM.
+  // Four warps (one query each) per CTA: with the 32-row x 64-column stages,
+  // six CTAs fit an SM.
   const int warps = 4;
   const size_t smem = static_cast<size_t>(warps) * (n2 * 8 + stage);
   HB_CUDA(cudaFuncSetAttribute(coarse_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));

@@ -309,7 +309,7 @@ inline unsigned blocks_for(size_t n, int tb = 256, unsigned cap = 148u * 64u) {
 using namespace sm100;
 
 constexpr int kMlpRows = 128;
-constexpr int kMlpThreads = 256;
+constexpr int kMlpThreads = 512;
 
 // W (N x K FP32, BF16-valued) -> Wb, the shared-memory image of the layer's
 // B operand: Npad rows x Kpad BF16 (zero padding), K-major in 64-column
@@ -427,9 +427,9 @@ __global__ void __launch_bounds__(kMlpThreads, 1) probe_mlp_tc_kernel(
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   // Epilogue mapping: warp w reads TMEM lanes 32 * (w % 4) (rows), columns
-  // [128 * (w / 4), +128).
+  // [64 * (w / 4), +64).
   const int row = (warp & 3) * 32 + (tid & 31);
-  const int cbase = (warp >> 2) * 128;
+  const int cbase = (warp >> 2) * 64;
   const uint32_t taddr = tmem + ((32u * static_cast<uint32_t>(warp & 3)) << 16);
   bool ok = true;
   uint32_t parity = 0;
@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) probe_mlp_tc_kernel(
     if (!ok) break;
     stage_weights(W, layer == 0 ? W2b : W3b, (layer == 0 ? 256u : 32u) * 256u * 2u, &wbar);
     const float* bias = layer == 0 ? b1 : b2;
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < 2; ++c) {
       uint32_t rr[32];
       tmem_ld32(taddr + static_cast<uint32_t>(cbase + c * 32), rr);
       tmem_ld_wait();

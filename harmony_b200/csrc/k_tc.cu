@@ -780,17 +780,29 @@ __global__ void __launch_bounds__(kRrWarps * 32) rerank_warp_kernel(
     __syncwarp();
     u_bits = warp_kth_smallest([&](int i) { return ubs[i]; }, c, k, s_h[wib], lane);
   }
+  // The candidates with lower bound <= U, compacted into buf (c <= 256:
+  // eight keys per lane, their loads in flight together).
   int m = 0;
-  for (int base = 0; base < c; base += 32) {
-    const int i = base + lane;
-    const uint64_t key = i < c ? src[i] : kEmpty;
-    const bool in = i < c && static_cast<uint32_t>(key >> 32) <= u_bits;
-    const unsigned bal = __ballot_sync(0xffffffffu, in);
-    if (in) buf[m + __popc(bal & ((1u << lane) - 1u))] = key;
-    m += __popc(bal);
+  {
+    uint64_t key[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) key[u] = 32 * u + lane < c ? src[32 * u + lane] : kEmpty;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const bool in = 32 * u + lane < c && static_cast<uint32_t>(key[u] >> 32) <= u_bits;
+      const unsigned bal = __ballot_sync(0xffffffffu, in);
+      if (in) buf[m + __popc(bal & ((1u << lane) - 1u))] = key[u];
+      m += __popc(bal);
+    }
   }
   __syncwarp();
   if (lane == 0) m_out[qi] = m;
+  // Every line of the rows to recompute requested at once (the lane loops
+  // below then wait for one DRAM round trip, not one per batch of loads).
+  for (int j = lane; j < m; j += 32) {
+    const char* rp = reinterpret_cast<const char*>(codes + static_cast<size_t>(key_tie(buf[j])) * dpad);
+    for (int o = 0; o < dpad * 4; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(rp + o));
+  }
   const float* qrow = q + static_cast<size_t>(qi) * dpad;
   const int e2n = pow2_ceil(m < 2 ? 2 : m);
   for (int j = lane; j < e2n; j += 32) {
@@ -874,17 +886,22 @@ __global__ void __launch_bounds__(kBigWarps * 32) rerank_big_bound_kernel(
     uint64_t* buf = cand + static_cast<size_t>(qi) * cap;
     const uint32_t* ubs = cand_ub + static_cast<size_t>(qi) * cap;
     const uint32_t lim_bits = warp_kth_smallest([&](int i) { return ubs[i]; }, c, k, s_h[wib], lane);
-    // In-place compaction: a block of 32 is read before any of it is
-    // written, and writes land at or below the read position.
+    // In-place compaction: a block of 256 keys (eight per lane, their loads
+    // in flight together) is read before any of it is written, and writes
+    // land at or below the read position.
     int m = 0;
-    for (int base = 0; base < c; base += 32) {
-      const int i = base + lane;
-      const uint64_t key = i < c ? buf[i] : kEmpty;
-      const bool in = i < c && static_cast<uint32_t>(key >> 32) <= lim_bits;
-      const unsigned bal = __ballot_sync(0xffffffffu, in);
+    for (int base = 0; base < c; base += 256) {
+      uint64_t key[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) key[u] = base + 32 * u + lane < c ? buf[base + 32 * u + lane] : kEmpty;
       __syncwarp();
-      if (in) buf[m + __popc(bal & ((1u << lane) - 1u))] = key;
-      m += __popc(bal);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const bool in = base + 32 * u + lane < c && static_cast<uint32_t>(key[u] >> 32) <= lim_bits;
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (in) buf[m + __popc(bal & ((1u << lane) - 1u))] = key[u];
+        m += __popc(bal);
+      }
     }
     if (lane == 0) m_out[qi] = m;
     __syncwarp();

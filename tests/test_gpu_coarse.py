@@ -44,6 +44,14 @@ def trained(d, nlist, nb, seed, offset=0.0):
     (64, 2048, 200, 256),
     (128, 200, 50, 200),   # nprobe = nlist: every centroid is a candidate
     (128, 300, 1, 290),    # candidates reach nlist through the margin
+    # The selection from 16-column chunk minima (nprobe + margin at most a
+    # quarter of the chunks): full chunks; a partial last chunk with TMA
+    # stores of the matrix; a partial last chunk with plain stores (nlist not
+    # a multiple of 4) and the CTA-per-query refinement.
+    (128, 2048, 700, 8),
+    (128, 1100, 600, 1),
+    (96, 3000, 520, 30),
+    (64, 4090, 300, 20),
 ])
 def test_tensor_coarse_matches_exact_and_oracle(restated, d, nlist, nq, P):
     ix, q = trained(d, nlist, max(4 * nlist, 3000), seed=d * 131 + nlist)
@@ -68,6 +76,17 @@ def test_fallback_rows_are_exact(restated):
     Pt2, _ = probes(ix, q, 32, CoarseQuantizer.TENSOR, margin=64)
     assert np.array_equal(Pt2, Pe)
     assert ix.coarse_fallbacks() < n_fb
+
+
+def test_fallback_rows_on_the_chunk_selection(restated):
+    """The chunk-minimum selection with margin 0: flagged rows are
+    recomputed exactly (their matrix rows and chunk minima rewritten) and the
+    probes still match the exact quantizer."""
+    ix, q = trained(128, 2048, 8192, seed=11)
+    Pt, Dt = probes(ix, q, 16, CoarseQuantizer.TENSOR, margin=0)
+    assert ix.coarse_fallbacks() > 0
+    Pe, De = probes(ix, q, 16, CoarseQuantizer.EXACT)
+    assert np.array_equal(Pt, Pe) and np.array_equal(Dt.view(np.uint32), De.view(np.uint32))
 
 
 def test_offset_data_large_norms(restated):

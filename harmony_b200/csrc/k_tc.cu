@@ -640,87 +640,6 @@ __global__ void residual_bf16_kernel(const float* __restrict__ codes, const int6
 
 constexpr int kSmallKth = 32;  // largest k for warp_kth_small8
 
-// The k-th smallest (k >= 1) of n 32-bit keys get(0 .. n-1), by one warp:
-// radix selection over four 8-bit digits with a 256-bin histogram h in
-// shared memory.  n >= k.  A digit that the smallest and the largest key
-// share (with everything above it) is every key's digit and needs no count:
-// keys of one query share their top bits, and counting those digits would
-// put every lane's atomic on one bin.
-template <class Get>
-__device__ uint32_t warp_kth_smallest(Get get, int n, int k, int* h, int lane) {
-  // Keys are read eight per lane at a time, the loads issued together.
-  constexpr int kB = 8;
-  uint32_t lo = 0xFFFFFFFFu, hi = 0u;
-  for (int i0 = 0; i0 < n; i0 += 32 * kB) {
-    uint32_t v[kB];
-#pragma unroll
-    for (int u = 0; u < kB; ++u) v[u] = i0 + 32 * u + lane < n ? get(i0 + 32 * u + lane) : 0u;
-#pragma unroll
-    for (int u = 0; u < kB; ++u)
-      if (i0 + 32 * u + lane < n) {
-        lo = min(lo, v[u]);
-        hi = max(hi, v[u]);
-      }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-  }
-  uint32_t prefix = 0u, pmask = 0u;
-  int need = k;  // rank of the wanted key among those matching the prefix
-  for (int shift = 24; shift >= 0; shift -= 8) {
-    if ((lo >> shift) == (hi >> shift)) {
-      prefix |= lo & (255u << shift);
-      pmask |= 255u << shift;
-      continue;
-    }
-    for (int i = lane; i < 256; i += 32) h[i] = 0;
-    __syncwarp();
-    for (int i0 = 0; i0 < n; i0 += 32 * kB) {
-      uint32_t v[kB];
-#pragma unroll
-      for (int u = 0; u < kB; ++u) v[u] = i0 + 32 * u + lane < n ? get(i0 + 32 * u + lane) : 0u;
-#pragma unroll
-      for (int u = 0; u < kB; ++u)
-        if (i0 + 32 * u + lane < n && (v[u] & pmask) == prefix) atomicAdd(&h[(v[u] >> shift) & 255u], 1);
-    }
-    __syncwarp();
-    int loc[8], sum = 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      loc[j] = h[8 * lane + j];
-      sum += loc[j];
-    }
-    int incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int x = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += x;
-    }
-    const int excl = incl - sum;
-    const unsigned hit = __ballot_sync(0xffffffffu, excl < need && need <= incl);
-    const int src_lane = __ffs(hit) - 1;
-    int bin = 0, before = excl;
-    if (lane == src_lane) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        if (before + loc[j] >= need) {
-          bin = 8 * lane + j;
-          break;
-        }
-        before += loc[j];
-      }
-    }
-    bin = __shfl_sync(0xffffffffu, bin, src_lane);
-    before = __shfl_sync(0xffffffffu, before, src_lane);
-    need -= before;
-    prefix |= static_cast<uint32_t>(bin) << shift;
-    pmask |= 255u << shift;
-    __syncwarp();
-  }
-  return prefix;
-}
 
 // Re-rank, one warp per query with at most kRrWarpCap candidates: U = the
 // k-th smallest upper bound among them (radix selection), the candidates

@@ -1,5 +1,5 @@
 // Blackwell (sm_100a) primitives as inline PTX: mbarriers with bounded
-// waits, TMA tiled loads (no multicast), bulk copies, tcgen05 TMEM
+// waits, TMA tiled loads (into this CTA only), bulk copies, tcgen05 TMEM
 // allocation, MMA, commit and loads.  Written from the PTX ISA
 // descriptions; every wait here gives up after a clock budget and reports
 // it through the caller's error flag instead of spinning forever.
@@ -78,7 +78,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
 // ---- TMA ------------------------------------------------------------------
 
 // 2-D tiled load of box (c0, c1) of `tmap` into shared memory, completing
-// `bytes` on `bar`.  Plain load: no multicast.
+// `bytes` on `bar`; the box lands in this CTA only.
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tmap, int c0, int c1, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::

@@ -960,11 +960,6 @@ __global__ void __launch_bounds__(kSeedWarps * 32, 4) seed_bound_kernel(
     const char* rp = reinterpret_cast<const char*>(codes + static_cast<size_t>(b + tid) * kpad);
     for (int o = 0; o < kpad * 2; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(rp + o));
   }
-  if (!by_query) {
-    bool mine = false;
-    for (int64_t e = e0 + tid; e < e1 && !mine; e += blockDim.x) mine = (list_q[e] & 0xffff) == 0;
-    if (!__syncthreads_or(mine)) return;
-  }
   const uint4* xrow = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(b + (row_ok ? tid : 0)) * kpad);
   const float xn = row_ok ? xnorm[b + tid] : 0.0f;
   for (int64_t r0 = e0; r0 < e1; r0 += blockDim.x) {
@@ -976,7 +971,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32, 4) seed_bound_kernel(
       if ((ent & 0xffff) == 0) s_qs[atomicAdd(&s_nq, 1)] = static_cast<int>(ent >> 16);
     }
     __syncthreads();
-    const int nqr = s_nq;
+    const int nqr = s_nq;  // 0 for a list that is no query's nearest: nothing to do
     for (int t0 = 0; t0 < nqr; t0 += kSeedQ) {
       const int nb = min(kSeedQ, nqr - t0);
       if (wib < nb) {

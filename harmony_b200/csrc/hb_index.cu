@@ -430,7 +430,7 @@ class IndexCore {
       cflags_.reserve(static_cast<size_t>(nq));
       launch_select_rows(dmat_.p, nq, static_cast<int>(nlist_), static_cast<int>(nlist_), P, probes_out, cdist_out,
                          st_, nullptr, cflags_.p);
-      launches_ += 2;
+      launches_ += 3;  // matrix, warp selection, its CTA kernel
       coarse_last_nq_ = 0;
       return;
     }
@@ -531,7 +531,10 @@ class IndexCore {
       launch_coarse_fallback(qpad, nq, static_cast<int>(dpad_), cent_.p, nl, P, cflags_.p, dmat_.p, probes_out, nullptr,
                              st_, npq_.p);
     }
-    launches_ += 13;
+    // narrow pass: query split, matrix, selection + its CTA kernel,
+    // refinement, fallback; widening pass: widths, selection, refinement,
+    // fallback (the predictor counts its own).
+    launches_ += 10;
     coarse_last_nq_ = nq;
   }
 
@@ -1115,8 +1118,8 @@ class IndexCore {
     launch_l2_matrix(qpad, nb, cent_.p, static_cast<int>(nlist_), static_cast<int>(dpad_), dmat,
                      static_cast<int>(nlist_), st_);
     launch_select_rows(dmat, nb, static_cast<int>(nlist_), static_cast<int>(nlist_), P, probes, nullptr, st_);
-    launch_build_work(probes, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt, list_qoff, cursor,
-                      list_q, item_off, slot_base, work_tmp, wtmp, st_);
+    const int nbw = launch_build_work(probes, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt, list_qoff,
+                                      cursor, list_q, item_off, slot_base, work_tmp, wtmp, st_);
     HB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st_));
     ScanArgs a{};
     a.codes = codes_.p;
@@ -1141,7 +1144,7 @@ class IndexCore {
     a.nseg = 1;
     launch_scan_exact(a, num_sms_, st_);
     launch_merge(part, slot_base, nb, P, static_cast<int>(k), ids_.p, D, I, st_);
-    launches_ += 8;
+    launches_ += 5 + nbw;  // pad, distance matrix, selection, scan, merge, work description
     HB_CUDA(cudaStreamSynchronize(st_));
   }
 
@@ -1302,10 +1305,10 @@ class IndexCore {
     work_tmp_.reserve(wtmp);
     {
       Scope sc(this, "build_work");
-      launch_build_work(probes, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt_.p, list_qoff_.p,
-                        list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+      launches_ += launch_build_work(probes, nb, P, list_off_.p, static_cast<int>(nlist_), cr, qg, list_cnt_.p,
+                                     list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p,
+                                     wtmp, st_);
     }
-    launches_ += 3;
     part_.reserve(max_slots(nb, P, cr) * static_cast<size_t>(k));
     counter_.reserve(1);
     HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
@@ -1426,8 +1429,9 @@ class IndexCore {
     }
     {
       Scope sc(this, "build_work");
-      launch_build_work(probes_a, nb, P_a, list_off_.p, static_cast<int>(nlist_), cr_a, 128, list_cnt_.p,
-                        list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, nullptr, work_tmp_.p, wtmp, st_);
+      launches_ += launch_build_work(probes_a, nb, P_a, list_off_.p, static_cast<int>(nlist_), cr_a, 128, list_cnt_.p,
+                                     list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, nullptr, work_tmp_.p, wtmp,
+                                     st_);
     }
     {
       Scope sc(this, "seed");
@@ -1474,8 +1478,9 @@ class IndexCore {
       }
       {
         Scope sc(this, "build_work");
-        launch_build_work(probes_rest_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p,
-                          list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, nullptr, work_tmp_.p, wtmp, st_);
+        launches_ += launch_build_work(probes_rest_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128,
+                                       list_cnt_.p, list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, nullptr,
+                                       work_tmp_.p, wtmp, st_);
       }
       HB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st_));
       a.chunk_rows = cr;
@@ -1483,14 +1488,16 @@ class IndexCore {
         Scope sc(this, "scan_bf16");
         launch_scan_bf16(tmap_, a, num_sms_, st_);
       }
-      launches_ += 5;
+      launches_ += 2;  // kth_bound, the second scan
     }
     {
       Scope sc(this, "rerank");
       launch_rerank_bf16(cbuf_.p, cbuf_ub_.p, ccnt_.p, cap, nb, k, codes_.p, qpad_.p, static_cast<int>(dpad_), ids_.p, Dd,
                          Id, cflag_.p, over_list_.p, over_n_.p, rr_m_.p, num_sms_, st_);
     }
-    launches_ += 8 + (cap > 256 ? 1 : 0);
+    // query prep, seed, scan, warp re-rank, and the three flat re-rank
+    // kernels when the buffers can hold more than a warp's candidates.
+    launches_ += 4 + (cap > 256 ? 3 : 0);
   }
 
   // ---- autotuner of the bounded scan ----------------------------------------
@@ -1662,10 +1669,10 @@ class IndexCore {
     work_tmp_.reserve(wtmp);
     {
       Scope sc(this, "build_work");
-      launch_build_work(probes_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p, list_qoff_.p,
-                        list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p, wtmp, st_);
+      launches_ += launch_build_work(probes_.p, nb, P, list_off_.p, static_cast<int>(nlist_), cr, 128, list_cnt_.p,
+                                     list_qoff_.p, list_cursor_.p, list_q_.p, item_off_.p, slot_base_.p, work_tmp_.p,
+                                     wtmp, st_);
     }
-    launches_ += 3;
     seg_.reserve(nqp + 1);
     {
       Scope sc(this, "cand_segments");

@@ -137,8 +137,9 @@ void launch_select_rows(const float* D, int nrows, int ncols, int ldD, int k, in
                         const uint32_t* cmins = nullptr);
 // Build the list-major work description from probes (nq x P, -1 = none).
 // slot_base (the exact scan's per-(query, probe) output slots) may be null:
-// it is then not built.
-void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist,
+// it is then not built.  Returns the number of this library's kernels it
+// launched.
+int launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist,
                        int chunk_rows, int qgroup, int32_t* list_cnt, int64_t* list_qoff,
                        int32_t* list_cursor, int32_t* list_q, int64_t* item_off, int64_t* slot_base,
                        void* scan_tmp, size_t scan_tmp_bytes, cudaStream_t st);

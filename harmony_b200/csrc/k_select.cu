@@ -792,7 +792,7 @@ size_t build_work_tmp_bytes(int nq, int P, int nlist) {
   return cub_bytes + (2 * n1 + n2) * sizeof(int64_t) + 256;
 }
 
-void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist, int chunk_rows,
+int launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list_off, int nlist, int chunk_rows,
                        int qgroup, int32_t* list_cnt, int64_t* list_qoff, int32_t* list_cursor, int32_t* list_q,
                        int64_t* item_off, int64_t* slot_base, void* scan_tmp, size_t scan_tmp_bytes,
                        cudaStream_t st) {
@@ -816,7 +816,7 @@ void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list
     build_work_small_kernel<<<1, kWorkThreads, smem, st>>>(probes, nqp, P, list_off, nlist, chunk_rows, qgroup,
                                                            list_cnt, list_qoff, list_q, item_off, slot_base);
     HB_CUDA(cudaGetLastError());
-    return;
+    return 1;
   }
   HB_CUDA(cudaMemsetAsync(list_cnt, 0, sizeof(int32_t) * nlist, st));
   HB_CUDA(cudaMemsetAsync(list_cursor, 0, sizeof(int32_t) * nlist, st));
@@ -841,6 +841,7 @@ void launch_build_work(const int32_t* probes, int nq, int P, const int64_t* list
   scatter_probes_kernel<<<(nqp + tb - 1) / tb, tb, 0, st>>>(probes, nqp, P, list_off, list_qoff, list_cursor,
                                                             list_q);
   HB_CUDA(cudaGetLastError());
+  return 3;  // count, the per-list sums, scatter (the CUB scans are library kernels)
 }
 
 void launch_merge(const uint64_t* part, const int64_t* slot_base, int nq, int P, int k, const int64_t* ids,

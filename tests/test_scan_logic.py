@@ -5,6 +5,8 @@ restated step for step in Python with a lane per list element:
   positions per round; the lanes at or under the item form a prefix), which
   must find the list l with item_off[l] <= item < item_off[l + 1], empty lists
   included;
+- the split of coarse_tc's (centroid tile, query tile) pairs over CTAs
+  (k_coarse_tc.cu coarse_range): contiguous ranges covering every pair once;
 - the chunk-minimum row selection (k_select.cu select_rows_chunk_kernel):
   the k-th smallest chunk minimum T bounds the row's k-th smallest value, so
   the values <= T of the chunks with minimum <= T hold the k smallest keys;
@@ -160,3 +162,25 @@ def test_chunk_minimum_selection_matches_sort():
         nch = (n + 15) // 16
         k = rng.randint(1, nch)
         assert select_by_chunk_minima(row, k) == sorted((v, j) for j, v in enumerate(row))[:k]
+
+
+def coarse_range(b, G, pairs):
+    return b * pairs // G, (b + 1) * pairs // G
+
+
+def test_coarse_pair_ranges_cover_every_pair_once():
+    rng = random.Random(6)
+    for _ in range(300):
+        qt, ct = rng.randint(1, 120), rng.randint(1, 64)
+        pairs = qt * ct
+        G = max(1, min(pairs, rng.choice([148, 132, 7, 1])))
+        seen, prev_end = [], 0
+        for b in range(G):
+            p0, p1 = coarse_range(b, G, pairs)
+            assert p0 == prev_end and p1 > p0  # contiguous, never empty (pairs >= G)
+            prev_end = p1
+            seen.extend(range(p0, p1))
+            # pairs are centroid-tile major: a CTA loads ceil-ish (range / qt) + 1 tiles at most
+            tiles = {p // qt for p in range(p0, p1)}
+            assert len(tiles) <= (p1 - p0 + qt - 1) // qt + 1
+        assert seen == list(range(pairs))
